@@ -1,0 +1,430 @@
+/*
+ * Test-oracle driver around the reference's OWN C code for the
+ * Shack-Hartmann physical-optics path.  Built by oracle/Makefile into
+ * oracle/_ref/libmaosref.so from the sources under the reference tree (which
+ * are compiled in place, never copied).  Test infrastructure only: the
+ * product never links or calls it.
+ *
+ * It includes the reference's maos/powfs.c so that the static setup routines
+ * (setup_shwfs_geom, setup_shwfs_prep_phy, setup_shwfs_dtf, setup_shwfs_etf,
+ * setup_powfs_llt, setup_shwfs_phygrad) run exactly as MAOS runs them, and it
+ * then calls the reference's per-frame routines:
+ *   wfsints()      maos/wfsints.c:79
+ *   shwfs_grad()   maos/utils.c:983
+ *   addnoise()     lib/libmisc.c:31
+ *   prop()         lib/accphi.c:223 (prop_grid_pts, lib/accphi_grid_do.c:408)
+ *   genscreen      lib/turbulence.c:214 (via genatm_simple, lib/turbulence.c:371)
+ *
+ * The flat API below (oref_*) is what tests/ and bench.py's CPU-baseline leg
+ * call through ctypes.  Arrays cross it as plain double pointers in MAOS
+ * column-major order.
+ */
+#include "powfs.c"  /* reference maos/powfs.c, for its static setup routines */
+#include <omp.h>
+/* maos/wfsints.c:79; declared in the reference only inside its simulator headers */
+void* wfsints(thread_t* thread_data);
+
+typedef struct oref_cfg_t{
+	double D, Din;        /* telescope diameter and central obstruction (m) */
+	int amp_binary;       /* 1: binary annular pupil map sampled on the OPD grid */
+	int order;            /* subapertures across the pupil */
+	double dsa;           /* subaperture size (m) */
+	double dx;            /* OPD sampling (m) */
+	double saat;          /* subaperture area threshold */
+	int embfac;           /* embedding factor, normally 2 */
+	int notf;             /* OTF size; 0 = automatic */
+	int pixpsa;           /* pixels per subaperture side */
+	double pixtheta;      /* pixel size (rad) */
+	double pixblur;       /* pixel blur sigma (fraction of pixel) */
+	double wvl;           /* wavelength (m) */
+	double hs;            /* guide star range (m); INFINITY for NGS */
+	double siglev;        /* photons per subaperture per frame */
+	double rne;           /* read noise (e-) */
+	double bkgrnd;        /* background (e-/pixel/frame) */
+	double bkgrndc;       /* calibrated fraction of background */
+	int phytype;          /* 1: matched filter, 2: CoG */
+	int sigmatch;         /* 0,1,2 */
+	int mtchcr;           /* matched filter constraint */
+	double cogthres, cogoff;
+	double r0, L0;        /* turbulence used for the matched filter i0 */
+	int has_llt;
+	double llt_d, llt_widthp, llt_ox, llt_oy;
+	int na_n;             /* sodium profile samples (evenly spaced) */
+	const double* na_h;   /* altitude (m) */
+	const double* na_p;   /* strength; sums to the signal scaling */
+	int nwfs;
+	const double* thetax; /* rad */
+	const double* thetay; /* rad */
+	int nthread;          /* NTHREAD for the reference's own threading */
+}oref_cfg_t;
+
+static parms_t* g_parms=NULL;
+static powfs_t* g_powfs=NULL;
+static dmat* g_wvl=NULL;
+
+static lmat* lvec(long n, long start){
+	lmat* v=lnew(n, 1);
+	for(long i=0; i<n; i++) P(v, i)=start+i;
+	return v;
+}
+
+/* Builds parms_t/powfs_t for one powfs with cfg->nwfs WFS and runs the
+   reference's SH setup. Returns the number of valid subapertures. */
+int oref_setup(const oref_cfg_t* c){
+	if(!global) global=mycalloc(1, global_t);
+	NTHREAD=c->nthread>0?c->nthread:1;
+	omp_set_num_threads(NTHREAD);
+	parms_t* parms=g_parms=mycalloc(1, parms_t);
+	parms->npowfs=1;
+	parms->nwfs=c->nwfs;
+	parms->powfs=mycalloc(1, powfs_cfg_t);
+	parms->wfs=mycalloc(c->nwfs, wfs_cfg_t);
+	parms->aper.d=c->D;
+	parms->aper.din=c->Din;
+	parms->aper.misreg=dnew(2, 1);
+	parms->sim.dt=1./800;
+	parms->sim.dtref=parms->sim.dt;
+	parms->sim.za=0;
+	parms->sim.htel=0;
+	parms->dbg.wfslinearity=-1;
+	parms->save.gradnf=lnew(c->nwfs, 1);
+	powfs_cfg_t* p=parms->powfs;
+	g_wvl=dnew(1, 1); P(g_wvl, 0)=c->wvl;
+	p->wvl=g_wvl;
+	p->wvlwts=dnew(1, 1); P(p->wvlwts, 0)=1;
+	p->nwvl=1;
+	p->wvlmean=c->wvl;
+	p->order=c->order;
+	p->dsa=c->dsa;
+	p->dx=c->dx;
+	p->saat=c->saat;
+	p->safill2d=1;
+	p->embfac=c->embfac;
+	p->notf=c->notf;
+	p->pixpsa=c->pixpsa;
+	p->pixtheta=c->pixtheta;
+	p->radpixtheta=c->pixtheta;
+	p->pixblur=c->pixblur;
+	p->hs=c->hs;
+	p->siglev=c->siglev;
+	p->rne=c->rne;
+	p->bkgrnd=c->bkgrnd;
+	p->bkgrndc=c->bkgrndc;
+	p->phytype_recon=c->phytype;
+	p->phytype_sim=c->phytype;
+	p->phyusenea=1;
+	p->sigmatch=c->sigmatch;
+	p->mtchcr=c->mtchcr;
+	p->cogthres=c->cogthres;
+	p->cogoff=c->cogoff;
+	p->r0=c->r0;
+	p->L0=c->L0;
+	p->dtrat=1;
+	p->usephy=1;
+	p->noisy=1;
+	p->nwfs=c->nwfs;
+	p->wfs=lvec(c->nwfs, 0);
+	p->wfsind=lvec(c->nwfs, 0);
+	p->siglevs=dnew(1, 1); P(p->siglevs, 0)=c->siglev;
+	for(int iwfs=0; iwfs<c->nwfs; iwfs++){
+		wfs_cfg_t* w=&parms->wfs[iwfs];
+		w->powfs=0;
+		w->thetax=c->thetax?c->thetax[iwfs]:0;
+		w->thetay=c->thetay?c->thetay[iwfs]:0;
+		w->hs=c->hs;
+		w->siglev=c->siglev;
+		w->sigsim=c->siglev;
+		w->wvlwts=dref(p->wvlwts);
+	}
+	if(c->has_llt){
+		llt_cfg_t* l=p->llt=mycalloc(1, llt_cfg_t);
+		l->d=c->llt_d;
+		l->widthp=c->llt_widthp;
+		l->ox=dnew(1, 1); P(l->ox, 0)=c->llt_ox;
+		l->oy=dnew(1, 1); P(l->oy, 0)=c->llt_oy;
+		l->misreg=dnew(2, 1);
+		l->i=lnew(c->nwfs, 1); /* every WFS uses LLT 0 */
+		l->nllt=1;
+		l->nhs=1;
+		l->na_interp=1;
+		p->trs=1;
+	}
+	global->parms=parms;
+	powfs_t* powfs=g_powfs=mycalloc(1, powfs_t);
+	global->powfs=powfs;
+
+	map_t* aper=NULL;
+	if(c->amp_binary){
+		/* Binary annulus on a grid whose nodes coincide with the OPD points,
+		   so the bilinear sampling in mkamp() returns the node values. */
+		const double dxo=c->dsa/(2*(int)round(0.5*c->dsa/c->dx));
+		long n=(long)ceil(c->D/dxo)+4;
+		aper=mapnew(n, n, dxo, dxo);
+		double off=((c->order&1)?-0.5*c->dsa:0)+0.5*dxo;
+		long k0=(long)ceil((0.5*c->D+2*dxo)/dxo);
+		aper->ox=off-k0*dxo;
+		aper->oy=off-k0*dxo;
+		for(long iy=0; iy<n; iy++){
+			double y=aper->oy+iy*dxo;
+			for(long ix=0; ix<n; ix++){
+				double x=aper->ox+ix*dxo;
+				double r2=x*x+y*y;
+				P(aper, ix, iy)=(r2<=0.25*c->D*c->D&&r2>=0.25*c->Din*c->Din)?1:0;
+			}
+		}
+	}
+	setup_shwfs_geom(powfs, parms, aper, 0);
+	setup_shwfs_prep_phy(powfs, parms, 0);
+	setup_shwfs_dtf(powfs, parms, 0);
+	if(c->has_llt){
+		dmat* na=dnew(c->na_n, 2);
+		for(int i=0; i<c->na_n; i++){
+			P(na, i, 0)=c->na_h[i];
+			P(na, i, 1)=c->na_p[i];
+		}
+		powfs[0].sodium=dcellnew(1, 1);
+		P(powfs[0].sodium, 0)=na;
+		setup_shwfs_etf(powfs, parms, 0, 1, 0, 0, 0);
+		setup_powfs_llt(powfs, parms, 0);
+	}
+	if(c->phytype==PTYPE_MF){
+		setup_shwfs_phygrad(powfs, parms, 0);
+	}
+	mapfree(aper);
+	return (int)powfs[0].saloc->nloc;
+}
+
+int oref_nsa(void){ return (int)g_powfs[0].saloc->nloc; }
+int oref_nopd(void){ return (int)g_powfs[0].pts->nxsa; }
+int oref_notf(void){ return g_powfs[0].notfx; }
+int oref_pixpsax(void){ return g_powfs[0].pixpsax; }
+int oref_pixpsay(void){ return g_powfs[0].pixpsay; }
+double oref_areascale(void){ return g_powfs[0].areascale; }
+double oref_dtheta(void){ return g_powfs[0].dtf[0].dtheta; }
+int oref_llt_nx(void){ return g_powfs[0].llt?(int)g_powfs[0].llt->pts->nxsa:0; }
+
+static void copy_vec(double* out, const double* in, long n){ memcpy(out, in, sizeof(double)*n); }
+
+void oref_get_saloc(double* x, double* y){
+	long n=g_powfs[0].saloc->nloc;
+	copy_vec(x, g_powfs[0].saloc->locx, n);
+	copy_vec(y, g_powfs[0].saloc->locy, n);
+}
+void oref_get_ptsorig(double* x, double* y){
+	long n=g_powfs[0].pts->nsa;
+	for(long i=0; i<n; i++){ x[i]=g_powfs[0].pts->origx[i]; y[i]=g_powfs[0].pts->origy[i]; }
+}
+double oref_get_ptsdx(void){ return g_powfs[0].pts->dx; }
+void oref_get_amp(double* amp){ dmat* a=P(g_powfs[0].amp, 0); copy_vec(amp, P(a), PN(a)); }
+void oref_get_saa(double* saa){ dmat* a=P(g_powfs[0].saa, 0); copy_vec(saa, P(a), PN(a)); }
+/* nominal DTF (treated, peak in corner with chess pattern) for subaperture isa */
+void oref_get_nominal(int isa, double* out){
+	dcell* nom=g_powfs[0].dtf[0].nominal;
+	dmat* n=PN(nom)==1?P(nom, 0):P(nom, isa);
+	copy_vec(out, P(n), PN(n));
+}
+/* pixel sampling matrix si (npix x notf^2) of subaperture isa, dense, column-major */
+void oref_get_si_dense(int isa, double* out){
+	dspcell* sis=g_powfs[0].dtf[0].si;
+	dsp* si=PN(sis)==1?P(sis, 0):P(sis, isa);
+	long nr=si->nx, nc=si->ny;
+	memset(out, 0, sizeof(double)*nr*nc);
+	for(long ic=0; ic<nc; ic++){
+		for(long k=si->pp[ic]; k<si->pp[ic+1]; k++){
+			out[si->pi[k]+ic*nr]+=si->px[k];
+		}
+	}
+}
+/* ETF with the nominal fused in, subaperture isa, interleaved complex notf^2 */
+void oref_get_etf(int isa, double* out){
+	cmat* e=P(g_powfs[0].etfsim[0].etf, isa, 0);
+	copy_vec(out, (double*)P(e), 2*PN(e));
+}
+void oref_get_srot(double* out){ dmat* a=P(g_powfs[0].srot, 0); copy_vec(out, P(a), PN(a)); }
+void oref_get_srsa(double* out){ dmat* a=P(g_powfs[0].srsa, 0); copy_vec(out, P(a), PN(a)); }
+void oref_get_lltamp(double* out){ copy_vec(out, P(g_powfs[0].llt->amp), PN(g_powfs[0].llt->amp)); }
+/* matched filter of subaperture isa: 2 x npix column-major */
+void oref_get_mtche(int isa, double* out){
+	dmat* m=P(g_powfs[0].intstat->mtche, isa, 0);
+	copy_vec(out, P(m), PN(m));
+}
+void oref_get_i0sum(double* out){
+	dmat* s=g_powfs[0].intstat->i0sum;
+	for(long i=0; i<NX(s); i++) out[i]=P(s, i, 0);
+}
+double oref_get_i0sumsum(void){ return P(g_powfs[0].intstat->i0sumsum, 0); }
+void oref_get_i0(int isa, double* i0, double* gx, double* gy){
+	intstat_t* st=g_powfs[0].intstat;
+	copy_vec(i0, P(P(st->i0, isa, 0)), PN(P(st->i0, isa, 0)));
+	if(gx) copy_vec(gx, P(P(st->gx, isa, 0)), PN(P(st->gx, isa, 0)));
+	if(gy) copy_vec(gy, P(P(st->gy, isa, 0)), PN(P(st->gy, isa, 0)));
+}
+
+/* One WFS frame of wfsints() over subapertures [isa0, isa1), single thread.
+   opd: nsa*nopd^2; lltopd: nlx^2 or NULL; ints: nsa*npix accumulated. */
+void oref_wfsints(int iwfs, const double* opd, const double* lltopd, double* ints, int isa0, int isa1, int isim){
+	const long nsa=g_powfs[0].saloc->nloc;
+	const long nopd=g_powfs[0].pts->nxsa;
+	const long npx=g_powfs[0].pixpsax, npy=g_powfs[0].pixpsay;
+	dmat* dopd=dnew_do(nsa*nopd*nopd, 1, (double*)opd, 0);
+	dmat* dllt=NULL;
+	if(lltopd){
+		long nlx=g_powfs[0].llt->pts->nxsa;
+		dllt=dnew_do(nlx, nlx, (double*)lltopd, 0);
+	}
+	dcell* dints=dcellnew(nsa, 1);
+	for(long isa=0; isa<nsa; isa++){
+		P(dints, isa)=dnew_do(npx, npy, ints+isa*npx*npy, 0);
+	}
+	wfsints_t data={0};
+	data.ints=dints;
+	data.opd=dopd;
+	data.lltopd=dllt;
+	data.iwfs=iwfs;
+	data.isim=isim;
+	thread_t thd={0};
+	thd.start=isa0;
+	thd.end=isa1;
+	thd.nthread=1;
+	thd.data=&data;
+	wfsints(&thd);
+	dcellfree(dints);
+	dfree(dopd);
+	dfree(dllt);
+}
+
+/* Gradients of one WFS from ints (nsa*npix); grad: 2*nsa (x then y). */
+void oref_shwfs_grad(int iwfs, const double* ints, double* grad){
+	const long nsa=g_powfs[0].saloc->nloc;
+	const long npx=g_powfs[0].pixpsax, npy=g_powfs[0].pixpsay;
+	dmat** pints=mycalloc(nsa, dmat*);
+	for(long isa=0; isa<nsa; isa++){
+		pints[isa]=dnew_do(npx, npy, (double*)ints+isa*npx*npy, 0);
+	}
+	dmat* g=dnew_do(2*nsa, 1, grad, 0);
+	shwfs_grad(&g, pints, g_parms, g_powfs, iwfs, g_parms->powfs[0].phytype_sim);
+	for(long isa=0; isa<nsa; isa++) dfree(pints[isa]);
+	free(pints);
+	dfree(g);
+}
+
+/* Photon + read noise on ints (nsa*npix) with the reference's MT19937 stream. */
+void oref_addnoise(double* ints, long n, unsigned int seed, double bkgrnd, double bkgrndc, double rne){
+	rand_t rstat;
+	seed_rand(&rstat, seed);
+	dmat* a=dnew_do(n, 1, ints, 0);
+	addnoise(a, &rstat, bkgrnd, bkgrndc, NULL, NULL, NULL, rne, 1.);
+	dfree(a);
+}
+
+/* Ray trace one layer into the WFS OPD points (accumulates into opd). */
+void oref_prop_layer(const double* screen, long nx, long ny, double dx, double ox, double oy, double ht,
+	double thetax, double thetay, double hs, double shiftx, double shifty, double alpha, int wrap,
+	double* opd, int isa0, int isa1){
+	map_t* m=mapnew(nx, ny, dx, dx);
+	memcpy(P(m), screen, sizeof(double)*nx*ny);
+	m->ox=ox; m->oy=oy; m->ht=ht;
+	prop_range(&(propdata_t){.mapin=m, .ptsout=g_powfs[0].pts, .phiout=opd, .alpha=alpha,
+		.hs=hs, .thetax=thetax, .thetay=thetay, .shiftx=shiftx, .shifty=shifty, .wrap=wrap}, isa0, isa1);
+	mapfree(m);
+}
+/* Ray trace one layer into the LLT pupil (nlx^2, accumulates) as maos/wfsgrad.c:337-365. */
+void oref_prop_llt(const double* screen, long nx, long ny, double dx, double ox, double oy, double ht,
+	double thetax, double thetay, double hs, double shiftx, double shifty, double* lltopd){
+	map_t* m=mapnew(nx, ny, dx, dx);
+	memcpy(P(m), screen, sizeof(double)*nx*ny);
+	m->ox=ox; m->oy=oy; m->ht=ht;
+	prop(&(propdata_t){.mapin=m, .ptsout=g_powfs[0].llt->pts, .phiout=lltopd, .alpha=1,
+		.hs=hs, .thetax=thetax, .thetay=thetay, .shiftx=shiftx, .shifty=shifty, .wrap=1});
+	mapfree(m);
+}
+
+/* The known-answer screen of test/cmocka_psd.c: genatm_simple(r0, L0, slope, dx, n, seed). */
+void oref_genatm_simple(double r0, double L0, double slope, double dx, long n, unsigned int seed, double* out){
+	dmat* s=genatm_simple(r0, L0, slope, dx, n, seed);
+	copy_vec(out, P(s), PN(s));
+	dfree(s);
+}
+
+/* Uniform and normal draws from the reference's RNG, for checking a restatement. */
+void oref_rand_stream(unsigned int seed, long n, double* u, double* g, long* pois, double pois_mean){
+	rand_t rstat;
+	seed_rand(&rstat, seed);
+	for(long i=0; i<n; i++){
+		if(u) u[i]=randu(&rstat);
+		if(g) g[i]=randn(&rstat);
+		if(pois) pois[i]=randp(&rstat, pois_mean);
+	}
+}
+
+/* The reference's multithreaded CPU frame for one WFS, as the MAOS time step
+   runs it: wfsints over thread_prep(0,nsa,NTHREAD) (maos/sim_utils.c:1072-1079),
+   then addnoise per subaperture and shwfs_grad.  Returns seconds spent. */
+double oref_frame_mt(int iwfs, const double* opd, const double* lltopd, double* ints, double* grad,
+	unsigned int seed, int noisy){
+	const long nsa=g_powfs[0].saloc->nloc;
+	const long nopd=g_powfs[0].pts->nxsa;
+	const long npx=g_powfs[0].pixpsax, npy=g_powfs[0].pixpsay;
+	double t0=omp_get_wtime();
+	dmat* dopd=dnew_do(nsa*nopd*nopd, 1, (double*)opd, 0);
+	dmat* dllt=NULL;
+	if(lltopd){
+		long nlx=g_powfs[0].llt->pts->nxsa;
+		dllt=dnew_do(nlx, nlx, (double*)lltopd, 0);
+	}
+	dcell* dints=dcellnew(nsa, 1);
+	for(long isa=0; isa<nsa; isa++){
+		P(dints, isa)=dnew_do(npx, npy, ints+isa*npx*npy, 0);
+		dzero(P(dints, isa));
+	}
+	wfsints_t data={0};
+	data.ints=dints;
+	data.opd=dopd;
+	data.lltopd=dllt;
+	data.iwfs=iwfs;
+	thread_t* thd=thread_prep(0, nsa, NTHREAD, wfsints, &data);
+	CALL_THREAD(thd, 1);
+	free(thd);
+	if(noisy){
+		rand_t rstat;
+		seed_rand(&rstat, seed);
+		const real bkgrnd=g_parms->powfs[0].bkgrnd;
+		const real bkgrndc=bkgrnd*g_parms->powfs[0].bkgrndc;
+		for(long isa=0; isa<nsa; isa++){
+			addnoise(P(dints, isa), &rstat, bkgrnd, bkgrndc, NULL, NULL, NULL, g_parms->powfs[0].rne, 1.);
+		}
+	}
+	dmat* g=dnew_do(2*nsa, 1, grad, 0);
+	shwfs_grad(&g, P(dints), g_parms, g_powfs, iwfs, g_parms->powfs[0].phytype_sim);
+	double t1=omp_get_wtime();
+	dfree(g);
+	dcellfree(dints);
+	dfree(dopd);
+	dfree(dllt);
+	return t1-t0;
+}
+
+/* The known-answer numbers of test/cmocka_psd.c for the screen
+   genatm_simple(0.186, 0, -11/3, 1/64, 128, seed=1):
+   out[0]=rms (nm), out[1]=psd2d_aniso integral (nm), out[2]=psd2d integral
+   (nm), out[3]=fitted r0, out[4]=fitted slope, out[5]=sum(stfun)*1e9,
+   out[6]=max(stfun)*1e13. */
+void oref_kat_psd(double* out){
+	dmat* screen=(dmat*)genatm_simple(0.186, 0, -11./3., 1./64., 128, 1);
+	dmat* psd=psd2d_aniso(screen, 1./64.);
+	out[1]=sqrt(psd_inte2(psd))*1e9;
+	dfree(psd);
+	dmat* extra=NULL;
+	psd=psd2d(&extra, screen, 1./64.);
+	out[2]=sqrt(psd_inte2(psd))*1e9;
+	out[0]=sqrt(dsumsq(screen)/PN(screen))*1e9;
+	out[3]=P(extra, 0);
+	out[4]=P(extra, 1);
+	dfree(extra);
+	dfree(psd);
+	dmat* st=stfun_batch(screen, NULL);
+	out[5]=dsum(st)*1e9;
+	out[6]=dmax(st)*1e13;
+	dfree(st);
+	dfree(screen);
+}
