@@ -1,0 +1,186 @@
+/*
+ * shwfs_b200.h -- C ABI of the B200 Shack-Hartmann wavefront-sensor frame.
+ *
+ * One frame of a physical-optics Shack-Hartmann WFS, per WFS:
+ *   (a) ray trace of the turbulence layers into the subaperture OPD points,
+ *   (b) field  amp*exp(i*2*pi*opd/wvl) embedded in an n_w x n_w grid,
+ *   (c) |FFT|^2 -> PSF -> FFT -> OTF x uplink OTF* x (ETF or DTF nominal)
+ *       -> inverse FFT -> real part sampled onto the detector pixels,
+ *   (d) photon (Poisson) and read-out (Gaussian) noise,
+ *   (e) centre-of-gravity or matched-filter gradients.
+ *
+ * The entry points replace the GPU seam of the reference simulator
+ * (cuda/sim/gpu_sim.h:39-48): the static data that the reference uploads in
+ * gpu_wfsgrad_init / gpu_wfsgrad_update_etf / gpu_wfsgrad_update_ref /
+ * gpu_atm2gpu / gpu_wfsgrad_seeding is passed here as plain arrays, and
+ * gpu_wfsgrad_queue + gpu_wfsgrad_sync become shwfs_frame_queue +
+ * shwfs_frame_sync.  All arrays use the reference's layouts: column-major
+ * (x fastest), subaperture-major, complex numbers as interleaved (re, im).
+ * Angles are in radians, lengths in metres.
+ *
+ * Every call returns 0 on success or a negative SHWFS_E* code; the message of
+ * the last failure on a context is returned by shwfs_last_error().  Calls on
+ * one context must not overlap from several host threads; distinct contexts
+ * are independent.
+ */
+#ifndef SHWFS_B200_H
+#define SHWFS_B200_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SHWFS_OK 0
+#define SHWFS_EINVAL (-1)   /* invalid argument or size */
+#define SHWFS_ECUDA (-2)    /* CUDA runtime error */
+#define SHWFS_ESTATE (-3)   /* call out of order (missing setup) */
+#define SHWFS_ENOMEM (-4)   /* device allocation failed or over budget */
+#define SHWFS_ETIMEOUT (-5) /* a bounded device wait expired */
+
+typedef struct shwfs_ctx shwfs_ctx;
+
+/* Gradient algorithms (maos/utils.c:983-1122, cuda/sim/wfsgrad.cu:413-478). */
+#define SHWFS_GRAD_MF 1   /* matched filter, PTYPE_MF */
+#define SHWFS_GRAD_COG 2  /* thresholded centre of gravity, PTYPE_COG */
+
+/* Imaging forms. */
+#define SHWFS_FORM_FFT 0  /* FP32 shared-memory/register FFT */
+#define SHWFS_FORM_TC 1   /* DFT as BF16x3 split products on tcgen05 tensor cores */
+
+/*
+ * Static description of one powfs (a group of identical WFS).  Mirrors the
+ * fields of the reference's powfs_cfg_t / powfs_t that the frame reads
+ * (maos/parms.h:152-330, maos/types.h powfs_t).
+ */
+typedef struct shwfs_powfs_desc {
+	int nsa;          /* valid subapertures (powfs.saloc->nloc) */
+	int nopd;         /* OPD points per subaperture side (pts->nxsa) */
+	int embfac;       /* embedding factor, n_w = nopd*embfac */
+	int notf;         /* OTF size n_f (powfs.notfx == notfy) */
+	int pixpsax;      /* detector pixels along x */
+	int pixpsay;      /* detector pixels along y */
+	double pixthetax; /* pixel size along x (radpixtheta) */
+	double pixthetay; /* pixel size along y (pixtheta) */
+	double wvl;       /* wavelength (single band) */
+	double dsa;       /* subaperture size (pts->dsa) */
+	double dx;        /* OPD sampling (pts->dx) */
+	double areascale; /* powfs.areascale */
+	double hs;        /* guide star range; INFINITY for NGS */
+	int has_etf;      /* 1: per-subaperture ETF with the nominal fused (LGS) */
+	int has_llt;      /* 1: compute the uplink OTF from the LLT OPD each frame */
+	int llt_nx;       /* LLT pupil points per side (llt->pts->nxsa) */
+	double llt_ox, llt_oy; /* LLT position in the pupil */
+	double llt_origx, llt_origy; /* llt->pts->origx[0], origy[0] */
+	int gradtype;     /* SHWFS_GRAD_MF or SHWFS_GRAD_COG */
+	int sigmatch;     /* 0, 1 or 2 (powfs.sigmatch) */
+	double cogthres;  /* powfs.cogthres */
+	double cogoff;    /* powfs.cogoff */
+	double rne;       /* read noise per pixel (e-) */
+	double bkgrnd;    /* background per pixel per frame (bkgrnd*dtrat) */
+	double bkgrndc;   /* calibrated background per pixel per frame (bkgrnd*dtrat*bkgrndc) */
+	double saat;      /* subaperture area threshold (CoG skips saa<saat) */
+	double sigtot_cog;/* expected signal for sigmatch==0 CoG (siglev*dtrat) */
+} shwfs_powfs_desc;
+
+/* One WFS of a powfs (maos/parms.h wfs_cfg_t). */
+typedef struct shwfs_wfs_desc {
+	int ipowfs;
+	double thetax, thetay; /* direction */
+	double hs;             /* range of the star (INFINITY for NGS) */
+	double hc;             /* conjugation height of the pupil (0) */
+	double misregx, misregy;
+	double sigsim;         /* photons per full subaperture per frame */
+	double wvlwt;          /* wavelength weight (single band: 1) */
+	int noisy;             /* add photon and read noise */
+} shwfs_wfs_desc;
+
+/* One turbulence layer (map_t with wind; cuda/sim/atm.cu). */
+typedef struct shwfs_layer_desc {
+	long nx, ny;      /* screen size (x fastest) */
+	double dx;        /* screen sampling */
+	double ox, oy;    /* coordinate of screen element (0,0) */
+	double ht;        /* altitude */
+	double vx, vy;    /* wind velocity */
+	double alpha;     /* scaling (atmscale*wt) */
+} shwfs_layer_desc;
+
+/* ---- context ---- */
+int shwfs_create(shwfs_ctx** pctx, int device);
+int shwfs_destroy(shwfs_ctx* ctx);
+const char* shwfs_last_error(const shwfs_ctx* ctx);
+/* Version string of the library build. */
+const char* shwfs_version(void);
+
+/* ---- static data (replaces gpu_wfsgrad_init, cuda/sim/wfsinit.cu:159) ---- */
+/* Declares a powfs; *ipowfs receives its index. */
+int shwfs_powfs_add(shwfs_ctx* ctx, const shwfs_powfs_desc* desc, int* ipowfs);
+/* Subaperture OPD-grid origins pts->origx/origy (nsa each) and the amplitude
+   map powfs.amp (namp x nsa*nopd^2; namp is 1 or the number of WFS). */
+int shwfs_powfs_set_geom(shwfs_ctx* ctx, int ipowfs, const double* origx, const double* origy,
+	const double* amp, int namp, const double* saa);
+/* DTF nominal (dtf[0].nominal, notf^2 real, treated: peak in corner with the
+   fftshift folded in, lib/mkdtf.c:26-80); nnominal is 1 or nsa. */
+int shwfs_powfs_set_nominal(shwfs_ctx* ctx, int ipowfs, const double* nominal, int nnominal);
+/* Pixel sampling map (dtf[0].si, lib/mkdtf.c:158-161 via lib/mkh.c:62):
+   for each of nmap maps (1 or nsa) and each pixel, up to 4 (index, weight)
+   pairs into the notf^2 PSF; index -1 marks an unused slot.
+   idx/wt: nmap*npix*4 entries. */
+int shwfs_powfs_set_simap(shwfs_ctx* ctx, int ipowfs, const int* idx, const double* wt, int nmap);
+/* Elongation transfer function with the nominal fused in
+   (etfsim[0].etf, nsa x notf^2 complex; lib/mkdtf.c:186-396).
+   slot 0 = etf[0]; slot 1 = second profile for time interpolation
+   (gpu_wfsgrad_update_etf, cuda/sim/wfsinit.cu:32). */
+int shwfs_powfs_set_etf(shwfs_ctx* ctx, int ipowfs, const double* etf, int slot);
+/* LLT pupil amplitude (llt->amp, llt_nx^2). */
+int shwfs_powfs_set_lltamp(shwfs_ctx* ctx, int ipowfs, const double* lltamp);
+
+/* Declares a WFS; *iwfs receives its index. */
+int shwfs_wfs_add(shwfs_ctx* ctx, const shwfs_wfs_desc* desc, int* iwfs);
+/* Matched filter mtche (nsa x 2 x npix, each subaperture a 2 x npix
+   column-major block), i0sum (nsa) and i0sumsum (gpu_wfsgrad_update_ref,
+   cuda/sim/wfsinit.cu:107). i0sum may be NULL for CoG. */
+int shwfs_wfs_set_mtche(shwfs_ctx* ctx, int iwfs, const double* mtche, const double* i0sum, double i0sumsum);
+/* Noise seed of one WFS (gpu_wfsgrad_seeding, cuda/sim/wfsinit.cu:532). */
+int shwfs_wfs_seed(shwfs_ctx* ctx, int iwfs, uint64_t seed);
+
+/* Turbulence screens (gpu_atm2gpu, cuda/sim/atm.cu:106): nlayer layers, FP64
+   host screens converted to FP32 device screens (screens[i] has nx*ny). */
+int shwfs_atm_set(shwfs_ctx* ctx, int nlayer, const shwfs_layer_desc* layers, const double* const* screens);
+
+/* Imaging form used by the frame calls (default SHWFS_FORM_FFT). */
+int shwfs_set_form(shwfs_ctx* ctx, int form);
+/* Wind shift time step: frame isim shifts layer l by -v*dt*isim. */
+int shwfs_set_dt(shwfs_ctx* ctx, double dt);
+
+/* ---- per frame (replaces gpu_wfsgrad_queue / gpu_wfsgrad_sync) ---- */
+/* Queue one frame of every WFS in [iwfs0, iwfs1) on the context stream:
+   ray trace, imaging, noise, gradients.  Asynchronous. */
+int shwfs_frame_queue(shwfs_ctx* ctx, int isim, int iwfs0, int iwfs1);
+/* Wait for the queued frame and copy WFS iwfs's gradients (2*nsa: x then y)
+   and optionally its pixel intensities (nsa*npix) to host memory. */
+int shwfs_frame_sync(shwfs_ctx* ctx, int iwfs, double* grad, double* ints);
+
+/* ---- stage entry points (device pointers; used by callers that hold the
+        OPD already, and by the parity tests) ---- */
+/* (a) Ray trace of all layers for WFS iwfs at frame isim into opd
+   (device, nsa*nopd^2 FP32, overwritten). */
+int shwfs_raytrace_dev(shwfs_ctx* ctx, int iwfs, int isim, float* opd);
+/* (b)-(e) from a given OPD (device, nsa*nopd^2 FP32) and optional LLT OPD
+   (device, llt_nx^2 FP32 or NULL).  ints (device, nsa*npix FP32) and grad
+   (device, 2*nsa FP32) are overwritten; either may be NULL when not wanted,
+   except that gradients need ints internally.  isim selects the noise
+   counter; noise is added only if the WFS is noisy and add_noise != 0. */
+int shwfs_ints_grad_dev(shwfs_ctx* ctx, int iwfs, int isim, const float* opd, const float* lltopd,
+	float* ints, float* grad, int add_noise);
+/* (e) alone: gradients (device, 2*nsa) from pixel intensities (device, nsa*npix). */
+int shwfs_grad_dev(shwfs_ctx* ctx, int iwfs, const float* ints, float* grad);
+/* Synchronise the context stream; returns the first error of queued work. */
+int shwfs_sync(shwfs_ctx* ctx);
+/* The CUDA stream the context launches on (cudaStream_t as void*). */
+void* shwfs_stream(shwfs_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

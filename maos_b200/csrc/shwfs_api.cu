@@ -1,0 +1,707 @@
+// C ABI of the B200 Shack-Hartmann frame (declared in include/shwfs_b200.h).
+//
+// The context owns device copies of the static data that the reference
+// uploads in gpu_wfsgrad_init (cuda/sim/wfsinit.cu:159-462), the per-WFS
+// frame buffers (cuwfs_t, cuda/sim/wfs.h:72-138) and the FP32 screens
+// (gpu_atm2gpu, cuda/sim/atm.cu:106).  Host data arrive in FP64 and MAOS
+// layouts; the ETF, DTF nominal and uplink OTF are stored transposed
+// (fy fastest) so that the imaging kernel reads them coalesced.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+#include <string>
+#include <vector>
+#include "../../include/shwfs_b200.h"
+#include "shwfs_kernels.cuh"
+
+using namespace shwfs;
+
+namespace {
+
+template <typename T>
+struct DevBuf {
+	T* p = nullptr;
+	size_t n = 0;
+	void free_() {
+		if (p) cudaFree(p);
+		p = nullptr;
+		n = 0;
+	}
+};
+
+struct PowfsState {
+	shwfs_powfs_desc d;
+	DevBuf<double> origx, origy;
+	DevBuf<float> amp;  // namp*nsa*nopd^2
+	int namp = 0;
+	DevBuf<float> saa;
+	DevBuf<float> nominalT;
+	int nnominal = 0;
+	DevBuf<int> simap_idx;
+	DevBuf<float> simap_wt;
+	int nsimap = 0;
+	DevBuf<float2> etfT[2];
+	float etfwt[2] = {1.f, 0.f};
+	DevBuf<float> lltamp;
+	DevBuf<double> lltorig;  // {llt origx, llt origy}
+	std::vector<double> origx_h, origy_h;
+};
+
+struct WfsState {
+	shwfs_wfs_desc d;
+	int wfsind = 0;  // index among the WFS of its powfs
+	DevBuf<float> mtche, i0sum;
+	double i0sumsum = 0;
+	DevBuf<float> opd, lltopd, ints, grad;
+	DevBuf<float2> lotfT;
+	uint64_t seed = 1;
+	float* grad_h = nullptr;  // pinned staging
+	float* ints_h = nullptr;
+};
+
+struct LayerState {
+	shwfs_layer_desc d;
+	DevBuf<float> screen;
+};
+
+}  // namespace
+
+struct shwfs_ctx {
+	int device = 0;
+	cudaStream_t stream = nullptr;
+	std::string err;
+	std::vector<PowfsState> powfs;
+	std::vector<WfsState> wfs;
+	std::vector<LayerState> atm;
+	double dt = 1.0 / 800;
+	int form = SHWFS_FORM_FFT;
+	DevBuf<WfsDev> wfsdev;  // staging for per-launch WFS descriptors
+	std::vector<WfsDev> wfsdev_h;
+	DevBuf<const float*> llt_in;
+	DevBuf<float2*> llt_out;
+};
+
+static int fail(shwfs_ctx* c, int code, const char* fmt, ...) {
+	char buf[512];
+	va_list ap;
+	va_start(ap, fmt);
+	vsnprintf(buf, sizeof(buf), fmt, ap);
+	va_end(ap);
+	if (c) c->err = buf;
+	return code;
+}
+#define CK(call)                                                                                        \
+	do {                                                                                                \
+		cudaError_t e_ = (call);                                                                        \
+		if (e_ != cudaSuccess) return fail(ctx, SHWFS_ECUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+	} while (0)
+
+template <typename T>
+static int dev_alloc(shwfs_ctx* ctx, DevBuf<T>& b, size_t n) {
+	if (b.n == n && b.p) return 0;
+	b.free_();
+	if (n == 0) return 0;
+	cudaError_t e = cudaMalloc(&b.p, n * sizeof(T));
+	if (e != cudaSuccess) {
+		b.p = nullptr;
+		return fail(ctx, SHWFS_ENOMEM, "cudaMalloc(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
+	}
+	b.n = n;
+	return 0;
+}
+template <typename T>
+static int dev_upload(shwfs_ctx* ctx, DevBuf<T>& b, const T* h, size_t n) {
+	int r = dev_alloc(ctx, b, n);
+	if (r) return r;
+	CK(cudaMemcpyAsync(b.p, h, n * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+	CK(cudaStreamSynchronize(ctx->stream));
+	return 0;
+}
+static int dev_upload_f(shwfs_ctx* ctx, DevBuf<float>& b, const double* h, size_t n) {
+	std::vector<float> t(n);
+	for (size_t i = 0; i < n; i++) t[i] = (float)h[i];
+	return dev_upload(ctx, b, t.data(), n);
+}
+
+static int set_device(shwfs_ctx* ctx) {
+	CK(cudaSetDevice(ctx->device));
+	return 0;
+}
+
+extern "C" {
+
+const char* shwfs_version(void) { return "shwfs_b200 1.0 (sm_100a)"; }
+
+int shwfs_create(shwfs_ctx** pctx, int device) {
+	if (!pctx) return SHWFS_EINVAL;
+	*pctx = nullptr;
+	shwfs_ctx* ctx = new shwfs_ctx();
+	ctx->device = device;
+	int ndev = 0;
+	cudaError_t e = cudaGetDeviceCount(&ndev);
+	if (e != cudaSuccess || device < 0 || device >= ndev) {
+		delete ctx;
+		return SHWFS_ECUDA;
+	}
+	if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+		delete ctx;
+		return SHWFS_ECUDA;
+	}
+	*pctx = ctx;
+	return 0;
+}
+
+int shwfs_destroy(shwfs_ctx* ctx) {
+	if (!ctx) return SHWFS_EINVAL;
+	cudaSetDevice(ctx->device);
+	cudaStreamSynchronize(ctx->stream);
+	for (auto& p : ctx->powfs) {
+		p.origx.free_();
+		p.origy.free_();
+		p.amp.free_();
+		p.saa.free_();
+		p.nominalT.free_();
+		p.simap_idx.free_();
+		p.simap_wt.free_();
+		p.etfT[0].free_();
+		p.etfT[1].free_();
+		p.lltamp.free_();
+		p.lltorig.free_();
+	}
+	for (auto& w : ctx->wfs) {
+		w.mtche.free_();
+		w.i0sum.free_();
+		w.opd.free_();
+		w.lltopd.free_();
+		w.ints.free_();
+		w.grad.free_();
+		w.lotfT.free_();
+		if (w.grad_h) cudaFreeHost(w.grad_h);
+		if (w.ints_h) cudaFreeHost(w.ints_h);
+	}
+	for (auto& l : ctx->atm) l.screen.free_();
+	ctx->wfsdev.free_();
+	ctx->llt_in.free_();
+	ctx->llt_out.free_();
+	cudaStreamDestroy(ctx->stream);
+	delete ctx;
+	return 0;
+}
+
+const char* shwfs_last_error(const shwfs_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+void* shwfs_stream(shwfs_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int shwfs_set_form(shwfs_ctx* ctx, int form) {
+	if (!ctx) return SHWFS_EINVAL;
+	if (form != SHWFS_FORM_FFT && form != SHWFS_FORM_TC) return fail(ctx, SHWFS_EINVAL, "unknown form %d", form);
+	ctx->form = form;
+	return 0;
+}
+int shwfs_set_dt(shwfs_ctx* ctx, double dt) {
+	if (!ctx || !(dt > 0)) return SHWFS_EINVAL;
+	ctx->dt = dt;
+	return 0;
+}
+
+int shwfs_powfs_add(shwfs_ctx* ctx, const shwfs_powfs_desc* d, int* ipowfs) {
+	if (!ctx || !d || !ipowfs) return SHWFS_EINVAL;
+	if (d->nsa <= 0 || d->nopd <= 0 || d->embfac <= 0 || d->notf <= 0 || d->pixpsax <= 0 || d->pixpsay <= 0)
+		return fail(ctx, SHWFS_EINVAL, "powfs: sizes must be positive");
+	const int nw = d->nopd * d->embfac;
+	if (!(d->nopd == 16 && nw == 32 && d->notf == 32))
+		return fail(ctx, SHWFS_EINVAL, "powfs: n_opd=%d n_w=%d n_f=%d not supported by this build (16/32/32)", d->nopd, nw,
+			d->notf);
+	if (d->pixpsax * d->pixpsay > 128) return fail(ctx, SHWFS_EINVAL, "powfs: at most 128 pixels per subaperture");
+	if (d->gradtype != SHWFS_GRAD_MF && d->gradtype != SHWFS_GRAD_COG)
+		return fail(ctx, SHWFS_EINVAL, "powfs: gradtype must be SHWFS_GRAD_MF or SHWFS_GRAD_COG");
+	if (d->sigmatch < 0 || d->sigmatch > 2) return fail(ctx, SHWFS_EINVAL, "powfs: sigmatch must be 0, 1 or 2");
+	if (d->has_llt && d->llt_nx * d->embfac != 32)
+		return fail(ctx, SHWFS_EINVAL, "powfs: LLT pupil of %d points is not supported (needs %d)", d->llt_nx, 32 / d->embfac);
+	int r = set_device(ctx);
+	if (r) return r;
+	ctx->powfs.emplace_back();
+	ctx->powfs.back().d = *d;
+	*ipowfs = (int)ctx->powfs.size() - 1;
+	return 0;
+}
+
+static PowfsState* get_powfs(shwfs_ctx* ctx, int ipowfs) {
+	if (!ctx || ipowfs < 0 || ipowfs >= (int)ctx->powfs.size()) return nullptr;
+	return &ctx->powfs[ipowfs];
+}
+static WfsState* get_wfs(shwfs_ctx* ctx, int iwfs) {
+	if (!ctx || iwfs < 0 || iwfs >= (int)ctx->wfs.size()) return nullptr;
+	return &ctx->wfs[iwfs];
+}
+
+int shwfs_powfs_set_geom(shwfs_ctx* ctx, int ipowfs, const double* origx, const double* origy, const double* amp,
+	int namp, const double* saa) {
+	PowfsState* p = get_powfs(ctx, ipowfs);
+	if (!p || !origx || !origy || !amp || namp <= 0) return ctx ? fail(ctx, SHWFS_EINVAL, "set_geom: bad arguments") : SHWFS_EINVAL;
+	int r = set_device(ctx);
+	if (r) return r;
+	const int nsa = p->d.nsa, n2 = p->d.nopd * p->d.nopd;
+	p->origx_h.assign(origx, origx + nsa);
+	p->origy_h.assign(origy, origy + nsa);
+	if ((r = dev_upload(ctx, p->origx, origx, nsa))) return r;
+	if ((r = dev_upload(ctx, p->origy, origy, nsa))) return r;
+	if ((r = dev_upload_f(ctx, p->amp, amp, (size_t)namp * nsa * n2))) return r;
+	p->namp = namp;
+	if (saa) {
+		if ((r = dev_upload_f(ctx, p->saa, saa, nsa))) return r;
+	}
+	return 0;
+}
+
+// transpose each notf x notf block: out[fy + n*fx] = in[fx + n*fy]
+static void transpose_blocks_real(const double* in, float* out, int nblk, int n) {
+	for (int b = 0; b < nblk; b++)
+		for (int fy = 0; fy < n; fy++)
+			for (int fx = 0; fx < n; fx++) out[(size_t)b * n * n + fy + n * fx] = (float)in[(size_t)b * n * n + fx + n * fy];
+}
+static void transpose_blocks_cplx(const double* in, float2* out, int nblk, int n) {
+	for (int b = 0; b < nblk; b++)
+		for (int fy = 0; fy < n; fy++)
+			for (int fx = 0; fx < n; fx++) {
+				const size_t i = (size_t)b * n * n + fx + n * fy;
+				out[(size_t)b * n * n + fy + n * fx] = make_float2((float)in[2 * i], (float)in[2 * i + 1]);
+			}
+}
+
+int shwfs_powfs_set_nominal(shwfs_ctx* ctx, int ipowfs, const double* nominal, int nnominal) {
+	PowfsState* p = get_powfs(ctx, ipowfs);
+	if (!p || !nominal || (nnominal != 1 && nnominal != p->d.nsa))
+		return ctx ? fail(ctx, SHWFS_EINVAL, "set_nominal: bad arguments") : SHWFS_EINVAL;
+	int r = set_device(ctx);
+	if (r) return r;
+	const int n = p->d.notf;
+	std::vector<float> t((size_t)nnominal * n * n);
+	transpose_blocks_real(nominal, t.data(), nnominal, n);
+	if ((r = dev_upload(ctx, p->nominalT, t.data(), t.size()))) return r;
+	p->nnominal = nnominal;
+	return 0;
+}
+
+int shwfs_powfs_set_simap(shwfs_ctx* ctx, int ipowfs, const int* idx, const double* wt, int nmap) {
+	PowfsState* p = get_powfs(ctx, ipowfs);
+	if (!p || !idx || !wt || (nmap != 1 && nmap != p->d.nsa)) return ctx ? fail(ctx, SHWFS_EINVAL, "set_simap: bad arguments") : SHWFS_EINVAL;
+	const int npix = p->d.pixpsax * p->d.pixpsay, n2 = p->d.notf * p->d.notf;
+	const size_t m = (size_t)nmap * npix * 4;
+	for (size_t i = 0; i < m; i++) {
+		if (idx[i] < -1 || idx[i] >= n2) return fail(ctx, SHWFS_EINVAL, "set_simap: index %d out of [-1,%d)", idx[i], n2);
+	}
+	int r = set_device(ctx);
+	if (r) return r;
+	if ((r = dev_upload(ctx, p->simap_idx, idx, m))) return r;
+	if ((r = dev_upload_f(ctx, p->simap_wt, wt, m))) return r;
+	p->nsimap = nmap;
+	return 0;
+}
+
+int shwfs_powfs_set_etf(shwfs_ctx* ctx, int ipowfs, const double* etf, int slot) {
+	PowfsState* p = get_powfs(ctx, ipowfs);
+	if (!p || !etf || slot < 0 || slot > 1) return ctx ? fail(ctx, SHWFS_EINVAL, "set_etf: bad arguments") : SHWFS_EINVAL;
+	int r = set_device(ctx);
+	if (r) return r;
+	const int n = p->d.notf;
+	std::vector<float2> t((size_t)p->d.nsa * n * n);
+	transpose_blocks_cplx(etf, t.data(), p->d.nsa, n);
+	if ((r = dev_upload(ctx, p->etfT[slot], t.data(), t.size()))) return r;
+	return 0;
+}
+
+int shwfs_powfs_set_lltamp(shwfs_ctx* ctx, int ipowfs, const double* lltamp) {
+	PowfsState* p = get_powfs(ctx, ipowfs);
+	if (!p || !lltamp || !p->d.has_llt) return ctx ? fail(ctx, SHWFS_EINVAL, "set_lltamp: bad arguments") : SHWFS_EINVAL;
+	int r = set_device(ctx);
+	if (r) return r;
+	const double orig[2] = {p->d.llt_origx, p->d.llt_origy};
+	if ((r = dev_upload(ctx, p->lltorig, orig, 2))) return r;
+	return dev_upload_f(ctx, p->lltamp, lltamp, (size_t)p->d.llt_nx * p->d.llt_nx);
+}
+
+int shwfs_wfs_add(shwfs_ctx* ctx, const shwfs_wfs_desc* d, int* iwfs) {
+	if (!ctx || !d || !iwfs) return SHWFS_EINVAL;
+	PowfsState* p = get_powfs(ctx, d->ipowfs);
+	if (!p) return fail(ctx, SHWFS_EINVAL, "wfs_add: unknown powfs %d", d->ipowfs);
+	int r = set_device(ctx);
+	if (r) return r;
+	ctx->wfs.emplace_back();
+	WfsState& w = ctx->wfs.back();
+	w.d = *d;
+	int count = 0;
+	for (size_t i = 0; i + 1 < ctx->wfs.size(); i++)
+		if (ctx->wfs[i].d.ipowfs == d->ipowfs) count++;
+	w.wfsind = count;
+	const int nsa = p->d.nsa, npix = p->d.pixpsax * p->d.pixpsay;
+	if ((r = dev_alloc(ctx, w.opd, (size_t)nsa * p->d.nopd * p->d.nopd))) return r;
+	if ((r = dev_alloc(ctx, w.ints, (size_t)nsa * npix))) return r;
+	if ((r = dev_alloc(ctx, w.grad, (size_t)2 * nsa))) return r;
+	CK(cudaMemsetAsync(w.grad.p, 0, sizeof(float) * 2 * nsa, ctx->stream));
+	if (p->d.has_llt) {
+		if ((r = dev_alloc(ctx, w.lltopd, (size_t)p->d.llt_nx * p->d.llt_nx))) return r;
+		if ((r = dev_alloc(ctx, w.lotfT, (size_t)p->d.notf * p->d.notf))) return r;
+	}
+	CK(cudaMallocHost(&w.grad_h, sizeof(float) * 2 * nsa));
+	CK(cudaMallocHost(&w.ints_h, sizeof(float) * nsa * npix));
+	CK(cudaStreamSynchronize(ctx->stream));
+	*iwfs = (int)ctx->wfs.size() - 1;
+	return 0;
+}
+
+int shwfs_wfs_set_mtche(shwfs_ctx* ctx, int iwfs, const double* mtche, const double* i0sum, double i0sumsum) {
+	WfsState* w = get_wfs(ctx, iwfs);
+	if (!w) return ctx ? fail(ctx, SHWFS_EINVAL, "set_mtche: unknown wfs %d", iwfs) : SHWFS_EINVAL;
+	PowfsState& p = ctx->powfs[w->d.ipowfs];
+	const int nsa = p.d.nsa, npix = p.d.pixpsax * p.d.pixpsay;
+	int r = set_device(ctx);
+	if (r) return r;
+	if (mtche && (r = dev_upload_f(ctx, w->mtche, mtche, (size_t)nsa * 2 * npix))) return r;
+	if (i0sum && (r = dev_upload_f(ctx, w->i0sum, i0sum, nsa))) return r;
+	w->i0sumsum = i0sumsum;
+	return 0;
+}
+
+int shwfs_wfs_seed(shwfs_ctx* ctx, int iwfs, uint64_t seed) {
+	WfsState* w = get_wfs(ctx, iwfs);
+	if (!w) return ctx ? fail(ctx, SHWFS_EINVAL, "wfs_seed: unknown wfs %d", iwfs) : SHWFS_EINVAL;
+	w->seed = seed;
+	return 0;
+}
+
+int shwfs_atm_set(shwfs_ctx* ctx, int nlayer, const shwfs_layer_desc* layers, const double* const* screens) {
+	if (!ctx || nlayer < 0 || nlayer > SHWFS_MAX_LAYERS || (nlayer && (!layers || !screens)))
+		return ctx ? fail(ctx, SHWFS_EINVAL, "atm_set: 0..%d layers", SHWFS_MAX_LAYERS) : SHWFS_EINVAL;
+	int r = set_device(ctx);
+	if (r) return r;
+	for (auto& l : ctx->atm) l.screen.free_();
+	ctx->atm.clear();
+	ctx->atm.resize(nlayer);
+	for (int i = 0; i < nlayer; i++) {
+		if (layers[i].nx < 2 || layers[i].ny < 2 || !(layers[i].dx > 0) || !screens[i])
+			return fail(ctx, SHWFS_EINVAL, "atm_set: layer %d is invalid", i);
+		ctx->atm[i].d = layers[i];
+		if ((r = dev_upload_f(ctx, ctx->atm[i].screen, screens[i], (size_t)layers[i].nx * layers[i].ny))) return r;
+	}
+	return 0;
+}
+
+}  // extern "C"
+
+// ---- frame machinery ----
+
+// Layer geometry of prop_range (lib/accphi.c:223-244) and prop_grid_pts
+// (lib/accphi_grid_do.c:408-434), FP64 on the host.
+static int build_raytrace(shwfs_ctx* ctx, const PowfsState& p, double thetax, double thetay, double hs, double hc,
+	double misregx, double misregy, double extra_shiftx, double extra_shifty, int isim, const double* origx,
+	const double* origy, int nsa, int nopd, double dx, float* out, RaytraceParams& rp) {
+	rp.origx = origx;
+	rp.origy = origy;
+	rp.dx = dx;
+	rp.nopd = nopd;
+	rp.nsa = nsa;
+	rp.opd = out;
+	rp.nlayer = 0;
+	for (const auto& L : ctx->atm) {
+		const shwfs_layer_desc& a = L.d;
+		const double ht = a.ht;
+		if (isfinite(hs) && hs != 0 && (hc > hs || ht > hs)) continue;
+		const double scale = (isfinite(hs) && hs != 0) ? 1. - (ht - hc) / (hs - hc) : 1.;
+		if (scale < 0) continue;
+		const double shiftx = -a.vx * ctx->dt * isim + extra_shiftx;
+		const double shifty = -a.vy * ctx->dt * isim + extra_shifty;
+		const double displacex = ht * thetax + scale * misregx + shiftx;
+		const double displacey = ht * thetay + scale * misregy + shifty;
+		LayerGeom& g = rp.layer[rp.nlayer++];
+		g.screen = L.screen.p;
+		g.nx = (int)a.nx;
+		g.ny = (int)a.ny;
+		const double dx_in1 = 1. / a.dx;
+		g.sx = scale * dx_in1;
+		g.dispx = (displacex - a.ox) * dx_in1;
+		g.dispy = (displacey - a.oy) * dx_in1;
+		g.alpha = (float)a.alpha;
+	}
+	(void)p;
+	return 0;
+}
+
+static int launch_raytrace(shwfs_ctx* ctx, WfsState& w, int isim, float* opd) {
+	PowfsState& p = ctx->powfs[w.d.ipowfs];
+	RaytraceParams rp;
+	build_raytrace(ctx, p, w.d.thetax, w.d.thetay, w.d.hs, w.d.hc, w.d.misregx, w.d.misregy, 0, 0, isim, p.origx.p,
+		p.origy.p, p.d.nsa, p.d.nopd, p.d.dx, opd, rp);
+	if (rp.nlayer == 0) {
+		CK(cudaMemsetAsync(opd, 0, sizeof(float) * p.d.nsa * p.d.nopd * p.d.nopd, ctx->stream));
+		return 0;
+	}
+	raytrace_kernel<<<p.d.nsa, p.d.nopd * p.d.nopd, 0, ctx->stream>>>(rp);
+	CK(cudaGetLastError());
+	return 0;
+}
+
+// LLT OPD (maos/wfsgrad.c:337-365): thetax - ox/hs, shift ox - v*dt*isim, wrap.
+// The LLT pupil is traced as one subaperture with origin llt->pts->origx/y.
+static int launch_lltopd(shwfs_ctx* ctx, WfsState& w, int isim) {
+	PowfsState& p = ctx->powfs[w.d.ipowfs];
+	RaytraceParams rp;
+	build_raytrace(ctx, p, w.d.thetax - p.d.llt_ox / w.d.hs, w.d.thetay - p.d.llt_oy / w.d.hs, w.d.hs, 0, 0, 0,
+		p.d.llt_ox, p.d.llt_oy, isim, p.lltorig.p, p.lltorig.p + 1, 1, p.d.llt_nx, p.d.dx, w.lltopd.p, rp);
+	if (rp.nlayer == 0) {
+		CK(cudaMemsetAsync(w.lltopd.p, 0, sizeof(float) * p.d.llt_nx * p.d.llt_nx, ctx->stream));
+		return 0;
+	}
+	raytrace_kernel<<<1, p.d.llt_nx * p.d.llt_nx, 0, ctx->stream>>>(rp);
+	CK(cudaGetLastError());
+	return 0;
+}
+
+static float norm_ints(const PowfsState& p, const WfsState& w) {
+	const double nwvf = (double)p.d.nopd * p.d.embfac;
+	const double norm_psf = sqrt(p.d.areascale) / ((double)p.d.nopd * nwvf);
+	return (float)(w.d.sigsim * w.d.wvlwt * norm_psf * norm_psf / ((double)p.d.notf * p.d.notf));
+}
+
+static PowfsDev make_powfs_dev(const PowfsState& p, int isim) {
+	PowfsDev P;
+	memset(&P, 0, sizeof(P));
+	P.nsa = p.d.nsa;
+	P.pixpsax = p.d.pixpsax;
+	P.pixpsay = p.d.pixpsay;
+	P.npix = p.d.pixpsax * p.d.pixpsay;
+	P.etfT1 = p.d.has_etf ? p.etfT[0].p : nullptr;
+	P.etfT2 = (p.d.has_etf && p.etfT[1].p) ? p.etfT[1].p : nullptr;
+	P.etfwt1 = p.etfwt[0];
+	P.etfwt2 = p.etfwt[1];
+	P.nominalT = p.d.has_etf ? nullptr : p.nominalT.p;
+	P.nominal_per_sa = p.nnominal > 1;
+	P.simap_idx = p.simap_idx.p;
+	P.simap_wt = p.simap_wt.p;
+	P.simap_per_sa = p.nsimap > 1;
+	P.gradtype = p.d.gradtype;
+	P.sigmatch = p.d.sigmatch;
+	P.cogthres = (float)p.d.cogthres;
+	P.cogoff = (float)p.d.cogoff;
+	P.pixthetax = (float)p.d.pixthetax;
+	P.pixthetay = (float)p.d.pixthetay;
+	P.saat = (float)p.d.saat;
+	P.sigtot = (float)p.d.sigtot_cog;
+	P.saa = p.saa.p;
+	P.twoinvwvl = (float)(2.0 / p.d.wvl);
+	P.rne = (float)p.d.rne;
+	P.bkgrnd = (float)p.d.bkgrnd;
+	P.bkgrndc = (float)p.d.bkgrndc;
+	P.isim = isim;
+	P.lltnorm = (float)(1.0 / ((double)p.d.llt_nx * p.d.embfac * p.d.llt_nx * p.d.embfac));
+	return P;
+}
+
+static int check_ready(shwfs_ctx* ctx, const PowfsState& p, const WfsState& w) {
+	if (!p.amp.p || !p.origx.p) return fail(ctx, SHWFS_ESTATE, "powfs geometry not set");
+	if (!p.simap_idx.p) return fail(ctx, SHWFS_ESTATE, "pixel sampling map not set");
+	if (p.d.has_etf && !p.etfT[0].p) return fail(ctx, SHWFS_ESTATE, "ETF not set");
+	if (!p.d.has_etf && !p.nominalT.p) return fail(ctx, SHWFS_ESTATE, "DTF nominal not set");
+	if (p.d.has_llt && !p.lltamp.p) return fail(ctx, SHWFS_ESTATE, "LLT amplitude not set");
+	if (p.d.gradtype == SHWFS_GRAD_MF && !w.mtche.p) return fail(ctx, SHWFS_ESTATE, "matched filter not set");
+	if (p.d.gradtype == SHWFS_GRAD_MF && p.d.sigmatch == 1 && !w.i0sum.p) return fail(ctx, SHWFS_ESTATE, "i0sum not set");
+	if (p.d.sigmatch == 2) return fail(ctx, SHWFS_EINVAL, "sigmatch=2 is not supported by this build");
+	return 0;
+}
+
+// (b)-(e) for a set of WFS of one powfs sharing the launch.
+static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist, int isim,
+	const std::vector<const float*>& opds, const std::vector<const float2*>& lotfs, const std::vector<float*>& ints,
+	const std::vector<float*>& grads, const std::vector<int>& noisy) {
+	PowfsState& p = ctx->powfs[ipowfs];
+	const int nw = (int)wlist.size();
+	if (nw == 0) return 0;
+	PowfsDev P = make_powfs_dev(p, isim);
+	std::vector<WfsDev> wd(nw);
+	for (int k = 0; k < nw; k++) {
+		WfsState& w = ctx->wfs[wlist[k]];
+		int r = check_ready(ctx, p, w);
+		if (r) return r;
+		WfsDev& d = wd[k];
+		d.opd = opds[k];
+		d.amp = p.amp.p + (p.namp > 1 ? (size_t)w.wfsind * p.d.nsa * p.d.nopd * p.d.nopd : 0);
+		d.lotfT = lotfs[k];
+		d.mtche = w.mtche.p;
+		d.i0sum = w.i0sum.p;
+		d.ints = ints[k];
+		d.grad = grads[k];
+		d.alpha = norm_ints(p, w);
+		d.noisy = noisy[k];
+		d.wfs_id = (uint32_t)wlist[k];
+		d.seed = w.seed;
+	}
+	// per-launch descriptors live in a device ring so queued launches never
+	// see them overwritten
+	const size_t need = ctx->wfsdev_h.size() + nw;
+	if (ctx->wfsdev.n < need) {
+		CK(cudaStreamSynchronize(ctx->stream));
+		ctx->wfsdev_h.clear();
+		int r = dev_alloc(ctx, ctx->wfsdev, need < 4096 ? 4096 : need * 2);
+		if (r) return r;
+	}
+	if (ctx->wfsdev_h.size() + nw > ctx->wfsdev.n) {
+		CK(cudaStreamSynchronize(ctx->stream));
+		ctx->wfsdev_h.clear();
+	}
+	const size_t off = ctx->wfsdev_h.size();
+	ctx->wfsdev_h.insert(ctx->wfsdev_h.end(), wd.begin(), wd.end());
+	CK(cudaMemcpyAsync(ctx->wfsdev.p + off, wd.data(), sizeof(WfsDev) * nw, cudaMemcpyHostToDevice, ctx->stream));
+	const int nitem = p.d.nsa * nw;
+	const int nblk = (nitem + 3) / 4;
+	const int npix = P.npix;
+	if (npix <= 32) {
+		ints_n32_kernel<1><<<nblk, 128, 0, ctx->stream>>>(P, ctx->wfsdev.p + off, nw, nitem);
+	} else if (npix <= 64) {
+		ints_n32_kernel<2><<<nblk, 128, 0, ctx->stream>>>(P, ctx->wfsdev.p + off, nw, nitem);
+	} else {
+		ints_n32_kernel<4><<<nblk, 128, 0, ctx->stream>>>(P, ctx->wfsdev.p + off, nw, nitem);
+	}
+	CK(cudaGetLastError());
+	return 0;
+}
+
+static int launch_uplink(shwfs_ctx* ctx, const std::vector<int>& wlist, const std::vector<const float*>& lltopd,
+	std::vector<const float2*>& lotfs) {
+	if (wlist.empty()) return 0;
+	PowfsState& p = ctx->powfs[ctx->wfs[wlist[0]].d.ipowfs];
+	const int nw = (int)wlist.size();
+	std::vector<const float*> in(nw);
+	std::vector<float2*> out(nw);
+	for (int k = 0; k < nw; k++) {
+		in[k] = lltopd[k];
+		out[k] = ctx->wfs[wlist[k]].lotfT.p;
+		lotfs[k] = out[k];
+	}
+	CK(cudaStreamSynchronize(ctx->stream));
+	int r;
+	if ((r = dev_alloc(ctx, ctx->llt_in, (size_t)nw))) return r;
+	if ((r = dev_alloc(ctx, ctx->llt_out, (size_t)nw))) return r;
+	CK(cudaMemcpyAsync(ctx->llt_in.p, in.data(), sizeof(float*) * nw, cudaMemcpyHostToDevice, ctx->stream));
+	CK(cudaMemcpyAsync(ctx->llt_out.p, out.data(), sizeof(float2*) * nw, cudaMemcpyHostToDevice, ctx->stream));
+	const float twoinvwvl = (float)(2.0 / p.d.wvl);
+	const float lltnorm = (float)(1.0 / ((double)p.d.llt_nx * p.d.embfac * p.d.llt_nx * p.d.embfac));
+	uplink_otf_n32_kernel<<<(nw + 3) / 4, 128, 0, ctx->stream>>>(ctx->llt_in.p, p.lltamp.p, ctx->llt_out.p, nw, twoinvwvl,
+		lltnorm);
+	CK(cudaGetLastError());
+	return 0;
+}
+
+extern "C" {
+
+int shwfs_raytrace_dev(shwfs_ctx* ctx, int iwfs, int isim, float* opd) {
+	WfsState* w = get_wfs(ctx, iwfs);
+	if (!w || !opd) return ctx ? fail(ctx, SHWFS_EINVAL, "raytrace: bad arguments") : SHWFS_EINVAL;
+	int r = set_device(ctx);
+	if (r) return r;
+	return launch_raytrace(ctx, *w, isim, opd);
+}
+
+int shwfs_ints_grad_dev(shwfs_ctx* ctx, int iwfs, int isim, const float* opd, const float* lltopd, float* ints,
+	float* grad, int add_noise) {
+	WfsState* w = get_wfs(ctx, iwfs);
+	if (!w || !opd) return ctx ? fail(ctx, SHWFS_EINVAL, "ints_grad: bad arguments") : SHWFS_EINVAL;
+	int r = set_device(ctx);
+	if (r) return r;
+	PowfsState& p = ctx->powfs[w->d.ipowfs];
+	std::vector<int> wl{iwfs};
+	std::vector<const float2*> lotf{nullptr};
+	if (p.d.has_llt) {
+		if (!lltopd) return fail(ctx, SHWFS_EINVAL, "ints_grad: LGS powfs needs the LLT OPD");
+		if (!p.lltamp.p) return fail(ctx, SHWFS_ESTATE, "LLT amplitude not set");
+		std::vector<const float*> lin{lltopd};
+		if ((r = launch_uplink(ctx, wl, lin, lotf))) return r;
+	}
+	std::vector<const float*> opds{opd};
+	std::vector<float*> in{ints}, gr{grad};
+	std::vector<int> nz{(add_noise && w->d.noisy) ? 1 : 0};
+	return launch_ints(ctx, w->d.ipowfs, wl, isim, opds, lotf, in, gr, nz);
+}
+
+int shwfs_grad_dev(shwfs_ctx* ctx, int iwfs, const float* ints, float* grad) {
+	WfsState* w = get_wfs(ctx, iwfs);
+	if (!w || !ints || !grad) return ctx ? fail(ctx, SHWFS_EINVAL, "grad: bad arguments") : SHWFS_EINVAL;
+	int r = set_device(ctx);
+	if (r) return r;
+	PowfsState& p = ctx->powfs[w->d.ipowfs];
+	if (p.d.gradtype == SHWFS_GRAD_MF && !w->mtche.p) return fail(ctx, SHWFS_ESTATE, "matched filter not set");
+	if (p.d.sigmatch == 2) return fail(ctx, SHWFS_EINVAL, "sigmatch=2 is not supported by this build");
+	PowfsDev P = make_powfs_dev(p, 0);
+	const int nblk = (p.d.nsa + 3) / 4;
+	if (P.npix <= 32)
+		grad_kernel<1><<<nblk, 128, 0, ctx->stream>>>(P, ints, w->mtche.p, w->i0sum.p, grad);
+	else if (P.npix <= 64)
+		grad_kernel<2><<<nblk, 128, 0, ctx->stream>>>(P, ints, w->mtche.p, w->i0sum.p, grad);
+	else
+		grad_kernel<4><<<nblk, 128, 0, ctx->stream>>>(P, ints, w->mtche.p, w->i0sum.p, grad);
+	CK(cudaGetLastError());
+	return 0;
+}
+
+int shwfs_frame_queue(shwfs_ctx* ctx, int isim, int iwfs0, int iwfs1) {
+	if (!ctx || iwfs0 < 0 || iwfs1 > (int)ctx->wfs.size() || iwfs0 >= iwfs1)
+		return ctx ? fail(ctx, SHWFS_EINVAL, "frame_queue: bad WFS range") : SHWFS_EINVAL;
+	int r = set_device(ctx);
+	if (r) return r;
+	for (size_t ip = 0; ip < ctx->powfs.size(); ip++) {
+		std::vector<int> wl;
+		for (int i = iwfs0; i < iwfs1; i++)
+			if (ctx->wfs[i].d.ipowfs == (int)ip) wl.push_back(i);
+		if (wl.empty()) continue;
+		PowfsState& p = ctx->powfs[ip];
+		std::vector<const float*> opds, llts;
+		std::vector<const float2*> lotf(wl.size(), nullptr);
+		std::vector<float*> in, gr;
+		std::vector<int> nz;
+		for (int i : wl) {
+			WfsState& w = ctx->wfs[i];
+			if ((r = launch_raytrace(ctx, w, isim, w.opd.p))) return r;
+			if (p.d.has_llt) {
+				if ((r = launch_lltopd(ctx, w, isim))) return r;
+				llts.push_back(w.lltopd.p);
+			}
+			opds.push_back(w.opd.p);
+			in.push_back(w.ints.p);
+			gr.push_back(w.grad.p);
+			nz.push_back(w.d.noisy);
+		}
+		if (p.d.has_llt && (r = launch_uplink(ctx, wl, llts, lotf))) return r;
+		if ((r = launch_ints(ctx, (int)ip, wl, isim, opds, lotf, in, gr, nz))) return r;
+	}
+	return 0;
+}
+
+int shwfs_frame_sync(shwfs_ctx* ctx, int iwfs, double* grad, double* ints) {
+	WfsState* w = get_wfs(ctx, iwfs);
+	if (!w) return ctx ? fail(ctx, SHWFS_EINVAL, "frame_sync: unknown wfs %d", iwfs) : SHWFS_EINVAL;
+	int r = set_device(ctx);
+	if (r) return r;
+	PowfsState& p = ctx->powfs[w->d.ipowfs];
+	const int nsa = p.d.nsa, npix = p.d.pixpsax * p.d.pixpsay;
+	if (grad) CK(cudaMemcpyAsync(w->grad_h, w->grad.p, sizeof(float) * 2 * nsa, cudaMemcpyDeviceToHost, ctx->stream));
+	if (ints) CK(cudaMemcpyAsync(w->ints_h, w->ints.p, sizeof(float) * nsa * npix, cudaMemcpyDeviceToHost, ctx->stream));
+	CK(cudaStreamSynchronize(ctx->stream));
+	ctx->wfsdev_h.clear();
+	if (grad)
+		for (int i = 0; i < 2 * nsa; i++) grad[i] = w->grad_h[i];
+	if (ints)
+		for (int i = 0; i < nsa * npix; i++) ints[i] = w->ints_h[i];
+	return 0;
+}
+
+int shwfs_sync(shwfs_ctx* ctx) {
+	if (!ctx) return SHWFS_EINVAL;
+	int r = set_device(ctx);
+	if (r) return r;
+	CK(cudaStreamSynchronize(ctx->stream));
+	ctx->wfsdev_h.clear();
+	return 0;
+}
+
+}  // extern "C"

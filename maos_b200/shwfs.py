@@ -1,0 +1,264 @@
+"""ctypes binding of the C ABI declared in include/shwfs_b200.h.
+
+This is the host-side mirror of the reference's GPU WFS seam
+(cuda/sim/gpu_sim.h:39-48): a :class:`Context` holds the static data of the
+powfs/WFS (what gpu_wfsgrad_init uploads), the turbulence screens (what
+gpu_atm2gpu uploads) and runs frames (gpu_wfsgrad_queue/sync).  Errors are
+raised as :class:`ShwfsError`, mirroring the reference's ``error()`` abort.
+
+There is no CPU fallback: if the native library is missing the import of this
+module fails.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libshwfs_b200.so")
+
+SHWFS_GRAD_MF = 1
+SHWFS_GRAD_COG = 2
+SHWFS_FORM_FFT = 0
+SHWFS_FORM_TC = 1
+
+
+class ShwfsError(RuntimeError):
+    pass
+
+
+class PowfsDesc(C.Structure):
+    _fields_ = [
+        ("nsa", C.c_int), ("nopd", C.c_int), ("embfac", C.c_int), ("notf", C.c_int),
+        ("pixpsax", C.c_int), ("pixpsay", C.c_int),
+        ("pixthetax", C.c_double), ("pixthetay", C.c_double),
+        ("wvl", C.c_double), ("dsa", C.c_double), ("dx", C.c_double), ("areascale", C.c_double),
+        ("hs", C.c_double),
+        ("has_etf", C.c_int), ("has_llt", C.c_int), ("llt_nx", C.c_int),
+        ("llt_ox", C.c_double), ("llt_oy", C.c_double), ("llt_origx", C.c_double), ("llt_origy", C.c_double),
+        ("gradtype", C.c_int), ("sigmatch", C.c_int),
+        ("cogthres", C.c_double), ("cogoff", C.c_double),
+        ("rne", C.c_double), ("bkgrnd", C.c_double), ("bkgrndc", C.c_double),
+        ("saat", C.c_double), ("sigtot_cog", C.c_double),
+    ]
+
+
+class WfsDesc(C.Structure):
+    _fields_ = [
+        ("ipowfs", C.c_int),
+        ("thetax", C.c_double), ("thetay", C.c_double),
+        ("hs", C.c_double), ("hc", C.c_double),
+        ("misregx", C.c_double), ("misregy", C.c_double),
+        ("sigsim", C.c_double), ("wvlwt", C.c_double),
+        ("noisy", C.c_int),
+    ]
+
+
+class LayerDesc(C.Structure):
+    _fields_ = [
+        ("nx", C.c_long), ("ny", C.c_long),
+        ("dx", C.c_double), ("ox", C.c_double), ("oy", C.c_double),
+        ("ht", C.c_double), ("vx", C.c_double), ("vy", C.c_double),
+        ("alpha", C.c_double),
+    ]
+
+
+def _load() -> C.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"native library {LIB_PATH} is missing; build it with `python -m maos_b200.build`")
+    lib = C.CDLL(LIB_PATH)
+    vp, ip, dp, i = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_int
+    sig = {
+        "shwfs_create": [C.POINTER(vp), i],
+        "shwfs_destroy": [vp],
+        "shwfs_powfs_add": [vp, C.POINTER(PowfsDesc), ip],
+        "shwfs_powfs_set_geom": [vp, i, dp, dp, dp, i, dp],
+        "shwfs_powfs_set_nominal": [vp, i, dp, i],
+        "shwfs_powfs_set_simap": [vp, i, ip, dp, i],
+        "shwfs_powfs_set_etf": [vp, i, dp, i],
+        "shwfs_powfs_set_lltamp": [vp, i, dp],
+        "shwfs_wfs_add": [vp, C.POINTER(WfsDesc), ip],
+        "shwfs_wfs_set_mtche": [vp, i, dp, dp, C.c_double],
+        "shwfs_wfs_seed": [vp, i, C.c_uint64],
+        "shwfs_atm_set": [vp, i, C.POINTER(LayerDesc), C.POINTER(dp)],
+        "shwfs_set_form": [vp, i],
+        "shwfs_set_dt": [vp, C.c_double],
+        "shwfs_frame_queue": [vp, i, i, i],
+        "shwfs_frame_sync": [vp, i, dp, dp],
+        "shwfs_raytrace_dev": [vp, i, i, vp],
+        "shwfs_ints_grad_dev": [vp, i, i, vp, vp, vp, vp, i],
+        "shwfs_grad_dev": [vp, i, vp, vp],
+        "shwfs_sync": [vp],
+    }
+    for name, args in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = C.c_int
+    lib.shwfs_last_error.argtypes = [vp]
+    lib.shwfs_last_error.restype = C.c_char_p
+    lib.shwfs_version.argtypes = []
+    lib.shwfs_version.restype = C.c_char_p
+    lib.shwfs_stream.argtypes = [vp]
+    lib.shwfs_stream.restype = vp
+    return lib
+
+
+_lib: Optional[C.CDLL] = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        _lib = _load()
+    return _lib
+
+
+def _dptr(a: Optional[np.ndarray]):
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _devptr(t) -> Optional[int]:
+    """Device address of a torch tensor (or an int address)."""
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return t
+    return int(t.data_ptr())
+
+
+class Context:
+    """One device context: static powfs/WFS data, screens and frame buffers."""
+
+    def __init__(self, device: int = 0):
+        self._L = lib()
+        h = C.c_void_p()
+        rc = self._L.shwfs_create(C.byref(h), device)
+        if rc != 0:
+            raise ShwfsError(f"shwfs_create(device={device}) failed with {rc}")
+        self._h = h
+        self.npix = {}
+        self.nsa = {}
+
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            msg = self._L.shwfs_last_error(self._h)
+            raise ShwfsError(f"{what}: {msg.decode() if msg else rc} (status {rc})")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.shwfs_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def stream(self) -> int:
+        return int(self._L.shwfs_stream(self._h) or 0)
+
+    # ---- static data ----
+    def powfs_add(self, **kw) -> int:
+        d = PowfsDesc(**kw)
+        out = C.c_int()
+        self._check(self._L.shwfs_powfs_add(self._h, C.byref(d), C.byref(out)), "powfs_add")
+        self.npix[out.value] = d.pixpsax * d.pixpsay
+        self.nsa[out.value] = d.nsa
+        return out.value
+
+    def powfs_set_geom(self, ipowfs, origx, origy, amp, saa=None, namp=1):
+        ox, oy, am = _f64(origx), _f64(origy), _f64(amp)
+        sa = _f64(saa) if saa is not None else None
+        self._check(self._L.shwfs_powfs_set_geom(self._h, ipowfs, _dptr(ox), _dptr(oy), _dptr(am), namp, _dptr(sa)),
+                    "powfs_set_geom")
+
+    def powfs_set_nominal(self, ipowfs, nominal, nnominal=1):
+        a = _f64(nominal)
+        self._check(self._L.shwfs_powfs_set_nominal(self._h, ipowfs, _dptr(a), nnominal), "powfs_set_nominal")
+
+    def powfs_set_simap(self, ipowfs, idx, wt, nmap=1):
+        ii = np.ascontiguousarray(idx, dtype=np.int32)
+        ww = _f64(wt)
+        self._check(self._L.shwfs_powfs_set_simap(self._h, ipowfs, ii.ctypes.data_as(C.POINTER(C.c_int)), _dptr(ww),
+                                                   nmap), "powfs_set_simap")
+
+    def powfs_set_etf(self, ipowfs, etf, slot=0):
+        a = np.ascontiguousarray(etf, dtype=np.complex128).view(np.float64)
+        self._check(self._L.shwfs_powfs_set_etf(self._h, ipowfs, _dptr(a), slot), "powfs_set_etf")
+
+    def powfs_set_lltamp(self, ipowfs, lltamp):
+        a = _f64(lltamp)
+        self._check(self._L.shwfs_powfs_set_lltamp(self._h, ipowfs, _dptr(a)), "powfs_set_lltamp")
+
+    def wfs_add(self, **kw) -> int:
+        d = WfsDesc(**kw)
+        out = C.c_int()
+        self._check(self._L.shwfs_wfs_add(self._h, C.byref(d), C.byref(out)), "wfs_add")
+        return out.value
+
+    def wfs_set_mtche(self, iwfs, mtche, i0sum=None, i0sumsum=0.0):
+        m = _f64(mtche) if mtche is not None else None
+        s = _f64(i0sum) if i0sum is not None else None
+        self._check(self._L.shwfs_wfs_set_mtche(self._h, iwfs, _dptr(m), _dptr(s), float(i0sumsum)), "wfs_set_mtche")
+
+    def wfs_seed(self, iwfs, seed):
+        self._check(self._L.shwfs_wfs_seed(self._h, iwfs, int(seed) & 0xFFFFFFFFFFFFFFFF), "wfs_seed")
+
+    def atm_set(self, layers: Sequence[dict], screens: Sequence[np.ndarray]):
+        n = len(layers)
+        descs = (LayerDesc * max(n, 1))(*[LayerDesc(**l) for l in layers])
+        keep = [_f64(s) for s in screens]
+        ptrs = (C.POINTER(C.c_double) * max(n, 1))(*[_dptr(s) for s in keep])
+        self._check(self._L.shwfs_atm_set(self._h, n, descs, ptrs), "atm_set")
+
+    def set_form(self, form: int):
+        self._check(self._L.shwfs_set_form(self._h, form), "set_form")
+
+    def set_dt(self, dt: float):
+        self._check(self._L.shwfs_set_dt(self._h, float(dt)), "set_dt")
+
+    # ---- frames ----
+    def frame_queue(self, isim: int, iwfs0: int, iwfs1: int):
+        self._check(self._L.shwfs_frame_queue(self._h, isim, iwfs0, iwfs1), "frame_queue")
+
+    def frame_sync(self, iwfs: int, ipowfs: int, want_ints: bool = False):
+        nsa = self.nsa[ipowfs]
+        g = np.zeros(2 * nsa)
+        ints = np.zeros(nsa * self.npix[ipowfs]) if want_ints else None
+        self._check(self._L.shwfs_frame_sync(self._h, iwfs, _dptr(g), _dptr(ints)), "frame_sync")
+        return (g, ints) if want_ints else g
+
+    def raytrace_dev(self, iwfs, isim, opd):
+        self._check(self._L.shwfs_raytrace_dev(self._h, iwfs, isim, _devptr(opd)), "raytrace_dev")
+
+    def ints_grad_dev(self, iwfs, isim, opd, lltopd=None, ints=None, grad=None, add_noise=False):
+        self._check(self._L.shwfs_ints_grad_dev(self._h, iwfs, isim, _devptr(opd), _devptr(lltopd), _devptr(ints),
+                                                _devptr(grad), 1 if add_noise else 0), "ints_grad_dev")
+
+    def grad_dev(self, iwfs, ints, grad):
+        self._check(self._L.shwfs_grad_dev(self._h, iwfs, _devptr(ints), _devptr(grad)), "grad_dev")
+
+    def sync(self):
+        self._check(self._L.shwfs_sync(self._h), "sync")
+
+
+def version() -> str:
+    return lib().shwfs_version().decode()

@@ -1,0 +1,233 @@
+"""ctypes driver of the reference's own C code (oracle/_ref/libmaosref.so).
+
+Test infrastructure.  The library is the reference's maos/, lib/, math/ and
+sys/ sources compiled in place by ``make -C oracle ref`` with stand-ins for the
+absent FFTW and BLAS/LAPACK (oracle/refbuild/).  :class:`RefPowfs` runs the
+reference's SH setup (maos/powfs.c: setup_shwfs_geom, setup_shwfs_prep_phy,
+setup_shwfs_dtf, setup_shwfs_etf, setup_powfs_llt, setup_shwfs_phygrad) and
+exposes its outputs and per-frame routines (wfsints, shwfs_grad, addnoise,
+prop).  The library holds one powfs at a time (global state, as in MAOS).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_LIB = os.path.join(HERE, "_ref", "libmaosref.so")
+
+
+class OrefCfg(C.Structure):
+    _fields_ = [("D", C.c_double), ("Din", C.c_double), ("amp_binary", C.c_int), ("order", C.c_int),
+                ("dsa", C.c_double), ("dx", C.c_double), ("saat", C.c_double), ("embfac", C.c_int),
+                ("notf", C.c_int), ("pixpsa", C.c_int), ("pixtheta", C.c_double), ("pixblur", C.c_double),
+                ("wvl", C.c_double), ("hs", C.c_double), ("siglev", C.c_double), ("rne", C.c_double),
+                ("bkgrnd", C.c_double), ("bkgrndc", C.c_double), ("phytype", C.c_int), ("sigmatch", C.c_int),
+                ("mtchcr", C.c_int), ("cogthres", C.c_double), ("cogoff", C.c_double), ("r0", C.c_double),
+                ("L0", C.c_double), ("has_llt", C.c_int), ("llt_d", C.c_double), ("llt_widthp", C.c_double),
+                ("llt_ox", C.c_double), ("llt_oy", C.c_double), ("na_n", C.c_int), ("na_h", C.c_void_p),
+                ("na_p", C.c_void_p), ("nwfs", C.c_int), ("thetax", C.c_void_p), ("thetay", C.c_void_p),
+                ("nthread", C.c_int)]
+
+
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not available():
+            raise FileNotFoundError(f"{REF_LIB} is not built (make -C oracle ref)")
+        L = C.CDLL(REF_LIB)
+        for name in ("oref_nsa", "oref_nopd", "oref_notf", "oref_pixpsax", "oref_pixpsay", "oref_llt_nx", "oref_setup"):
+            getattr(L, name).restype = C.c_int
+        for name in ("oref_areascale", "oref_dtheta", "oref_get_ptsdx", "oref_get_i0sumsum", "oref_frame_mt"):
+            getattr(L, name).restype = C.c_double
+        _lib = L
+    return _lib
+
+
+def _p(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class RefPowfs:
+    """One powfs set up by the reference's own code from a config dict."""
+
+    def __init__(self, cfg: dict, nthread: int = 1):
+        self.cfg = cfg
+        L = lib()
+        keep = []
+        na_h = na_p = None
+        if cfg.get("has_llt"):
+            from maos_b200.configs import sodium_gaussian
+            s = cfg["sodium"]
+            na_h, na_p = sodium_gaussian(s["centers"], s["fwhms"], s["weights"])
+            keep += [na_h, na_p]
+        tx = np.asarray(cfg["thetax"], dtype=np.float64)
+        ty = np.asarray(cfg["thetay"], dtype=np.float64)
+        keep += [tx, ty]
+        c = OrefCfg(D=cfg["D"], Din=cfg["Din"], amp_binary=cfg.get("amp_binary", 0), order=cfg["order"],
+                    dsa=cfg["dsa"], dx=cfg["dx"], saat=cfg["saat"], embfac=cfg["embfac"], notf=cfg["notf"],
+                    pixpsa=cfg["pixpsa"], pixtheta=cfg["pixtheta"], pixblur=cfg["pixblur"], wvl=cfg["wvl"],
+                    hs=cfg["hs"], siglev=cfg["siglev"], rne=cfg["rne"], bkgrnd=cfg.get("bkgrnd", 0.0),
+                    bkgrndc=cfg.get("bkgrndc", 0.0), phytype=cfg["phytype"], sigmatch=cfg["sigmatch"],
+                    mtchcr=cfg.get("mtchcr", 0), cogthres=cfg.get("cogthres", 0.0), cogoff=cfg.get("cogoff", 0.0),
+                    r0=cfg["r0"], L0=cfg["L0"], has_llt=cfg.get("has_llt", 0), llt_d=cfg.get("llt_d", 0.0),
+                    llt_widthp=cfg.get("llt_widthp", 0.0), llt_ox=cfg.get("llt_ox", 0.0),
+                    llt_oy=cfg.get("llt_oy", 0.0), na_n=0 if na_h is None else len(na_h), na_h=_p(na_h),
+                    na_p=_p(na_p), nwfs=cfg["nwfs"], thetax=_p(tx), thetay=_p(ty), nthread=nthread)
+        self._keep = keep
+        self.nsa = L.oref_setup(C.byref(c))
+        self.nopd = L.oref_nopd()
+        self.notf = L.oref_notf()
+        self.pixpsax = L.oref_pixpsax()
+        self.pixpsay = L.oref_pixpsay()
+        self.npix = self.pixpsax * self.pixpsay
+        self.areascale = L.oref_areascale()
+        self.dtheta = L.oref_dtheta()
+        self.llt_nx = L.oref_llt_nx()
+
+    # ---- setup outputs ----
+    def saloc(self):
+        x = np.zeros(self.nsa); y = np.zeros(self.nsa)
+        lib().oref_get_saloc(_p(x), _p(y))
+        return x, y
+
+    def ptsorig(self):
+        x = np.zeros(self.nsa); y = np.zeros(self.nsa)
+        lib().oref_get_ptsorig(_p(x), _p(y))
+        return x, y
+
+    def ptsdx(self) -> float:
+        return lib().oref_get_ptsdx()
+
+    def amp(self):
+        a = np.zeros(self.nsa * self.nopd ** 2)
+        lib().oref_get_amp(_p(a))
+        return a
+
+    def saa(self):
+        a = np.zeros(self.nsa)
+        lib().oref_get_saa(_p(a))
+        return a
+
+    def nominal(self, isa: int = 0):
+        a = np.zeros(self.notf ** 2)
+        lib().oref_get_nominal(C.c_int(isa), _p(a))
+        return a
+
+    def si_dense(self, isa: int = 0):
+        a = np.zeros(self.npix * self.notf ** 2)
+        lib().oref_get_si_dense(C.c_int(isa), _p(a))
+        return a.reshape(self.notf ** 2, self.npix).T  # [pixel, psf index]
+
+    def etf(self):
+        n2 = self.notf ** 2
+        out = np.zeros((self.nsa, n2), dtype=np.complex128)
+        buf = np.zeros(2 * n2)
+        for isa in range(self.nsa):
+            lib().oref_get_etf(C.c_int(isa), _p(buf))
+            out[isa] = buf[0::2] + 1j * buf[1::2]
+        return out
+
+    def srot(self):
+        a = np.zeros(self.nsa); lib().oref_get_srot(_p(a)); return a
+
+    def srsa(self):
+        a = np.zeros(self.nsa); lib().oref_get_srsa(_p(a)); return a
+
+    def lltamp(self):
+        a = np.zeros(self.llt_nx ** 2); lib().oref_get_lltamp(_p(a)); return a
+
+    def mtche(self):
+        out = np.zeros((self.nsa, 2 * self.npix))
+        buf = np.zeros(2 * self.npix)
+        for isa in range(self.nsa):
+            lib().oref_get_mtche(C.c_int(isa), _p(buf))
+            out[isa] = buf
+        return out
+
+    def i0sum(self):
+        a = np.zeros(self.nsa); lib().oref_get_i0sum(_p(a)); return a
+
+    def i0sumsum(self) -> float:
+        return lib().oref_get_i0sumsum()
+
+    # ---- per-frame routines ----
+    def wfsints(self, opd, lltopd=None, iwfs=0, isa0=0, isa1=None, isim=0):
+        ints = np.zeros(self.nsa * self.npix)
+        opd = np.ascontiguousarray(opd, dtype=np.float64)
+        llt = None if lltopd is None else np.ascontiguousarray(lltopd, dtype=np.float64)
+        lib().oref_wfsints(C.c_int(iwfs), _p(opd), _p(llt), _p(ints), C.c_int(isa0),
+                           C.c_int(self.nsa if isa1 is None else isa1), C.c_int(isim))
+        return ints
+
+    def grad(self, ints, iwfs=0):
+        g = np.zeros(2 * self.nsa)
+        ints = np.ascontiguousarray(ints, dtype=np.float64)
+        lib().oref_shwfs_grad(C.c_int(iwfs), _p(ints), _p(g))
+        return g
+
+    def prop_layer(self, screen, dx, ox, oy, ht, thetax, thetay, hs, shiftx, shifty, opd=None, alpha=1.0, wrap=1):
+        scr = np.ascontiguousarray(screen, dtype=np.float64)
+        ny, nx = scr.shape
+        if opd is None:
+            opd = np.zeros(self.nsa * self.nopd ** 2)
+        lib().oref_prop_layer(_p(scr), C.c_long(nx), C.c_long(ny), C.c_double(dx), C.c_double(ox), C.c_double(oy),
+                              C.c_double(ht), C.c_double(thetax), C.c_double(thetay), C.c_double(hs),
+                              C.c_double(shiftx), C.c_double(shifty), C.c_double(alpha), C.c_int(wrap), _p(opd),
+                              C.c_int(0), C.c_int(self.nsa))
+        return opd
+
+    def prop_llt(self, screen, dx, ox, oy, ht, thetax, thetay, hs, shiftx, shifty, lltopd=None):
+        scr = np.ascontiguousarray(screen, dtype=np.float64)
+        ny, nx = scr.shape
+        if lltopd is None:
+            lltopd = np.zeros(self.llt_nx ** 2)
+        lib().oref_prop_llt(_p(scr), C.c_long(nx), C.c_long(ny), C.c_double(dx), C.c_double(ox), C.c_double(oy),
+                            C.c_double(ht), C.c_double(thetax), C.c_double(thetay), C.c_double(hs),
+                            C.c_double(shiftx), C.c_double(shifty), _p(lltopd))
+        return lltopd
+
+    def frame_mt(self, opd, lltopd, seed=1, noisy=False, iwfs=0):
+        ints = np.zeros(self.nsa * self.npix)
+        g = np.zeros(2 * self.nsa)
+        opd = np.ascontiguousarray(opd, dtype=np.float64)
+        llt = None if lltopd is None else np.ascontiguousarray(lltopd, dtype=np.float64)
+        t = lib().oref_frame_mt(C.c_int(iwfs), _p(opd), _p(llt), _p(ints), _p(g), C.c_uint(seed), C.c_int(int(noisy)))
+        return ints, g, t
+
+
+def si_to_taps(si_dense: np.ndarray):
+    """Pixel sampling matrix (npix x notf^2) -> 4-tap (index, weight) arrays."""
+    npix = si_dense.shape[0]
+    idx = -np.ones((npix, 4), dtype=np.int32)
+    wt = np.zeros((npix, 4))
+    for p in range(npix):
+        nz = np.nonzero(si_dense[p])[0]
+        if len(nz) > 4:
+            raise ValueError(f"pixel {p} has {len(nz)} taps")
+        idx[p, :len(nz)] = nz
+        wt[p, :len(nz)] = si_dense[p, nz]
+    return idx, wt
+
+
+def kat_psd() -> np.ndarray:
+    out = np.zeros(7)
+    lib().oref_kat_psd(_p(out))
+    return out
+
+
+def genatm_simple(r0, L0, slope, dx, n, seed):
+    out = np.zeros(n * n)
+    lib().oref_genatm_simple(C.c_double(r0), C.c_double(L0), C.c_double(slope), C.c_double(dx), C.c_long(n),
+                             C.c_uint(seed), _p(out))
+    return out.reshape(n, n)
