@@ -1,0 +1,361 @@
+#!/usr/bin/env python
+"""Benchmark of the physical-optics Shack-Hartmann WFS frame.
+
+Workload (default): NFIRAOS-like LGS, 30 m telescope with 3.6 m obstruction,
+6 LGS WFS at 35" radius, 60x60 subapertures of 0.5 m (2820 valid), 16x16 OPD
+points, 32x32 FFT, 6x6 pixels of 1", 7 von Karman layers on 2048^2 FP32
+screens (synthetic, seeded), Gaussian sodium layer at 90 km (10 km FWHM) from
+an LLT 8 m off axis, 500 photons/subaperture with 3 e- read noise, matched
+filter gradients.  One step = one frame of all 6 WFS: ray trace, uplink OTF,
+imaging, noise, gradients.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+The b200 arm prints one JSON line with the device-timed throughput (value),
+the end-to-end throughput through the C ABI with host results (e2e), the
+roofline of the dominant kernel and the reference's own CPU path timed on
+this host (cpu_baseline).  The reference arm times the reference's own C for
+the path (oracle/_ref, all host threads) on the same workload.  Under
+torchrun each rank runs an independent replica (no collective on the data
+path); the job value is the units of all ranks over the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thr = threading.Thread(target=self._read, daemon=True)
+            self.thr.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=None)
+    return ws, rank, local
+
+
+def allreduce_max(x: float, ws: int, device) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws: int, device):
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+        dist.barrier(device_ids=[device.index])
+        torch.cuda.synchronize(device)
+
+
+# ---------------------------------------------------------------------------
+def algorithmic_traffic(cfg, nsa, npix, nopd, notf, nwfs, nlayer):
+    """Algorithmic bytes per launch of the two main kernels (minimum traffic)."""
+    ints = (nsa * notf * notf * 8 if cfg.get("has_llt") else notf * notf * 4)  # ETF (shared) or nominal
+    ints += nsa * nopd * nopd * 4                                             # amplitude (shared)
+    ints += nwfs * nsa * nopd * nopd * 4                                      # OPD of every WFS
+    ints += nwfs * nsa * npix * (4 + 8)                                       # ints out + matched filter
+    ints += nwfs * (nsa * 4 + nsa * 8)                                        # i0sum + gradients
+    ray = nsa * nopd * nopd * (nlayer * 4 + 4)                                # per WFS launch
+    return ints, ray
+
+
+def fft_flops_per_image(notf):
+    """Nominal FFT flop count per subaperture image: three 2-D transforms."""
+    n2 = notf * notf
+    return 3 * 5 * n2 * math.log2(n2)
+
+
+def cpu_baseline(cfg, wl_layers, screens, seconds=15.0, max_frames=40):
+    from oracle import ref
+    ncpu = os.cpu_count() or 1
+    r = ref.RefPowfs(cfg, nthread=ncpu)
+    ref.atm_set(screens, wl_layers)
+    dt = cfg.get("dt", 1.0 / 800)
+    ref.frame_full_mt(r, 0, 0, dt)  # warm plans and caches
+    t = 0.0
+    n = 0
+    while t < seconds and n < max_frames:
+        _, _, dt_s = ref.frame_full_mt(r, n % cfg["nwfs"], n + 1, dt, seed=n + 1, noisy=True)
+        t += dt_s
+        n += 1
+    return {"value": r.nsa * n / t, "unit": "subap-images/s", "cores": ncpu, "kind": "reference",
+            "sample": f"{n} single-WFS frames of {cfg['name']} ({r.nsa} subapertures each): 7-layer ray trace, "
+                      f"LLT uplink, wfsints, addnoise, matched filter; reference C (oracle/_ref), FFT stand-in "
+                      f"for FFTW, NTHREAD={ncpu}"}
+
+
+def run_reference(args, cfg):
+    ws, rank, local = dist_init()
+    if rank != 0:
+        return 0
+    from oracle import ref
+    from maos_b200.setup import screens as mkscreens
+    from maos_b200.workload import wind
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libmaosref.so is not built"}))
+        return 0
+    ncpu = os.cpu_count() or 1
+    r = ref.RefPowfs(cfg, nthread=ncpu)
+    a = cfg["atm"]
+    n = a["nx"]
+    scr = mkscreens(n, n, a["dx"], a["r0"], a["L0"], a["wt"], 1)
+    vx, vy = wind(cfg, 1)
+    o = -n / 2 * a["dx"]
+    layers = [dict(nx=n, ny=n, dx=a["dx"], ox=o, oy=o, ht=float(h), vx=float(vx[i]), vy=float(vy[i]))
+              for i, h in enumerate(a["ht"])]
+    ref.atm_set(scr, layers)
+    dt = cfg.get("dt", 1.0 / 800)
+    for i in range(args.warmup):
+        ref.frame_full_mt(r, i % cfg["nwfs"], i, dt, seed=i + 1)
+    times = []
+    for k in range(args.steps):
+        _, _, t = ref.frame_full_mt(r, k % cfg["nwfs"], args.warmup + k, dt, seed=k + 7)
+        times.append(t)
+    tot = sum(times)
+    value = r.nsa * args.steps / tot
+    line = {
+        "impl": "reference", "metric": "subaperture images/s", "value": value, "unit": "subap-images/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": cfg["name"], "step": "one single-WFS frame (reference CPU path)"},
+        "cpu_baseline": {"value": value, "unit": "subap-images/s", "cores": ncpu, "kind": "reference",
+                         "sample": f"{args.steps} single-WFS frames of {cfg['name']} ({r.nsa} subapertures)"},
+        "e2e": {"value": value, "unit": "subap-images/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_b200(args, cfg):
+    import torch
+    from maos_b200 import shwfs
+    from maos_b200.workload import build
+    ws, rank, local = dist_init()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    form = shwfs.SHWFS_FORM_TC if args.form == "tc" else shwfs.SHWFS_FORM_FFT
+    wl = build(cfg, device=local, seed=1 + rank, noisy=True, form=form)
+    ctx = wl.ctx
+    nwfs = len(wl.wfs)
+    units_per_step = nwfs * wl.nsa
+    ext = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    isim = 0
+    for _ in range(args.warmup):
+        wl.frame(isim)
+        isim += 1
+    ctx.sync()
+    barrier(ws, dev)
+    clk = ClockSampler(local)
+    clk.start()
+    time.sleep(0.5)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with torch.cuda.stream(ext):
+        for k in range(args.steps):
+            flush.zero_()  # L2 flush between timed steps (not timed)
+            starts[k].record(ext)
+            wl.frame(isim)
+            ends[k].record(ext)
+            isim += 1
+    ctx.sync()
+    torch.cuda.synchronize(dev)
+    clocks = clk.stop()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    tot_ms = allreduce_max(sum(step_ms), ws, dev)
+    barrier(ws, dev)
+    value = units_per_step * args.steps * ws / (tot_ms * 1e-3)
+
+    # stage timing of the same frames (profiled pass, separate from the timed one)
+    ctx.profile_enable(True)
+    nprof = min(args.steps, 20)
+    with torch.cuda.stream(ext):
+        for k in range(nprof):
+            flush.zero_()
+            wl.frame(isim)
+            isim += 1
+    ctx.sync()
+    stages = ctx.profile_read()
+    ctx.profile_enable(False)
+    launches_per_step = sum(n for _, n in stages.values()) / nprof
+
+    # end to end through the C ABI: queue + sync with host gradients each step
+    ctx.copy_counters()
+    e2e_s = 0.0
+    for k in range(args.steps):
+        with torch.cuda.stream(ext):
+            flush.zero_()
+        ctx.sync()
+        t0 = time.perf_counter()
+        wl.frame(isim)
+        wl.frame_sync()
+        e2e_s += time.perf_counter() - t0
+        isim += 1
+    h2d, d2h = ctx.copy_counters()
+    e2e_s = allreduce_max(e2e_s, ws, dev)
+    e2e = units_per_step * args.steps * ws / e2e_s
+
+    # roofline of the dominant kernel
+    hbm, bf16, src = _peaks()
+    nlayer = len(cfg["atm"]["ht"])
+    ints_bytes, ray_bytes = algorithmic_traffic(cfg, wl.nsa, wl.npix, wl.setup.nopd, wl.setup.notf, nwfs, nlayer)
+    st = {k: dict(ms_per_launch=(ms / n if n else 0.0), launches_per_step=n / nprof, ms_per_step=ms / nprof)
+          for k, (ms, n) in stages.items()}
+    ints_ms = st["ints"]["ms_per_launch"]
+    ray_ms = st["raytrace"]["ms_per_launch"]
+    ints_gbs = ints_bytes / (ints_ms * 1e-3) / 1e9 if ints_ms else 0.0
+    ray_gbs = ray_bytes / (ray_ms * 1e-3) / 1e9 if ray_ms else 0.0
+    flops = fft_flops_per_image(wl.setup.notf) * units_per_step
+    fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal FP32 CUDA-core peak, TFLOP/s
+    ints_tf = flops / (ints_ms * 1e-3) / 1e12 if ints_ms else 0.0
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            traffic = json.load(f).get(f"{cfg['name']}:{args.form}:ints")
+    roofline = {"kernel": "ints_n32_kernel (fused imaging, noise, gradients)", "bound": "hbm",
+                "achieved": ints_gbs, "peak": hbm, "unit": "GB/s", "frac": ints_gbs / hbm,
+                "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else "fallback",
+                "traffic": traffic, "algorithmic_bytes_per_launch": ints_bytes,
+                "compute": {"achieved": ints_tf, "peak": fp32_peak, "unit": "TFLOP/s",
+                            "frac": ints_tf / fp32_peak,
+                            "note": "nominal FFT flops (3 x 5 N^2 log2 N^2 per image) vs nominal FP32 CUDA-core peak"},
+                "raytrace": {"achieved": ray_gbs, "peak": hbm, "unit": "GB/s", "frac": ray_gbs / hbm,
+                             "algorithmic_bytes_per_launch": ray_bytes}}
+    p50 = float(np.percentile(step_ms, 50))
+    p99 = float(np.percentile(step_ms, 99))
+    line = {
+        "metric": "subaperture images/s", "value": value, "unit": "subap-images/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": cfg["name"], "wfs": nwfs, "subapertures_per_wfs": wl.nsa,
+                   "fft": wl.setup.notf, "pixels": f"{wl.setup.npix}", "layers": nlayer,
+                   "screen": f"{cfg['atm']['nx']}^2 FP32", "form": args.form, "noise": True,
+                   "gradients": "matched filter" if cfg["phytype"] == 1 else "CoG",
+                   "l2": "flushed (256 MiB write) before every timed step", "parallelism": f"replicas x{ws}"},
+        "frame_latency_ms": {"p50": p50, "p99": p99},
+        "stages": st,
+        "gpu_launches": int(round(launches_per_step * args.steps)),
+        "e2e": {"value": e2e, "unit": "subap-images/s", "h2d_bytes_per_step": h2d // args.steps,
+                "d2h_bytes_per_step": d2h // args.steps},
+        "roofline": roofline,
+        "clocks": clocks,
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(cfg, wl.layers, wl.screens)
+        except Exception as e:  # the oracle library may be absent on a foreign host
+            line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+    if rank == 0:
+        print(json.dumps(line))
+    wl.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="lgs30_6x60x60_mf")
+    ap.add_argument("--form", default="fft", choices=["fft", "tc"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    from maos_b200.configs import CONFIGS
+    cfg = CONFIGS[args.config]
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args, cfg)
+    return run_b200(args, cfg)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

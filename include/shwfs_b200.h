@@ -175,6 +175,22 @@ int shwfs_ints_grad_dev(shwfs_ctx* ctx, int iwfs, int isim, const float* opd, co
 	float* ints, float* grad, int add_noise);
 /* (e) alone: gradients (device, 2*nsa) from pixel intensities (device, nsa*npix). */
 int shwfs_grad_dev(shwfs_ctx* ctx, int iwfs, const float* ints, float* grad);
+/* ---- stage timing: CUDA events around every launch on the context stream,
+        as the reference's ctoc instrumentation (cuda/math/common.h:233-267) ---- */
+#define SHWFS_STAGE_RAYTRACE 0 /* (a) ray trace into the subaperture OPD */
+#define SHWFS_STAGE_UPLINK 1   /* LLT ray trace and uplink OTF */
+#define SHWFS_STAGE_INTS 2     /* (b)-(e) fused imaging, noise, gradients */
+#define SHWFS_NSTAGE 3
+int shwfs_profile_enable(shwfs_ctx* ctx, int enable);
+/* Waits for queued work, then returns per stage the summed device time (ms)
+   and the number of kernel launches since the previous read, and resets. */
+int shwfs_profile_read(shwfs_ctx* ctx, double* ms, int* launches);
+
+/* Bytes the context has copied host->device and device->host on the frame
+   path (descriptor tables, gradients, intensities) since the previous call;
+   resets the counters. */
+int shwfs_copy_counters(shwfs_ctx* ctx, uint64_t* h2d, uint64_t* d2h);
+
 /* Synchronise the context stream; returns the first error of queued work. */
 int shwfs_sync(shwfs_ctx* ctx);
 /* The CUDA stream the context launches on (cudaStream_t as void*). */

@@ -81,6 +81,45 @@ struct shwfs_ctx {
 	std::vector<WfsDev> wfsdev_h;
 	DevBuf<const float*> llt_in;
 	DevBuf<float2*> llt_out;
+	uint64_t h2d_bytes = 0, d2h_bytes = 0;
+	// stage timing
+	int profiling = 0;
+	std::vector<cudaEvent_t> ev_pool;
+	struct Mark {
+		int stage;
+		cudaEvent_t a, b;
+	};
+	std::vector<Mark> marks;
+};
+
+static cudaEvent_t ev_get(shwfs_ctx* ctx) {
+	if (!ctx->ev_pool.empty()) {
+		cudaEvent_t e = ctx->ev_pool.back();
+		ctx->ev_pool.pop_back();
+		return e;
+	}
+	cudaEvent_t e = nullptr;
+	cudaEventCreate(&e);
+	return e;
+}
+// Brackets one launch with events when profiling is on.
+struct StageMark {
+	shwfs_ctx* ctx;
+	int stage;
+	cudaEvent_t a = nullptr;
+	StageMark(shwfs_ctx* c, int s) : ctx(c), stage(s) {
+		if (ctx->profiling) {
+			a = ev_get(ctx);
+			cudaEventRecord(a, ctx->stream);
+		}
+	}
+	~StageMark() {
+		if (a) {
+			cudaEvent_t b = ev_get(ctx);
+			cudaEventRecord(b, ctx->stream);
+			ctx->marks.push_back({stage, a, b});
+		}
+	}
 };
 
 static int fail(shwfs_ctx* c, int code, const char* fmt, ...) {
@@ -182,6 +221,11 @@ int shwfs_destroy(shwfs_ctx* ctx) {
 		if (w.ints_h) cudaFreeHost(w.ints_h);
 	}
 	for (auto& l : ctx->atm) l.screen.free_();
+	for (auto& m : ctx->marks) {
+		cudaEventDestroy(m.a);
+		cudaEventDestroy(m.b);
+	}
+	for (auto e : ctx->ev_pool) cudaEventDestroy(e);
 	ctx->wfsdev.free_();
 	ctx->llt_in.free_();
 	ctx->llt_out.free_();
@@ -438,7 +482,10 @@ static int launch_raytrace(shwfs_ctx* ctx, WfsState& w, int isim, float* opd) {
 		CK(cudaMemsetAsync(opd, 0, sizeof(float) * p.d.nsa * p.d.nopd * p.d.nopd, ctx->stream));
 		return 0;
 	}
-	raytrace_kernel<<<p.d.nsa, p.d.nopd * p.d.nopd, 0, ctx->stream>>>(rp);
+	{
+		StageMark m(ctx, SHWFS_STAGE_RAYTRACE);
+		raytrace_kernel<<<p.d.nsa, p.d.nopd * p.d.nopd, 0, ctx->stream>>>(rp);
+	}
 	CK(cudaGetLastError());
 	return 0;
 }
@@ -454,7 +501,10 @@ static int launch_lltopd(shwfs_ctx* ctx, WfsState& w, int isim) {
 		CK(cudaMemsetAsync(w.lltopd.p, 0, sizeof(float) * p.d.llt_nx * p.d.llt_nx, ctx->stream));
 		return 0;
 	}
-	raytrace_kernel<<<1, p.d.llt_nx * p.d.llt_nx, 0, ctx->stream>>>(rp);
+	{
+		StageMark m(ctx, SHWFS_STAGE_UPLINK);
+		raytrace_kernel<<<1, p.d.llt_nx * p.d.llt_nx, 0, ctx->stream>>>(rp);
+	}
 	CK(cudaGetLastError());
 	return 0;
 }
@@ -553,9 +603,11 @@ static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist
 	const size_t off = ctx->wfsdev_h.size();
 	ctx->wfsdev_h.insert(ctx->wfsdev_h.end(), wd.begin(), wd.end());
 	CK(cudaMemcpyAsync(ctx->wfsdev.p + off, wd.data(), sizeof(WfsDev) * nw, cudaMemcpyHostToDevice, ctx->stream));
+	ctx->h2d_bytes += sizeof(WfsDev) * nw;
 	const int nitem = p.d.nsa * nw;
 	const int nblk = (nitem + 3) / 4;
 	const int npix = P.npix;
+	StageMark mark(ctx, SHWFS_STAGE_INTS);
 	if (npix <= 32) {
 		ints_n32_kernel<1><<<nblk, 128, 0, ctx->stream>>>(P, ctx->wfsdev.p + off, nw, nitem);
 	} else if (npix <= 64) {
@@ -585,10 +637,14 @@ static int launch_uplink(shwfs_ctx* ctx, const std::vector<int>& wlist, const st
 	if ((r = dev_alloc(ctx, ctx->llt_out, (size_t)nw))) return r;
 	CK(cudaMemcpyAsync(ctx->llt_in.p, in.data(), sizeof(float*) * nw, cudaMemcpyHostToDevice, ctx->stream));
 	CK(cudaMemcpyAsync(ctx->llt_out.p, out.data(), sizeof(float2*) * nw, cudaMemcpyHostToDevice, ctx->stream));
+	ctx->h2d_bytes += (sizeof(float*) + sizeof(float2*)) * nw;
 	const float twoinvwvl = (float)(2.0 / p.d.wvl);
 	const float lltnorm = (float)(1.0 / ((double)p.d.llt_nx * p.d.embfac * p.d.llt_nx * p.d.embfac));
-	uplink_otf_n32_kernel<<<(nw + 3) / 4, 128, 0, ctx->stream>>>(ctx->llt_in.p, p.lltamp.p, ctx->llt_out.p, nw, twoinvwvl,
-		lltnorm);
+	{
+		StageMark m(ctx, SHWFS_STAGE_UPLINK);
+		uplink_otf_n32_kernel<<<(nw + 3) / 4, 128, 0, ctx->stream>>>(ctx->llt_in.p, p.lltamp.p, ctx->llt_out.p, nw,
+			twoinvwvl, lltnorm);
+	}
 	CK(cudaGetLastError());
 	return 0;
 }
@@ -684,14 +740,55 @@ int shwfs_frame_sync(shwfs_ctx* ctx, int iwfs, double* grad, double* ints) {
 	if (r) return r;
 	PowfsState& p = ctx->powfs[w->d.ipowfs];
 	const int nsa = p.d.nsa, npix = p.d.pixpsax * p.d.pixpsay;
-	if (grad) CK(cudaMemcpyAsync(w->grad_h, w->grad.p, sizeof(float) * 2 * nsa, cudaMemcpyDeviceToHost, ctx->stream));
-	if (ints) CK(cudaMemcpyAsync(w->ints_h, w->ints.p, sizeof(float) * nsa * npix, cudaMemcpyDeviceToHost, ctx->stream));
+	if (grad) {
+		CK(cudaMemcpyAsync(w->grad_h, w->grad.p, sizeof(float) * 2 * nsa, cudaMemcpyDeviceToHost, ctx->stream));
+		ctx->d2h_bytes += sizeof(float) * 2 * nsa;
+	}
+	if (ints) {
+		CK(cudaMemcpyAsync(w->ints_h, w->ints.p, sizeof(float) * nsa * npix, cudaMemcpyDeviceToHost, ctx->stream));
+		ctx->d2h_bytes += sizeof(float) * nsa * npix;
+	}
 	CK(cudaStreamSynchronize(ctx->stream));
 	ctx->wfsdev_h.clear();
 	if (grad)
 		for (int i = 0; i < 2 * nsa; i++) grad[i] = w->grad_h[i];
 	if (ints)
 		for (int i = 0; i < nsa * npix; i++) ints[i] = w->ints_h[i];
+	return 0;
+}
+
+int shwfs_copy_counters(shwfs_ctx* ctx, uint64_t* h2d, uint64_t* d2h) {
+	if (!ctx) return SHWFS_EINVAL;
+	if (h2d) *h2d = ctx->h2d_bytes;
+	if (d2h) *d2h = ctx->d2h_bytes;
+	ctx->h2d_bytes = ctx->d2h_bytes = 0;
+	return 0;
+}
+
+int shwfs_profile_enable(shwfs_ctx* ctx, int enable) {
+	if (!ctx) return SHWFS_EINVAL;
+	ctx->profiling = enable ? 1 : 0;
+	return 0;
+}
+
+int shwfs_profile_read(shwfs_ctx* ctx, double* ms, int* launches) {
+	if (!ctx || !ms || !launches) return SHWFS_EINVAL;
+	int r = set_device(ctx);
+	if (r) return r;
+	CK(cudaStreamSynchronize(ctx->stream));
+	for (int i = 0; i < SHWFS_NSTAGE; i++) {
+		ms[i] = 0;
+		launches[i] = 0;
+	}
+	for (auto& m : ctx->marks) {
+		float t = 0;
+		CK(cudaEventElapsedTime(&t, m.a, m.b));
+		ms[m.stage] += t;
+		launches[m.stage]++;
+		ctx->ev_pool.push_back(m.a);
+		ctx->ev_pool.push_back(m.b);
+	}
+	ctx->marks.clear();
 	return 0;
 }
 

@@ -93,6 +93,9 @@ def _load() -> C.CDLL:
         "shwfs_ints_grad_dev": [vp, i, i, vp, vp, vp, vp, i],
         "shwfs_grad_dev": [vp, i, vp, vp],
         "shwfs_sync": [vp],
+        "shwfs_profile_enable": [vp, i],
+        "shwfs_profile_read": [vp, dp, ip],
+        "shwfs_copy_counters": [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)],
     }
     for name, args in sig.items():
         f = getattr(lib, name)
@@ -258,6 +261,24 @@ class Context:
 
     def sync(self):
         self._check(self._L.shwfs_sync(self._h), "sync")
+
+    def copy_counters(self):
+        """(host->device bytes, device->host bytes) copied on the frame path since the last call."""
+        a, b = C.c_uint64(), C.c_uint64()
+        self._check(self._L.shwfs_copy_counters(self._h, C.byref(a), C.byref(b)), "copy_counters")
+        return a.value, b.value
+
+    STAGES = ("raytrace", "uplink", "ints")
+
+    def profile_enable(self, on: bool = True):
+        self._check(self._L.shwfs_profile_enable(self._h, 1 if on else 0), "profile_enable")
+
+    def profile_read(self):
+        """{stage: (device ms summed, launches)} since the previous read."""
+        ms = (C.c_double * 3)()
+        n = (C.c_int * 3)()
+        self._check(self._L.shwfs_profile_read(self._h, ms, n), "profile_read")
+        return {k: (ms[i], n[i]) for i, k in enumerate(self.STAGES)}
 
 
 def version() -> str:

@@ -1,0 +1,87 @@
+"""Assemble a complete Shack-Hartmann simulation on one device from a config.
+
+:func:`build` runs the host setup (maos_b200.setup), makes the von Karman
+screens with seeded wind directions, declares every WFS and loads the matched
+filter; the returned :class:`Workload` runs frames through the C ABI.  It is
+the standalone counterpart of the reference's maos_setup + gpu_wfsgrad_init +
+gpu_atm2gpu sequence (maos/setup.c:56-203, maos/sim.c:79).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import List
+
+import numpy as np
+
+from . import shwfs
+from .setup import Setup, screens
+
+
+@dataclass
+class Workload:
+    cfg: dict
+    ctx: "shwfs.Context"
+    setup: Setup
+    ipowfs: int
+    wfs: List[int]
+    layers: List[dict] = field(default_factory=list)
+    screens: List[np.ndarray] = field(default_factory=list)
+
+    @property
+    def nsa(self) -> int:
+        return self.setup.nsa
+
+    @property
+    def npix(self) -> int:
+        return self.setup.npix
+
+    def frame(self, isim: int):
+        """Queue one frame of every WFS (asynchronous)."""
+        self.ctx.frame_queue(isim, self.wfs[0], self.wfs[-1] + 1)
+
+    def frame_sync(self, want_ints: bool = False):
+        return [self.ctx.frame_sync(i, self.ipowfs, want_ints) for i in self.wfs]
+
+    def close(self):
+        self.ctx.close()
+        self.setup.close()
+
+
+def wind(cfg: dict, seed: int):
+    """Per-layer wind vectors: speeds from the config, directions seeded."""
+    a = cfg["atm"]
+    rng = np.random.default_rng(seed)
+    nl = len(a["ht"])
+    if a.get("wdir_deg") is not None:
+        ang = np.deg2rad(np.asarray(a["wdir_deg"], dtype=float))
+    else:
+        ang = rng.uniform(0, 2 * math.pi, nl)
+    ws = np.asarray(a["ws"], dtype=float)
+    return ws * np.cos(ang), ws * np.sin(ang)
+
+
+def build(cfg: dict, device: int = 0, seed: int = 1, noisy: bool = True, nx: int = None,
+          form: int = shwfs.SHWFS_FORM_FFT) -> Workload:
+    setup = Setup(cfg)
+    ctx = shwfs.Context(device)
+    ctx.set_form(form)
+    ctx.set_dt(cfg.get("dt", 1.0 / 800))
+    ip = setup.load(ctx)
+    wl = []
+    for k in range(cfg["nwfs"]):
+        i = ctx.wfs_add(ipowfs=ip, thetax=cfg["thetax"][k], thetay=cfg["thetay"][k], hs=cfg["hs"], hc=0.0,
+                        misregx=0.0, misregy=0.0, sigsim=cfg["siglev"], wvlwt=1.0, noisy=1 if noisy else 0)
+        setup.load_wfs(ctx, i)
+        ctx.wfs_seed(i, seed * 1000003 + k)
+        wl.append(i)
+    a = cfg["atm"]
+    n = nx or a["nx"]
+    dx = a["dx"]
+    scr = screens(n, n, dx, a["r0"], a["L0"], a["wt"], seed)
+    vx, vy = wind(cfg, seed)
+    o = -n / 2 * dx
+    layers = [dict(nx=n, ny=n, dx=dx, ox=o, oy=o, ht=float(h), vx=float(vx[i]), vy=float(vy[i]), alpha=1.0)
+              for i, h in enumerate(a["ht"])]
+    ctx.atm_set(layers, scr)
+    return Workload(cfg=cfg, ctx=ctx, setup=setup, ipowfs=ip, wfs=wl, layers=layers, screens=scr)

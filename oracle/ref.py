@@ -48,7 +48,8 @@ def lib():
         L = C.CDLL(REF_LIB)
         for name in ("oref_nsa", "oref_nopd", "oref_notf", "oref_pixpsax", "oref_pixpsay", "oref_llt_nx", "oref_setup"):
             getattr(L, name).restype = C.c_int
-        for name in ("oref_areascale", "oref_dtheta", "oref_get_ptsdx", "oref_get_i0sumsum", "oref_frame_mt"):
+        for name in ("oref_areascale", "oref_dtheta", "oref_get_ptsdx", "oref_get_i0sumsum", "oref_frame_mt",
+                     "oref_frame_full_mt"):
             getattr(L, name).restype = C.c_double
         _lib = L
     return _lib
@@ -204,6 +205,27 @@ class RefPowfs:
         llt = None if lltopd is None else np.ascontiguousarray(lltopd, dtype=np.float64)
         t = lib().oref_frame_mt(C.c_int(iwfs), _p(opd), _p(llt), _p(ints), _p(g), C.c_uint(seed), C.c_int(int(noisy)))
         return ints, g, t
+
+
+def atm_set(screens, layers):
+    """Give the reference's full-frame path its turbulence (list of (ny,nx) screens,
+    layer dicts with nx, ny, dx, ox, oy, ht, vx, vy)."""
+    n = len(screens)
+    keep = [np.ascontiguousarray(sc, dtype=np.float64) for sc in screens]
+    ptrs = (C.c_void_p * n)(*[k.ctypes.data for k in keep])
+    arr = lambda key, t=np.float64: np.ascontiguousarray([l[key] for l in layers], dtype=t)
+    nx, ny = arr("nx", np.int64), arr("ny", np.int64)
+    dx, ox, oy, ht, vx, vy = (arr(k) for k in ("dx", "ox", "oy", "ht", "vx", "vy"))
+    lib().oref_atm_set(C.c_int(n), ptrs, _p(nx), _p(ny), _p(dx), _p(ox), _p(oy), _p(ht), _p(vx), _p(vy))
+
+
+def frame_full_mt(ref: "RefPowfs", iwfs: int, isim: int, dt: float, seed: int = 1, noisy: bool = True):
+    """One complete WFS frame of the reference CPU path; returns (ints, grad, seconds)."""
+    ints = np.zeros(ref.nsa * ref.npix)
+    g = np.zeros(2 * ref.nsa)
+    t = lib().oref_frame_full_mt(C.c_int(iwfs), C.c_int(isim), C.c_double(dt), _p(ints), _p(g), C.c_uint(seed),
+                                 C.c_int(int(noisy)))
+    return ints, g, t
 
 
 def si_to_taps(si_dense: np.ndarray):

@@ -428,3 +428,69 @@ void oref_kat_psd(double* out){
 	dfree(st);
 	dfree(screen);
 }
+
+/* Turbulence for the full-frame CPU path: nlayer screens kept as map_t. */
+static map_t** g_atm=NULL;
+static int g_natm=0;
+void oref_atm_set(int nlayer, const double* const* screens, const long* nx, const long* ny, const double* dx,
+	const double* ox, const double* oy, const double* ht, const double* vx, const double* vy){
+	for(int i=0; i<g_natm; i++) mapfree(g_atm[i]);
+	free(g_atm);
+	g_natm=nlayer;
+	g_atm=mycalloc(nlayer, map_t*);
+	for(int i=0; i<nlayer; i++){
+		map_t* m=g_atm[i]=mapnew(nx[i], ny[i], dx[i], dx[i]);
+		memcpy(P(m), screens[i], sizeof(double)*nx[i]*ny[i]);
+		m->ox=ox[i]; m->oy=oy[i]; m->ht=ht[i]; m->vx=vx[i]; m->vy=vy[i];
+	}
+}
+
+/* One complete WFS frame of the reference CPU path at step isim, as
+   wfsgrad_iwfs runs it (maos/wfsgrad.c:170-194, 330-473): the ray trace of
+   every layer split over 8 threads (LGS) or 2 (NGS) per layer
+   (maos/sim_utils.c:1031), the LLT OPD for LGS, wfsints over
+   thread_prep(0,nsa,NTHREAD), addnoise and shwfs_grad.  Returns seconds. */
+double oref_frame_full_mt(int iwfs, int isim, double dt, double* ints, double* grad, unsigned int seed, int noisy){
+	const parms_t* parms=g_parms;
+	powfs_t* powfs=g_powfs;
+	const long nsa=powfs[0].saloc->nloc;
+	const long nopd=powfs[0].pts->nxsa;
+	const real hs=parms->wfs[iwfs].hs;
+	double t0=omp_get_wtime();
+	dmat* opd=dnew(nsa*nopd*nopd, 1);
+	const int nth=isinf(hs)?2:8;
+	for(int ips=0; ips<g_natm; ips++){
+		propdata_t pd={0};
+		pd.mapin=g_atm[ips];
+		pd.ptsout=powfs[0].pts;
+		pd.phiout=P(opd);
+		pd.alpha=1;
+		pd.hs=hs;
+		pd.thetax=parms->wfs[iwfs].thetax;
+		pd.thetay=parms->wfs[iwfs].thetay;
+		pd.shiftx=-g_atm[ips]->vx*dt*isim;
+		pd.shifty=-g_atm[ips]->vy*dt*isim;
+		pd.wrap=1;
+		thread_t* thd=thread_prep(0, nsa, nth, prop_thread, &pd);
+		CALL_THREAD(thd, 1);
+		free(thd);
+	}
+	dmat* lltopd=NULL;
+	if(powfs[0].llt){
+		lltopd=dnew(powfs[0].llt->pts->nxsa, powfs[0].llt->pts->nysa);
+		const real ox=P(parms->powfs[0].llt->ox, 0);
+		const real oy=P(parms->powfs[0].llt->oy, 0);
+		for(int ips=0; ips<g_natm; ips++){
+			const real scale=1.-g_atm[ips]->ht/hs;
+			if(scale<0) continue;
+			prop(&(propdata_t){.mapin=g_atm[ips], .ptsout=powfs[0].llt->pts, .phiout=P(lltopd), .alpha=1,
+				.hs=hs, .thetax=parms->wfs[iwfs].thetax-ox/hs, .thetay=parms->wfs[iwfs].thetay-oy/hs,
+				.shiftx=ox-g_atm[ips]->vx*isim*dt, .shifty=oy-g_atm[ips]->vy*isim*dt, .wrap=1});
+		}
+	}
+	double t1=omp_get_wtime();
+	double t=oref_frame_mt(iwfs, P(opd), lltopd?P(lltopd):NULL, ints, grad, seed, noisy);
+	dfree(opd);
+	dfree(lltopd);
+	return (t1-t0)+t;
+}
