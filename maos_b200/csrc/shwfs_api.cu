@@ -46,6 +46,7 @@ struct PowfsState {
 	float etfwt[2] = {1.f, 0.f};
 	DevBuf<float> lltamp;
 	DevBuf<double> lltorig;  // {llt origx, llt origy}
+	int variant = 0;         // imaging-kernel variant chosen by shwfs_autotune
 	std::vector<double> origx_h, origy_h;
 };
 
@@ -437,75 +438,92 @@ int shwfs_atm_set(shwfs_ctx* ctx, int nlayer, const shwfs_layer_desc* layers, co
 
 // ---- frame machinery ----
 
-// Layer geometry of prop_range (lib/accphi.c:223-244) and prop_grid_pts
+// Appends one pupil to a batched ray-trace launch: per-layer geometry of
+// prop_range (lib/accphi.c:223-244) and prop_grid_pts
 // (lib/accphi_grid_do.c:408-434), FP64 on the host.
-static int build_raytrace(shwfs_ctx* ctx, const PowfsState& p, double thetax, double thetay, double hs, double hc,
+static int add_geom_entry(shwfs_ctx* ctx, GeomParams& gp, double thetax, double thetay, double hs, double hc,
 	double misregx, double misregy, double extra_shiftx, double extra_shifty, int isim, const double* origx,
-	const double* origy, int nsa, int nopd, double dx, float* out, RaytraceParams& rp) {
-	rp.origx = origx;
-	rp.origy = origy;
-	rp.dx = dx;
-	rp.nopd = nopd;
-	rp.nsa = nsa;
-	rp.opd = out;
-	rp.nlayer = 0;
-	for (const auto& L : ctx->atm) {
-		const shwfs_layer_desc& a = L.d;
+	const double* origy, int nsa, int nopd, double dx, float* out) {
+	if (gp.nentry >= SHWFS_MAX_ENTRIES) return fail(ctx, SHWFS_EINVAL, "too many pupils in one ray-trace launch");
+	GeomEntry& e = gp.e[gp.nentry++];
+	memset(&e, 0, sizeof(e));
+	e.origx = origx;
+	e.origy = origy;
+	e.opd = out;
+	e.nsa = nsa;
+	e.nopd = nopd;
+	e.dx = dx;
+	e.use = 0;
+	for (int l = 0; l < (int)ctx->atm.size(); l++) {
+		const shwfs_layer_desc& a = ctx->atm[l].d;
 		const double ht = a.ht;
-		if (isfinite(hs) && hs != 0 && (hc > hs || ht > hs)) continue;
-		const double scale = (isfinite(hs) && hs != 0) ? 1. - (ht - hc) / (hs - hc) : 1.;
+		const bool finite_hs = isfinite(hs) && hs != 0;
+		if (finite_hs && (hc > hs || ht > hs)) continue;
+		const double scale = finite_hs ? 1. - (ht - hc) / (hs - hc) : 1.;
 		if (scale < 0) continue;
 		const double shiftx = -a.vx * ctx->dt * isim + extra_shiftx;
 		const double shifty = -a.vy * ctx->dt * isim + extra_shifty;
 		const double displacex = ht * thetax + scale * misregx + shiftx;
 		const double displacey = ht * thetay + scale * misregy + shifty;
-		LayerGeom& g = rp.layer[rp.nlayer++];
-		g.screen = L.screen.p;
-		g.nx = (int)a.nx;
-		g.ny = (int)a.ny;
 		const double dx_in1 = 1. / a.dx;
-		g.sx = scale * dx_in1;
-		g.dispx = (displacex - a.ox) * dx_in1;
-		g.dispy = (displacey - a.oy) * dx_in1;
-		g.alpha = (float)a.alpha;
+		e.sx[l] = scale * dx_in1;
+		e.dispx[l] = (displacex - a.ox) * dx_in1;
+		e.dispy[l] = (displacey - a.oy) * dx_in1;
+		e.use |= 1u << l;
 	}
-	(void)p;
 	return 0;
 }
 
-static int launch_raytrace(shwfs_ctx* ctx, WfsState& w, int isim, float* opd) {
-	PowfsState& p = ctx->powfs[w.d.ipowfs];
-	RaytraceParams rp;
-	build_raytrace(ctx, p, w.d.thetax, w.d.thetay, w.d.hs, w.d.hc, w.d.misregx, w.d.misregy, 0, 0, isim, p.origx.p,
-		p.origy.p, p.d.nsa, p.d.nopd, p.d.dx, opd, rp);
-	if (rp.nlayer == 0) {
-		CK(cudaMemsetAsync(opd, 0, sizeof(float) * p.d.nsa * p.d.nopd * p.d.nopd, ctx->stream));
-		return 0;
+static void geom_init(shwfs_ctx* ctx, GeomParams& gp) {
+	memset(&gp, 0, sizeof(gp));
+	gp.nlayer = (int)ctx->atm.size();
+	for (int l = 0; l < gp.nlayer; l++) {
+		gp.screen[l] = ctx->atm[l].screen.p;
+		gp.nx[l] = (int)ctx->atm[l].d.nx;
+		gp.ny[l] = (int)ctx->atm[l].d.ny;
+		gp.alpha[l] = (float)ctx->atm[l].d.alpha;
+	}
+}
+
+static int launch_geom(shwfs_ctx* ctx, GeomParams& gp) {
+	int nblk = 0;
+	for (int i = 0; i < gp.nentry; i++) {
+		gp.e[i].item0 = nblk;
+		nblk += gp.e[i].nsa;
+	}
+	if (nblk == 0) return 0;
+	if (gp.nlayer == 0) {  // no turbulence: zero OPD and a flat-wavefront uplink
+		for (int i = 0; i < gp.nentry; i++)
+			if (gp.e[i].opd)
+				CK(cudaMemsetAsync(gp.e[i].opd, 0, sizeof(float) * gp.e[i].nsa * gp.e[i].nopd * gp.e[i].nopd, ctx->stream));
 	}
 	{
 		StageMark m(ctx, SHWFS_STAGE_RAYTRACE);
-		raytrace_kernel<<<p.d.nsa, p.d.nopd * p.d.nopd, 0, ctx->stream>>>(rp);
+		geom_kernel<<<nblk, 256, 0, ctx->stream>>>(gp);
 	}
 	CK(cudaGetLastError());
 	return 0;
 }
 
-// LLT OPD (maos/wfsgrad.c:337-365): thetax - ox/hs, shift ox - v*dt*isim, wrap.
-// The LLT pupil is traced as one subaperture with origin llt->pts->origx/y.
-static int launch_lltopd(shwfs_ctx* ctx, WfsState& w, int isim) {
+// The ray-trace entry of one WFS.
+static int add_wfs_entry(shwfs_ctx* ctx, GeomParams& gp, WfsState& w, int isim, float* opd) {
 	PowfsState& p = ctx->powfs[w.d.ipowfs];
-	RaytraceParams rp;
-	build_raytrace(ctx, p, w.d.thetax - p.d.llt_ox / w.d.hs, w.d.thetay - p.d.llt_oy / w.d.hs, w.d.hs, 0, 0, 0,
-		p.d.llt_ox, p.d.llt_oy, isim, p.lltorig.p, p.lltorig.p + 1, 1, p.d.llt_nx, p.d.dx, w.lltopd.p, rp);
-	if (rp.nlayer == 0) {
-		CK(cudaMemsetAsync(w.lltopd.p, 0, sizeof(float) * p.d.llt_nx * p.d.llt_nx, ctx->stream));
-		return 0;
-	}
-	{
-		StageMark m(ctx, SHWFS_STAGE_UPLINK);
-		raytrace_kernel<<<1, p.d.llt_nx * p.d.llt_nx, 0, ctx->stream>>>(rp);
-	}
-	CK(cudaGetLastError());
+	return add_geom_entry(ctx, gp, w.d.thetax, w.d.thetay, w.d.hs, w.d.hc, w.d.misregx, w.d.misregy, 0, 0, isim,
+		p.origx.p, p.origy.p, p.d.nsa, p.d.nopd, p.d.dx, opd);
+}
+// The LLT pupil of one LGS WFS (maos/wfsgrad.c:337-365): direction
+// theta - llt_o/hs, shift llt_o - v*dt*isim, cone of the star, wrap; the
+// block then forms the uplink OTF.
+static int add_llt_entry(shwfs_ctx* ctx, GeomParams& gp, WfsState& w, int isim) {
+	PowfsState& p = ctx->powfs[w.d.ipowfs];
+	int r = add_geom_entry(ctx, gp, w.d.thetax - p.d.llt_ox / w.d.hs, w.d.thetay - p.d.llt_oy / w.d.hs, w.d.hs, 0, 0,
+		0, p.d.llt_ox, p.d.llt_oy, isim, p.lltorig.p, p.lltorig.p + 1, 1, p.d.llt_nx, p.d.dx, w.lltopd.p);
+	if (r) return r;
+	GeomEntry& e = gp.e[gp.nentry - 1];
+	e.lltamp = p.lltamp.p;
+	e.lotfT = w.lotfT.p;
+	e.twoinvwvl = (float)(2.0 / p.d.wvl);
+	e.lltnorm = (float)(1.0 / ((double)p.d.llt_nx * p.d.embfac * p.d.llt_nx * p.d.embfac));
 	return 0;
 }
 
@@ -608,12 +626,21 @@ static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist
 	const int nblk = (nitem + 3) / 4;
 	const int npix = P.npix;
 	StageMark mark(ctx, SHWFS_STAGE_INTS);
+	const WfsDev* wdev = ctx->wfsdev.p + off;
+	auto go = [&](auto kern) { kern<<<nblk, 128, 0, ctx->stream>>>(P, wdev, nw, nitem); };
+	const int v = p.variant;
 	if (npix <= 32) {
-		ints_n32_kernel<1><<<nblk, 128, 0, ctx->stream>>>(P, ctx->wfsdev.p + off, nw, nitem);
+		if (v == 1) go(ints_n32_kernel<1, 5>);
+		else if (v == 2) go(ints_n32_kernel<1, 6>);
+		else go(ints_n32_kernel<1, 4>);
 	} else if (npix <= 64) {
-		ints_n32_kernel<2><<<nblk, 128, 0, ctx->stream>>>(P, ctx->wfsdev.p + off, nw, nitem);
+		if (v == 1) go(ints_n32_kernel<2, 5>);
+		else if (v == 2) go(ints_n32_kernel<2, 6>);
+		else go(ints_n32_kernel<2, 4>);
 	} else {
-		ints_n32_kernel<4><<<nblk, 128, 0, ctx->stream>>>(P, ctx->wfsdev.p + off, nw, nitem);
+		if (v == 1) go(ints_n32_kernel<4, 5>);
+		else if (v == 2) go(ints_n32_kernel<4, 6>);
+		else go(ints_n32_kernel<4, 4>);
 	}
 	CK(cudaGetLastError());
 	return 0;
@@ -656,7 +683,10 @@ int shwfs_raytrace_dev(shwfs_ctx* ctx, int iwfs, int isim, float* opd) {
 	if (!w || !opd) return ctx ? fail(ctx, SHWFS_EINVAL, "raytrace: bad arguments") : SHWFS_EINVAL;
 	int r = set_device(ctx);
 	if (r) return r;
-	return launch_raytrace(ctx, *w, isim, opd);
+	GeomParams gp;
+	geom_init(ctx, gp);
+	if ((r = add_wfs_entry(ctx, gp, *w, isim, opd))) return r;
+	return launch_geom(ctx, gp);
 }
 
 int shwfs_ints_grad_dev(shwfs_ctx* ctx, int iwfs, int isim, const float* opd, const float* lltopd, float* ints,
@@ -706,28 +736,39 @@ int shwfs_frame_queue(shwfs_ctx* ctx, int isim, int iwfs0, int iwfs1) {
 	int r = set_device(ctx);
 	if (r) return r;
 	for (size_t ip = 0; ip < ctx->powfs.size(); ip++) {
+		PowfsState& p = ctx->powfs[ip];
 		std::vector<int> wl;
 		for (int i = iwfs0; i < iwfs1; i++)
-			if (ctx->wfs[i].d.ipowfs == (int)ip) wl.push_back(i);
+			if (ctx->wfs[i].d.ipowfs == (int)ip) {
+				if ((r = check_ready(ctx, p, ctx->wfs[i]))) return r;
+				wl.push_back(i);
+			}
 		if (wl.empty()) continue;
-		PowfsState& p = ctx->powfs[ip];
-		std::vector<const float*> opds, llts;
-		std::vector<const float2*> lotf(wl.size(), nullptr);
+		// (a) one ray-trace launch per batch of pupils (WFS + LLT)
+		const int per = p.d.has_llt ? SHWFS_MAX_ENTRIES / 2 : SHWFS_MAX_ENTRIES;
+		for (size_t b = 0; b < wl.size(); b += per) {
+			GeomParams gp;
+			geom_init(ctx, gp);
+			for (size_t k = b; k < wl.size() && k < b + per; k++) {
+				WfsState& w = ctx->wfs[wl[k]];
+				if ((r = add_wfs_entry(ctx, gp, w, isim, w.opd.p))) return r;
+				if (p.d.has_llt && (r = add_llt_entry(ctx, gp, w, isim))) return r;
+			}
+			if ((r = launch_geom(ctx, gp))) return r;
+		}
+		// (b)-(e)
+		std::vector<const float*> opds;
+		std::vector<const float2*> lotf;
 		std::vector<float*> in, gr;
 		std::vector<int> nz;
 		for (int i : wl) {
 			WfsState& w = ctx->wfs[i];
-			if ((r = launch_raytrace(ctx, w, isim, w.opd.p))) return r;
-			if (p.d.has_llt) {
-				if ((r = launch_lltopd(ctx, w, isim))) return r;
-				llts.push_back(w.lltopd.p);
-			}
 			opds.push_back(w.opd.p);
+			lotf.push_back(p.d.has_llt ? w.lotfT.p : nullptr);
 			in.push_back(w.ints.p);
 			gr.push_back(w.grad.p);
 			nz.push_back(w.d.noisy);
 		}
-		if (p.d.has_llt && (r = launch_uplink(ctx, wl, llts, lotf))) return r;
 		if ((r = launch_ints(ctx, (int)ip, wl, isim, opds, lotf, in, gr, nz))) return r;
 	}
 	return 0;
@@ -754,6 +795,46 @@ int shwfs_frame_sync(shwfs_ctx* ctx, int iwfs, double* grad, double* ints) {
 		for (int i = 0; i < 2 * nsa; i++) grad[i] = w->grad_h[i];
 	if (ints)
 		for (int i = 0; i < nsa * npix; i++) ints[i] = w->ints_h[i];
+	return 0;
+}
+
+int shwfs_autotune(shwfs_ctx* ctx, int iwfs0, int iwfs1, int nrep, int* chosen) {
+	if (!ctx || iwfs0 < 0 || iwfs1 > (int)ctx->wfs.size() || iwfs0 >= iwfs1 || nrep <= 0)
+		return ctx ? fail(ctx, SHWFS_EINVAL, "autotune: bad arguments") : SHWFS_EINVAL;
+	int r = set_device(ctx);
+	if (r) return r;
+	const int ipowfs = ctx->wfs[iwfs0].d.ipowfs;
+	PowfsState& p = ctx->powfs[ipowfs];
+	const int saved = ctx->profiling;
+	ctx->profiling = 1;
+	double best = 1e300;
+	int bestv = 0;
+	double ms[SHWFS_NSTAGE];
+	int n[SHWFS_NSTAGE];
+	if ((r = shwfs_profile_read(ctx, ms, n))) return r;  // drain
+	for (int v = 0; v < SHWFS_NVARIANT; v++) {
+		p.variant = v;
+		if ((r = shwfs_frame_queue(ctx, 0, iwfs0, iwfs1))) return r;  // warm
+		if ((r = shwfs_profile_read(ctx, ms, n))) return r;
+		for (int k = 0; k < nrep; k++)
+			if ((r = shwfs_frame_queue(ctx, k, iwfs0, iwfs1))) return r;
+		if ((r = shwfs_profile_read(ctx, ms, n))) return r;
+		const double t = ms[SHWFS_STAGE_INTS] / (n[SHWFS_STAGE_INTS] ? n[SHWFS_STAGE_INTS] : 1);
+		if (t < best) {
+			best = t;
+			bestv = v;
+		}
+	}
+	p.variant = bestv;
+	ctx->profiling = saved;
+	if (chosen) *chosen = bestv;
+	return 0;
+}
+
+int shwfs_set_variant(shwfs_ctx* ctx, int ipowfs, int variant) {
+	PowfsState* p = get_powfs(ctx, ipowfs);
+	if (!p || variant < 0 || variant >= SHWFS_NVARIANT) return ctx ? fail(ctx, SHWFS_EINVAL, "set_variant: bad arguments") : SHWFS_EINVAL;
+	p->variant = variant;
 	return 0;
 }
 

@@ -1,8 +1,8 @@
 // Device kernels of the Shack-Hartmann frame.
 //
-//   raytrace_kernel     (a) bilinear gather of every turbulence layer into the
-//                           subaperture OPD points, FP64 offsets
-//   uplink_otf_kernel   LGS uplink OTF from the LLT OPD (one warp per WFS)
+//   geom_kernel         (a) bilinear gather of every turbulence layer into the
+//                           subaperture OPD points of every WFS of the frame
+//                           (FP64 offsets), and the LGS uplink OTF
 //   ints_n32_kernel     (b)-(e) fused per subaperture for n_w = n_f = 32,
 //                           n_opd = 16: field, pruned 2-D FFT, |.|^2, FFT,
 //                           x conj(uplink OTF) x ETF/DTF, inverse FFT, pixel
@@ -39,8 +39,10 @@ __device__ __forceinline__ u32x4 philox4x32_10(u32x4 c, uint32_t k0, uint32_t k1
 	}
 	return c;
 }
-// uniform in (0, 1]: never 0, so a running product of draws stays positive
-__device__ __forceinline__ float u01(uint32_t v) { return ((v >> 8) + 1u) * (1.0f / 16777216.0f); }
+// uniform in [0, 1) with 24-bit resolution
+__device__ __forceinline__ float u01(uint32_t v) { return (v >> 8) * (1.0f / 16777216.0f); }
+// uniform in (0, 1], for logarithms
+__device__ __forceinline__ float u01_nz(uint32_t v) { return ((v >> 8) + 1u) * (1.0f / 16777216.0f); }
 
 // Stream of uniforms for one pixel: counter (n, pixel, wfs, frame).
 struct PixelRng {
@@ -49,18 +51,19 @@ struct PixelRng {
 	int used;
 	__device__ __forceinline__ PixelRng(uint64_t seed, uint32_t pix_, uint32_t wfs_, uint32_t frame_)
 		: k0((uint32_t)seed), k1((uint32_t)(seed >> 32)), pix(pix_), wfs(wfs_), frame(frame_), n(0), used(4) {}
-	__device__ __forceinline__ float next() {
+	__device__ __forceinline__ uint32_t bits() {
 		if (used == 4) {
 			buf = philox4x32_10(u32x4{n++, pix, wfs, frame}, k0, k1);
 			used = 0;
 		}
 		uint32_t v = used == 0 ? buf.x : used == 1 ? buf.y : used == 2 ? buf.z : buf.w;
 		used++;
-		return u01(v);
+		return v;
 	}
+	__device__ __forceinline__ float next() { return u01(bits()); }
 	// standard normal by Box-Muller
 	__device__ __forceinline__ float normal() {
-		float u1 = next(), u2 = next();
+		float u1 = u01_nz(bits()), u2 = next();
 		float r = sqrtf(-2.f * logf(u1));
 		float s, c;
 		sincospif(2.f * u2, &s, &c);
@@ -68,28 +71,38 @@ struct PixelRng {
 	}
 };
 
-// Poisson draw with the reference's method (math/random.c:186-209): a
-// Gaussian approximation above 200, otherwise products of uniforms in chunks
-// of at most 12.  The inner loop is capped; a draw that reaches the cap
-// returns the count so far (probability below 1e-30 for these means).
+// Poisson draw.  As the reference (math/random.c:186-209) it uses a Gaussian
+// approximation above a mean of 200 and otherwise splits the mean into chunks
+// of at most 12 whose counts add up; each chunk is drawn exactly by inversion
+// of its cumulative distribution (one uniform per chunk) instead of the
+// reference's product of uniforms, which needs about mean+1 uniforms.  Both
+// give Poisson variates; the inversion is accumulated in FP64 so that the
+// computed distribution reaches 1 - 1e-15 > the largest uniform 1 - 2^-24.
+struct InvTable {
+	double v[81];
+	__host__ __device__ constexpr InvTable() : v() {
+		for (int k = 1; k <= 80; k++) v[k] = 1.0 / k;
+	}
+};
+__constant__ InvTable c_invk = InvTable();
+
 __device__ __forceinline__ float poisson_draw(PixelRng& rng, float xm) {
 	if (xm > 200.f) {
 		return rintf(xm + rng.normal() * sqrtf(xm));
 	}
 	int x = 0;
-	int guard = 0;
-	while (xm > 0.f && guard < 4096) {
+	while (xm > 0.f) {
 		const float xmu = xm > 12.f ? 12.f : xm;
 		xm -= xmu;
-		const float g = expf(-xmu);
-		int xu = -1;
-		float t = 1.f;
-		while (t > g && guard < 4096) {
-			xu++;
-			t *= rng.next();
-			guard++;
+		const double u = rng.next();
+		double p = exp(-(double)xmu), F = p;
+		int k = 0;
+		while (u > F && k < 80) {
+			k++;
+			p *= (double)xmu * c_invk.v[k];
+			F += p;
 		}
-		x += xu;
+		x += k;
 	}
 	return (float)x;
 }
@@ -97,25 +110,34 @@ __device__ __forceinline__ float poisson_draw(PixelRng& rng, float xm) {
 // ---------------------------------------------------------------------------
 // Parameters
 // ---------------------------------------------------------------------------
-// Per-layer ray-trace geometry for one WFS at one frame, computed on the host
-// in FP64 (lib/accphi.c:241-244 and lib/accphi_grid_do.c:424-434).
-struct LayerGeom {
-	const float* screen;
-	int nx, ny;
-	double dispx, dispy;  // (displacement - screen origin)/screen dx, in screen pixels
-	double sx;            // scale/screen dx   (multiplies point coordinates)
-	float alpha;
-};
 #define SHWFS_MAX_LAYERS 16
+#define SHWFS_MAX_ENTRIES 16
 
-struct RaytraceParams {
-	const double* origx;  // nsa
+// One pupil to ray trace in a frame: the subapertures of a WFS, or the LLT
+// pupil of an LGS (one "subaperture"), with the per-layer geometry of
+// prop_range (lib/accphi.c:241-244) and prop_grid_pts
+// (lib/accphi_grid_do.c:424-434), computed on the host in FP64.
+struct GeomEntry {
+	const double* origx;   // nsa subaperture origins
 	const double* origy;
-	double dx;            // pts->dx
-	int nopd, nsa;
-	int nlayer;
-	LayerGeom layer[SHWFS_MAX_LAYERS];
-	float* opd;           // nsa*nopd^2
+	float* opd;            // nsa*nopd^2 output (may be null for LLT entries)
+	int nsa, nopd, item0;  // item0: first block of this entry
+	double dx;             // OPD sampling
+	double sx[SHWFS_MAX_LAYERS];    // scale / screen dx
+	double dispx[SHWFS_MAX_LAYERS]; // (displacement - screen origin) / screen dx
+	double dispy[SHWFS_MAX_LAYERS];
+	unsigned use;          // bit l: layer l contributes (below the star)
+	// LLT entry: uplink OTF (maos/wfsints.c:149-199) written transposed
+	const float* lltamp;   // nopd^2, or null for a WFS entry
+	float2* lotfT;
+	float twoinvwvl, lltnorm;
+};
+struct GeomParams {
+	int nentry, nlayer;
+	const float* screen[SHWFS_MAX_LAYERS];
+	int nx[SHWFS_MAX_LAYERS], ny[SHWFS_MAX_LAYERS];
+	float alpha[SHWFS_MAX_LAYERS];
+	GeomEntry e[SHWFS_MAX_ENTRIES];
 };
 
 struct WfsDev {
@@ -152,52 +174,6 @@ struct PowfsDev {
 };
 
 // ---------------------------------------------------------------------------
-// (a) ray trace
-// ---------------------------------------------------------------------------
-// One thread per OPD point, looping over layers; block = one subaperture's
-// nopd^2 points (blockDim.x = nopd*nopd <= 1024).  The per-subaperture start
-// coordinate is formed and wrapped in FP64; only the in-subaperture offset
-// (< nopd screen pixels) is carried in FP32.
-__global__ void raytrace_kernel(RaytraceParams p) {
-	const int isa = blockIdx.x;
-	const int ip = threadIdx.x;
-	if (isa >= p.nsa || ip >= p.nopd * p.nopd) return;
-	const int ix = ip % p.nopd, iy = ip / p.nopd;
-	const double ox = p.origx[isa], oy = p.origy[isa];
-	float acc = 0.f;
-	for (int l = 0; l < p.nlayer; l++) {
-		const LayerGeom& g = p.layer[l];
-		// start of this subaperture in screen pixels, wrapped into [0, n)
-		double x0 = ox * g.sx + g.dispx;
-		double y0 = oy * g.sx + g.dispy;
-		if (!isfinite(x0) || !isfinite(y0)) continue;
-		x0 -= floor(x0 / g.nx) * g.nx;
-		y0 -= floor(y0 / g.ny) * g.ny;
-		const int ix0 = (int)floor(x0), iy0 = (int)floor(y0);
-		const float fx0 = (float)(x0 - ix0), fy0 = (float)(y0 - iy0);
-		const float step = (float)(p.dx * g.sx);
-		const float xf = fx0 + ix * step;
-		const float yf = fy0 + iy * step;
-		const float flx = floorf(xf), fly = floorf(yf);
-		int jx = ix0 + (int)flx, jy = iy0 + (int)fly;
-		const float wx = xf - flx, wy = yf - fly;
-		while (jx >= g.nx) jx -= g.nx;
-		while (jy >= g.ny) jy -= g.ny;
-		while (jx < 0) jx += g.nx;
-		while (jy < 0) jy += g.ny;
-		const int jx1 = jx == g.nx - 1 ? 0 : jx + 1;
-		const int jy1 = jy == g.ny - 1 ? 0 : jy + 1;
-		const float* s = g.screen;
-		const float m00 = __ldg(s + jx + (size_t)g.nx * jy);
-		const float m10 = __ldg(s + jx1 + (size_t)g.nx * jy);
-		const float m01 = __ldg(s + jx + (size_t)g.nx * jy1);
-		const float m11 = __ldg(s + jx1 + (size_t)g.nx * jy1);
-		acc += g.alpha * ((m00 + (m10 - m00) * wx) * (1.f - wy) + (m01 + (m11 - m01) * wx) * wy);
-	}
-	p.opd[(size_t)isa * p.nopd * p.nopd + ip] = acc;
-}
-
-// ---------------------------------------------------------------------------
 // Shared pieces of the 32-point pipeline (one warp).
 // ---------------------------------------------------------------------------
 constexpr int N32 = 32;
@@ -207,15 +183,15 @@ constexpr int LD = 33;  // padded leading dimension of the warp tile (float2)
 // forward FFT, pruned to the 16 non-zero rows and columns.  On return lane l
 // holds F(kx=l, ky=0..31).  opd/amp are the subaperture's 256 values
 // (x fastest); tile is the warp's 32x33 float2 scratch.
-__device__ __forceinline__ void field_fft_n32(const float* __restrict__ opd, const float* __restrict__ amp,
+__device__ __forceinline__ void field_fft_n32(const float* opd, const float* __restrict__ amp,
 	float twoinvwvl, float2* tile, int lane, float2 (&F)[32]) {
 	// (b) field. lane holds elements e = j*32 + lane: ix = lane&15, iy = 2j + lane/16
 	float o[8], a[8];
 	float s = 0.f;
 #pragma unroll
 	for (int j = 0; j < 8; j++) {
-		o[j] = __ldg(opd + j * 32 + lane);
-		a[j] = __ldg(amp + j * 32 + lane);
+		o[j] = opd[j * 32 + lane];
+		a[j] = amp[j * 32 + lane];
 		s += o[j];
 	}
 	// remove the subaperture piston before forming the phase: a constant phase
@@ -291,10 +267,89 @@ __device__ __forceinline__ void psf_to_otf_n32(float2 (&F)[32], float scale, flo
 }
 
 // ---------------------------------------------------------------------------
-// LGS uplink OTF (maos/wfsints.c:149-199 with nlwvf == nwvf == notf):
-// lotf = FFT(|FFT(embed(lltamp*exp(i*2*pi*lltopd/wvl)))|^2 / nlwvf^2).
-// One warp per WFS.  Output transposed: lotfT[fy + 32*fx].
+// (a) ray trace of every pupil of the frame in one launch, and the LGS uplink
+// OTF.  Block b belongs to the entry whose [item0, item0+nsa) holds b; it
+// traces one subaperture's nopd^2 points through every layer.  The start of
+// the subaperture in each screen is formed and wrapped once per layer in FP64
+// (threads l < nlayer), then every point adds its bilinear sample with FP32
+// in-subaperture offsets (< nopd screen pixels).  An LLT block keeps the OPD
+// in shared memory and its first warp turns it into the uplink OTF:
+// lotf = FFT(|FFT(embed(lltamp*exp(i*2*pi*opd/wvl)))|^2 / nlwvf^2), stored
+// transposed (fy fastest).
 // ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomParams P) {
+	__shared__ int s_ix0[SHWFS_MAX_LAYERS], s_iy0[SHWFS_MAX_LAYERS];
+	__shared__ float s_fx0[SHWFS_MAX_LAYERS], s_fy0[SHWFS_MAX_LAYERS], s_step[SHWFS_MAX_LAYERS];
+	__shared__ float s_opd[256];
+	__shared__ float2 s_tile[32 * LD];
+	int ie = 0;
+	while (ie + 1 < P.nentry && (int)blockIdx.x >= P.e[ie + 1].item0) ie++;
+	const GeomEntry& E = P.e[ie];
+	const int isa = blockIdx.x - E.item0;
+	if (isa < 0 || isa >= E.nsa) return;
+	const int tid = threadIdx.x;
+	if (tid < P.nlayer) {
+		const int l = tid;
+		double x0 = E.origx[isa] * E.sx[l] + E.dispx[l];
+		double y0 = E.origy[isa] * E.sx[l] + E.dispy[l];
+		const int nx = P.nx[l], ny = P.ny[l];
+		if (!isfinite(x0) || !isfinite(y0)) {
+			x0 = 0;
+			y0 = 0;
+		}
+		x0 -= floor(x0 / nx) * nx;
+		y0 -= floor(y0 / ny) * ny;
+		int ix0 = (int)floor(x0), iy0 = (int)floor(y0);
+		float fx0 = (float)(x0 - ix0), fy0 = (float)(y0 - iy0);
+		if (ix0 >= nx) ix0 -= nx;
+		if (iy0 >= ny) iy0 -= ny;
+		s_ix0[l] = ix0;
+		s_iy0[l] = iy0;
+		s_fx0[l] = fx0;
+		s_fy0[l] = fy0;
+		s_step[l] = (float)(E.dx * E.sx[l]);
+	}
+	__syncthreads();
+	const int np = E.nopd * E.nopd;
+	for (int ip = tid; ip < np; ip += blockDim.x) {
+		const int ix = ip % E.nopd, iy = ip / E.nopd;
+		float acc = 0.f;
+		for (int l = 0; l < P.nlayer; l++) {
+			if (!((E.use >> l) & 1u)) continue;
+			const int nx = P.nx[l], ny = P.ny[l];
+			const float xf = s_fx0[l] + ix * s_step[l];
+			const float yf = s_fy0[l] + iy * s_step[l];
+			const float flx = floorf(xf), fly = floorf(yf);
+			int jx = s_ix0[l] + (int)flx, jy = s_iy0[l] + (int)fly;
+			const float wx = xf - flx, wy = yf - fly;
+			while (jx >= nx) jx -= nx;
+			while (jy >= ny) jy -= ny;
+			const int jx1 = jx == nx - 1 ? 0 : jx + 1;
+			const int jy1 = jy == ny - 1 ? 0 : jy + 1;
+			const float* sc = P.screen[l];
+			const float m00 = __ldg(sc + jx + (size_t)nx * jy);
+			const float m10 = __ldg(sc + jx1 + (size_t)nx * jy);
+			const float m01 = __ldg(sc + jx + (size_t)nx * jy1);
+			const float m11 = __ldg(sc + jx1 + (size_t)nx * jy1);
+			acc += P.alpha[l] * ((m00 + (m10 - m00) * wx) * (1.f - wy) + (m01 + (m11 - m01) * wx) * wy);
+		}
+		if (E.opd) E.opd[(size_t)isa * np + ip] = acc;
+		if (E.lltamp && ip < 256) s_opd[ip] = acc;
+	}
+	if (E.lltamp) {  // uplink OTF (needs nopd == 16: checked on the host)
+		__syncthreads();
+		if (tid < 32) {
+			float2 F[32];
+			field_fft_n32(s_opd, E.lltamp, E.twoinvwvl, s_tile, tid, F);
+			psf_to_otf_n32(F, E.lltnorm, s_tile, tid);
+#pragma unroll
+			for (int fx = 0; fx < 32; fx++) E.lotfT[tid + 32 * fx] = F[fx];
+		}
+	}
+}
+
+// Uplink OTF from a given LLT OPD (one warp per WFS), for callers that hold
+// the LLT OPD already (shwfs_ints_grad_dev).
 __global__ void uplink_otf_n32_kernel(const float* const* lltopd, const float* lltamp, float2* const* lotfT,
 	int nwfs, float twoinvwvl, float lltnorm) {
 	__shared__ float2 tiles[4][32 * LD];
@@ -388,8 +443,11 @@ __device__ __forceinline__ void grad_from_pixels(const float (&pix)[NPQ], int np
 // (b)-(e) fused, n_opd=16, n_w=n_f=32.  Work item w -> (isa = w / nw, wfs =
 // wlist[w % nw]) so the WFS that share a subaperture's ETF run together.
 // ---------------------------------------------------------------------------
-template <int NPQ>  // pixel slots per lane: ceil(npix/32)
-__global__ void __launch_bounds__(128) ints_n32_kernel(PowfsDev P, const WfsDev* __restrict__ wfs, int nw, int nitem) {
+// NPQ: pixel slots per lane, ceil(npix/32).  MINB: resident blocks per SM the
+// register allocation must allow (occupancy/spill trade-off, picked by the
+// autotuner).
+template <int NPQ, int MINB>
+__global__ void __launch_bounds__(128, MINB) ints_n32_kernel(PowfsDev P, const WfsDev* __restrict__ wfs, int nw, int nitem) {
 	__shared__ float2 tiles[4][32 * LD];
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	const int item = blockIdx.x * 4 + warp;

@@ -96,6 +96,8 @@ def _load() -> C.CDLL:
         "shwfs_profile_enable": [vp, i],
         "shwfs_profile_read": [vp, dp, ip],
         "shwfs_copy_counters": [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)],
+        "shwfs_autotune": [vp, i, i, i, ip],
+        "shwfs_set_variant": [vp, i, i],
     }
     for name, args in sig.items():
         f = getattr(lib, name)
@@ -267,6 +269,15 @@ class Context:
         a, b = C.c_uint64(), C.c_uint64()
         self._check(self._L.shwfs_copy_counters(self._h, C.byref(a), C.byref(b)), "copy_counters")
         return a.value, b.value
+
+    def autotune(self, iwfs0: int, iwfs1: int, nrep: int = 5) -> int:
+        """Pick the fastest imaging-kernel variant on the real frames; returns its index."""
+        out = C.c_int()
+        self._check(self._L.shwfs_autotune(self._h, iwfs0, iwfs1, nrep, C.byref(out)), "autotune")
+        return out.value
+
+    def set_variant(self, ipowfs: int, variant: int):
+        self._check(self._L.shwfs_set_variant(self._h, ipowfs, variant), "set_variant")
 
     STAGES = ("raytrace", "uplink", "ints")
 
