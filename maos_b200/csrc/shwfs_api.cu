@@ -12,9 +12,11 @@
 #include <stdio.h>
 #include <string.h>
 #include <string>
+#include <algorithm>
 #include <vector>
 #include "../../include/shwfs_b200.h"
 #include "shwfs_kernels.cuh"
+#include "shwfs_tc.cuh"
 
 using namespace shwfs;
 
@@ -47,6 +49,11 @@ struct PowfsState {
 	DevBuf<float> lltamp;
 	DevBuf<double> lltorig;  // {llt origx, llt origy}
 	int variant = 0;         // imaging-kernel variant chosen by shwfs_autotune
+	std::vector<int> simap_idx_h;     // host copies of the pixel map (TC tables)
+	std::vector<double> simap_wt_h;
+	DevBuf<uint4> tc_bmat;            // tensor-core B operands (bf16 images)
+	DevBuf<float2> tc_gx;             // Gx(ix, fx)
+	int tc_ready = 0;
 	std::vector<double> origx_h, origy_h;
 };
 
@@ -72,6 +79,8 @@ struct LayerState {
 struct shwfs_ctx {
 	int device = 0;
 	cudaStream_t stream = nullptr;
+	cudaStream_t aux = nullptr;          // LLT/uplink work beside the main ray trace
+	cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 	std::string err;
 	std::vector<PowfsState> powfs;
 	std::vector<WfsState> wfs;
@@ -82,6 +91,7 @@ struct shwfs_ctx {
 	std::vector<WfsDev> wfsdev_h;
 	DevBuf<const float*> llt_in;
 	DevBuf<float2*> llt_out;
+	DevBuf<int> errflag;                 // bounded device waits record expiry here
 	uint64_t h2d_bytes = 0, d2h_bytes = 0;
 	// stage timing
 	int profiling = 0;
@@ -107,17 +117,18 @@ static cudaEvent_t ev_get(shwfs_ctx* ctx) {
 struct StageMark {
 	shwfs_ctx* ctx;
 	int stage;
+	cudaStream_t st;
 	cudaEvent_t a = nullptr;
-	StageMark(shwfs_ctx* c, int s) : ctx(c), stage(s) {
+	StageMark(shwfs_ctx* c, int s, cudaStream_t stream = nullptr) : ctx(c), stage(s), st(stream ? stream : c->stream) {
 		if (ctx->profiling) {
 			a = ev_get(ctx);
-			cudaEventRecord(a, ctx->stream);
+			cudaEventRecord(a, st);
 		}
 	}
 	~StageMark() {
 		if (a) {
 			cudaEvent_t b = ev_get(ctx);
-			cudaEventRecord(b, ctx->stream);
+			cudaEventRecord(b, st);
 			ctx->marks.push_back({stage, a, b});
 		}
 	}
@@ -165,6 +176,17 @@ static int dev_upload_f(shwfs_ctx* ctx, DevBuf<float>& b, const double* h, size_
 	return dev_upload(ctx, b, t.data(), n);
 }
 
+static int check_errflag(shwfs_ctx* ctx) {
+	if (!ctx->errflag.p) return 0;
+	int v = 0;
+	CK(cudaMemcpy(&v, ctx->errflag.p, sizeof(int), cudaMemcpyDeviceToHost));
+	if (v) {
+		CK(cudaMemset(ctx->errflag.p, 0, sizeof(int)));
+		return fail(ctx, SHWFS_ETIMEOUT, "a bounded tensor-core wait expired in the imaging kernel");
+	}
+	return 0;
+}
+
 static int set_device(shwfs_ctx* ctx) {
 	CK(cudaSetDevice(ctx->device));
 	return 0;
@@ -185,7 +207,10 @@ int shwfs_create(shwfs_ctx** pctx, int device) {
 		delete ctx;
 		return SHWFS_ECUDA;
 	}
-	if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+	if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+		cudaStreamCreateWithFlags(&ctx->aux, cudaStreamNonBlocking) != cudaSuccess ||
+		cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+		cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming) != cudaSuccess) {
 		delete ctx;
 		return SHWFS_ECUDA;
 	}
@@ -209,6 +234,8 @@ int shwfs_destroy(shwfs_ctx* ctx) {
 		p.etfT[1].free_();
 		p.lltamp.free_();
 		p.lltorig.free_();
+		p.tc_bmat.free_();
+		p.tc_gx.free_();
 	}
 	for (auto& w : ctx->wfs) {
 		w.mtche.free_();
@@ -228,8 +255,13 @@ int shwfs_destroy(shwfs_ctx* ctx) {
 	}
 	for (auto e : ctx->ev_pool) cudaEventDestroy(e);
 	ctx->wfsdev.free_();
+	ctx->errflag.free_();
 	ctx->llt_in.free_();
 	ctx->llt_out.free_();
+	cudaStreamSynchronize(ctx->aux);
+	cudaEventDestroy(ctx->ev_fork);
+	cudaEventDestroy(ctx->ev_join);
+	cudaStreamDestroy(ctx->aux);
 	cudaStreamDestroy(ctx->stream);
 	delete ctx;
 	return 0;
@@ -263,6 +295,8 @@ int shwfs_powfs_add(shwfs_ctx* ctx, const shwfs_powfs_desc* d, int* ipowfs) {
 	if (d->gradtype != SHWFS_GRAD_MF && d->gradtype != SHWFS_GRAD_COG)
 		return fail(ctx, SHWFS_EINVAL, "powfs: gradtype must be SHWFS_GRAD_MF or SHWFS_GRAD_COG");
 	if (d->sigmatch < 0 || d->sigmatch > 2) return fail(ctx, SHWFS_EINVAL, "powfs: sigmatch must be 0, 1 or 2");
+	if (d->has_llt && d->llt_nx != d->nopd)
+		return fail(ctx, SHWFS_EINVAL, "powfs: LLT pupil sampling (%d) must equal the subaperture's (%d)", d->llt_nx, d->nopd);
 	if (d->has_llt && d->llt_nx * d->embfac != 32)
 		return fail(ctx, SHWFS_EINVAL, "powfs: LLT pupil of %d points is not supported (needs %d)", d->llt_nx, 32 / d->embfac);
 	int r = set_device(ctx);
@@ -343,6 +377,9 @@ int shwfs_powfs_set_simap(shwfs_ctx* ctx, int ipowfs, const int* idx, const doub
 	if ((r = dev_upload(ctx, p->simap_idx, idx, m))) return r;
 	if ((r = dev_upload_f(ctx, p->simap_wt, wt, m))) return r;
 	p->nsimap = nmap;
+	p->simap_idx_h.assign(idx, idx + m);
+	p->simap_wt_h.assign(wt, wt + m);
+	p->tc_ready = 0;
 	return 0;
 }
 
@@ -438,6 +475,8 @@ int shwfs_atm_set(shwfs_ctx* ctx, int nlayer, const shwfs_layer_desc* layers, co
 
 // ---- frame machinery ----
 
+static int launch_geom_wfs(shwfs_ctx* ctx, GeomParams& gp);
+
 // Appends one pupil to a batched ray-trace launch: per-layer geometry of
 // prop_range (lib/accphi.c:223-244) and prop_grid_pts
 // (lib/accphi_grid_do.c:408-434), FP64 on the host.
@@ -485,13 +524,42 @@ static void geom_init(shwfs_ctx* ctx, GeomParams& gp) {
 	}
 }
 
-static int launch_geom(shwfs_ctx* ctx, GeomParams& gp) {
-	int nblk = 0;
-	for (int i = 0; i < gp.nentry; i++) {
-		gp.e[i].item0 = nblk;
-		nblk += gp.e[i].nsa;
+// LLT pupils go to llt_uplink_kernel on the aux stream (forked from and
+// joined back into the main stream); subaperture pupils to geom_kernel.
+static int launch_geom(shwfs_ctx* ctx, GeomParams& all) {
+	GeomParams gp, lp;
+	memcpy(&gp, &all, sizeof(GeomParams));
+	memcpy(&lp, &all, sizeof(GeomParams));
+	gp.nentry = lp.nentry = 0;
+	for (int i = 0; i < all.nentry; i++) {
+		if (all.e[i].lltamp) lp.e[lp.nentry++] = all.e[i];
+		else gp.e[gp.nentry++] = all.e[i];
 	}
-	if (nblk == 0) return 0;
+	if (lp.nentry) {
+		CK(cudaEventRecord(ctx->ev_fork, ctx->stream));
+		CK(cudaStreamWaitEvent(ctx->aux, ctx->ev_fork, 0));
+		{
+			StageMark m(ctx, SHWFS_STAGE_UPLINK, ctx->aux);
+			llt_uplink_kernel<<<lp.nentry, 256, 0, ctx->aux>>>(lp);
+		}
+		CK(cudaGetLastError());
+		CK(cudaEventRecord(ctx->ev_join, ctx->aux));
+	}
+	int r = launch_geom_wfs(ctx, gp);
+	if (lp.nentry) CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
+	return r;
+}
+
+static int launch_geom_wfs(shwfs_ctx* ctx, GeomParams& gp) {
+	int nitem = 0;
+	const int nopd = gp.nentry ? gp.e[0].nopd : 0;
+	for (int i = 0; i < gp.nentry; i++) {
+		if (gp.e[i].nopd != nopd) return fail(ctx, SHWFS_EINVAL, "ray trace: pupils of one launch need the same sampling");
+		gp.e[i].item0 = nitem;
+		nitem += gp.e[i].nsa;
+	}
+	if (nitem == 0) return 0;
+	const int nblk = nitem;
 	if (gp.nlayer == 0) {  // no turbulence: zero OPD and a flat-wavefront uplink
 		for (int i = 0; i < gp.nentry; i++)
 			if (gp.e[i].opd)
@@ -499,7 +567,7 @@ static int launch_geom(shwfs_ctx* ctx, GeomParams& gp) {
 	}
 	{
 		StageMark m(ctx, SHWFS_STAGE_RAYTRACE);
-		geom_kernel<<<nblk, 256, 0, ctx->stream>>>(gp);
+		geom_kernel<<<nblk, 256, 0, ctx->stream>>>(gp, nopd, nitem);
 	}
 	CK(cudaGetLastError());
 	return 0;
@@ -579,6 +647,168 @@ static int check_ready(shwfs_ctx* ctx, const PowfsState& p, const WfsState& w) {
 	return 0;
 }
 
+// ---- tensor-core form tables ----
+// float -> bf16, round to nearest even
+static uint16_t f2bf(float f) {
+	uint32_t u;
+	memcpy(&u, &f, 4);
+	if ((u & 0x7fffffffu) > 0x7f800000u) return 0x7fc0;
+	u += 0x7fffu + ((u >> 16) & 1u);
+	return (uint16_t)(u >> 16);
+}
+static float bf2f(uint16_t h) {
+	uint32_t u = (uint32_t)h << 16;
+	float f;
+	memcpy(&f, &u, 4);
+	return f;
+}
+// Writes the hi/lo image of a real N x K matrix m(n, k) into the canonical
+// K-major layout with 2K/8 chunks per row group (hi chunks first).
+static void put_bmat(std::vector<uint16_t>& img, size_t byte0, int N, int K, const std::vector<double>& m) {
+	const int kc = 2 * K / 8;
+	for (int n = 0; n < N; n++)
+		for (int k = 0; k < K; k++) {
+			const float v = (float)m[(size_t)n * K + k];
+			const uint16_t h = f2bf(v);
+			const uint16_t l = f2bf(v - bf2f(h));
+			const size_t oh = byte0 + tc_off(n, k / 8, kc) + (k % 8) * 2;
+			const size_t ol = byte0 + tc_off(n, K / 8 + k / 8, kc) + (k % 8) * 2;
+			img[oh / 2] = h;
+			img[ol / 2] = l;
+		}
+}
+// Real block form of a complex matrix M (nout x nin) for C = A B^T with A rows
+// [re | im] of length 2*nin: rows n < nout give Re, rows nhalf+n give Im.
+static void complex_block(std::vector<double>& m, int N, int K, int nhalf, int nout, int nin,
+	const std::vector<double>& mr, const std::vector<double>& mi) {
+	m.assign((size_t)N * K, 0.0);
+	for (int n = 0; n < nout; n++)
+		for (int j = 0; j < nin; j++) {
+			const double a = mr[(size_t)n * nin + j], b = mi[(size_t)n * nin + j];
+			m[(size_t)n * K + j] = a;
+			m[(size_t)n * K + nin + j] = -b;
+			m[(size_t)(nhalf + n) * K + j] = b;
+			m[(size_t)(nhalf + n) * K + nin + j] = a;
+		}
+}
+
+// Builds B1 (16-into-32 DFT), B2 (32-point DFT), B3 (Gy) and Gx for a powfs.
+// The pixel weights come from the pixel geometry in separable form and must
+// reproduce the uploaded pixel map tap for tap.
+static int build_tc_tables(shwfs_ctx* ctx, PowfsState& p) {
+	const shwfs_powfs_desc& d = p.d;
+	const int n = d.notf, n2 = n / 2, npx = d.pixpsax, npy = d.pixpsay, npix = npx * npy;
+	if (!(d.nopd == 16 && n == 32)) return fail(ctx, SHWFS_EINVAL, "TC form: needs 16x16 OPD points and a 32x32 OTF");
+	if (npx > 8 || npy > 8) return fail(ctx, SHWFS_EINVAL, "TC form: at most 8x8 pixels in this build");
+	if (p.nsimap != 1 || p.simap_idx_h.empty()) return fail(ctx, SHWFS_EINVAL, "TC form: needs one pixel map shared by all subapertures");
+	const double dtheta = d.wvl / (d.dsa * d.embfac);
+	const double dx_in1 = 1. / dtheta, disp = (0 - (-n2 * dtheta)) * dx_in1;
+	// 1-D bilinear taps of every pixel column / row (lib/mkh.c:96-140 in separable form)
+	auto taps = [&](int np, double pth, int i, int* g, double* w) {
+		const double po = -(np * 0.5 - 0.5) * pth;
+		double f = (i * pth + po) * dx_in1 + disp;
+		const int fl = (int)floor(f);
+		f -= fl;
+		g[0] = fl;
+		g[1] = fl + 1;
+		w[0] = 1. - f;
+		w[1] = f;
+	};
+	std::vector<double> Wx((size_t)npx * n, 0.0), Wy((size_t)npy * n, 0.0);
+	for (int ix = 0; ix < npx; ix++) {
+		int g[2];
+		double w[2];
+		taps(npx, d.pixthetax, ix, g, w);
+		for (int iy = 0; iy < npy; iy++) {
+			int gy[2];
+			double wy[2];
+			taps(npy, d.pixthetay, iy, gy, wy);
+			// the product taps must equal the uploaded map of pixel (ix, iy)
+			std::vector<std::pair<int, double>> mine, theirs;
+			for (int b = 0; b < 2; b++)
+				for (int a = 0; a < 2; a++) {
+					const double wt = w[a] * wy[b];
+					if (wt > 1e-15 && g[a] >= 0 && g[a] < n && gy[b] >= 0 && gy[b] < n) mine.push_back({g[a] + gy[b] * n, wt});
+				}
+			const int pix = ix + iy * npx;
+			for (int c = 0; c < 4; c++)
+				if (p.simap_idx_h[4 * pix + c] >= 0) theirs.push_back({p.simap_idx_h[4 * pix + c], p.simap_wt_h[4 * pix + c]});
+			std::sort(mine.begin(), mine.end());
+			std::sort(theirs.begin(), theirs.end());
+			bool same = mine.size() == theirs.size();
+			for (size_t t = 0; same && t < mine.size(); t++)
+				same = mine[t].first == theirs[t].first && fabs(mine[t].second - theirs[t].second) <= 1e-9;
+			if (!same) return fail(ctx, SHWFS_EINVAL, "TC form: the pixel map of pixel %d is not separable bilinear", pix);
+		}
+		for (int a = 0; a < 2; a++)
+			if (g[a] >= 0 && g[a] < n) Wx[(size_t)ix * n + g[a]] += w[a];
+	}
+	for (int iy = 0; iy < npy; iy++) {
+		int g[2];
+		double w[2];
+		taps(npy, d.pixthetay, iy, g, w);
+		for (int a = 0; a < 2; a++)
+			if (g[a] >= 0 && g[a] < n) Wy[(size_t)iy * n + g[a]] += w[a];
+	}
+	// G(i, f) = sum_x W(i, x) exp(+2 pi i f x / n)
+	auto Gmat = [&](const std::vector<double>& W, int ni, std::vector<double>& gr, std::vector<double>& gi) {
+		gr.assign((size_t)ni * n, 0.0);
+		gi.assign((size_t)ni * n, 0.0);
+		for (int i = 0; i < ni; i++)
+			for (int f = 0; f < n; f++)
+				for (int x = 0; x < n; x++) {
+					const double w = W[(size_t)i * n + x];
+					if (w == 0) continue;
+					const double ang = 2 * M_PI * (double)((f * x) % n) / n;
+					gr[(size_t)i * n + f] += w * cos(ang);
+					gi[(size_t)i * n + f] += w * sin(ang);
+				}
+	};
+	std::vector<double> gxr, gxi, gyr, gyi;
+	Gmat(Wx, npx, gxr, gxi);
+	Gmat(Wy, npy, gyr, gyi);
+	// forward DFT matrices, w = exp(-2 pi i / 32)
+	std::vector<double> m1r(32 * 16), m1i(32 * 16), m2r(32 * 32), m2i(32 * 32);
+	for (int k = 0; k < 32; k++) {
+		for (int j = 0; j < 16; j++) {
+			const int e = (k * (j + 8)) % 32;
+			m1r[k * 16 + j] = cos(2 * M_PI * e / 32);
+			m1i[k * 16 + j] = -sin(2 * M_PI * e / 32);
+		}
+		for (int j = 0; j < 32; j++) {
+			const int e = (k * j) % 32;
+			m2r[k * 32 + j] = cos(2 * M_PI * e / 32);
+			m2i[k * 32 + j] = -sin(2 * M_PI * e / 32);
+		}
+	}
+	std::vector<double> b1, b2, b3;
+	complex_block(b1, 64, 32, 32, 32, 16, m1r, m1i);
+	complex_block(b2, 64, 64, 32, 32, 32, m2r, m2i);
+	complex_block(b3, 32, 64, 16, npy, 32, gyr, gyi);
+	std::vector<uint16_t> img(TC_B_BYTES / 2, 0);
+	put_bmat(img, 0, 64, 32, b1);
+	put_bmat(img, TC_B1_BYTES, 64, 64, b2);
+	put_bmat(img, TC_B1_BYTES + TC_B2_BYTES, 32, 64, b3);
+	int r;
+	if ((r = dev_upload(ctx, p.tc_bmat, reinterpret_cast<const uint4*>(img.data()), TC_B_BYTES / 16))) return r;
+	std::vector<float2> gx((size_t)npx * 32);
+	for (int i = 0; i < npx; i++)
+		for (int f = 0; f < 32; f++) gx[(size_t)i * 32 + f] = make_float2((float)gxr[(size_t)i * n + f], (float)gxi[(size_t)i * n + f]);
+	if ((r = dev_upload(ctx, p.tc_gx, gx.data(), gx.size()))) return r;
+	(void)npix;
+	p.tc_ready = 1;
+	return 0;
+}
+
+static int tc_sm_count(shwfs_ctx* ctx) {
+	static int nsm[64] = {0};
+	if (ctx->device < 64 && nsm[ctx->device]) return nsm[ctx->device];
+	int v = 148;
+	cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, ctx->device);
+	if (ctx->device < 64) nsm[ctx->device] = v;
+	return v;
+}
+
 // (b)-(e) for a set of WFS of one powfs sharing the launch.
 static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist, int isim,
 	const std::vector<const float*>& opds, const std::vector<const float2*>& lotfs, const std::vector<float*>& ints,
@@ -627,6 +857,32 @@ static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist
 	const int npix = P.npix;
 	StageMark mark(ctx, SHWFS_STAGE_INTS);
 	const WfsDev* wdev = ctx->wfsdev.p + off;
+	if (ctx->form == SHWFS_FORM_TC) {
+		if (!p.tc_ready) {
+			int r = build_tc_tables(ctx, p);
+			if (r) return r;
+		}
+		if (!ctx->errflag.p) {
+			int r = dev_alloc(ctx, ctx->errflag, 1);
+			if (r) return r;
+			CK(cudaMemsetAsync(ctx->errflag.p, 0, sizeof(int), ctx->stream));
+		}
+		static bool attr_set[64] = {false};
+		if (ctx->device < 64 && !attr_set[ctx->device]) {
+			CK(cudaFuncSetAttribute(ints_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES));
+			CK(cudaFuncSetAttribute(ints_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES));
+			attr_set[ctx->device] = true;
+		}
+		TcTables T{p.tc_bmat.p, p.tc_gx.p};
+		const int ntile = (nitem + 3) / 4;
+		const int grid = std::min(ntile, tc_sm_count(ctx) * 3);
+		if (npix <= 32)
+			ints_tc_kernel<1><<<grid, 128, TC_SMEM_BYTES, ctx->stream>>>(P, wdev, nw, nitem, T, ctx->errflag.p);
+		else
+			ints_tc_kernel<2><<<grid, 128, TC_SMEM_BYTES, ctx->stream>>>(P, wdev, nw, nitem, T, ctx->errflag.p);
+		CK(cudaGetLastError());
+		return 0;
+	}
 	auto go = [&](auto kern) { kern<<<nblk, 128, 0, ctx->stream>>>(P, wdev, nw, nitem); };
 	const int v = p.variant;
 	if (npix <= 32) {
@@ -791,6 +1047,7 @@ int shwfs_frame_sync(shwfs_ctx* ctx, int iwfs, double* grad, double* ints) {
 	}
 	CK(cudaStreamSynchronize(ctx->stream));
 	ctx->wfsdev_h.clear();
+	if ((r = check_errflag(ctx))) return r;
 	if (grad)
 		for (int i = 0; i < 2 * nsa; i++) grad[i] = w->grad_h[i];
 	if (ints)
@@ -857,6 +1114,7 @@ int shwfs_profile_read(shwfs_ctx* ctx, double* ms, int* launches) {
 	int r = set_device(ctx);
 	if (r) return r;
 	CK(cudaStreamSynchronize(ctx->stream));
+	CK(cudaStreamSynchronize(ctx->aux));
 	for (int i = 0; i < SHWFS_NSTAGE; i++) {
 		ms[i] = 0;
 		launches[i] = 0;
@@ -879,7 +1137,7 @@ int shwfs_sync(shwfs_ctx* ctx) {
 	if (r) return r;
 	CK(cudaStreamSynchronize(ctx->stream));
 	ctx->wfsdev_h.clear();
-	return 0;
+	return check_errflag(ctx);
 }
 
 }  // extern "C"

@@ -277,16 +277,22 @@ __device__ __forceinline__ void psf_to_otf_n32(float2 (&F)[32], float scale, flo
 // lotf = FFT(|FFT(embed(lltamp*exp(i*2*pi*opd/wvl)))|^2 / nlwvf^2), stored
 // transposed (fy fastest).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomParams P) {
-	__shared__ int s_ix0[SHWFS_MAX_LAYERS], s_iy0[SHWFS_MAX_LAYERS];
+// Thread layout: one block of 256 threads per subaperture, one OPD point per
+// thread and pass (points p = threadIdx.x + 256*k), so the 32 lanes of a warp
+// read contiguous runs of a screen row.  The start of the subaperture in each
+// screen is formed and wrapped once per layer in FP64 (threads l < nlayer);
+// the points add their bilinear samples with FP32 in-subaperture offsets
+// (< nopd screen pixels).  A layer whose footprint lies inside the screen
+// skips the periodic-wrap arithmetic.
+__global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomParams P, int nopd, int nitem) {
+	__shared__ int s_ix0[SHWFS_MAX_LAYERS], s_iy0[SHWFS_MAX_LAYERS], s_fast[SHWFS_MAX_LAYERS];
 	__shared__ float s_fx0[SHWFS_MAX_LAYERS], s_fy0[SHWFS_MAX_LAYERS], s_step[SHWFS_MAX_LAYERS];
-	__shared__ float s_opd[256];
-	__shared__ float2 s_tile[32 * LD];
+	const int item = blockIdx.x;
+	if (item >= nitem) return;
 	int ie = 0;
-	while (ie + 1 < P.nentry && (int)blockIdx.x >= P.e[ie + 1].item0) ie++;
+	while (ie + 1 < P.nentry && item >= P.e[ie + 1].item0) ie++;
 	const GeomEntry& E = P.e[ie];
-	const int isa = blockIdx.x - E.item0;
-	if (isa < 0 || isa >= E.nsa) return;
+	const int isa = item - E.item0;
 	const int tid = threadIdx.x;
 	if (tid < P.nlayer) {
 		const int l = tid;
@@ -300,51 +306,95 @@ __global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomP
 		x0 -= floor(x0 / nx) * nx;
 		y0 -= floor(y0 / ny) * ny;
 		int ix0 = (int)floor(x0), iy0 = (int)floor(y0);
-		float fx0 = (float)(x0 - ix0), fy0 = (float)(y0 - iy0);
+		const float fx0 = (float)(x0 - ix0), fy0 = (float)(y0 - iy0);
 		if (ix0 >= nx) ix0 -= nx;
 		if (iy0 >= ny) iy0 -= ny;
+		const float step = (float)(E.dx * E.sx[l]);
 		s_ix0[l] = ix0;
 		s_iy0[l] = iy0;
 		s_fx0[l] = fx0;
 		s_fy0[l] = fy0;
-		s_step[l] = (float)(E.dx * E.sx[l]);
+		s_step[l] = step;
+		const float ext = (nopd - 1) * step + 2.f;
+		s_fast[l] = (ix0 + fx0 + ext < (float)(nx - 1)) && (iy0 + fy0 + ext < (float)(ny - 1));
 	}
 	__syncthreads();
-	const int np = E.nopd * E.nopd;
-	for (int ip = tid; ip < np; ip += blockDim.x) {
-		const int ix = ip % E.nopd, iy = ip / E.nopd;
+	const int np = nopd * nopd;
+	for (int ip = tid; ip < np; ip += 256) {
+		const int ix = ip % nopd, iy = ip / nopd;
 		float acc = 0.f;
 		for (int l = 0; l < P.nlayer; l++) {
 			if (!((E.use >> l) & 1u)) continue;
 			const int nx = P.nx[l], ny = P.ny[l];
-			const float xf = s_fx0[l] + ix * s_step[l];
-			const float yf = s_fy0[l] + iy * s_step[l];
+			const float step = s_step[l];
+			const float xf = s_fx0[l] + ix * step, yf = s_fy0[l] + iy * step;
 			const float flx = floorf(xf), fly = floorf(yf);
-			int jx = s_ix0[l] + (int)flx, jy = s_iy0[l] + (int)fly;
 			const float wx = xf - flx, wy = yf - fly;
-			while (jx >= nx) jx -= nx;
-			while (jy >= ny) jy -= ny;
-			const int jx1 = jx == nx - 1 ? 0 : jx + 1;
-			const int jy1 = jy == ny - 1 ? 0 : jy + 1;
-			const float* sc = P.screen[l];
-			const float m00 = __ldg(sc + jx + (size_t)nx * jy);
-			const float m10 = __ldg(sc + jx1 + (size_t)nx * jy);
-			const float m01 = __ldg(sc + jx + (size_t)nx * jy1);
-			const float m11 = __ldg(sc + jx1 + (size_t)nx * jy1);
-			acc += P.alpha[l] * ((m00 + (m10 - m00) * wx) * (1.f - wy) + (m01 + (m11 - m01) * wx) * wy);
+			int jx = s_ix0[l] + (int)flx, jy = s_iy0[l] + (int)fly;
+			const float* __restrict__ sc = P.screen[l];
+			float m00, m10, m01, m11;
+			if (s_fast[l]) {
+				const float* r0 = sc + (size_t)jy * nx + jx;
+				m00 = __ldg(r0);
+				m10 = __ldg(r0 + 1);
+				m01 = __ldg(r0 + nx);
+				m11 = __ldg(r0 + nx + 1);
+			} else {  // periodic wrap (data->wrap=1, maos/sim_utils.c:1017)
+				while (jx >= nx) jx -= nx;
+				while (jy >= ny) jy -= ny;
+				const int jx1 = jx == nx - 1 ? 0 : jx + 1, jy1 = jy == ny - 1 ? 0 : jy + 1;
+				m00 = __ldg(sc + jx + (size_t)nx * jy);
+				m10 = __ldg(sc + jx1 + (size_t)nx * jy);
+				m01 = __ldg(sc + jx + (size_t)nx * jy1);
+				m11 = __ldg(sc + jx1 + (size_t)nx * jy1);
+			}
+			acc = fmaf(P.alpha[l], (m00 + (m10 - m00) * wx) * (1.f - wy) + (m01 + (m11 - m01) * wx) * wy, acc);
 		}
-		if (E.opd) E.opd[(size_t)isa * np + ip] = acc;
-		if (E.lltamp && ip < 256) s_opd[ip] = acc;
+		E.opd[(size_t)isa * np + ip] = acc;
 	}
-	if (E.lltamp) {  // uplink OTF (needs nopd == 16: checked on the host)
-		__syncthreads();
-		if (tid < 32) {
-			float2 F[32];
-			field_fft_n32(s_opd, E.lltamp, E.twoinvwvl, s_tile, tid, F);
-			psf_to_otf_n32(F, E.lltnorm, s_tile, tid);
+}
+
+// LGS uplink: ray trace of each LLT pupil (one block of 256 threads per
+// pupil, nopd == 16) into shared memory, then its first warp forms the
+// uplink OTF.  Runs beside geom_kernel on a second stream.
+__global__ void __launch_bounds__(256) llt_uplink_kernel(const __grid_constant__ GeomParams P) {
+	__shared__ float s_opd[256];
+	__shared__ float2 s_tile[32 * LD];
+	const GeomEntry& E = P.e[blockIdx.x];
+	const int ip = threadIdx.x;
+	const int ix = ip & 15, iy = ip >> 4;
+	float acc = 0.f;
+	for (int l = 0; l < P.nlayer; l++) {
+		if (!((E.use >> l) & 1u)) continue;
+		const int nx = P.nx[l], ny = P.ny[l];
+		double x0 = E.origx[0] * E.sx[l] + E.dispx[l];
+		double y0 = E.origy[0] * E.sx[l] + E.dispy[l];
+		if (!isfinite(x0) || !isfinite(y0)) continue;
+		x0 -= floor(x0 / nx) * nx;
+		y0 -= floor(y0 / ny) * ny;
+		const int ix0 = (int)floor(x0), iy0 = (int)floor(y0);
+		const float step = (float)(E.dx * E.sx[l]);
+		const float xf = (float)(x0 - ix0) + ix * step, yf = (float)(y0 - iy0) + iy * step;
+		const float flx = floorf(xf), fly = floorf(yf);
+		int jx = ix0 + (int)flx, jy = iy0 + (int)fly;
+		const float wx = xf - flx, wy = yf - fly;
+		while (jx >= nx) jx -= nx;
+		while (jy >= ny) jy -= ny;
+		const int jx1 = jx == nx - 1 ? 0 : jx + 1, jy1 = jy == ny - 1 ? 0 : jy + 1;
+		const float* sc = P.screen[l];
+		const float m00 = __ldg(sc + jx + (size_t)nx * jy), m10 = __ldg(sc + jx1 + (size_t)nx * jy);
+		const float m01 = __ldg(sc + jx + (size_t)nx * jy1), m11 = __ldg(sc + jx1 + (size_t)nx * jy1);
+		acc += P.alpha[l] * ((m00 + (m10 - m00) * wx) * (1.f - wy) + (m01 + (m11 - m01) * wx) * wy);
+	}
+	s_opd[ip] = acc;
+	if (E.opd) E.opd[ip] = acc;
+	__syncthreads();
+	if (ip < 32) {
+		float2 F[32];
+		field_fft_n32(s_opd, E.lltamp, E.twoinvwvl, s_tile, ip, F);
+		psf_to_otf_n32(F, E.lltnorm, s_tile, ip);
 #pragma unroll
-			for (int fx = 0; fx < 32; fx++) E.lotfT[tid + 32 * fx] = F[fx];
-		}
+		for (int fx = 0; fx < 32; fx++) E.lotfT[ip + 32 * fx] = F[fx];
 	}
 }
 
