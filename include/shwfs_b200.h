@@ -199,6 +199,23 @@ int shwfs_set_variant(shwfs_ctx* ctx, int ipowfs, int variant);
    resets the counters. */
 int shwfs_copy_counters(shwfs_ctx* ctx, uint64_t* h2d, uint64_t* d2h);
 
+/* ---- allocation-free frame (no counterpart in the reference) ----
+   One frame of WFS iwfs -- ray trace, uplink OTF, imaging, noise,
+   gradients -- that allocates no device memory: its scratch (OPD, LLT OPD,
+   uplink OTF, launch descriptor) lives in one file-scope device array of
+   about 4 MiB that every GPU loading the library keeps until exit.  For
+   callers that cannot call cudaMalloc once running (real-time loops that
+   forbid allocation after start-up, stream capture into a CUDA graph,
+   externally managed memory).  ints (nsa*npix) and grad (2*nsa) are device
+   pointers owned by the caller; either may be NULL, not both.  Limits: at
+   most SHWFS_NOALLOC_MAX_NSA subapertures of at most 16x16 OPD points;
+   larger WFS are rejected with SHWFS_EINVAL.  The first call on a device
+   looks up the array's device address (cudaGetSymbolAddress), so make it
+   before any stream capture.  Calls share the array: calls whose work
+   overlaps on the GPU race; queue them on one stream. */
+#define SHWFS_NOALLOC_MAX_NSA 4096
+int shwfs_frame_noalloc(shwfs_ctx* ctx, int iwfs, int isim, float* ints, float* grad);
+
 /* Synchronise the context stream; returns the first error of queued work. */
 int shwfs_sync(shwfs_ctx* ctx);
 /* The CUDA stream the context launches on (cudaStream_t as void*). */

@@ -1141,3 +1141,128 @@ int shwfs_sync(shwfs_ctx* ctx) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free frame.
+//
+// For callers that must not allocate device memory once they run: a
+// real-time control loop that forbids allocation after start-up, code that
+// records the frame into a CUDA graph (cudaMalloc is not allowed while a
+// stream is being captured), or a host whose memory pool is handed out by
+// someone else.  The ordinary frame keeps its scratch (the ray-traced OPD,
+// the LLT OPD, the uplink OTF and the launch descriptor) in buffers the
+// context allocates; this variant keeps them in one file-scope device array
+// instead, so a call allocates nothing.
+//
+// The array is SHWFS_NOALLOC_SCRATCH_FLOATS floats (about 4 MiB) and every
+// GPU that loads the library holds it until the process exits.  Its host-side
+// name is only a stand-in for the device symbol, so the device address is
+// looked up with cudaGetSymbolAddress once per device, with that device
+// current, the first time the entry point runs on it.  All calls on a device
+// share the array: every element a call reads is first written by the same
+// call, so nothing needs clearing between calls, but calls whose work
+// overlaps on the GPU (two streams, two contexts, two threads) race on it.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+#define NOALLOC_OPD_FLOATS (SHWFS_NOALLOC_MAX_NSA * 256)
+#define NOALLOC_LLT_OFF NOALLOC_OPD_FLOATS
+#define NOALLOC_LOTF_OFF (NOALLOC_LLT_OFF + 256)
+#define NOALLOC_DESC_OFF (NOALLOC_LOTF_OFF + 2048)
+#define SHWFS_NOALLOC_SCRATCH_FLOATS (NOALLOC_DESC_OFF + 64)
+
+static __device__ __align__(256) float g_noalloc_scratch[SHWFS_NOALLOC_SCRATCH_FLOATS];
+
+namespace {
+std::mutex g_noalloc_mutex;
+float* g_noalloc_ptr[64] = {nullptr};
+}  // namespace
+
+__global__ void noalloc_desc_kernel(WfsDev wd, WfsDev* dst) { *dst = wd; }
+
+static int noalloc_scratch(shwfs_ctx* ctx, float** out) {
+	if (ctx->device < 0 || ctx->device >= 64) return fail(ctx, SHWFS_EINVAL, "frame_noalloc: device %d out of range", ctx->device);
+	std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+	if (!g_noalloc_ptr[ctx->device]) {
+		void* p = nullptr;
+		cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+		if (e != cudaSuccess || !p)
+			return fail(ctx, SHWFS_ECUDA, "frame_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+		g_noalloc_ptr[ctx->device] = (float*)p;
+	}
+	*out = g_noalloc_ptr[ctx->device];
+	return 0;
+}
+
+extern "C" {
+
+int shwfs_frame_noalloc(shwfs_ctx* ctx, int iwfs, int isim, float* ints, float* grad) {
+	WfsState* w = get_wfs(ctx, iwfs);
+	if (!w || (!ints && !grad)) return ctx ? fail(ctx, SHWFS_EINVAL, "frame_noalloc: bad arguments") : SHWFS_EINVAL;
+	PowfsState& p = ctx->powfs[w->d.ipowfs];
+	if (p.d.nsa > SHWFS_NOALLOC_MAX_NSA)
+		return fail(ctx, SHWFS_EINVAL, "frame_noalloc: %d subapertures exceed the allocation-free maximum of %d",
+			p.d.nsa, SHWFS_NOALLOC_MAX_NSA);
+	if (p.d.nopd * p.d.nopd > 256)
+		return fail(ctx, SHWFS_EINVAL, "frame_noalloc: %dx%d OPD points per subaperture exceed the maximum of 16x16",
+			p.d.nopd, p.d.nopd);
+	int r = set_device(ctx);
+	if (r) return r;
+	if ((r = check_ready(ctx, p, *w))) return r;
+	float* scratch = nullptr;
+	if ((r = noalloc_scratch(ctx, &scratch))) return r;
+	// stage timing would create CUDA events: keep it off for this call
+	struct ProfileOff {
+		shwfs_ctx* c;
+		int saved;
+		~ProfileOff() { c->profiling = saved; }
+	} prof_off{ctx, ctx->profiling};
+	ctx->profiling = 0;
+	float* opd = scratch;
+	float* lltopd = scratch + NOALLOC_LLT_OFF;
+	float2* lotfT = reinterpret_cast<float2*>(scratch + NOALLOC_LOTF_OFF);
+	WfsDev* desc = reinterpret_cast<WfsDev*>(scratch + NOALLOC_DESC_OFF);
+	// (a) ray trace (and the LGS uplink) into the scratch array
+	GeomParams gp;
+	geom_init(ctx, gp);
+	if ((r = add_wfs_entry(ctx, gp, *w, isim, opd))) return r;
+	if (p.d.has_llt) {
+		if ((r = add_geom_entry(ctx, gp, w->d.thetax - p.d.llt_ox / w->d.hs, w->d.thetay - p.d.llt_oy / w->d.hs, w->d.hs,
+				 0, 0, 0, p.d.llt_ox, p.d.llt_oy, isim, p.lltorig.p, p.lltorig.p + 1, 1, p.d.llt_nx, p.d.dx, lltopd)))
+			return r;
+		GeomEntry& e = gp.e[gp.nentry - 1];
+		e.lltamp = p.lltamp.p;
+		e.lotfT = lotfT;
+		e.twoinvwvl = (float)(2.0 / p.d.wvl);
+		e.lltnorm = (float)(1.0 / ((double)p.d.llt_nx * p.d.embfac * p.d.llt_nx * p.d.embfac));
+	}
+	if ((r = launch_geom(ctx, gp))) return r;
+	// (b)-(e) with the launch descriptor written on the device
+	WfsDev wd;
+	memset(&wd, 0, sizeof(wd));
+	wd.opd = opd;
+	wd.amp = p.amp.p + (p.namp > 1 ? (size_t)w->wfsind * p.d.nsa * p.d.nopd * p.d.nopd : 0);
+	wd.lotfT = p.d.has_llt ? lotfT : nullptr;
+	wd.mtche = w->mtche.p;
+	wd.i0sum = w->i0sum.p;
+	wd.ints = ints;
+	wd.grad = grad;
+	wd.alpha = norm_ints(p, *w);
+	wd.noisy = w->d.noisy;
+	wd.wfs_id = (uint32_t)iwfs;
+	wd.seed = w->seed;
+	noalloc_desc_kernel<<<1, 1, 0, ctx->stream>>>(wd, desc);
+	CK(cudaGetLastError());
+	PowfsDev P = make_powfs_dev(p, isim);
+	const int nitem = p.d.nsa, nblk = (nitem + 3) / 4;
+	if (P.npix <= 32)
+		ints_n32_kernel<1, 4><<<nblk, 128, 0, ctx->stream>>>(P, desc, 1, nitem);
+	else if (P.npix <= 64)
+		ints_n32_kernel<2, 4><<<nblk, 128, 0, ctx->stream>>>(P, desc, 1, nitem);
+	else
+		ints_n32_kernel<4, 4><<<nblk, 128, 0, ctx->stream>>>(P, desc, 1, nitem);
+	CK(cudaGetLastError());
+	return 0;
+}
+
+}  // extern "C"

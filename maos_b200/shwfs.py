@@ -98,6 +98,7 @@ def _load() -> C.CDLL:
         "shwfs_copy_counters": [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)],
         "shwfs_autotune": [vp, i, i, i, ip],
         "shwfs_set_variant": [vp, i, i],
+        "shwfs_frame_noalloc": [vp, i, i, vp, vp],
     }
     for name, args in sig.items():
         f = getattr(lib, name)
@@ -257,6 +258,11 @@ class Context:
     def ints_grad_dev(self, iwfs, isim, opd, lltopd=None, ints=None, grad=None, add_noise=False):
         self._check(self._L.shwfs_ints_grad_dev(self._h, iwfs, isim, _devptr(opd), _devptr(lltopd), _devptr(ints),
                                                 _devptr(grad), 1 if add_noise else 0), "ints_grad_dev")
+
+    def frame_noalloc(self, iwfs, isim, ints=None, grad=None):
+        """One frame of WFS iwfs that allocates no device memory (scratch in a
+        static device array); ints/grad are caller-owned device tensors."""
+        self._check(self._L.shwfs_frame_noalloc(self._h, iwfs, isim, _devptr(ints), _devptr(grad)), "frame_noalloc")
 
     def grad_dev(self, iwfs, ints, grad):
         self._check(self._L.shwfs_grad_dev(self._h, iwfs, _devptr(ints), _devptr(grad)), "grad_dev")
