@@ -52,7 +52,6 @@ struct PowfsState {
 	std::vector<int> simap_idx_h;     // host copies of the pixel map (TC tables)
 	std::vector<double> simap_wt_h;
 	DevBuf<uint4> tc_bmat;            // tensor-core B operands (bf16 images)
-	DevBuf<float2> tc_gx;             // Gx(ix, fx)
 	int tc_ready = 0;
 	std::vector<double> origx_h, origy_h;
 };
@@ -235,7 +234,6 @@ int shwfs_destroy(shwfs_ctx* ctx) {
 		p.lltamp.free_();
 		p.lltorig.free_();
 		p.tc_bmat.free_();
-		p.tc_gx.free_();
 	}
 	for (auto& w : ctx->wfs) {
 		w.mtche.free_();
@@ -692,7 +690,7 @@ static void complex_block(std::vector<double>& m, int N, int K, int nhalf, int n
 		}
 }
 
-// Builds B1 (16-into-32 DFT), B2 (32-point DFT), B3 (Gy) and Gx for a powfs.
+// Builds B1 (16-into-32 DFT), B2 (32-point DFT), B3 (Gy) and B4 (Gx) for a powfs.
 // The pixel weights come from the pixel geometry in separable form and must
 // reproduce the uploaded pixel map tap for tap.
 static int build_tc_tables(shwfs_ctx* ctx, PowfsState& p) {
@@ -781,20 +779,23 @@ static int build_tc_tables(shwfs_ctx* ctx, PowfsState& p) {
 			m2i[k * 32 + j] = -sin(2 * M_PI * e / 32);
 		}
 	}
-	std::vector<double> b1, b2, b3;
+	std::vector<double> b1, b2, b3, b4((size_t)16 * 64, 0.0);
 	complex_block(b1, 64, 32, 32, 32, 16, m1r, m1i);
 	complex_block(b2, 64, 64, 32, 32, 32, m2r, m2i);
 	complex_block(b3, 32, 64, 16, npy, 32, gyr, gyi);
+	// 6b: I(ix, iy) = sum_fx Re T(fx, iy) Re Gx(ix, fx) - Im T(fx, iy) Im Gx(ix, fx)
+	for (int i = 0; i < npx; i++)
+		for (int f = 0; f < 32; f++) {
+			b4[(size_t)i * 64 + f] = gxr[(size_t)i * n + f];
+			b4[(size_t)i * 64 + 32 + f] = -gxi[(size_t)i * n + f];
+		}
 	std::vector<uint16_t> img(TC_B_BYTES / 2, 0);
 	put_bmat(img, 0, 64, 32, b1);
 	put_bmat(img, TC_B1_BYTES, 64, 64, b2);
 	put_bmat(img, TC_B1_BYTES + TC_B2_BYTES, 32, 64, b3);
+	put_bmat(img, TC_B1_BYTES + TC_B2_BYTES + TC_B3_BYTES, 16, 64, b4);
 	int r;
 	if ((r = dev_upload(ctx, p.tc_bmat, reinterpret_cast<const uint4*>(img.data()), TC_B_BYTES / 16))) return r;
-	std::vector<float2> gx((size_t)npx * 32);
-	for (int i = 0; i < npx; i++)
-		for (int f = 0; f < 32; f++) gx[(size_t)i * 32 + f] = make_float2((float)gxr[(size_t)i * n + f], (float)gxi[(size_t)i * n + f]);
-	if ((r = dev_upload(ctx, p.tc_gx, gx.data(), gx.size()))) return r;
 	(void)npix;
 	p.tc_ready = 1;
 	return 0;
@@ -873,13 +874,14 @@ static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist
 			CK(cudaFuncSetAttribute(ints_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES));
 			attr_set[ctx->device] = true;
 		}
-		TcTables T{p.tc_bmat.p, p.tc_gx.p};
+		TcTables T{p.tc_bmat.p};
+		// persistent: TC_CTAS_PER_SM CTAs of TC_GROUPS tile groups per SM
 		const int ntile = (nitem + 3) / 4;
-		const int grid = std::min(ntile, tc_sm_count(ctx) * 3);
+		const int grid = std::min((ntile + TC_GROUPS - 1) / TC_GROUPS, tc_sm_count(ctx) * TC_CTAS_PER_SM);
 		if (npix <= 32)
-			ints_tc_kernel<1><<<grid, 128, TC_SMEM_BYTES, ctx->stream>>>(P, wdev, nw, nitem, T, ctx->errflag.p);
+			ints_tc_kernel<1><<<grid, TC_THREADS, TC_SMEM_BYTES, ctx->stream>>>(P, wdev, nw, nitem, T, ctx->errflag.p);
 		else
-			ints_tc_kernel<2><<<grid, 128, TC_SMEM_BYTES, ctx->stream>>>(P, wdev, nw, nitem, T, ctx->errflag.p);
+			ints_tc_kernel<2><<<grid, TC_THREADS, TC_SMEM_BYTES, ctx->stream>>>(P, wdev, nw, nitem, T, ctx->errflag.p);
 		CK(cudaGetLastError());
 		return 0;
 	}

@@ -4,27 +4,39 @@
 // tensor cores with BF16 operands split in three terms (a*b ~ ah*bh + ah*bl +
 // al*bh, x = xh + xl, xl = bf16(x - xh)) and FP32 accumulators in TMEM:
 //
-//   2a  F1(x, ky)  = sum_y  E(x, y)  w32^(ky(y+8))     rows (s, x),  K = y
-//   2b  F(kx, ky)  = sum_x  F1(x,ky) w32^(kx(x+8))     rows (s, ky), K = x
-//   4a  Q(ky, fx)  = sum_kx P(kx,ky) w32^(fx kx)       rows (s, ky), K = kx  (P = |F|^2)
-//   4b  O(fx, fy)  = sum_ky Q(ky,fx) w32^(fy ky)       rows (s, fx), K = ky
-//   6a  T(fx, iy)  = sum_fy O'(fx,fy) Gy(iy, fy)       rows (s, fx), K = fy  (O' = O x conj(uplink) x ETF)
-//                                                       N = 32: Re iy in columns 0..15, Im in 16..31
-//   6b  I(ix, iy)  = Re sum_fx Gx(ix, fx) T(fx, iy)    FP32 warp reduction
+//   2a  F1(x, ky)  = sum_y  E(x, y)  w32^(ky(y+8))     rows (s, x),  K = y   A in TMEM
+//   2b  F(kx, ky)  = sum_x  F1(x,ky) w32^(kx(x+8))     rows (s, ky), K = x   A in smem, MN-major
+//   4a  Q(ky, fx)  = sum_kx P(kx,ky) w32^(fx kx)       rows (s, ky), K = kx  A in TMEM  (P = |F|^2)
+//   4b  O(fx, fy)  = sum_ky Q(ky,fx) w32^(fy ky)       rows (s, fx), K = ky  A in smem, MN-major
+//   6a  T(fx, iy)  = sum_fy O'(fx,fy) Gy(iy, fy)       rows (s, fx), K = fy  A in TMEM  (O' = O x conj(uplink) x ETF)
+//   6b  I(ix, iy)  = Re sum_fx T(fx,iy) Gx(ix, fx)     rows (s, iy), K = fx  A in smem, MN-major
 //
 // with w32 = exp(-2 pi i / 32) (FFTW's forward sign) and G = the inverse DFT
 // premultiplied by the separable bilinear pixel weights, so the inverse
 // transform and the pixel sampling of maos/wfsints.c:284-286 collapse into
-// 6a/6b.  A tile is 4 subapertures = 128 GEMM rows; warp w owns subaperture w
-// of the tile and TMEM lanes 32w..32w+31.  One elected thread issues the MMAs
-// and commits them to an mbarrier that every thread waits on (bounded wait:
-// on expiry the kernel records SHWFS_ETIMEOUT, frees its TMEM and returns).
+// 6a/6b.  Complex operands are real blocks: K = [re | im], N = [re | im].
 //
-// Shared memory per CTA: a 32 KB operand region (warp w's 8 KB slice holds its
-// 32 A-rows, and doubles as its FP32 transpose tile between stages) and the
-// 32 KB of constant B operands.  Operands use the K-major, no-swizzle
-// canonical layout: core matrices of 8 rows x 16 bytes, 128 bytes apart
-// along K (LBO) and 16 x 128 bytes apart along rows (SBO).
+// Each stage leaves its output in TMEM, one GEMM row per lane.  Where that row
+// is a row of the next A operand (field -> 2a, 2b -> 4a, 4b -> 6a) the lane
+// writes it back to TMEM with tcgen05.st; where it is a K-row of the next A
+// operand (2a -> 2b, 4a -> 4b, 6a -> 6b) the lane writes it to shared memory
+// in the MN-major layout.  No stage transposes through shared memory.  The 6b
+// rows (s, iy) with iy >= 8 read stale operand data and are never read back.
+//
+// A tile is 4 subapertures = 128 GEMM rows; warp w of a tile group owns
+// subaperture w and TMEM lanes 32w..32w+31.  A CTA holds two independent
+// tile groups (4 warps each) that share the constant B operands; each group
+// has its own TMEM columns (64 accumulator + 64 A-operand), its own 32 KB
+// MN-major operand buffer and its own mbarrier.  One thread per group issues
+// the MMAs, commits them to the group's mbarrier and waits on it with a 2 s
+// bound (on expiry the kernel records SHWFS_ETIMEOUT, frees its TMEM and
+// returns); the rest of the group waits at a named barrier.
+//
+// Operand layouts (SWIZZLE_NONE, core matrices of 8 rows x 16 bytes):
+//   K-major (B):  chunk (row r, k-chunk c) at ((r/8)*kc + c)*128 + (r%8)*16
+//   MN-major (A): chunk (m-chunk mg, K-row k) at (mg*nkg + k/8)*128 + (k%8)*16
+// LBO = 128 B is the stride along K, SBO the stride along M/N.  A TMEM A
+// operand holds K pairs per 32-bit column (even K in the low half).
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -36,22 +48,31 @@ namespace shwfs {
 constexpr int SHWFS_ETIMEOUT_CODE = -5;  // SHWFS_ETIMEOUT of shwfs_b200.h
 
 // ---- constants of the operand layouts ----
-constexpr int TC_A_BYTES = 128 * 16 * 16;  // 128 rows x 16 chunks x 16 B
-constexpr int TC_B1_BYTES = 64 * 8 * 16;   // N=64, K=32 (h|l: 8 chunks)
-constexpr int TC_B2_BYTES = 64 * 16 * 16;  // N=64, K=64 (h|l: 16 chunks)
-constexpr int TC_B3_BYTES = 32 * 16 * 16;  // N=32 (16 re + 16 im pixel rows), K=64
-constexpr int TC_B_BYTES = TC_B1_BYTES + TC_B2_BYTES + TC_B3_BYTES;
-constexpr int TC_SMEM_BYTES = TC_A_BYTES + TC_B_BYTES + 64;
-constexpr int TC_TMEM_COLS = 64;
+constexpr int TC_B1_BYTES = 64 * 8 * 16;   // N=64, K=32 (h|l: 8 chunks)   16-into-32 DFT
+constexpr int TC_B2_BYTES = 64 * 16 * 16;  // N=64, K=64 (h|l: 16 chunks)  32-point DFT
+constexpr int TC_B3_BYTES = 32 * 16 * 16;  // N=32 (16 re + 16 im pixel rows), K=64: Gy
+constexpr int TC_B4_BYTES = 16 * 16 * 16;  // N=16 (pixel columns), K=64: [Re Gx | -Im Gx]
+constexpr int TC_B_BYTES = TC_B1_BYTES + TC_B2_BYTES + TC_B3_BYTES + TC_B4_BYTES;
+constexpr int TC_A_BYTES = 16 * 16 * 128;  // one group's MN-major A: 16 m-chunks x 16 k-groups
+constexpr int TC_GROUPS = 2;               // tile groups per CTA
+constexpr int TC_THREADS = 128 * TC_GROUPS;
+constexpr int TC_PIX_BYTES = TC_THREADS / 32 * 64 * 4;  // 64 staged pixels per warp
+constexpr int TC_MISC_OFF = TC_B_BYTES + TC_GROUPS * TC_A_BYTES + TC_PIX_BYTES;
+constexpr int TC_SMEM_BYTES = TC_MISC_OFF + 64;
+constexpr int TC_TMEM_COLS = 128 * TC_GROUPS;  // per group: 64 accumulator + 64 A operand
+constexpr int TC_CTAS_PER_SM = 2;
 
-// byte offset of (row r, 16-byte chunk c) in an operand with kc chunks per row group
+// byte offset of (row r, 16-byte chunk c) in a K-major operand with kc chunks per row group
 __host__ __device__ constexpr uint32_t tc_off(int r, int c, int kc) {
 	return (uint32_t)(((r >> 3) * kc + c) * 128 + (r & 7) * 16);
 }
+// byte offset of (m-chunk mg, K-row k) in an MN-major operand with nkg k-groups
+__host__ __device__ constexpr uint32_t mn_off(int mg, int k, int nkg) {
+	return (uint32_t)((mg * nkg + (k >> 3)) * 128 + (k & 7) * 16);
+}
 
 struct TcTables {
-	const uint4* bmat;  // TC_B_BYTES of B1|B2|B3 images (bf16, canonical layout)
-	const float2* gx;   // pixpsax x 32 : Gx(ix, fx)
+	const uint4* bmat;  // TC_B_BYTES of B1|B2|B3|B4 images (bf16, canonical K-major layout)
 };
 
 // ---- PTX wrappers ----
@@ -70,16 +91,26 @@ __device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32
 	d |= (uint64_t)1 << 46;  // descriptor version for sm_100; SWIZZLE_NONE, base offset 0
 	return d;
 }
-// kind::f16 instruction descriptor: D=F32, A=B=BF16, both K-major, M=128
-__host__ __device__ constexpr uint32_t tc_idesc(int n) {
-	return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+// kind::f16 instruction descriptor: D=F32, A=B=BF16, B K-major, M=128; A
+// MN-major when a_mn (bit 15)
+__host__ __device__ constexpr uint32_t tc_idesc(int n, bool a_mn) {
+	return (1u << 4) | (1u << 7) | (1u << 10) | (a_mn ? (1u << 15) : 0u) | ((uint32_t)(n >> 3) << 17) |
+		   ((uint32_t)(128 >> 4) << 24);
 }
 
-__device__ __forceinline__ void tc_mma(uint32_t dtmem, uint64_t ad, uint64_t bd, uint32_t idesc, uint32_t acc) {
+// A from shared memory (descriptor)
+__device__ __forceinline__ void tc_mma_ss(uint32_t dtmem, uint64_t ad, uint64_t bd, uint32_t idesc, uint32_t acc) {
 	asm volatile(
 		"{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
 		"tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dtmem),
 		"l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+}
+// A from tensor memory
+__device__ __forceinline__ void tc_mma_ts(uint32_t dtmem, uint32_t atmem, uint64_t bd, uint32_t idesc, uint32_t acc) {
+	asm volatile(
+		"{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+		"tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}\n" ::"r"(dtmem),
+		"r"(atmem), "l"(bd), "r"(idesc), "r"(acc));
 }
 __device__ __forceinline__ void tc_commit(uint64_t* mbar) {
 	asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mbar))
@@ -88,6 +119,7 @@ __device__ __forceinline__ void tc_commit(uint64_t* mbar) {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void group_sync(int id) { asm volatile("barrier.sync %0, 128;" ::"r"(id) : "memory"); }
 
 __device__ __forceinline__ void mbar_init(uint64_t* m, uint32_t count) {
 	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(m)), "r"(count) : "memory");
@@ -102,7 +134,7 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* m, uint32_t parity) {
 	return ok != 0;
 }
 
-// 16 consecutive TMEM columns of this warp's 32 lanes -> 16 registers per thread
+// 16 / 8 consecutive TMEM columns of this warp's 32 lanes <-> registers
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 	uint32_t r[16];
 	asm volatile(
@@ -113,76 +145,115 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 #pragma unroll
 	for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
+	uint32_t r[8];
+	asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+				 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+				 : "r"(taddr));
+#pragma unroll
+	for (int i = 0; i < 8; i++) v[i] = __uint_as_float(r[i]);
+}
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16]) {
+	asm volatile(
+		"tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
+			taddr),
+		"r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]),
+		"r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+		: "memory");
+}
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&r)[8]) {
+	asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr), "r"(r[0]),
+				 "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+				 : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
-// ---- operand writers ----
-// bf16 hi/lo split of 8 floats packed as two 16-byte chunks
+// ---- operand split ----
+// (a, b) -> packed bf16 pair hi = (bf16(a), bf16(b)) and lo = bf16 of the
+// remainders; the first element sits in the low half.
+__device__ __forceinline__ void split_pair(float a, float b, uint32_t& hi, uint32_t& lo) {
+	const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+	const uint32_t hu = *reinterpret_cast<const uint32_t*>(&h);
+	const float ha = __uint_as_float(hu << 16), hb = __uint_as_float(hu & 0xffff0000u);
+	const __nv_bfloat162 l = __floats2bfloat162_rn(a - ha, b - hb);
+	hi = hu;
+	lo = *reinterpret_cast<const uint32_t*>(&l);
+}
+// 8 floats -> one 16-byte hi chunk and one lo chunk
 __device__ __forceinline__ void split8(const float* x, uint4& hi, uint4& lo) {
-	uint32_t h[4], l[4];
-#pragma unroll
-	for (int i = 0; i < 4; i++) {
-		const __nv_bfloat16 h0 = __float2bfloat16_rn(x[2 * i]), h1 = __float2bfloat16_rn(x[2 * i + 1]);
-		const __nv_bfloat16 l0 = __float2bfloat16_rn(x[2 * i] - __bfloat162float(h0));
-		const __nv_bfloat16 l1 = __float2bfloat16_rn(x[2 * i + 1] - __bfloat162float(h1));
-		h[i] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
-		l[i] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
-	}
-	hi = make_uint4(h[0], h[1], h[2], h[3]);
-	lo = make_uint4(l[0], l[1], l[2], l[3]);
+	split_pair(x[0], x[1], hi.x, lo.x);
+	split_pair(x[2], x[3], hi.y, lo.y);
+	split_pair(x[4], x[5], hi.z, lo.z);
+	split_pair(x[6], x[7], hi.w, lo.w);
 }
-// Writes row r of the A operand from K real values x[0..K): hi chunks 0..K/8-1,
-// lo chunks 8..8+K/8-1 (K = 32 or 64).
-template <int K>
-__device__ __forceinline__ void write_arow(unsigned char* abuf, int r, const float* x) {
-#pragma unroll
-	for (int c = 0; c < K / 8; c++) {
-		uint4 hi, lo;
-		split8(x + 8 * c, hi, lo);
-		*reinterpret_cast<uint4*>(abuf + tc_off(r, c, 16)) = hi;
-		*reinterpret_cast<uint4*>(abuf + tc_off(r, 8 + c, 16)) = lo;
-	}
+__device__ __forceinline__ void sts128(unsigned char* base, uint32_t off, const uint4& v) {
+	*reinterpret_cast<uint4*>(base + off) = v;
 }
 
-// Issues the 3-term split product over nks K-steps (16 real K each):
-// D = sum_j Ah_j Bh_j + Ah_j Bl_j + Al_j Bh_j.  bbase: B image, bkc: its
-// chunks per row group, blo: chunk index of its lo half.
-__device__ __forceinline__ void tc_gemm(uint32_t dtmem, uint32_t abase, uint32_t bbase, int bkc, int blo, int nks,
-	uint32_t idesc) {
-	const uint32_t asbo = 16 * 128, bsbo = (uint32_t)bkc * 128;
-	uint32_t acc = 0;
+// sin(pi t), cos(pi t): t reduced exactly to [-1, 1] (t - 2 rint(t/2) is
+// exact in FP32), then the hardware sine/cosine, whose absolute error on
+// [-pi, pi] (about 4e-7) is far below the BF16x3 products' (about 1e-5).
+__device__ __forceinline__ void sincospi_fast(float t, float& s, float& c) {
+	const float r = fmaf(-2.f, rintf(0.5f * t), t);
+	__sincosf(3.14159265358979f * r, &s, &c);
+}
+
+// ---- GEMM issue (one thread) ----
+// D = sum_j Ah_j Bh_j + Ah_j Bl_j + Al_j Bh_j over nks K-steps of 16.
+// B: K-major image at bbase with bkc chunks per row group, lo half at chunk blo.
+__device__ __forceinline__ uint64_t bdesc_hi(uint32_t bbase, int bkc, int j) {
+	return tc_desc(bbase + (uint32_t)(2 * j) * 128, 128, (uint32_t)bkc * 128);
+}
+__device__ __forceinline__ uint64_t bdesc_lo(uint32_t bbase, int bkc, int blo, int j) {
+	return tc_desc(bbase + (uint32_t)(blo + 2 * j) * 128, 128, (uint32_t)bkc * 128);
+}
+// A in TMEM: hi K pairs in columns [acol, acol+alo), lo in [acol+alo, ...)
+__device__ __forceinline__ void tc_gemm_ts(uint32_t dt, uint32_t acol, int alo, uint32_t bbase, int bkc, int blo,
+	int nks, uint32_t idesc) {
 	for (int j = 0; j < nks; j++) {
-		const uint64_t ah = tc_desc(abase + (2 * j) * 128, 128, asbo);
-		const uint64_t al = tc_desc(abase + (8 + 2 * j) * 128, 128, asbo);
-		const uint64_t bh = tc_desc(bbase + (2 * j) * 128, 128, bsbo);
-		const uint64_t bl = tc_desc(bbase + (blo + 2 * j) * 128, 128, bsbo);
-		tc_mma(dtmem, ah, bh, idesc, acc);
-		acc = 1;
-		tc_mma(dtmem, ah, bl, idesc, 1);
-		tc_mma(dtmem, al, bh, idesc, 1);
+		const uint32_t ah = acol + 8 * j, al = acol + alo + 8 * j;
+		const uint64_t bh = bdesc_hi(bbase, bkc, j), bl = bdesc_lo(bbase, bkc, blo, j);
+		tc_mma_ts(dt, ah, bh, idesc, j > 0 ? 1u : 0u);
+		tc_mma_ts(dt, ah, bl, idesc, 1u);
+		tc_mma_ts(dt, al, bh, idesc, 1u);
 	}
 }
-
-// FP32 transpose tile of one warp: 32 x 32 float2 with an XOR swizzle so that
-// both row and column accesses are bank-conflict free.
-__device__ __forceinline__ float2* tile_at(float2* t, int row, int col) { return t + row * 32 + (col ^ row); }
+// A in shared memory, MN-major with nkg k-groups: hi K-rows from k-group 0,
+// lo K-rows from k-group nkg/2
+__device__ __forceinline__ void tc_gemm_ss(uint32_t dt, uint32_t abase, int nkg, uint32_t bbase, int bkc, int blo,
+	int nks, uint32_t idesc) {
+	const uint32_t sbo = (uint32_t)nkg * 128;
+	for (int j = 0; j < nks; j++) {
+		const uint64_t ah = tc_desc(abase + (uint32_t)(2 * j) * 128, 128, sbo);
+		const uint64_t al = tc_desc(abase + (uint32_t)(nkg / 2 + 2 * j) * 128, 128, sbo);
+		const uint64_t bh = bdesc_hi(bbase, bkc, j), bl = bdesc_lo(bbase, bkc, blo, j);
+		tc_mma_ss(dt, ah, bh, idesc, j > 0 ? 1u : 0u);
+		tc_mma_ss(dt, ah, bl, idesc, 1u);
+		tc_mma_ss(dt, al, bh, idesc, 1u);
+	}
+}
 
 // ---------------------------------------------------------------------------
 template <int NPQ>
-__global__ void __launch_bounds__(128) ints_tc_kernel(PowfsDev P, const WfsDev* __restrict__ wfs, int nw, int nitem,
-	TcTables T, int* errflag) {
+__global__ void __launch_bounds__(TC_THREADS, TC_CTAS_PER_SM) ints_tc_kernel(PowfsDev P,
+	const WfsDev* __restrict__ wfs, int nw, int nitem, TcTables T, int* errflag) {
 	extern __shared__ __align__(128) unsigned char smem[];
-	unsigned char* abuf = smem;                        // 32 KB: A operands / transpose tiles
-	unsigned char* bbuf = smem + TC_A_BYTES;           // 28 KB: B1 | B2 | B3
-	uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + TC_A_BYTES + TC_B_BYTES);
-	uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + TC_A_BYTES + TC_B_BYTES + 8);
-	int* bail = reinterpret_cast<int*>(smem + TC_A_BYTES + TC_B_BYTES + 16);
 	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+	const int g = warp >> 2, wq = warp & 3;  // tile group, warp within the group
+	unsigned char* bbuf = smem;               // B1 | B2 | B3 | B4
+	unsigned char* abuf = smem + TC_B_BYTES + g * TC_A_BYTES;
+	float* pixbuf = reinterpret_cast<float*>(smem + TC_B_BYTES + TC_GROUPS * TC_A_BYTES) + warp * 64;
+	uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + TC_MISC_OFF) + g;
+	uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + TC_MISC_OFF + 16);
+	int* bail = reinterpret_cast<int*>(smem + TC_MISC_OFF + 32) + g;
 
-	// constant B operands into shared memory
-	for (int i = tid; i < TC_B_BYTES / 16; i += 128) reinterpret_cast<uint4*>(bbuf)[i] = T.bmat[i];
+	for (int i = tid; i < TC_B_BYTES / 16; i += TC_THREADS) reinterpret_cast<uint4*>(bbuf)[i] = T.bmat[i];
 	if (tid == 0) {
-		mbar_init(mbar, 1);
-		*bail = 0;
+		for (int k = 0; k < TC_GROUPS; k++) {
+			mbar_init(reinterpret_cast<uint64_t*>(smem + TC_MISC_OFF) + k, 1);
+			reinterpret_cast<int*>(smem + TC_MISC_OFF + 32)[k] = 0;
+		}
 		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 	}
 	if (warp == 0) {
@@ -195,228 +266,257 @@ __global__ void __launch_bounds__(128) ints_tc_kernel(PowfsDev P, const WfsDev* 
 	__syncthreads();
 	tc_fence_after();
 	const uint32_t tmem = *tslot;
-	const uint32_t tlane = tmem + ((uint32_t)(32 * warp) << 16);  // this warp's lanes
+	const uint32_t dcol = tmem + 128 * g;  // accumulator columns of this group (lane 0)
+	const uint32_t acol = dcol + 64;       // A-operand columns of this group
+	const uint32_t tl = (uint32_t)(32 * wq) << 16;  // this warp's lane quarter
 	const uint32_t a_s = smem_u32(abuf), b1_s = smem_u32(bbuf), b2_s = b1_s + TC_B1_BYTES,
-				   b3_s = b2_s + TC_B2_BYTES;
-	unsigned char* myslice = abuf + warp * 8192;  // rows 32*warp.. of the A operand
-	float2* tile = reinterpret_cast<float2*>(myslice);
+				   b3_s = b2_s + TC_B2_BYTES, b4_s = b3_s + TC_B3_BYTES;
+	const bool issuer = (tid & 127) == 0;
+	const int bar_id = 1 + g;
 	uint32_t phase = 0;
 
-	// one MMA stage: operands written -> issue -> wait
-	auto run_stage = [&](uint32_t bbase, int bkc, int blo, int nks, int n) -> bool {
-		fence_async_smem();
+	// operands written (tcgen05.st waited / generic smem fenced by the caller)
+	// -> one thread issues and waits -> the group proceeds with the result
+	auto finish_stage = [&](auto issue) -> bool {
 		tc_fence_before();
-		__syncthreads();
-		if (tid == 0) {
+		group_sync(bar_id);
+		if (issuer) {
 			tc_fence_after();
-			tc_gemm(tmem, a_s, bbase, bkc, blo, nks, tc_idesc(n));
+			issue();
 			tc_commit(mbar);
-		}
-		// bounded wait: 2 s of wall time, then record the expiry and leave
-		const uint64_t t0 = globaltimer_ns();
-		while (!mbar_try_wait(mbar, phase)) {
-			if (globaltimer_ns() - t0 > 2000000000ull) {
-				atomicExch(errflag, SHWFS_ETIMEOUT_CODE);
-				*bail = 1;
-				break;
+			const uint64_t t0 = globaltimer_ns();
+			while (!mbar_try_wait(mbar, phase)) {
+				if (globaltimer_ns() - t0 > 2000000000ull) {
+					atomicExch(errflag, SHWFS_ETIMEOUT_CODE);
+					*bail = 1;
+					break;
+				}
 			}
 		}
 		phase ^= 1u;
+		group_sync(bar_id);
 		tc_fence_after();
 		return *bail == 0;
 	};
 
 	const int ntile = (nitem + 3) / 4;
-	for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
-		const int item = 4 * t + warp;
+	for (int t = TC_GROUPS * blockIdx.x + g; t < ntile; t += TC_GROUPS * gridDim.x) {
+		const int item = 4 * t + wq;
 		const bool valid = item < nitem;
 		const int isa = valid ? item / nw : 0;
 		const WfsDev W = wfs[valid ? item % nw : 0];
-		// ---- (b) field: row x = lane holds E(x-8, y) for x in [8,24), else 0
+		// ---- (b) field -> A(2a) in TMEM: row x = lane holds E(x-8, y), zero outside [8,24)
 		{
-			const float* opd = W.opd + (size_t)isa * 256;
-			const float* amp = W.amp + (size_t)isa * 256;
 			const int xp = lane - 8;
 			const bool live = valid && xp >= 0 && xp < 16;
+			const size_t base = (size_t)isa * 256 + (live ? xp : 0);
 			float o[16], a[16];
 			float s = 0.f;
 #pragma unroll
 			for (int y = 0; y < 16; y++) {
-				o[y] = live ? __ldg(opd + y * 16 + xp) : 0.f;
-				a[y] = live ? __ldg(amp + y * 16 + xp) : 0.f;
+				o[y] = live ? __ldg(W.opd + base + y * 16) : 0.f;
+				a[y] = live ? __ldg(W.amp + base + y * 16) : 0.f;
 				s += o[y];
 			}
 #pragma unroll
 			for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
 			const float piston = s * (1.f / 256.f);
-			float row[32];
+			uint32_t hw[16], lw[16];
 #pragma unroll
-			for (int y = 0; y < 16; y++) {
-				float sn, cs;
-				sincospif(P.twoinvwvl * (o[y] - piston), &sn, &cs);
-				row[y] = live ? a[y] * cs : 0.f;
-				row[16 + y] = live ? a[y] * sn : 0.f;
+			for (int y = 0; y < 16; y += 2) {
+				float s0, c0, s1, c1;
+				sincospi_fast(P.twoinvwvl * (o[y] - piston), s0, c0);
+				sincospi_fast(P.twoinvwvl * (o[y + 1] - piston), s1, c1);
+				split_pair(a[y] * c0, a[y + 1] * c1, hw[y / 2], lw[y / 2]);          // re: K = y
+				split_pair(a[y] * s0, a[y + 1] * s1, hw[8 + y / 2], lw[8 + y / 2]);  // im: K = 16 + y
 			}
-			write_arow<32>(abuf, 32 * warp + lane, row);
+			tmem_st16(acol + tl, hw);
+			tmem_st16(acol + tl + 16, lw);
+			tmem_wait_st();
 		}
-		if (!run_stage(b1_s, 8, 4, 2, 64)) break;  // 2a
-		// ---- 2a out (row x) -> transpose -> 2b in (row ky), K = x-8
+		if (!finish_stage([&] { tc_gemm_ts(dcol, acol, 16, b1_s, 8, 4, 2, tc_idesc(64, false)); })) break;  // 2a
+		// ---- 2a out: row x holds F1(x-8, ky) -> K-rows x-8 (re), 16+x-8 (im) of A(2b), M = (s, ky)
 		{
-			float v[16];
+			const int xp = lane - 8;
+			const bool live = xp >= 0 && xp < 16;
 #pragma unroll
-			for (int q = 0; q < 4; q++) {  // columns 16q..16q+15: re ky 0..31 then im
-				tmem_ld16(tlane + 16 * q, v);
+			for (int h = 0; h < 2; h++) {
+				float re[16], im[16];
+				tmem_ld16(dcol + tl + 16 * h, re);
+				tmem_ld16(dcol + tl + 32 + 16 * h, im);
 				tmem_wait_ld();
-				if (lane >= 8 && lane < 24) {
 #pragma unroll
-					for (int i = 0; i < 16; i++) {
-						const int c = 16 * q + i, ky = c & 31;
-						float2* e = tile_at(tile, ky, lane - 8);
-						if (c < 32) e->x = v[i];
-						else e->y = v[i];
+				for (int c = 0; c < 2; c++) {
+					const int mg = 4 * wq + 2 * h + c;
+					uint4 rh, rl, ih, il;
+					split8(re + 8 * c, rh, rl);
+					split8(im + 8 * c, ih, il);
+					if (live) {
+						sts128(abuf, mn_off(mg, xp, 8), rh);
+						sts128(abuf, mn_off(mg, 16 + xp, 8), ih);
+						sts128(abuf, mn_off(mg, 32 + xp, 8), rl);
+						sts128(abuf, mn_off(mg, 48 + xp, 8), il);
 					}
 				}
 			}
-			__syncwarp();
-			float row[32];
-#pragma unroll
-			for (int xp = 0; xp < 16; xp++) {
-				const float2 e = *tile_at(tile, lane, xp);
-				row[xp] = e.x;
-				row[16 + xp] = e.y;
-			}
-			__syncwarp();
-			write_arow<32>(abuf, 32 * warp + lane, row);
+			fence_async_smem();
 		}
-		if (!run_stage(b1_s, 8, 4, 2, 64)) break;  // 2b
-		// ---- 2b out (row ky: F(kx, ky)) -> |F|^2 -> 4a in (row ky), K = kx
+		if (!finish_stage([&] { tc_gemm_ss(dcol, a_s, 8, b1_s, 8, 4, 2, tc_idesc(64, true)); })) break;  // 2b
+		// ---- 2b out: row ky holds F(kx, ky) -> P = |F|^2 -> A(4a) in TMEM, K = kx
 		{
-			float re[16], im[16], row[32];
+			uint32_t hw[16], lw[16];
 #pragma unroll
 			for (int h = 0; h < 2; h++) {
-				tmem_ld16(tlane + 16 * h, re);
-				tmem_ld16(tlane + 32 + 16 * h, im);
+				float re[16], im[16];
+				tmem_ld16(dcol + tl + 16 * h, re);
+				tmem_ld16(dcol + tl + 32 + 16 * h, im);
 				tmem_wait_ld();
 #pragma unroll
-				for (int i = 0; i < 16; i++) row[16 * h + i] = re[i] * re[i] + im[i] * im[i];
-			}
-			write_arow<32>(abuf, 32 * warp + lane, row);
-		}
-		if (!run_stage(b2_s, 16, 8, 2, 64)) break;  // 4a (real K: first half of B2)
-		// ---- 4a out (row ky: Q(ky, fx)) -> transpose -> 4b in (row fx), K = ky (complex)
-		{
-			float v[16];
-#pragma unroll
-			for (int q = 0; q < 4; q++) {
-				tmem_ld16(tlane + 16 * q, v);
-				tmem_wait_ld();
-#pragma unroll
-				for (int i = 0; i < 16; i++) {
-					const int c = 16 * q + i, fx = c & 31;
-					float2* e = tile_at(tile, fx, lane);
-					if (c < 32) e->x = v[i];
-					else e->y = v[i];
+				for (int i = 0; i < 16; i += 2) {
+					const float p0 = fmaf(re[i], re[i], im[i] * im[i]);
+					const float p1 = fmaf(re[i + 1], re[i + 1], im[i + 1] * im[i + 1]);
+					split_pair(p0, p1, hw[8 * h + i / 2], lw[8 * h + i / 2]);
 				}
 			}
-			__syncwarp();
-			float row[64];
-#pragma unroll
-			for (int ky = 0; ky < 32; ky++) {
-				const float2 e = *tile_at(tile, lane, ky);
-				row[ky] = e.x;
-				row[32 + ky] = e.y;
-			}
-			__syncwarp();
-			write_arow<64>(abuf, 32 * warp + lane, row);
+			tmem_st16(acol + tl, hw);
+			tmem_st16(acol + tl + 16, lw);
+			tmem_wait_st();
 		}
-		if (!run_stage(b2_s, 16, 8, 4, 64)) break;  // 4b
-		// ---- 4b out (row fx: OTF(fx, fy)) x conj(uplink) x ETF -> 6a in (row fx), K = fy
+		if (!finish_stage([&] { tc_gemm_ts(dcol, acol, 16, b2_s, 16, 8, 2, tc_idesc(64, false)); })) break;  // 4a
+		// ---- 4a out: row ky holds Q(ky, fx) -> K-rows ky (re), 32+ky (im) of A(4b), M = (s, fx)
 		{
-			float row[64];
-			float re[16], im[16];
 #pragma unroll
 			for (int h = 0; h < 2; h++) {
-				tmem_ld16(tlane + 16 * h, re);
-				tmem_ld16(tlane + 32 + 16 * h, im);
+				float re[16], im[16];
+				tmem_ld16(dcol + tl + 16 * h, re);
+				tmem_ld16(dcol + tl + 32 + 16 * h, im);
 				tmem_wait_ld();
 #pragma unroll
-				for (int i = 0; i < 16; i++) {
-					row[16 * h + i] = re[i];
-					row[32 + 16 * h + i] = im[i];
+				for (int c = 0; c < 2; c++) {
+					const int mg = 4 * wq + 2 * h + c;
+					uint4 rh, rl, ih, il;
+					split8(re + 8 * c, rh, rl);
+					split8(im + 8 * c, ih, il);
+					sts128(abuf, mn_off(mg, lane, 16), rh);
+					sts128(abuf, mn_off(mg, 32 + lane, 16), ih);
+					sts128(abuf, mn_off(mg, 64 + lane, 16), rl);
+					sts128(abuf, mn_off(mg, 96 + lane, 16), il);
 				}
 			}
+			fence_async_smem();
+		}
+		if (!finish_stage([&] { tc_gemm_ss(dcol, a_s, 16, b2_s, 16, 8, 4, tc_idesc(64, true)); })) break;  // 4b
+		// ---- 4b out: row fx holds OTF(fx, fy) x conj(uplink) x ETF -> A(6a) in TMEM, K = fy
+		{
 			const int fx = lane;
-			if (valid) {
-				if (W.lotfT) {
-					const float2* l = W.lotfT + 32 * fx;
 #pragma unroll
-					for (int fy = 0; fy < 32; fy++) {
-						const float2 c = __ldg(l + fy);
-						const float a = row[fy], b = row[32 + fy];
-						row[fy] = fmaf(a, c.x, b * c.y);
-						row[32 + fy] = fmaf(b, c.x, -a * c.y);
-					}
-				}
-				if (P.etfT1) {
-					const float2* e1 = P.etfT1 + (size_t)isa * 1024 + 32 * fx;
+			for (int h = 0; h < 2; h++) {
+				float re[16], im[16];
+				tmem_ld16(dcol + tl + 16 * h, re);
+				tmem_ld16(dcol + tl + 32 + 16 * h, im);
+				tmem_wait_ld();
+				if (valid) {
+					if (W.lotfT) {
+						const float4* l = reinterpret_cast<const float4*>(W.lotfT + 32 * fx + 16 * h);
 #pragma unroll
-					for (int fy = 0; fy < 32; fy++) {
-						float2 c = __ldg(e1 + fy);
-						if (P.etfT2) {
-							const float2 c2 = __ldg(P.etfT2 + (size_t)isa * 1024 + 32 * fx + fy);
-							c = make_float2(c.x * P.etfwt1 + c2.x * P.etfwt2, c.y * P.etfwt1 + c2.y * P.etfwt2);
+						for (int i = 0; i < 16; i += 2) {
+							const float4 c = __ldg(l + i / 2);
+							float a = re[i], b = im[i];
+							re[i] = fmaf(a, c.x, b * c.y);
+							im[i] = fmaf(b, c.x, -a * c.y);
+							a = re[i + 1];
+							b = im[i + 1];
+							re[i + 1] = fmaf(a, c.z, b * c.w);
+							im[i + 1] = fmaf(b, c.z, -a * c.w);
 						}
-						const float a = row[fy], b = row[32 + fy];
-						row[fy] = fmaf(a, c.x, -b * c.y);
-						row[32 + fy] = fmaf(a, c.y, b * c.x);
 					}
-				} else if (P.nominalT) {
-					const float* nm = P.nominalT + (P.nominal_per_sa ? (size_t)isa * 1024 : 0) + 32 * fx;
+					if (P.etfT1) {
+						const float4* e1 =
+							reinterpret_cast<const float4*>(P.etfT1 + (size_t)isa * 1024 + 32 * fx + 16 * h);
+						const float4* e2 =
+							P.etfT2 ? reinterpret_cast<const float4*>(P.etfT2 + (size_t)isa * 1024 + 32 * fx + 16 * h)
+									: nullptr;
 #pragma unroll
-					for (int fy = 0; fy < 32; fy++) {
-						const float d = __ldg(nm + fy);
-						row[fy] *= d;
-						row[32 + fy] *= d;
+						for (int i = 0; i < 16; i += 2) {
+							float4 c = __ldg(e1 + i / 2);
+							if (e2) {
+								const float4 c2 = __ldg(e2 + i / 2);
+								c = make_float4(c.x * P.etfwt1 + c2.x * P.etfwt2, c.y * P.etfwt1 + c2.y * P.etfwt2,
+									c.z * P.etfwt1 + c2.z * P.etfwt2, c.w * P.etfwt1 + c2.w * P.etfwt2);
+							}
+							float a = re[i], b = im[i];
+							re[i] = fmaf(a, c.x, -b * c.y);
+							im[i] = fmaf(a, c.y, b * c.x);
+							a = re[i + 1];
+							b = im[i + 1];
+							re[i + 1] = fmaf(a, c.z, -b * c.w);
+							im[i + 1] = fmaf(a, c.w, b * c.z);
+						}
+					} else if (P.nominalT) {
+						const float4* nm = reinterpret_cast<const float4*>(
+							P.nominalT + (P.nominal_per_sa ? (size_t)isa * 1024 : 0) + 32 * fx + 16 * h);
+#pragma unroll
+						for (int i = 0; i < 16; i += 4) {
+							const float4 d = __ldg(nm + i / 4);
+							re[i] *= d.x;
+							im[i] *= d.x;
+							re[i + 1] *= d.y;
+							im[i + 1] *= d.y;
+							re[i + 2] *= d.z;
+							im[i + 2] *= d.z;
+							re[i + 3] *= d.w;
+							im[i + 3] *= d.w;
+						}
 					}
 				}
+				uint32_t rh[8], rl[8], ih[8], il[8];
+#pragma unroll
+				for (int i = 0; i < 16; i += 2) {
+					split_pair(re[i], re[i + 1], rh[i / 2], rl[i / 2]);
+					split_pair(im[i], im[i + 1], ih[i / 2], il[i / 2]);
+				}
+				tmem_st8(acol + tl + 8 * h, rh);       // re fy: K 0..31  -> hi columns 0..15
+				tmem_st8(acol + tl + 16 + 8 * h, ih);  // im fy: K 32..63 -> hi columns 16..31
+				tmem_st8(acol + tl + 32 + 8 * h, rl);  // lo columns 32..63
+				tmem_st8(acol + tl + 48 + 8 * h, il);
 			}
-			write_arow<64>(abuf, 32 * warp + lane, row);
+			tmem_wait_st();
 		}
-		if (!run_stage(b3_s, 16, 8, 4, 32)) break;  // 6a
-		// ---- 6a out (row fx: T(fx, iy)) -> 6b: I(ix,iy) = Re sum_fx Gx(ix,fx) T(fx,iy)
+		if (!finish_stage([&] { tc_gemm_ts(dcol, acol, 32, b3_s, 16, 8, 4, tc_idesc(32, false)); })) break;  // 6a
+		// ---- 6a out: row fx holds T(fx, iy) -> K-rows fx (re), 32+fx (im) of A(6b), M = (s, iy < 8)
+		{
+			float re[8], im[8];
+			tmem_ld8(dcol + tl, re);
+			tmem_ld8(dcol + tl + 16, im);
+			tmem_wait_ld();
+			uint4 rh, rl, ih, il;
+			split8(re, rh, rl);
+			split8(im, ih, il);
+			const int mg = 4 * wq;
+			sts128(abuf, mn_off(mg, lane, 16), rh);
+			sts128(abuf, mn_off(mg, 32 + lane, 16), ih);
+			sts128(abuf, mn_off(mg, 64 + lane, 16), rl);
+			sts128(abuf, mn_off(mg, 96 + lane, 16), il);
+			fence_async_smem();
+		}
+		if (!finish_stage([&] { tc_gemm_ss(dcol, a_s, 16, b4_s, 16, 8, 4, tc_idesc(16, true)); })) break;  // 6b
+		// ---- 6b out: row iy (lanes 0..7) holds I(ix, iy) -> pixels of this warp's subaperture
 		float pix[NPQ];
 		{
-			float v[32];  // cols 0..15 re iy, 16..31 im iy
-			{
-				float a[16], b[16];
-				tmem_ld16(tlane, a);
-				tmem_ld16(tlane + 16, b);
-				tmem_wait_ld();
-#pragma unroll
-				for (int i = 0; i < 16; i++) {
-					v[i] = a[i];
-					v[16 + i] = b[i];
-				}
-			}
+			float v[8];
+			tmem_ld8(dcol + tl, v);
+			tmem_wait_ld();
 			const int npx = P.pixpsax, npy = P.pixpsay, npix = P.npix;
-			float* red = reinterpret_cast<float*>(myslice);  // [32 lanes][npix] partial sums
-#pragma unroll 1
-			for (int ix = 0; ix < npx; ix++) {
-				const float2 g = __ldg(T.gx + ix * 32 + lane);
+			if (lane < npy) {
 #pragma unroll
-				for (int iy = 0; iy < 16; iy++) {
-					if (iy < npy) red[lane * npix + ix + iy * npx] = fmaf(g.x, v[iy], -g.y * v[16 + iy]);
-				}
+				for (int ix = 0; ix < 8; ix++)
+					if (ix < npx) pixbuf[lane * npx + ix] = v[ix] * W.alpha;
 			}
 			__syncwarp();
 #pragma unroll
 			for (int q = 0; q < NPQ; q++) {
 				const int p = lane + 32 * q;
-				float sum = 0.f;
-				if (p < npix) {
-					for (int f = 0; f < 32; f++) sum += red[f * npix + p];
-				}
-				pix[q] = p < npix ? sum * W.alpha : 0.f;
+				pix[q] = p < npix ? pixbuf[p] : 0.f;
 			}
 			__syncwarp();
 		}
