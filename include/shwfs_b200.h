@@ -175,6 +175,16 @@ int shwfs_ints_grad_dev(shwfs_ctx* ctx, int iwfs, int isim, const float* opd, co
 	float* ints, float* grad, int add_noise);
 /* (e) alone: gradients (device, 2*nsa) from pixel intensities (device, nsa*npix). */
 int shwfs_grad_dev(shwfs_ctx* ctx, int iwfs, const float* ints, float* grad);
+/* Photon and read noise added in place to n pixel intensities on the device:
+   the rule of addnoise (lib/libmisc.c:31-55), with the optional per-pixel
+   arrays bkgrnd2, bkgrnd2c and qe (device, n FP32, or NULL) and excess < 1
+   taken as 1.  The draws are those of the frame kernels (Poisson by
+   inversion below a mean of 10, transformed rejection up to 200, the
+   reference's Gaussian rule above), from the counter (seed, pixel index,
+   stream, frame), so the result depends on nothing else.  n < 2^32. */
+int shwfs_addnoise_dev(shwfs_ctx* ctx, float* ints, long n, const float* bkgrnd2, const float* bkgrnd2c,
+	const float* qe, double bkgrnd, double bkgrndc, double rne, double excess, uint64_t seed, uint32_t stream,
+	uint32_t frame);
 /* ---- stage timing: CUDA events around every launch on the context stream,
         as the reference's ctoc instrumentation (cuda/math/common.h:233-267) ---- */
 #define SHWFS_STAGE_RAYTRACE 0 /* (a) ray trace into the subaperture OPD */

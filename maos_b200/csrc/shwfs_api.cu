@@ -988,6 +988,22 @@ int shwfs_grad_dev(shwfs_ctx* ctx, int iwfs, const float* ints, float* grad) {
 	return 0;
 }
 
+int shwfs_addnoise_dev(shwfs_ctx* ctx, float* ints, long n, const float* bkgrnd2, const float* bkgrnd2c,
+	const float* qe, double bkgrnd, double bkgrndc, double rne, double excess, uint64_t seed, uint32_t stream,
+	uint32_t frame) {
+	if (!ctx || n < 0 || (n > 0 && !ints) || n > 0xffffffffL)
+		return ctx ? fail(ctx, SHWFS_EINVAL, "addnoise: bad arguments") : SHWFS_EINVAL;
+	int r = set_device(ctx);
+	if (r) return r;
+	if (n == 0) return 0;
+	if (excess < 1) excess = 1;
+	const long nblk = std::min((n + 255) / 256, (long)tc_sm_count(ctx) * 8);
+	addnoise_kernel<<<(int)nblk, 256, 0, ctx->stream>>>(ints, n, bkgrnd2, bkgrnd2c, qe, (float)bkgrnd,
+		(float)bkgrndc, (float)rne, (float)excess, seed, stream, frame);
+	CK(cudaGetLastError());
+	return 0;
+}
+
 int shwfs_frame_queue(shwfs_ctx* ctx, int isim, int iwfs0, int iwfs1) {
 	if (!ctx || iwfs0 < 0 || iwfs1 > (int)ctx->wfs.size() || iwfs0 >= iwfs1)
 		return ctx ? fail(ctx, SHWFS_EINVAL, "frame_queue: bad WFS range") : SHWFS_EINVAL;

@@ -61,50 +61,68 @@ struct PixelRng {
 		return v;
 	}
 	__device__ __forceinline__ float next() { return u01(bits()); }
-	// standard normal by Box-Muller
+	// standard normal by Box-Muller: r cos(theta) with theta = pi (2 u2 - 1)
+	// uniform on [-pi, pi), the range where the hardware cosine is accurate
 	__device__ __forceinline__ float normal() {
-		float u1 = u01_nz(bits()), u2 = next();
-		float r = sqrtf(-2.f * logf(u1));
-		float s, c;
-		sincospif(2.f * u2, &s, &c);
-		return r * c;
+		const float u1 = u01_nz(bits()), u2 = next();
+		const float r = sqrtf(-2.f * __logf(u1));
+		return r * __cosf(3.14159265358979f * fmaf(2.f, u2, -1.f));
 	}
 };
 
-// Poisson draw.  As the reference (math/random.c:186-209) it uses a Gaussian
-// approximation above a mean of 200 and otherwise splits the mean into chunks
-// of at most 12 whose counts add up; each chunk is drawn exactly by inversion
-// of its cumulative distribution (one uniform per chunk) instead of the
-// reference's product of uniforms, which needs about mean+1 uniforms.  Both
-// give Poisson variates; the inversion is accumulated in FP64 so that the
-// computed distribution reaches 1 - 1e-15 > the largest uniform 1 - 2^-24.
-struct InvTable {
-	double v[81];
-	__host__ __device__ constexpr InvTable() : v() {
-		for (int k = 1; k <= 80; k++) v[k] = 1.0 / k;
+// Poisson draw of mean xm >= 0.  As the reference (math/random.c:186-209) it
+// uses a Gaussian approximation above a mean of 200; below it draws exact
+// Poisson variates by another method than the reference's product of
+// uniforms (about mean+1 uniforms per draw):
+//  - mean < 10: inversion, the smallest k with u < F(k), tested as
+//    u e^xm < sum_{j<=k} xm^j / j! so that no small exponential is formed; the
+//    walk stops where the next term no longer changes the FP32 sum, beyond
+//    which the tail holds less than about 1e-7 of the mass;
+//  - 10 <= mean <= 200: transformed rejection with squeeze (W. Hormann, "The
+//    transformed rejection method for generating Poisson random variables",
+//    Insurance: Mathematics and Economics 12 (1993) 39-45, algorithm PTRS),
+//    about 1.1 uniform pairs per draw; the rejection loop is bounded.
+struct InvTableF {
+	float v[65];
+	__host__ __device__ constexpr InvTableF() : v() {
+		for (int k = 1; k <= 64; k++) v[k] = 1.0f / (float)k;
 	}
 };
-__constant__ InvTable c_invk = InvTable();
+__constant__ InvTableF c_invkf = InvTableF();
+
+__device__ __forceinline__ float poisson_ptrs(PixelRng& rng, float lam) {
+	const float slam = sqrtf(lam), loglam = logf(lam);
+	const float b = 0.931f + 2.53f * slam;
+	const float a = -0.059f + 0.02483f * b;
+	const float invalpha = 1.1239f + 1.1328f / (b - 3.4f);
+	const float vr = 0.9277f - 3.6224f / (b - 2.f);
+	for (int it = 0; it < 64; it++) {
+		const float U = rng.next() - 0.5f, V = rng.next();
+		const float us = 0.5f - fabsf(U);
+		if (us <= 0.f) continue;  // U = -1/2 exactly: no variate
+		const float k = floorf((2.f * a / us + b) * U + lam + 0.43f);
+		if (us >= 0.07f && V <= vr) return k;
+		if (k < 0.f || (us < 0.013f && V > us)) continue;
+		if (logf(V) + logf(invalpha) - logf(a / (us * us) + b) <= -lam + k * loglam - lgammaf(k + 1.f)) return k;
+	}
+	return rintf(lam);  // 64 rejections in a row: probability below 1e-60
+}
 
 __device__ __forceinline__ float poisson_draw(PixelRng& rng, float xm) {
-	if (xm > 200.f) {
-		return rintf(xm + rng.normal() * sqrtf(xm));
+	if (xm > 200.f) return rintf(xm + rng.normal() * sqrtf(xm));
+	if (xm >= 10.f) return poisson_ptrs(rng, xm);
+	if (!(xm > 0.f)) return 0.f;
+	const float t = rng.next() * expf(xm);
+	float term = 1.f, S = 1.f;
+	int k = 0;
+	while (t >= S && k < 64) {
+		k++;
+		term *= xm * c_invkf.v[k];
+		const float S1 = S + term;
+		if (S1 == S) break;
+		S = S1;
 	}
-	int x = 0;
-	while (xm > 0.f) {
-		const float xmu = xm > 12.f ? 12.f : xm;
-		xm -= xmu;
-		const double u = rng.next();
-		double p = exp(-(double)xmu), F = p;
-		int k = 0;
-		while (u > F && k < 80) {
-			k++;
-			p *= (double)xmu * c_invk.v[k];
-			F += p;
-		}
-		x += k;
-	}
-	return (float)x;
+	return (float)k;
 }
 
 // ---------------------------------------------------------------------------
@@ -609,6 +627,27 @@ __global__ void grad_kernel(PowfsDev P, const float* __restrict__ ints, const fl
 	}
 	grad_from_pixels<NPQ>(pix, P.npix, P.pixpsax, P.pixpsay, P, mtche ? mtche + (size_t)isa * 2 * P.npix : nullptr,
 		i0sum, isa, lane, grad, P.nsa);
+}
+
+// Photon and read noise on n intensities in place, the rule of addnoise
+// (lib/libmisc.c:31-55): tot = x + bkgrnd + bkgrnd2[i], times qe[i] when
+// given; x = (Poisson(tot excess) + tot (1 - excess) + rne N(0,1)) qe[i]
+// - (bkgrndc + bkgrnd2c[i]).  Draws come from the counter (seed, i, stream, frame).
+__global__ void addnoise_kernel(float* __restrict__ x, long n, const float* __restrict__ bkgrnd2,
+	const float* __restrict__ bkgrnd2c, const float* __restrict__ qe, float bkgrnd, float bkgrndc, float rne,
+	float excess, uint64_t seed, uint32_t stream, uint32_t frame) {
+	for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+		float tot = x[i] + bkgrnd + (bkgrnd2 ? bkgrnd2[i] : 0.f);
+		const float corr = bkgrndc + (bkgrnd2c ? bkgrnd2c[i] : 0.f);
+		float scale = 1.f;
+		if (qe) {
+			tot *= qe[i];
+			scale = 1.f / qe[i];
+		}
+		PixelRng rng(seed, (uint32_t)i, stream, frame);
+		const float ph = poisson_draw(rng, tot * excess);
+		x[i] = (ph + tot * (1.f - excess) + rne * rng.normal()) / scale - corr;
+	}
 }
 
 }  // namespace shwfs

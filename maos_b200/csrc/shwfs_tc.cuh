@@ -187,6 +187,7 @@ __device__ __forceinline__ void split8(const float* x, uint4& hi, uint4& lo) {
 	split_pair(x[4], x[5], hi.z, lo.z);
 	split_pair(x[6], x[7], hi.w, lo.w);
 }
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 __device__ __forceinline__ void sts128(unsigned char* base, uint32_t off, const uint4& v) {
 	*reinterpret_cast<uint4*>(base + off) = v;
 }
@@ -305,6 +306,16 @@ __global__ void __launch_bounds__(TC_THREADS, TC_CTAS_PER_SM) ints_tc_kernel(Pow
 		const bool valid = item < nitem;
 		const int isa = valid ? item / nw : 0;
 		const WfsDev W = wfs[valid ? item % nw : 0];
+		// the ETF row this lane multiplies at 4b -> 6a, fetched into L2 now
+		if (valid && P.etfT1) {
+			const float2* e = P.etfT1 + (size_t)isa * 1024 + 32 * lane;
+			prefetch_l2(e);
+			prefetch_l2(e + 16);
+			if (P.etfT2) {
+				prefetch_l2(P.etfT2 + (size_t)isa * 1024 + 32 * lane);
+				prefetch_l2(P.etfT2 + (size_t)isa * 1024 + 32 * lane + 16);
+			}
+		}
 		// ---- (b) field -> A(2a) in TMEM: row x = lane holds E(x-8, y), zero outside [8,24)
 		{
 			const int xp = lane - 8;

@@ -92,6 +92,8 @@ def _load() -> C.CDLL:
         "shwfs_raytrace_dev": [vp, i, i, vp],
         "shwfs_ints_grad_dev": [vp, i, i, vp, vp, vp, vp, i],
         "shwfs_grad_dev": [vp, i, vp, vp],
+        "shwfs_addnoise_dev": [vp, vp, C.c_long, vp, vp, vp, C.c_double, C.c_double, C.c_double, C.c_double,
+                               C.c_uint64, C.c_uint32, C.c_uint32],
         "shwfs_sync": [vp],
         "shwfs_profile_enable": [vp, i],
         "shwfs_profile_read": [vp, dp, ip],
@@ -266,6 +268,13 @@ class Context:
 
     def grad_dev(self, iwfs, ints, grad):
         self._check(self._L.shwfs_grad_dev(self._h, iwfs, _devptr(ints), _devptr(grad)), "grad_dev")
+
+    def addnoise_dev(self, ints, seed: int, stream: int = 0, frame: int = 0, bkgrnd: float = 0.0,
+                     bkgrndc: float = 0.0, rne: float = 0.0, excess: float = 1.0, bkgrnd2=None, bkgrnd2c=None, qe=None):
+        """Photon and read noise in place on a CUDA float32 tensor (addnoise, lib/libmisc.c:31)."""
+        self._check(self._L.shwfs_addnoise_dev(self._h, _devptr(ints), ints.numel(), _devptr(bkgrnd2),
+                                               _devptr(bkgrnd2c), _devptr(qe), bkgrnd, bkgrndc, rne, excess,
+                                               seed, stream, frame), "addnoise_dev")
 
     def sync(self):
         self._check(self._L.shwfs_sync(self._h), "sync")
