@@ -817,6 +817,16 @@ static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist
 	PowfsState& p = ctx->powfs[ipowfs];
 	const int nw = (int)wlist.size();
 	if (nw == 0) return 0;
+	if (ctx->form == SHWFS_FORM_TC && nw > TC_MAX_WFS) {
+		// the tensor-core launch holds at most TC_MAX_WFS WFS descriptors in shared memory
+		for (int k0 = 0; k0 < nw; k0 += TC_MAX_WFS) {
+			const int k1 = std::min(nw, k0 + TC_MAX_WFS);
+			auto cut = [&](const auto& v) { return std::vector<typename std::decay_t<decltype(v)>::value_type>(v.begin() + k0, v.begin() + k1); };
+			int r = launch_ints(ctx, ipowfs, cut(wlist), isim, cut(opds), cut(lotfs), cut(ints), cut(grads), cut(noisy));
+			if (r) return r;
+		}
+		return 0;
+	}
 	PowfsDev P = make_powfs_dev(p, isim);
 	std::vector<WfsDev> wd(nw);
 	for (int k = 0; k < nw; k++) {
@@ -830,6 +840,11 @@ static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist
 		d.mtche = w.mtche.p;
 		d.i0sum = w.i0sum.p;
 		d.ints = ints[k];
+		// the tensor-core form passes intensities to its noise/gradient kernel
+		if (ctx->form == SHWFS_FORM_TC && !d.ints && grads[k]) {
+			if (!w.ints.p) return fail(ctx, SHWFS_ESTATE, "TC form: WFS %d has no intensity buffer", wlist[k]);
+			d.ints = w.ints.p;
+		}
 		d.grad = grads[k];
 		d.alpha = norm_ints(p, w);
 		d.noisy = noisy[k];
@@ -870,19 +885,31 @@ static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist
 		}
 		static bool attr_set[64] = {false};
 		if (ctx->device < 64 && !attr_set[ctx->device]) {
-			CK(cudaFuncSetAttribute(ints_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES));
-			CK(cudaFuncSetAttribute(ints_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES));
+			CK(cudaFuncSetAttribute(ints_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+				tc_smem_bytes(TC_MAX_WFS)));
 			attr_set[ctx->device] = true;
 		}
 		TcTables T{p.tc_bmat.p};
+		bool all_lotf = true, any_out = false;
+		for (int k = 0; k < nw; k++) {
+			all_lotf = all_lotf && wd[k].lotfT;
+			any_out = any_out || wd[k].ints;
+		}
+		const int nlotf = all_lotf ? nw : 0;
 		// persistent: TC_CTAS_PER_SM CTAs of TC_GROUPS tile groups per SM
 		const int ntile = (nitem + 3) / 4;
 		const int grid = std::min((ntile + TC_GROUPS - 1) / TC_GROUPS, tc_sm_count(ctx) * TC_CTAS_PER_SM);
-		if (npix <= 32)
-			ints_tc_kernel<1><<<grid, TC_THREADS, TC_SMEM_BYTES, ctx->stream>>>(P, wdev, nw, nitem, T, ctx->errflag.p);
-		else
-			ints_tc_kernel<2><<<grid, TC_THREADS, TC_SMEM_BYTES, ctx->stream>>>(P, wdev, nw, nitem, T, ctx->errflag.p);
+		if (any_out)
+			ints_tc_kernel<<<grid, TC_THREADS, tc_smem_bytes(nlotf), ctx->stream>>>(P, wdev, nw, nitem, nlotf, T,
+				ctx->errflag.p);
 		CK(cudaGetLastError());
+		bool post = false;
+		for (int k = 0; k < nw; k++) post = post || (wd[k].ints && (wd[k].noisy || wd[k].grad));
+		if (post) {
+			if (npix <= 32) noise_grad_kernel<1><<<nblk, 128, 0, ctx->stream>>>(P, wdev, nw, nitem);
+			else noise_grad_kernel<2><<<nblk, 128, 0, ctx->stream>>>(P, wdev, nw, nitem);
+			CK(cudaGetLastError());
+		}
 		return 0;
 	}
 	auto go = [&](auto kern) { kern<<<nblk, 128, 0, ctx->stream>>>(P, wdev, nw, nitem); };

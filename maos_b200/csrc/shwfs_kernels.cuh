@@ -612,6 +612,40 @@ __global__ void __launch_bounds__(128, MINB) ints_n32_kernel(PowfsDev P, const W
 	}
 }
 
+// (d)-(e) after an imaging kernel that stored noise-free intensities (the
+// tensor-core form): photon/read noise in place, then CoG / matched filter.
+// One warp per work item, items ordered as in the imaging launch.
+template <int NPQ>
+__global__ void noise_grad_kernel(PowfsDev P, const WfsDev* __restrict__ wfs, int nw, int nitem) {
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int item = blockIdx.x * (blockDim.x >> 5) + warp;
+	if (item >= nitem) return;
+	const int isa = item / nw;
+	const WfsDev& W = wfs[item % nw];
+	const int npix = P.npix;
+	float* o = W.ints + (size_t)isa * npix;
+	float pix[NPQ];
+#pragma unroll
+	for (int q = 0; q < NPQ; q++) {
+		const int p = lane + 32 * q;
+		pix[q] = p < npix ? o[p] : 0.f;
+	}
+	if (W.noisy) {
+#pragma unroll
+		for (int q = 0; q < NPQ; q++) {
+			const int p = lane + 32 * q;
+			if (p < npix) {
+				PixelRng rng(W.seed, (uint32_t)(isa * npix + p), W.wfs_id, (uint32_t)P.isim);
+				pix[q] = poisson_draw(rng, pix[q] + P.bkgrnd) + P.rne * rng.normal() - P.bkgrndc;
+				o[p] = pix[q];
+			}
+		}
+	}
+	if (W.grad)
+		grad_from_pixels<NPQ>(pix, npix, P.pixpsax, P.pixpsay, P, W.mtche + (size_t)isa * 2 * npix, W.i0sum, isa,
+			lane, W.grad, P.nsa);
+}
+
 // (e) alone: one warp per subaperture from stored intensities.
 template <int NPQ>
 __global__ void grad_kernel(PowfsDev P, const float* __restrict__ ints, const float* __restrict__ mtche,

@@ -24,13 +24,16 @@
 // rows (s, iy) with iy >= 8 read stale operand data and are never read back.
 //
 // A tile is 4 subapertures = 128 GEMM rows; warp w of a tile group owns
-// subaperture w and TMEM lanes 32w..32w+31.  A CTA holds two independent
-// tile groups (4 warps each) that share the constant B operands; each group
-// has its own TMEM columns (64 accumulator + 64 A-operand), its own 32 KB
-// MN-major operand buffer and its own mbarrier.  One thread per group issues
-// the MMAs, commits them to the group's mbarrier and waits on it with a 2 s
-// bound (on expiry the kernel records SHWFS_ETIMEOUT, frees its TMEM and
-// returns); the rest of the group waits at a named barrier.
+// subaperture w and TMEM lanes 32w..32w+31.  One CTA per SM holds four
+// independent tile groups (4 warps each) that share the constant B operands,
+// the WFS descriptors and the uplink OTFs in shared memory; each group has its
+// own TMEM columns (64 accumulator + 64 A-operand), its own 32 KB MN-major
+// operand buffer and its own mbarrier.  One thread per group issues the MMAs,
+// commits them to the group's mbarrier and waits on it with a 2 s bound (on
+// expiry the kernel records SHWFS_ETIMEOUT, frees its TMEM and returns); the
+// rest of the group waits at a named barrier.  The kernel stores noise-free
+// pixel intensities; photon/read noise and the gradients run in a separate
+// one-warp-per-image kernel, whose occupancy hides their latency.
 //
 // Operand layouts (SWIZZLE_NONE, core matrices of 8 rows x 16 bytes):
 //   K-major (B):  chunk (row r, k-chunk c) at ((r/8)*kc + c)*128 + (r%8)*16
@@ -54,13 +57,17 @@ constexpr int TC_B3_BYTES = 32 * 16 * 16;  // N=32 (16 re + 16 im pixel rows), K
 constexpr int TC_B4_BYTES = 16 * 16 * 16;  // N=16 (pixel columns), K=64: [Re Gx | -Im Gx]
 constexpr int TC_B_BYTES = TC_B1_BYTES + TC_B2_BYTES + TC_B3_BYTES + TC_B4_BYTES;
 constexpr int TC_A_BYTES = 16 * 16 * 128;  // one group's MN-major A: 16 m-chunks x 16 k-groups
-constexpr int TC_GROUPS = 2;               // tile groups per CTA
+constexpr int TC_GROUPS = 4;               // tile groups per CTA (one CTA per SM)
 constexpr int TC_THREADS = 128 * TC_GROUPS;
-constexpr int TC_PIX_BYTES = TC_THREADS / 32 * 64 * 4;  // 64 staged pixels per warp
-constexpr int TC_MISC_OFF = TC_B_BYTES + TC_GROUPS * TC_A_BYTES + TC_PIX_BYTES;
-constexpr int TC_SMEM_BYTES = TC_MISC_OFF + 64;
+constexpr int TC_MAX_WFS = 6;              // WFS per launch (descriptors and uplink OTFs in smem)
+constexpr int TC_LOTF_BYTES = 32 * 32 * 8; // one uplink OTF, 32 rows of 16 swizzled 16-byte chunks
+constexpr int TC_WDESC_OFF = TC_B_BYTES + TC_GROUPS * TC_A_BYTES;
+constexpr int TC_MISC_OFF = TC_WDESC_OFF + 640;  // >= TC_MAX_WFS * sizeof(WfsDev)
+constexpr int TC_LOTF_OFF = TC_MISC_OFF + 128;
+// dynamic shared memory of a launch caching nlotf uplink OTFs
+__host__ __device__ constexpr int tc_smem_bytes(int nlotf) { return TC_LOTF_OFF + nlotf * TC_LOTF_BYTES; }
 constexpr int TC_TMEM_COLS = 128 * TC_GROUPS;  // per group: 64 accumulator + 64 A operand
-constexpr int TC_CTAS_PER_SM = 2;
+constexpr int TC_CTAS_PER_SM = 1;
 
 // byte offset of (row r, 16-byte chunk c) in a K-major operand with kc chunks per row group
 __host__ __device__ constexpr uint32_t tc_off(int r, int c, int kc) {
@@ -167,7 +174,37 @@ __device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&r)[8])
 				 "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
 				 : "memory");
 }
+__device__ __forceinline__ void tmem_st4(uint32_t taddr, const uint32_t (&r)[4]) {
+	asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1,%2,%3,%4};" ::"r"(taddr), "r"(r[0]), "r"(r[1]),
+				 "r"(r[2]), "r"(r[3])
+				 : "memory");
+}
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// Transfer-function factors of one quarter (8 spatial frequencies fy) of an
+// OTF row, as complex pairs: (x, y) for fy, (z, w) for fy + 1.  l: uplink OTF
+// (applied conjugated), e: ETF, or the real DTF nominal as (d, 0), or 1.
+struct TfQuarter {
+	float4 l[4], e[4];
+};
+__device__ __forceinline__ void tf_load(TfQuarter& t, const unsigned char* lrow_s, int swz, const float4* lrow,
+	const float4* erow, const float2* nrow, int q) {
+#pragma unroll
+	for (int i = 0; i < 4; i++) {
+		if (lrow_s)
+			t.l[i] = *reinterpret_cast<const float4*>(lrow_s + (((4 * q + i) ^ swz) << 4));
+		else
+			t.l[i] = lrow ? __ldg(lrow + 4 * q + i) : make_float4(1.f, 0.f, 1.f, 0.f);
+		if (erow) {
+			t.e[i] = __ldg(erow + 4 * q + i);
+		} else if (nrow) {
+			const float2 d = __ldg(nrow + 4 * q + i);
+			t.e[i] = make_float4(d.x, 0.f, d.y, 0.f);
+		} else {
+			t.e[i] = make_float4(1.f, 0.f, 1.f, 0.f);
+		}
+	}
+}
 
 // ---- operand split ----
 // (a, b) -> packed bf16 pair hi = (bf16(a), bf16(b)) and lo = bf16 of the
@@ -201,34 +238,30 @@ __device__ __forceinline__ void sincospi_fast(float t, float& s, float& c) {
 }
 
 // ---- GEMM issue (one thread) ----
-// D = sum_j Ah_j Bh_j + Ah_j Bl_j + Al_j Bh_j over nks K-steps of 16.
-// B: K-major image at bbase with bkc chunks per row group, lo half at chunk blo.
-__device__ __forceinline__ uint64_t bdesc_hi(uint32_t bbase, int bkc, int j) {
-	return tc_desc(bbase + (uint32_t)(2 * j) * 128, 128, (uint32_t)bkc * 128);
-}
-__device__ __forceinline__ uint64_t bdesc_lo(uint32_t bbase, int bkc, int blo, int j) {
-	return tc_desc(bbase + (uint32_t)(blo + 2 * j) * 128, 128, (uint32_t)bkc * 128);
-}
+// D = sum_j Ah_j Bh_j + Ah_j Bl_j + Al_j Bh_j over nks K-steps of 16.  The
+// descriptors are formed once per kernel; a K-step of 16 advances a start
+// address by 256 B, i.e. the descriptor's start field by 16 (smem addresses
+// are below 2^18, so the 14-bit field never carries).
+// B: descriptor of its K-major image (SBO = chunks per row group x 128 B),
+// lo half blo chunks further on.
 // A in TMEM: hi K pairs in columns [acol, acol+alo), lo in [acol+alo, ...)
-__device__ __forceinline__ void tc_gemm_ts(uint32_t dt, uint32_t acol, int alo, uint32_t bbase, int bkc, int blo,
-	int nks, uint32_t idesc) {
+__device__ __forceinline__ void tc_gemm_ts(uint32_t dt, uint32_t acol, int alo, uint64_t bd, int blo, int nks,
+	uint32_t idesc) {
 	for (int j = 0; j < nks; j++) {
 		const uint32_t ah = acol + 8 * j, al = acol + alo + 8 * j;
-		const uint64_t bh = bdesc_hi(bbase, bkc, j), bl = bdesc_lo(bbase, bkc, blo, j);
+		const uint64_t bh = bd + (uint64_t)(16 * j), bl = bd + (uint64_t)(8 * blo + 16 * j);
 		tc_mma_ts(dt, ah, bh, idesc, j > 0 ? 1u : 0u);
 		tc_mma_ts(dt, ah, bl, idesc, 1u);
 		tc_mma_ts(dt, al, bh, idesc, 1u);
 	}
 }
-// A in shared memory, MN-major with nkg k-groups: hi K-rows from k-group 0,
-// lo K-rows from k-group nkg/2
-__device__ __forceinline__ void tc_gemm_ss(uint32_t dt, uint32_t abase, int nkg, uint32_t bbase, int bkc, int blo,
-	int nks, uint32_t idesc) {
-	const uint32_t sbo = (uint32_t)nkg * 128;
+// A in shared memory, MN-major with nkg k-groups (descriptor ad, SBO = nkg x
+// 128 B): hi K-rows from k-group 0, lo K-rows from k-group nkg/2
+__device__ __forceinline__ void tc_gemm_ss(uint32_t dt, uint64_t ad, int nkg, uint64_t bd, int blo, int nks,
+	uint32_t idesc) {
 	for (int j = 0; j < nks; j++) {
-		const uint64_t ah = tc_desc(abase + (uint32_t)(2 * j) * 128, 128, sbo);
-		const uint64_t al = tc_desc(abase + (uint32_t)(nkg / 2 + 2 * j) * 128, 128, sbo);
-		const uint64_t bh = bdesc_hi(bbase, bkc, j), bl = bdesc_lo(bbase, bkc, blo, j);
+		const uint64_t ah = ad + (uint64_t)(16 * j), al = ad + (uint64_t)(4 * nkg + 16 * j);
+		const uint64_t bh = bd + (uint64_t)(16 * j), bl = bd + (uint64_t)(8 * blo + 16 * j);
 		tc_mma_ss(dt, ah, bh, idesc, j > 0 ? 1u : 0u);
 		tc_mma_ss(dt, ah, bl, idesc, 1u);
 		tc_mma_ss(dt, al, bh, idesc, 1u);
@@ -236,24 +269,42 @@ __device__ __forceinline__ void tc_gemm_ss(uint32_t dt, uint32_t abase, int nkg,
 }
 
 // ---------------------------------------------------------------------------
-template <int NPQ>
+// Noise-free pixel intensities of nitem = nsa x nw subaperture images (item
+// i -> subaperture i / nw of WFS i % nw, nw <= TC_MAX_WFS) into wfs[].ints;
+// photon/read noise and gradients follow in noise_grad_kernel.  nlotf: 0, or
+// nw when every WFS of the launch has an uplink OTF, which is then cached in
+// shared memory.
 __global__ void __launch_bounds__(TC_THREADS, TC_CTAS_PER_SM) ints_tc_kernel(PowfsDev P,
-	const WfsDev* __restrict__ wfs, int nw, int nitem, TcTables T, int* errflag) {
+	const WfsDev* __restrict__ wfs, int nw, int nitem, int nlotf, TcTables T, int* errflag) {
+	static_assert(TC_MAX_WFS * sizeof(WfsDev) <= 640, "WFS descriptor area");
 	extern __shared__ __align__(128) unsigned char smem[];
 	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 	const int g = warp >> 2, wq = warp & 3;  // tile group, warp within the group
 	unsigned char* bbuf = smem;               // B1 | B2 | B3 | B4
 	unsigned char* abuf = smem + TC_B_BYTES + g * TC_A_BYTES;
-	float* pixbuf = reinterpret_cast<float*>(smem + TC_B_BYTES + TC_GROUPS * TC_A_BYTES) + warp * 64;
+	WfsDev* wsm = reinterpret_cast<WfsDev*>(smem + TC_WDESC_OFF);
+	const unsigned char* lotf_s = smem + TC_LOTF_OFF;
 	uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + TC_MISC_OFF) + g;
-	uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + TC_MISC_OFF + 16);
-	int* bail = reinterpret_cast<int*>(smem + TC_MISC_OFF + 32) + g;
+	uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + TC_MISC_OFF + 32);
+	int* bail = reinterpret_cast<int*>(smem + TC_MISC_OFF + 64) + g;
 
 	for (int i = tid; i < TC_B_BYTES / 16; i += TC_THREADS) reinterpret_cast<uint4*>(bbuf)[i] = T.bmat[i];
+	for (int i = tid; i < nw * (int)(sizeof(WfsDev) / 4); i += TC_THREADS)
+		reinterpret_cast<uint32_t*>(wsm)[i] = reinterpret_cast<const uint32_t*>(wfs)[i];
+	// uplink OTFs: row fx holds 16 chunks of 2 complex values, chunk c stored
+	// at c ^ (fx & 15) so that the 32 rows read by a warp hit distinct banks
+	for (int k = 0; k < nlotf; k++) {
+		const uint4* src = reinterpret_cast<const uint4*>(wfs[k].lotfT);
+		for (int i = tid; i < 512; i += TC_THREADS) {
+			const int fx = i >> 4, c = i & 15;
+			*reinterpret_cast<uint4*>(smem + TC_LOTF_OFF + k * TC_LOTF_BYTES + fx * 256 + ((c ^ (fx & 15)) << 4)) =
+				src[i];
+		}
+	}
 	if (tid == 0) {
 		for (int k = 0; k < TC_GROUPS; k++) {
 			mbar_init(reinterpret_cast<uint64_t*>(smem + TC_MISC_OFF) + k, 1);
-			reinterpret_cast<int*>(smem + TC_MISC_OFF + 32)[k] = 0;
+			reinterpret_cast<int*>(smem + TC_MISC_OFF + 64)[k] = 0;
 		}
 		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 	}
@@ -272,6 +323,9 @@ __global__ void __launch_bounds__(TC_THREADS, TC_CTAS_PER_SM) ints_tc_kernel(Pow
 	const uint32_t tl = (uint32_t)(32 * wq) << 16;  // this warp's lane quarter
 	const uint32_t a_s = smem_u32(abuf), b1_s = smem_u32(bbuf), b2_s = b1_s + TC_B1_BYTES,
 				   b3_s = b2_s + TC_B2_BYTES, b4_s = b3_s + TC_B3_BYTES;
+	const uint64_t bd1 = tc_desc(b1_s, 128, 8 * 128), bd2 = tc_desc(b2_s, 128, 16 * 128),
+				   bd3 = tc_desc(b3_s, 128, 16 * 128), bd4 = tc_desc(b4_s, 128, 16 * 128);
+	const uint64_t ad8 = tc_desc(a_s, 128, 8 * 128), ad16 = tc_desc(a_s, 128, 16 * 128);
 	const bool issuer = (tid & 127) == 0;
 	const int bar_id = 1 + g;
 	uint32_t phase = 0;
@@ -305,7 +359,8 @@ __global__ void __launch_bounds__(TC_THREADS, TC_CTAS_PER_SM) ints_tc_kernel(Pow
 		const int item = 4 * t + wq;
 		const bool valid = item < nitem;
 		const int isa = valid ? item / nw : 0;
-		const WfsDev W = wfs[valid ? item % nw : 0];
+		const int iw = valid ? item % nw : 0;
+		const WfsDev& W = wsm[iw];
 		// the ETF row this lane multiplies at 4b -> 6a, fetched into L2 now
 		if (valid && P.etfT1) {
 			const float2* e = P.etfT1 + (size_t)isa * 1024 + 32 * lane;
@@ -316,6 +371,7 @@ __global__ void __launch_bounds__(TC_THREADS, TC_CTAS_PER_SM) ints_tc_kernel(Pow
 				prefetch_l2(P.etfT2 + (size_t)isa * 1024 + 32 * lane + 16);
 			}
 		}
+		if (valid && W.grad && W.mtche && 32 * lane < 2 * P.npix) prefetch_l2(W.mtche + (size_t)isa * 2 * P.npix + 32 * lane);
 		// ---- (b) field -> A(2a) in TMEM: row x = lane holds E(x-8, y), zero outside [8,24)
 		{
 			const int xp = lane - 8;
@@ -345,7 +401,7 @@ __global__ void __launch_bounds__(TC_THREADS, TC_CTAS_PER_SM) ints_tc_kernel(Pow
 			tmem_st16(acol + tl + 16, lw);
 			tmem_wait_st();
 		}
-		if (!finish_stage([&] { tc_gemm_ts(dcol, acol, 16, b1_s, 8, 4, 2, tc_idesc(64, false)); })) break;  // 2a
+		if (!finish_stage([&] { tc_gemm_ts(dcol, acol, 16, bd1, 4, 2, tc_idesc(64, false)); })) break;  // 2a
 		// ---- 2a out: row x holds F1(x-8, ky) -> K-rows x-8 (re), 16+x-8 (im) of A(2b), M = (s, ky)
 		{
 			const int xp = lane - 8;
@@ -372,7 +428,7 @@ __global__ void __launch_bounds__(TC_THREADS, TC_CTAS_PER_SM) ints_tc_kernel(Pow
 			}
 			fence_async_smem();
 		}
-		if (!finish_stage([&] { tc_gemm_ss(dcol, a_s, 8, b1_s, 8, 4, 2, tc_idesc(64, true)); })) break;  // 2b
+		if (!finish_stage([&] { tc_gemm_ss(dcol, ad8, 8, bd1, 4, 2, tc_idesc(64, true)); })) break;  // 2b
 		// ---- 2b out: row ky holds F(kx, ky) -> P = |F|^2 -> A(4a) in TMEM, K = kx
 		{
 			uint32_t hw[16], lw[16];
@@ -393,7 +449,7 @@ __global__ void __launch_bounds__(TC_THREADS, TC_CTAS_PER_SM) ints_tc_kernel(Pow
 			tmem_st16(acol + tl + 16, lw);
 			tmem_wait_st();
 		}
-		if (!finish_stage([&] { tc_gemm_ts(dcol, acol, 16, b2_s, 16, 8, 2, tc_idesc(64, false)); })) break;  // 4a
+		if (!finish_stage([&] { tc_gemm_ts(dcol, acol, 16, bd2, 8, 2, tc_idesc(64, false)); })) break;  // 4a
 		// ---- 4a out: row ky holds Q(ky, fx) -> K-rows ky (re), 32+ky (im) of A(4b), M = (s, fx)
 		{
 #pragma unroll
@@ -416,84 +472,68 @@ __global__ void __launch_bounds__(TC_THREADS, TC_CTAS_PER_SM) ints_tc_kernel(Pow
 			}
 			fence_async_smem();
 		}
-		if (!finish_stage([&] { tc_gemm_ss(dcol, a_s, 16, b2_s, 16, 8, 4, tc_idesc(64, true)); })) break;  // 4b
+		// the transfer function of 4b -> 6a in quarters of 8 fy: the loads of
+		// quarter 0 are in flight during the 4b GEMM, those of quarter q+1
+		// during the arithmetic of quarter q
+		const unsigned char* lrow_s = (valid && nlotf) ? lotf_s + iw * TC_LOTF_BYTES + lane * 256 : nullptr;
+		const float4* lrow =
+			(valid && !nlotf && W.lotfT) ? reinterpret_cast<const float4*>(W.lotfT + 32 * lane) : nullptr;
+		const float4* erow =
+			(valid && P.etfT1) ? reinterpret_cast<const float4*>(P.etfT1 + (size_t)isa * 1024 + 32 * lane) : nullptr;
+		const float4* erow2 =
+			(erow && P.etfT2) ? reinterpret_cast<const float4*>(P.etfT2 + (size_t)isa * 1024 + 32 * lane) : nullptr;
+		const float2* nrow = (valid && !P.etfT1 && P.nominalT)
+								 ? reinterpret_cast<const float2*>(
+									   P.nominalT + (P.nominal_per_sa ? (size_t)isa * 1024 : 0) + 32 * lane)
+								 : nullptr;
+		TfQuarter tq;
+		tf_load(tq, lrow_s, lane & 15, lrow, erow, nrow, 0);
+		if (!finish_stage([&] { tc_gemm_ss(dcol, ad16, 16, bd2, 8, 4, tc_idesc(64, true)); })) break;  // 4b
 		// ---- 4b out: row fx holds OTF(fx, fy) x conj(uplink) x ETF -> A(6a) in TMEM, K = fy
 		{
-			const int fx = lane;
 #pragma unroll
-			for (int h = 0; h < 2; h++) {
-				float re[16], im[16];
-				tmem_ld16(dcol + tl + 16 * h, re);
-				tmem_ld16(dcol + tl + 32 + 16 * h, im);
+			for (int q = 0; q < 4; q++) {
+				float re[8], im[8];
+				tmem_ld8(dcol + tl + 8 * q, re);
+				tmem_ld8(dcol + tl + 32 + 8 * q, im);
+				TfQuarter tn;
+				if (q < 3) tf_load(tn, lrow_s, lane & 15, lrow, erow, nrow, q + 1);
 				tmem_wait_ld();
-				if (valid) {
-					if (W.lotfT) {
-						const float4* l = reinterpret_cast<const float4*>(W.lotfT + 32 * fx + 16 * h);
 #pragma unroll
-						for (int i = 0; i < 16; i += 2) {
-							const float4 c = __ldg(l + i / 2);
-							float a = re[i], b = im[i];
-							re[i] = fmaf(a, c.x, b * c.y);
-							im[i] = fmaf(b, c.x, -a * c.y);
-							a = re[i + 1];
-							b = im[i + 1];
-							re[i + 1] = fmaf(a, c.z, b * c.w);
-							im[i + 1] = fmaf(b, c.z, -a * c.w);
-						}
+				for (int i = 0; i < 4; i++) {
+					const float4 l = tq.l[i];
+					float4 e = tq.e[i];
+					if (erow2) {  // ETF interpolated between two sodium profiles
+						const float4 e2 = __ldg(erow2 + 4 * q + i);
+						e = make_float4(e.x * P.etfwt1 + e2.x * P.etfwt2, e.y * P.etfwt1 + e2.y * P.etfwt2,
+							e.z * P.etfwt1 + e2.z * P.etfwt2, e.w * P.etfwt1 + e2.w * P.etfwt2);
 					}
-					if (P.etfT1) {
-						const float4* e1 =
-							reinterpret_cast<const float4*>(P.etfT1 + (size_t)isa * 1024 + 32 * fx + 16 * h);
-						const float4* e2 =
-							P.etfT2 ? reinterpret_cast<const float4*>(P.etfT2 + (size_t)isa * 1024 + 32 * fx + 16 * h)
-									: nullptr;
-#pragma unroll
-						for (int i = 0; i < 16; i += 2) {
-							float4 c = __ldg(e1 + i / 2);
-							if (e2) {
-								const float4 c2 = __ldg(e2 + i / 2);
-								c = make_float4(c.x * P.etfwt1 + c2.x * P.etfwt2, c.y * P.etfwt1 + c2.y * P.etfwt2,
-									c.z * P.etfwt1 + c2.z * P.etfwt2, c.w * P.etfwt1 + c2.w * P.etfwt2);
-							}
-							float a = re[i], b = im[i];
-							re[i] = fmaf(a, c.x, -b * c.y);
-							im[i] = fmaf(a, c.y, b * c.x);
-							a = re[i + 1];
-							b = im[i + 1];
-							re[i + 1] = fmaf(a, c.z, -b * c.w);
-							im[i + 1] = fmaf(a, c.w, b * c.z);
-						}
-					} else if (P.nominalT) {
-						const float4* nm = reinterpret_cast<const float4*>(
-							P.nominalT + (P.nominal_per_sa ? (size_t)isa * 1024 : 0) + 32 * fx + 16 * h);
-#pragma unroll
-						for (int i = 0; i < 16; i += 4) {
-							const float4 d = __ldg(nm + i / 4);
-							re[i] *= d.x;
-							im[i] *= d.x;
-							re[i + 1] *= d.y;
-							im[i + 1] *= d.y;
-							re[i + 2] *= d.z;
-							im[i + 2] *= d.z;
-							re[i + 3] *= d.w;
-							im[i + 3] *= d.w;
-						}
-					}
+					float a = re[2 * i], b = im[2 * i];
+					float a1 = fmaf(a, l.x, b * l.y), b1 = fmaf(b, l.x, -a * l.y);
+					re[2 * i] = fmaf(a1, e.x, -b1 * e.y);
+					im[2 * i] = fmaf(a1, e.y, b1 * e.x);
+					a = re[2 * i + 1];
+					b = im[2 * i + 1];
+					a1 = fmaf(a, l.z, b * l.w);
+					b1 = fmaf(b, l.z, -a * l.w);
+					re[2 * i + 1] = fmaf(a1, e.z, -b1 * e.w);
+					im[2 * i + 1] = fmaf(a1, e.w, b1 * e.z);
 				}
-				uint32_t rh[8], rl[8], ih[8], il[8];
+				uint32_t rh[4], rl[4], ih[4], il[4];
 #pragma unroll
-				for (int i = 0; i < 16; i += 2) {
-					split_pair(re[i], re[i + 1], rh[i / 2], rl[i / 2]);
-					split_pair(im[i], im[i + 1], ih[i / 2], il[i / 2]);
+				for (int i = 0; i < 4; i++) {
+					split_pair(re[2 * i], re[2 * i + 1], rh[i], rl[i]);
+					split_pair(im[2 * i], im[2 * i + 1], ih[i], il[i]);
 				}
-				tmem_st8(acol + tl + 8 * h, rh);       // re fy: K 0..31  -> hi columns 0..15
-				tmem_st8(acol + tl + 16 + 8 * h, ih);  // im fy: K 32..63 -> hi columns 16..31
-				tmem_st8(acol + tl + 32 + 8 * h, rl);  // lo columns 32..63
-				tmem_st8(acol + tl + 48 + 8 * h, il);
+				tmem_st4(acol + tl + 4 * q, rh);       // re fy: K 0..31  -> hi columns 0..15
+				tmem_st4(acol + tl + 16 + 4 * q, ih);  // im fy: K 32..63 -> hi columns 16..31
+				tmem_st4(acol + tl + 32 + 4 * q, rl);  // lo columns 32..63
+				tmem_st4(acol + tl + 48 + 4 * q, il);
+				if (q < 3) tq = tn;
 			}
 			tmem_wait_st();
 		}
-		if (!finish_stage([&] { tc_gemm_ts(dcol, acol, 32, b3_s, 16, 8, 4, tc_idesc(32, false)); })) break;  // 6a
+		if (!finish_stage([&] { tc_gemm_ts(dcol, acol, 32, bd3, 8, 4, tc_idesc(32, false)); })) break;  // 6a
 		// ---- 6a out: row fx holds T(fx, iy) -> K-rows fx (re), 32+fx (im) of A(6b), M = (s, iy < 8)
 		{
 			float re[8], im[8];
@@ -510,49 +550,20 @@ __global__ void __launch_bounds__(TC_THREADS, TC_CTAS_PER_SM) ints_tc_kernel(Pow
 			sts128(abuf, mn_off(mg, 96 + lane, 16), il);
 			fence_async_smem();
 		}
-		if (!finish_stage([&] { tc_gemm_ss(dcol, a_s, 16, b4_s, 16, 8, 4, tc_idesc(16, true)); })) break;  // 6b
-		// ---- 6b out: row iy (lanes 0..7) holds I(ix, iy) -> pixels of this warp's subaperture
-		float pix[NPQ];
+		if (!finish_stage([&] { tc_gemm_ss(dcol, ad16, 16, bd4, 8, 4, tc_idesc(16, true)); })) break;  // 6b
+		// ---- 6b out: row iy (lanes 0..7) holds I(ix, iy) -> noise-free pixels of this warp's subaperture
 		{
 			float v[8];
 			tmem_ld8(dcol + tl, v);
 			tmem_wait_ld();
-			const int npx = P.pixpsax, npy = P.pixpsay, npix = P.npix;
-			if (lane < npy) {
+			const int npx = P.pixpsax, npy = P.pixpsay;
+			if (valid && W.ints && lane < npy) {
+				float* o = W.ints + (size_t)isa * P.npix + lane * npx;
+				const float alpha = W.alpha;
 #pragma unroll
 				for (int ix = 0; ix < 8; ix++)
-					if (ix < npx) pixbuf[lane * npx + ix] = v[ix] * W.alpha;
+					if (ix < npx) o[ix] = v[ix] * alpha;
 			}
-			__syncwarp();
-#pragma unroll
-			for (int q = 0; q < NPQ; q++) {
-				const int p = lane + 32 * q;
-				pix[q] = p < npix ? pixbuf[p] : 0.f;
-			}
-			__syncwarp();
-		}
-		if (valid) {
-			const int npix = P.npix;
-			if (W.noisy) {
-#pragma unroll
-				for (int q = 0; q < NPQ; q++) {
-					const int p = lane + 32 * q;
-					if (p < npix) {
-						PixelRng rng(W.seed, (uint32_t)(isa * npix + p), W.wfs_id, (uint32_t)P.isim);
-						pix[q] = poisson_draw(rng, pix[q] + P.bkgrnd) + P.rne * rng.normal() - P.bkgrndc;
-					}
-				}
-			}
-			if (W.ints) {
-#pragma unroll
-				for (int q = 0; q < NPQ; q++) {
-					const int p = lane + 32 * q;
-					if (p < npix) W.ints[(size_t)isa * npix + p] = pix[q];
-				}
-			}
-			if (W.grad)
-				grad_from_pixels<NPQ>(pix, npix, P.pixpsax, P.pixpsay, P, W.mtche + (size_t)isa * 2 * npix, W.i0sum,
-					isa, lane, W.grad, P.nsa);
 		}
 	}
 	tc_fence_before();
