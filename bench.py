@@ -148,6 +148,14 @@ def fft_flops_per_image(notf):
     return 3 * 5 * n2 * math.log2(n2)
 
 
+def tc_mma_flops_per_image():
+    """BF16 MMA flops the tensor-core imaging kernel executes per subaperture
+    image: per 4-image tile, 2a/2b/4a 6 MMAs and 4b 12 MMAs of 128x64x16, 6a 12
+    of 128x32x16 and 6b 12 of 128x16x16 (three split terms, zero padding included)."""
+    tile = 30 * 128 * 64 * 16 * 2 + 12 * 128 * 32 * 16 * 2 + 12 * 128 * 16 * 16 * 2
+    return tile / 4
+
+
 def cpu_baseline(cfg, wl_layers, screens, seconds=15.0, max_frames=40):
     from oracle import ref
     ncpu = os.cpu_count() or 1
@@ -297,15 +305,29 @@ def run_b200(args, cfg):
     if os.path.exists(tp):
         with open(tp) as f:
             traffic = json.load(f).get(f"{cfg['name']}:{args.form}:ints")
-    roofline = {"kernel": "ints_n32_kernel (fused imaging, noise, gradients)", "bound": "hbm",
-                "achieved": ints_gbs, "peak": hbm, "unit": "GB/s", "frac": ints_gbs / hbm,
-                "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else "fallback",
-                "traffic": traffic, "algorithmic_bytes_per_launch": ints_bytes,
-                "compute": {"achieved": ints_tf, "peak": fp32_peak, "unit": "TFLOP/s",
-                            "frac": ints_tf / fp32_peak,
-                            "note": "nominal FFT flops (3 x 5 N^2 log2 N^2 per image) vs nominal FP32 CUDA-core peak"},
-                "raytrace": {"achieved": ray_gbs, "peak": hbm, "unit": "GB/s", "frac": ray_gbs / hbm,
-                             "algorithmic_bytes_per_launch": ray_bytes}}
+    src_note = f"{src} (MEASURED_PEAKS.json)" if src == "measured" else "fallback"
+    raytrace = {"kernel": "geom_kernel", "achieved": ray_gbs, "peak": hbm, "unit": "GB/s", "frac": ray_gbs / hbm,
+                "algorithmic_bytes_per_launch": ray_bytes}
+    if args.form == "tc":
+        tflops = units_per_step * tc_mma_flops_per_image() / (ints_ms * 1e-3) / 1e12 if ints_ms else 0.0
+        post_ms = st["post"]["ms_per_launch"]
+        roofline = {"kernel": "ints_tc_kernel (tcgen05 BF16x3 DFT imaging)", "bound": "tensor",
+                    "achieved": tflops, "peak": bf16, "unit": "TFLOP/s", "frac": tflops / bf16,
+                    "peak_source": src_note + " bf16_tflops, burst", "traffic": traffic,
+                    "flops_per_launch": units_per_step * tc_mma_flops_per_image(),
+                    "hbm": {"achieved": ints_gbs, "peak": hbm, "unit": "GB/s", "frac": ints_gbs / hbm,
+                            "algorithmic_bytes_per_launch": ints_bytes},
+                    "post": {"kernel": "noise_grad_kernel", "ms_per_launch": post_ms},
+                    "raytrace": raytrace}
+    else:
+        roofline = {"kernel": "ints_n32_kernel (fused imaging, noise, gradients)", "bound": "hbm",
+                    "achieved": ints_gbs, "peak": hbm, "unit": "GB/s", "frac": ints_gbs / hbm,
+                    "peak_source": src_note + " hbm_gbs", "traffic": traffic,
+                    "algorithmic_bytes_per_launch": ints_bytes,
+                    "compute": {"achieved": ints_tf, "peak": fp32_peak, "unit": "TFLOP/s",
+                                "frac": ints_tf / fp32_peak,
+                                "note": "nominal FFT flops (3 x 5 N^2 log2 N^2 per image) vs nominal FP32 CUDA-core peak"},
+                    "raytrace": raytrace}
     p50 = float(np.percentile(step_ms, 50))
     p99 = float(np.percentile(step_ms, 99))
     line = {

@@ -189,8 +189,9 @@ int shwfs_addnoise_dev(shwfs_ctx* ctx, float* ints, long n, const float* bkgrnd2
         as the reference's ctoc instrumentation (cuda/math/common.h:233-267) ---- */
 #define SHWFS_STAGE_RAYTRACE 0 /* (a) ray trace into the subaperture OPD */
 #define SHWFS_STAGE_UPLINK 1   /* LLT ray trace and uplink OTF */
-#define SHWFS_STAGE_INTS 2     /* (b)-(e) fused imaging, noise, gradients */
-#define SHWFS_NSTAGE 3
+#define SHWFS_STAGE_INTS 2     /* (b)-(e) imaging (FFT form: with noise and gradients) */
+#define SHWFS_STAGE_POST 3     /* (d)-(e) noise and gradients after the tensor-core imaging */
+#define SHWFS_NSTAGE 4
 int shwfs_profile_enable(shwfs_ctx* ctx, int enable);
 /* Waits for queued work, then returns per stage the summed device time (ms)
    and the number of kernel launches since the previous read, and resets. */

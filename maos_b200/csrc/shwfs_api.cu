@@ -871,7 +871,6 @@ static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist
 	const int nitem = p.d.nsa * nw;
 	const int nblk = (nitem + 3) / 4;
 	const int npix = P.npix;
-	StageMark mark(ctx, SHWFS_STAGE_INTS);
 	const WfsDev* wdev = ctx->wfsdev.p + off;
 	if (ctx->form == SHWFS_FORM_TC) {
 		if (!p.tc_ready) {
@@ -899,19 +898,23 @@ static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist
 		// persistent: TC_CTAS_PER_SM CTAs of TC_GROUPS tile groups per SM
 		const int ntile = (nitem + 3) / 4;
 		const int grid = std::min((ntile + TC_GROUPS - 1) / TC_GROUPS, tc_sm_count(ctx) * TC_CTAS_PER_SM);
-		if (any_out)
+		if (any_out) {
+			StageMark mark(ctx, SHWFS_STAGE_INTS);
 			ints_tc_kernel<<<grid, TC_THREADS, tc_smem_bytes(nlotf), ctx->stream>>>(P, wdev, nw, nitem, nlotf, T,
 				ctx->errflag.p);
+		}
 		CK(cudaGetLastError());
 		bool post = false;
 		for (int k = 0; k < nw; k++) post = post || (wd[k].ints && (wd[k].noisy || wd[k].grad));
 		if (post) {
+			StageMark mark(ctx, SHWFS_STAGE_POST);
 			if (npix <= 32) noise_grad_kernel<1><<<nblk, 128, 0, ctx->stream>>>(P, wdev, nw, nitem);
 			else noise_grad_kernel<2><<<nblk, 128, 0, ctx->stream>>>(P, wdev, nw, nitem);
 			CK(cudaGetLastError());
 		}
 		return 0;
 	}
+	StageMark mark(ctx, SHWFS_STAGE_INTS);
 	auto go = [&](auto kern) { kern<<<nblk, 128, 0, ctx->stream>>>(P, wdev, nw, nitem); };
 	const int v = p.variant;
 	if (npix <= 32) {

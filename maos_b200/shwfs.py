@@ -294,15 +294,15 @@ class Context:
     def set_variant(self, ipowfs: int, variant: int):
         self._check(self._L.shwfs_set_variant(self._h, ipowfs, variant), "set_variant")
 
-    STAGES = ("raytrace", "uplink", "ints")
+    STAGES = ("raytrace", "uplink", "ints", "post")
 
     def profile_enable(self, on: bool = True):
         self._check(self._L.shwfs_profile_enable(self._h, 1 if on else 0), "profile_enable")
 
     def profile_read(self):
         """{stage: (device ms summed, launches)} since the previous read."""
-        ms = (C.c_double * 3)()
-        n = (C.c_int * 3)()
+        ms = (C.c_double * len(self.STAGES))()
+        n = (C.c_int * len(self.STAGES))()
         self._check(self._L.shwfs_profile_read(self._h, ms, n), "profile_read")
         return {k: (ms[i], n[i]) for i, k in enumerate(self.STAGES)}
 
