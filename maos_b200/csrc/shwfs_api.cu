@@ -548,6 +548,7 @@ static int launch_geom(shwfs_ctx* ctx, GeomParams& all) {
 	return r;
 }
 
+
 static int launch_geom_wfs(shwfs_ctx* ctx, GeomParams& gp) {
 	int nitem = 0;
 	const int nopd = gp.nentry ? gp.e[0].nopd : 0;
@@ -565,7 +566,10 @@ static int launch_geom_wfs(shwfs_ctx* ctx, GeomParams& gp) {
 	}
 	{
 		StageMark m(ctx, SHWFS_STAGE_RAYTRACE);
-		geom_kernel<<<nblk, 256, 0, ctx->stream>>>(gp, nopd, nitem);
+		const size_t smem = (size_t)gp.nlayer * nopd * 2 * sizeof(int4);
+		if (smem > 160 * 1024) return fail(ctx, SHWFS_EINVAL, "ray trace: %d layers x %d points too large", gp.nlayer, nopd);
+		if (smem > 48 * 1024) CK(cudaFuncSetAttribute(geom_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+		geom_kernel<<<nblk, 256, smem, ctx->stream>>>(gp, nopd, nitem);
 	}
 	CK(cudaGetLastError());
 	return 0;

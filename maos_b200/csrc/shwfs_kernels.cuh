@@ -302,70 +302,59 @@ __device__ __forceinline__ void psf_to_otf_n32(float2 (&F)[32], float scale, flo
 // the points add their bilinear samples with FP32 in-subaperture offsets
 // (< nopd screen pixels).  A layer whose footprint lies inside the screen
 // skips the periodic-wrap arithmetic.
+// ---- ray trace (a) ----
+// The bilinear coordinates of point (ix, iy) in layer l are separable: the
+// column index and weight depend on ix only, the row on iy only.  Each block
+// (one subaperture, one OPD point per thread) first tabulates them per layer
+// in shared memory: nopd column entries and nopd row entries, each thread
+// computing one entry from the FP64 footprint origin (prop_grid_pts,
+// lib/accphi_grid_do.c:424-434) with the wrapped neighbour (wrap=1,
+// maos/sim_utils.c:1017).  A point then costs two table reads, four gathers
+// and the interpolation per layer.  The entries are the same FP32 quantities a
+// direct per-point evaluation forms, so the OPD is the same to the bit.
+// Dynamic shared memory: nlayer * nopd * 2 * 16 bytes.
+//   column entry ix: (jx, jx1, wx, -)      row entry iy: (jy nx, jy1 nx, wy, -)
 __global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomParams P, int nopd, int nitem) {
-	__shared__ int s_ix0[SHWFS_MAX_LAYERS], s_iy0[SHWFS_MAX_LAYERS], s_fast[SHWFS_MAX_LAYERS];
-	__shared__ float s_fx0[SHWFS_MAX_LAYERS], s_fy0[SHWFS_MAX_LAYERS], s_step[SHWFS_MAX_LAYERS];
+	extern __shared__ int4 s_tab[];
 	const int item = blockIdx.x;
 	if (item >= nitem) return;
 	int ie = 0;
 	while (ie + 1 < P.nentry && item >= P.e[ie + 1].item0) ie++;
 	const GeomEntry& E = P.e[ie];
 	const int isa = item - E.item0;
-	const int tid = threadIdx.x;
-	if (tid < P.nlayer) {
-		const int l = tid;
-		double x0 = E.origx[isa] * E.sx[l] + E.dispx[l];
-		double y0 = E.origy[isa] * E.sx[l] + E.dispy[l];
-		const int nx = P.nx[l], ny = P.ny[l];
-		if (!isfinite(x0) || !isfinite(y0)) {
+	const int tid = threadIdx.x, nl = P.nlayer;
+	for (int k = tid; k < nl * 2 * nopd; k += blockDim.x) {
+		const int l = k / (2 * nopd), r = k - l * 2 * nopd;
+		const bool isy = r >= nopd;
+		const int i = isy ? r - nopd : r;
+		const int n = isy ? P.ny[l] : P.nx[l];
+		double x0 = (isy ? E.origy[isa] : E.origx[isa]) * E.sx[l] + (isy ? E.dispy[l] : E.dispx[l]);
+		if (!isfinite(x0) || !isfinite((isy ? E.origx[isa] : E.origy[isa]) * E.sx[l] + (isy ? E.dispx[l] : E.dispy[l])))
 			x0 = 0;
-			y0 = 0;
-		}
-		x0 -= floor(x0 / nx) * nx;
-		y0 -= floor(y0 / ny) * ny;
-		int ix0 = (int)floor(x0), iy0 = (int)floor(y0);
-		const float fx0 = (float)(x0 - ix0), fy0 = (float)(y0 - iy0);
-		if (ix0 >= nx) ix0 -= nx;
-		if (iy0 >= ny) iy0 -= ny;
-		const float step = (float)(E.dx * E.sx[l]);
-		s_ix0[l] = ix0;
-		s_iy0[l] = iy0;
-		s_fx0[l] = fx0;
-		s_fy0[l] = fy0;
-		s_step[l] = step;
-		const float ext = (nopd - 1) * step + 2.f;
-		s_fast[l] = (ix0 + fx0 + ext < (float)(nx - 1)) && (iy0 + fy0 + ext < (float)(ny - 1));
+		x0 -= floor(x0 / n) * n;
+		int j0 = (int)floor(x0);
+		const float f0 = (float)(x0 - j0);
+		if (j0 >= n) j0 -= n;
+		const float f = f0 + i * (float)(E.dx * E.sx[l]);
+		const float fl = floorf(f);
+		int j = j0 + (int)fl;
+		while (j >= n) j -= n;
+		const int j1 = j == n - 1 ? 0 : j + 1;
+		const int m = isy ? P.nx[l] : 1;
+		s_tab[k] = make_int4(j * m, j1 * m, __float_as_int(f - fl), 0);
 	}
 	__syncthreads();
 	const int np = nopd * nopd;
-	for (int ip = tid; ip < np; ip += 256) {
+	for (int ip = tid; ip < np; ip += blockDim.x) {
 		const int ix = ip % nopd, iy = ip / nopd;
 		float acc = 0.f;
-		for (int l = 0; l < P.nlayer; l++) {
+		for (int l = 0; l < nl; l++) {
 			if (!((E.use >> l) & 1u)) continue;
-			const int nx = P.nx[l], ny = P.ny[l];
-			const float step = s_step[l];
-			const float xf = s_fx0[l] + ix * step, yf = s_fy0[l] + iy * step;
-			const float flx = floorf(xf), fly = floorf(yf);
-			const float wx = xf - flx, wy = yf - fly;
-			int jx = s_ix0[l] + (int)flx, jy = s_iy0[l] + (int)fly;
+			const int4 tx = s_tab[l * 2 * nopd + ix], ty = s_tab[l * 2 * nopd + nopd + iy];
 			const float* __restrict__ sc = P.screen[l];
-			float m00, m10, m01, m11;
-			if (s_fast[l]) {
-				const float* r0 = sc + (size_t)jy * nx + jx;
-				m00 = __ldg(r0);
-				m10 = __ldg(r0 + 1);
-				m01 = __ldg(r0 + nx);
-				m11 = __ldg(r0 + nx + 1);
-			} else {  // periodic wrap (data->wrap=1, maos/sim_utils.c:1017)
-				while (jx >= nx) jx -= nx;
-				while (jy >= ny) jy -= ny;
-				const int jx1 = jx == nx - 1 ? 0 : jx + 1, jy1 = jy == ny - 1 ? 0 : jy + 1;
-				m00 = __ldg(sc + jx + (size_t)nx * jy);
-				m10 = __ldg(sc + jx1 + (size_t)nx * jy);
-				m01 = __ldg(sc + jx + (size_t)nx * jy1);
-				m11 = __ldg(sc + jx1 + (size_t)nx * jy1);
-			}
+			const float m00 = __ldg(sc + (ty.x + tx.x)), m10 = __ldg(sc + (ty.x + tx.y));
+			const float m01 = __ldg(sc + (ty.y + tx.x)), m11 = __ldg(sc + (ty.y + tx.y));
+			const float wx = __int_as_float(tx.z), wy = __int_as_float(ty.z);
 			acc = fmaf(P.alpha[l], (m00 + (m10 - m00) * wx) * (1.f - wy) + (m01 + (m11 - m01) * wx) * wy, acc);
 		}
 		E.opd[(size_t)isa * np + ip] = acc;
