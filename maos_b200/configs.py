@@ -63,4 +63,42 @@ LGS30 = dict(
     dt=1.0 / 800,
 )
 
-CONFIGS = {c["name"]: c for c in (NGS8, LGS30)}
+# Large-sampling stress: the LGS sensors of LGS30 sampled at 1/64 m (32x32 OPD
+# points per subaperture), FFT 64, 12x12 pixels of 0.8", a two-Gaussian sodium
+# layer at 88 and 94 km, screens of 4096^2 at 1/64 m.
+LGS30_N64 = dict(
+    LGS30, name="lgs30_6x60x60_n64",
+    dx=1.0 / 64, notf=64, pixpsa=12, pixtheta=0.8 * AS2RAD,
+    sodium=dict(centers=[88e3, 94e3], fwhms=[5e3, 5e3], weights=[0.6, 0.4]),
+    atm=dict(LGS30["atm"], nx=4096, dx=1.0 / 64),
+)
+
+# Uneven batch members beside the LGS30 sensors: one NGS of 2x2 subapertures
+# (64x64 OPD points each, FFT 128, 16x16 pixels of 4 mas) and two tip-tilt
+# NGS of 1x1 (128x128 points, FFT 256), both at 1.65 um, CoG gradients.
+NGS30_2X2 = dict(
+    name="ngs30_2x2_n128",
+    D=30.0, Din=3.6, amp_binary=0,
+    order=2, dsa=15.0, dx=15.0 / 64, saat=0.3, embfac=2, notf=128,
+    pixpsa=16, pixtheta=0.004 * AS2RAD, pixblur=0.3, wvl=1.65e-6, hs=math.inf,
+    siglev=1000.0, rne=3.0, bkgrnd=0.0, bkgrndc=0.0,
+    phytype=2, sigmatch=1, mtchcr=0, cogthres=0.0, cogoff=0.0,
+    r0=0.186, L0=30.0,
+    has_llt=0, nwfs=1, thetax=[0.0], thetay=[0.0],
+    atm=LGS30["atm"], dt=1.0 / 800,
+)
+TT30 = dict(
+    NGS30_2X2, name="tt30_1x1_n256",
+    order=1, dsa=30.0, dx=30.0 / 128, notf=256,
+    nwfs=2, thetax=[30.0 * AS2RAD, -30.0 * AS2RAD], thetay=[0.0, 0.0],
+)
+
+# Reduced copies for parity tests (the reference's CPU frame in seconds): an
+# 8 m telescope with 8x8 LGS subapertures at the stress sampling.
+LGS8_N64 = dict(
+    LGS30_N64, name="lgs8_2x8x8_n64",
+    D=4.0, Din=0.5, order=8, llt_ox=2.0, nwfs=2, thetax=[10.0 * AS2RAD, -10.0 * AS2RAD], thetay=[0.0, 5.0 * AS2RAD],
+    atm=dict(LGS30["atm"], nx=512, dx=1.0 / 64),
+)
+
+CONFIGS = {c["name"]: c for c in (NGS8, LGS30, LGS30_N64, NGS30_2X2, TT30, LGS8_N64)}

@@ -17,6 +17,7 @@
 #include "../../include/shwfs_b200.h"
 #include "shwfs_kernels.cuh"
 #include "shwfs_tc.cuh"
+#include "shwfs_gen.cuh"
 
 using namespace shwfs;
 
@@ -52,6 +53,7 @@ struct PowfsState {
 	std::vector<int> simap_idx_h;     // host copies of the pixel map (TC tables)
 	std::vector<double> simap_wt_h;
 	DevBuf<uint4> tc_bmat;            // tensor-core B operands (bf16 images)
+	DevBuf<float2> gen_buf, gen_lbuf, gen_tw;  // generic-size chain: scratch images (WFS, LLT), twiddles
 	int tc_ready = 0;
 	std::vector<double> origx_h, origy_h;
 };
@@ -234,6 +236,9 @@ int shwfs_destroy(shwfs_ctx* ctx) {
 		p.lltamp.free_();
 		p.lltorig.free_();
 		p.tc_bmat.free_();
+		p.gen_buf.free_();
+		p.gen_lbuf.free_();
+		p.gen_tw.free_();
 	}
 	for (auto& w : ctx->wfs) {
 		w.mtche.free_();
@@ -286,17 +291,22 @@ int shwfs_powfs_add(shwfs_ctx* ctx, const shwfs_powfs_desc* d, int* ipowfs) {
 	if (d->nsa <= 0 || d->nopd <= 0 || d->embfac <= 0 || d->notf <= 0 || d->pixpsax <= 0 || d->pixpsay <= 0)
 		return fail(ctx, SHWFS_EINVAL, "powfs: sizes must be positive");
 	const int nw = d->nopd * d->embfac;
-	if (!(d->nopd == 16 && nw == 32 && d->notf == 32))
-		return fail(ctx, SHWFS_EINVAL, "powfs: n_opd=%d n_w=%d n_f=%d not supported by this build (16/32/32)", d->nopd, nw,
-			d->notf);
-	if (d->pixpsax * d->pixpsay > 128) return fail(ctx, SHWFS_EINVAL, "powfs: at most 128 pixels per subaperture");
+	const bool n32 = d->nopd == 16 && nw == 32 && d->notf == 32;
+	const bool gen = nw == d->notf && (d->notf == 64 || d->notf == 128 || d->notf == 256);
+	if (!n32 && !gen)
+		return fail(ctx, SHWFS_EINVAL,
+			"powfs: n_opd=%d n_w=%d n_f=%d not supported by this build (16/32/32, or n_w = n_f in {64, 128, 256})",
+			d->nopd, nw, d->notf);
+	if (d->pixpsax * d->pixpsay > (n32 ? 128 : 256))
+		return fail(ctx, SHWFS_EINVAL, "powfs: at most %d pixels per subaperture", n32 ? 128 : 256);
 	if (d->gradtype != SHWFS_GRAD_MF && d->gradtype != SHWFS_GRAD_COG)
 		return fail(ctx, SHWFS_EINVAL, "powfs: gradtype must be SHWFS_GRAD_MF or SHWFS_GRAD_COG");
 	if (d->sigmatch < 0 || d->sigmatch > 2) return fail(ctx, SHWFS_EINVAL, "powfs: sigmatch must be 0, 1 or 2");
 	if (d->has_llt && d->llt_nx != d->nopd)
 		return fail(ctx, SHWFS_EINVAL, "powfs: LLT pupil sampling (%d) must equal the subaperture's (%d)", d->llt_nx, d->nopd);
-	if (d->has_llt && d->llt_nx * d->embfac != 32)
-		return fail(ctx, SHWFS_EINVAL, "powfs: LLT pupil of %d points is not supported (needs %d)", d->llt_nx, 32 / d->embfac);
+	if (d->has_llt && d->llt_nx * d->embfac != d->notf)
+		return fail(ctx, SHWFS_EINVAL, "powfs: LLT pupil of %d points is not supported (needs %d)", d->llt_nx,
+			d->notf / d->embfac);
 	int r = set_device(ctx);
 	if (r) return r;
 	ctx->powfs.emplace_back();
@@ -589,6 +599,7 @@ static int add_llt_entry(shwfs_ctx* ctx, GeomParams& gp, WfsState& w, int isim) 
 	int r = add_geom_entry(ctx, gp, w.d.thetax - p.d.llt_ox / w.d.hs, w.d.thetay - p.d.llt_oy / w.d.hs, w.d.hs, 0, 0,
 		0, p.d.llt_ox, p.d.llt_oy, isim, p.lltorig.p, p.lltorig.p + 1, 1, p.d.llt_nx, p.d.dx, w.lltopd.p);
 	if (r) return r;
+	if (p.d.notf != 32) return 0;  // the uplink OTF follows from the traced OPD (launch_uplink_gen)
 	GeomEntry& e = gp.e[gp.nentry - 1];
 	e.lltamp = p.lltamp.p;
 	e.lotfT = w.lotfT.p;
@@ -814,6 +825,109 @@ static int tc_sm_count(shwfs_ctx* ctx) {
 	return v;
 }
 
+// Per-launch WFS descriptors live in a device ring so that queued launches
+// never see them overwritten.
+static int push_wfsdev(shwfs_ctx* ctx, const std::vector<WfsDev>& wd, const WfsDev** out) {
+	const size_t nw = wd.size();
+	const size_t need = ctx->wfsdev_h.size() + nw;
+	if (ctx->wfsdev.n < need) {
+		CK(cudaStreamSynchronize(ctx->stream));
+		ctx->wfsdev_h.clear();
+		int r = dev_alloc(ctx, ctx->wfsdev, need < 4096 ? 4096 : need * 2);
+		if (r) return r;
+	}
+	if (ctx->wfsdev_h.size() + nw > ctx->wfsdev.n) {
+		CK(cudaStreamSynchronize(ctx->stream));
+		ctx->wfsdev_h.clear();
+	}
+	const size_t off = ctx->wfsdev_h.size();
+	ctx->wfsdev_h.insert(ctx->wfsdev_h.end(), wd.begin(), wd.end());
+	CK(cudaMemcpyAsync(ctx->wfsdev.p + off, wd.data(), sizeof(WfsDev) * nw, cudaMemcpyHostToDevice, ctx->stream));
+	ctx->h2d_bytes += sizeof(WfsDev) * nw;
+	*out = ctx->wfsdev.p + off;
+	return 0;
+}
+
+// The generic-size chain (n_f = n_w = N in {64, 128, 256}): FFT passes over
+// the scratch buf (nitem N^2), WFS or uplink mode.
+template <int N>
+static int launch_gen_n(shwfs_ctx* ctx, PowfsState& p, GenParams& G) {
+	const size_t smem = ((size_t)GEN_LINES * (N + 1) + N / 2) * sizeof(float2);
+	const dim3 full(G.nitem, N / GEN_LINES), field(G.nitem, (G.nopd + GEN_LINES - 1) / GEN_LINES);
+	gen_pass_kernel<N, GEN_FIELD_ROWS><<<field, GEN_THREADS, smem, ctx->stream>>>(G);
+	gen_pass_kernel<N, GEN_PSF_COLS><<<full, GEN_THREADS, smem, ctx->stream>>>(G);
+	gen_pass_kernel<N, GEN_OTF_ROWS><<<full, GEN_THREADS, smem, ctx->stream>>>(G);
+	gen_pass_kernel<N, GEN_OTF_COLS><<<full, GEN_THREADS, smem, ctx->stream>>>(G);
+	if (!G.uplink) {
+		gen_pass_kernel<N, GEN_INV_ROWS><<<full, GEN_THREADS, smem, ctx->stream>>>(G);
+		gen_pass_kernel<N, GEN_INV_COLS><<<full, GEN_THREADS, smem, ctx->stream>>>(G);
+	}
+	CK(cudaGetLastError());
+	(void)p;
+	return 0;
+}
+
+static int launch_gen(shwfs_ctx* ctx, PowfsState& p, const WfsDev* wdev, int nw, int nitem, int uplink,
+	DevBuf<float2>& buf, const PowfsDev& P) {
+	const int N = p.d.notf;
+	int r;
+	if (!p.gen_tw.p) {
+		std::vector<float2> tw(N / 2);
+		for (int k = 0; k < N / 2; k++) tw[k] = make_float2((float)cos(2 * M_PI * k / N), (float)-sin(2 * M_PI * k / N));
+		if ((r = dev_upload(ctx, p.gen_tw, tw.data(), tw.size()))) return r;
+	}
+	if (buf.n < (size_t)nitem * N * N) {
+		CK(cudaStreamSynchronize(ctx->stream));
+		if ((r = dev_alloc(ctx, buf, (size_t)nitem * N * N))) return r;
+	}
+	GenParams G;
+	memset(&G, 0, sizeof(G));
+	G.nitem = nitem;
+	G.nw = nw;
+	G.nopd = uplink ? p.d.llt_nx : p.d.nopd;
+	G.pad = (N - G.nopd) / 2;
+	G.uplink = uplink;
+	G.scale = uplink ? (float)(1.0 / ((double)N * N)) : 1.f;
+	G.twoinvwvl = (float)(2.0 / p.d.wvl);
+	G.buf = buf.p;
+	G.tw = p.gen_tw.p;
+	G.wfs = wdev;
+	if (!uplink) {
+		G.etfT1 = P.etfT1;
+		G.etfT2 = P.etfT2;
+		G.etfwt1 = P.etfwt1;
+		G.etfwt2 = P.etfwt2;
+		G.nominalT = P.nominalT;
+		G.nominal_per_sa = P.nominal_per_sa;
+	}
+	switch (N) {
+	case 64: return launch_gen_n<64>(ctx, p, G);
+	case 128: return launch_gen_n<128>(ctx, p, G);
+	case 256: return launch_gen_n<256>(ctx, p, G);
+	default: return fail(ctx, SHWFS_EINVAL, "no imaging path for n_f = %d", N);
+	}
+}
+
+// Uplink OTFs of the LLT pupils of a generic-size powfs from their traced
+// OPDs (maos/wfsints.c:149-199).
+static int launch_uplink_gen(shwfs_ctx* ctx, PowfsState& p, const std::vector<int>& wlist,
+	const std::vector<const float*>& lltopd) {
+	std::vector<WfsDev> wd(wlist.size());
+	for (size_t k = 0; k < wlist.size(); k++) {
+		memset(&wd[k], 0, sizeof(WfsDev));
+		wd[k].opd = lltopd[k];
+		wd[k].amp = p.lltamp.p;
+		wd[k].lotfT = ctx->wfs[wlist[k]].lotfT.p;
+	}
+	const WfsDev* wdev = nullptr;
+	int r = push_wfsdev(ctx, wd, &wdev);
+	if (r) return r;
+	PowfsDev P;
+	memset(&P, 0, sizeof(P));
+	StageMark m(ctx, SHWFS_STAGE_UPLINK);
+	return launch_gen(ctx, p, wdev, (int)wlist.size(), (int)wlist.size(), 1, p.gen_lbuf, P);
+}
+
 // (b)-(e) for a set of WFS of one powfs sharing the launch.
 static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist, int isim,
 	const std::vector<const float*>& opds, const std::vector<const float2*>& lotfs, const std::vector<float*>& ints,
@@ -855,27 +969,26 @@ static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist
 		d.wfs_id = (uint32_t)wlist[k];
 		d.seed = w.seed;
 	}
-	// per-launch descriptors live in a device ring so queued launches never
-	// see them overwritten
-	const size_t need = ctx->wfsdev_h.size() + nw;
-	if (ctx->wfsdev.n < need) {
-		CK(cudaStreamSynchronize(ctx->stream));
-		ctx->wfsdev_h.clear();
-		int r = dev_alloc(ctx, ctx->wfsdev, need < 4096 ? 4096 : need * 2);
+	const WfsDev* wdev = nullptr;
+	{
+		int r = push_wfsdev(ctx, wd, &wdev);
 		if (r) return r;
 	}
-	if (ctx->wfsdev_h.size() + nw > ctx->wfsdev.n) {
-		CK(cudaStreamSynchronize(ctx->stream));
-		ctx->wfsdev_h.clear();
-	}
-	const size_t off = ctx->wfsdev_h.size();
-	ctx->wfsdev_h.insert(ctx->wfsdev_h.end(), wd.begin(), wd.end());
-	CK(cudaMemcpyAsync(ctx->wfsdev.p + off, wd.data(), sizeof(WfsDev) * nw, cudaMemcpyHostToDevice, ctx->stream));
-	ctx->h2d_bytes += sizeof(WfsDev) * nw;
 	const int nitem = p.d.nsa * nw;
 	const int nblk = (nitem + 3) / 4;
 	const int npix = P.npix;
-	const WfsDev* wdev = ctx->wfsdev.p + off;
+	if (p.d.notf != 32) {  // generic sizes: FFT passes, then pixels, noise and gradients
+		StageMark mark(ctx, SHWFS_STAGE_INTS);
+		int r = launch_gen(ctx, p, wdev, nw, nitem, 0, p.gen_buf, P);
+		if (r) return r;
+		const int n2 = p.d.notf * p.d.notf;
+		if (npix <= 32) gen_pixels_kernel<1><<<nblk, 128, 0, ctx->stream>>>(P, wdev, nw, nitem, p.gen_buf.p, n2);
+		else if (npix <= 64) gen_pixels_kernel<2><<<nblk, 128, 0, ctx->stream>>>(P, wdev, nw, nitem, p.gen_buf.p, n2);
+		else if (npix <= 128) gen_pixels_kernel<4><<<nblk, 128, 0, ctx->stream>>>(P, wdev, nw, nitem, p.gen_buf.p, n2);
+		else gen_pixels_kernel<8><<<nblk, 128, 0, ctx->stream>>>(P, wdev, nw, nitem, p.gen_buf.p, n2);
+		CK(cudaGetLastError());
+		return 0;
+	}
 	if (ctx->form == SHWFS_FORM_TC) {
 		if (!p.tc_ready) {
 			int r = build_tc_tables(ctx, p);
@@ -943,6 +1056,10 @@ static int launch_uplink(shwfs_ctx* ctx, const std::vector<int>& wlist, const st
 	if (wlist.empty()) return 0;
 	PowfsState& p = ctx->powfs[ctx->wfs[wlist[0]].d.ipowfs];
 	const int nw = (int)wlist.size();
+	if (p.d.notf != 32) {
+		for (int k = 0; k < nw; k++) lotfs[k] = ctx->wfs[wlist[k]].lotfT.p;
+		return launch_uplink_gen(ctx, p, wlist, lltopd);
+	}
 	std::vector<const float*> in(nw);
 	std::vector<float2*> out(nw);
 	for (int k = 0; k < nw; k++) {
@@ -1063,6 +1180,15 @@ int shwfs_frame_queue(shwfs_ctx* ctx, int isim, int iwfs0, int iwfs1) {
 				if (p.d.has_llt && (r = add_llt_entry(ctx, gp, w, isim))) return r;
 			}
 			if ((r = launch_geom(ctx, gp))) return r;
+			if (p.d.has_llt && p.d.notf != 32) {
+				std::vector<int> bw;
+				std::vector<const float*> lo;
+				for (size_t k = b; k < wl.size() && k < b + per; k++) {
+					bw.push_back(wl[k]);
+					lo.push_back(ctx->wfs[wl[k]].lltopd.p);
+				}
+				if ((r = launch_uplink_gen(ctx, p, bw, lo))) return r;
+			}
 		}
 		// (b)-(e)
 		std::vector<const float*> opds;

@@ -5,7 +5,7 @@ screens are compared bit for bit."""
 import numpy as np
 import pytest
 
-from maos_b200.configs import NGS8, LGS30
+from maos_b200.configs import NGS8, LGS30, LGS8_N64, NGS30_2X2, TT30
 
 
 def _setup(cfg):
@@ -13,7 +13,7 @@ def _setup(cfg):
     return Setup(cfg)
 
 
-@pytest.mark.parametrize("cfg", [NGS8, LGS30], ids=lambda c: c["name"])
+@pytest.mark.parametrize("cfg", [NGS8, LGS30, LGS8_N64, NGS30_2X2, TT30], ids=lambda c: c["name"])
 def test_geometry_bit_exact(ref_lib, cfg):
     r = ref_lib.RefPowfs(cfg)
     s = _setup(cfg)
@@ -26,7 +26,7 @@ def test_geometry_bit_exact(ref_lib, cfg):
     assert np.array_equal(r.saa(), s.get("saa"))
 
 
-@pytest.mark.parametrize("cfg", [NGS8, LGS30], ids=lambda c: c["name"])
+@pytest.mark.parametrize("cfg", [NGS8, LGS30, LGS8_N64, NGS30_2X2, TT30], ids=lambda c: c["name"])
 def test_dtf_and_pixel_map_bit_exact(ref_lib, cfg):
     from oracle.ref import si_to_taps
     r = ref_lib.RefPowfs(cfg)
