@@ -362,6 +362,122 @@ def run_b200(args, cfg):
     return 0
 
 
+def run_batch(args, bcfg):
+    """The uneven batch: every member's WFS in one frame, replayed as one CUDA graph."""
+    import torch
+    from maos_b200 import shwfs
+    from maos_b200.workload import build_batch
+    ws, rank, local = dist_init()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    form = shwfs.SHWFS_FORM_TC if args.form == "tc" else shwfs.SHWFS_FORM_FFT
+    wl = build_batch(bcfg["members"], device=local, seed=1 + rank, noisy=True, form=form, graph=True)
+    ctx = wl.ctx
+    units_per_step = wl.images_per_frame
+    ext = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    lgs = wl.members[0]
+    variant = ctx.autotune(lgs[3][0], lgs[3][-1] + 1, nrep=5)
+    isim = 0
+    for _ in range(args.warmup):
+        wl.frame(isim)
+        isim += 1
+    ctx.sync()
+    barrier(ws, dev)
+    clk = ClockSampler(local)
+    clk.start()
+    time.sleep(0.5)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with torch.cuda.stream(ext):
+        for k in range(args.steps):
+            flush.zero_()  # L2 flush between timed steps (not timed)
+            starts[k].record(ext)
+            wl.frame(isim)
+            ends[k].record(ext)
+            isim += 1
+    ctx.sync()
+    torch.cuda.synchronize(dev)
+    clocks = clk.stop()
+    step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
+    tot_ms = allreduce_max(sum(step_ms), ws, dev)
+    barrier(ws, dev)
+    value = units_per_step * args.steps * ws / (tot_ms * 1e-3)
+    # stage timing (stream frames, profiling on; stages summed over the members)
+    wl.graph = False
+    ctx.profile_enable(True)
+    nprof = min(args.steps, 20)
+    with torch.cuda.stream(ext):
+        for k in range(nprof):
+            flush.zero_()
+            wl.frame(isim)
+            isim += 1
+    ctx.sync()
+    stages = ctx.profile_read()
+    ctx.profile_enable(False)
+    wl.graph = True
+    launches_per_step = sum(n for _, n in stages.values()) / nprof
+    st = {k: dict(ms_per_launch=(ms / n if n else 0.0), launches_per_step=n / nprof, ms_per_step=ms / nprof)
+          for k, (ms, n) in stages.items()}
+    # end to end: graph frame + host gradients of every WFS
+    ctx.copy_counters()
+    e2e_s = 0.0
+    for k in range(args.steps):
+        with torch.cuda.stream(ext):
+            flush.zero_()
+        ctx.sync()
+        t0 = time.perf_counter()
+        wl.frame(isim)
+        wl.frame_sync()
+        e2e_s += time.perf_counter() - t0
+        isim += 1
+    h2d, d2h = ctx.copy_counters()
+    e2e_s = allreduce_max(e2e_s, ws, dev)
+    e2e = units_per_step * args.steps * ws / e2e_s
+    hbm, bf16, src = _peaks()
+    lcfg = lgs[0]
+    nlayer = len(lcfg["atm"]["ht"])
+    ray_bytes = sum(m[1].nsa * len(m[3]) * m[1].nopd ** 2 * (nlayer * 4 + 4) for m in wl.members)
+    ray_ms = st["raytrace"]["ms_per_step"]
+    ray_gbs = ray_bytes / (ray_ms * 1e-3) / 1e9 if ray_ms else 0.0
+    members = [{"workload": m[0]["name"], "wfs": len(m[3]), "subapertures_per_wfs": m[1].nsa,
+                "opd_points": m[1].nopd, "fft": m[1].notf, "pixels": m[1].npix} for m in wl.members]
+    p50 = float(np.percentile(step_ms, 50))
+    p99 = float(np.percentile(step_ms, 99))
+    line = {
+        "metric": "subaperture images/s", "value": value, "unit": "subap-images/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": bcfg["name"], "members": members, "layers": nlayer,
+                   "screen": f"{lcfg['atm']['nx']}^2 FP32", "form": args.form, "noise": True,
+                   "frame": "one CUDA graph per frame, one branch per sensor type", "imaging_variant": variant,
+                   "l2": "flushed (256 MiB write) before every timed step", "parallelism": f"replicas x{ws}"},
+        "frame_latency_ms": {"p50": p50, "p99": p99},
+        "stages": st,
+        "gpu_launches": int(round(launches_per_step * args.steps)),
+        "e2e": {"value": e2e, "unit": "subap-images/s", "h2d_bytes_per_step": h2d // args.steps,
+                "d2h_bytes_per_step": d2h // args.steps},
+        "roofline": {"kernel": "geom_kernel (ray trace of all members)", "bound": "hbm", "achieved": ray_gbs,
+                     "peak": hbm, "unit": "GB/s", "frac": ray_gbs / hbm, "traffic": None,
+                     "peak_source": (f"{src} (MEASURED_PEAKS.json) hbm_gbs" if src == "measured" else "fallback"),
+                     "algorithmic_bytes_per_step": ray_bytes},
+        "clocks": clocks,
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(lcfg, wl.layers, wl.screens)
+            line["cpu_baseline"]["sample"] += " (the batch's dominant member)"
+        except Exception as e:
+            line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+    if rank == 0:
+        print(json.dumps(line))
+    wl.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -372,10 +488,15 @@ def main():
     ap.add_argument("--form", default="fft", choices=["fft", "tc"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
-    from maos_b200.configs import CONFIGS
-    cfg = CONFIGS[args.config]
+    from maos_b200.configs import CONFIGS, BATCHES
     if args.warmup < 3:
         args.warmup = 3
+    if args.config in BATCHES:
+        bcfg = BATCHES[args.config]
+        if args.impl == "reference":
+            return run_reference(args, bcfg["members"][0])
+        return run_batch(args, bcfg)
+    cfg = CONFIGS[args.config]
     if args.impl == "reference":
         return run_reference(args, cfg)
     return run_b200(args, cfg)

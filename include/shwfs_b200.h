@@ -160,6 +160,15 @@ int shwfs_frame_queue(shwfs_ctx* ctx, int isim, int iwfs0, int iwfs1);
 /* Wait for the queued frame and copy WFS iwfs's gradients (2*nsa: x then y)
    and optionally its pixel intensities (nsa*npix) to host memory. */
 int shwfs_frame_sync(shwfs_ctx* ctx, int iwfs, double* grad, double* ints);
+/* The frame of shwfs_frame_queue as one CUDA graph: the first call for a WFS
+   range runs the frame normally (allocations, descriptor uploads, stream
+   branches); later calls capture the frame's launches, update the
+   instantiated graph with this frame's parameters and launch it.  The WFS of
+   several powfs run as parallel branches of the graph.  Results are read
+   with shwfs_frame_sync as after shwfs_frame_queue.  Stage profiling must be
+   off.  Replaces the per-WFS gpu_wfsgrad_queue threads of
+   cuda/sim/gpu_sim.h:45 for a whole frame. */
+int shwfs_frame_graph(shwfs_ctx* ctx, int isim, int iwfs0, int iwfs1);
 
 /* ---- stage entry points (device pointers; used by callers that hold the
         OPD already, and by the parity tests) ---- */

@@ -102,3 +102,8 @@ LGS8_N64 = dict(
 )
 
 CONFIGS = {c["name"]: c for c in (NGS8, LGS30, LGS30_N64, NGS30_2X2, TT30, LGS8_N64)}
+
+# The uneven batch: six LGS of LGS30 (FFT 32), the 2x2 NGS (FFT 128) and the
+# two tip-tilt sensors (FFT 256) in one frame, on the LGS30 atmosphere.
+UNEVEN_BATCH = dict(name="uneven_batch_lgs6_ngs1_tt2", members=[LGS30, NGS30_2X2, TT30])
+BATCHES = {UNEVEN_BATCH["name"]: UNEVEN_BATCH}

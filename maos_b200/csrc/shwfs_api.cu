@@ -90,6 +90,21 @@ struct shwfs_ctx {
 	int form = SHWFS_FORM_FFT;
 	DevBuf<WfsDev> wfsdev;  // staging for per-launch WFS descriptors
 	std::vector<WfsDev> wfsdev_h;
+	// frame path: descriptors that repeat from frame to frame are uploaded once
+	// and served from here (no host-to-device copy, nothing to synchronise)
+	struct DescCache {
+		std::vector<WfsDev> h;
+		DevBuf<WfsDev> d;
+	};
+	std::vector<DescCache> desc_cache;
+	int cache_desc = 0;
+	// one stream branch per powfs of a frame, forked from and joined to `stream`
+	std::vector<cudaStream_t> pstream;
+	std::vector<cudaEvent_t> ev_pfork, ev_pjoin;
+	// CUDA graph of a frame (shwfs_frame_graph)
+	cudaGraphExec_t gexec = nullptr;
+	int g_i0 = -1, g_i1 = -1, g_warm = 0;
+	int capturing = 0;
 	DevBuf<const float*> llt_in;
 	DevBuf<float2*> llt_out;
 	DevBuf<int> errflag;                 // bounded device waits record expiry here
@@ -239,6 +254,14 @@ int shwfs_destroy(shwfs_ctx* ctx) {
 		p.gen_buf.free_();
 		p.gen_lbuf.free_();
 		p.gen_tw.free_();
+	}
+	for (auto& c : ctx->desc_cache) c.d.free_();
+	if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+	for (size_t i = 0; i < ctx->pstream.size(); i++) {
+		cudaStreamSynchronize(ctx->pstream[i]);
+		cudaStreamDestroy(ctx->pstream[i]);
+		cudaEventDestroy(ctx->ev_pfork[i]);
+		cudaEventDestroy(ctx->ev_pjoin[i]);
 	}
 	for (auto& w : ctx->wfs) {
 		w.mtche.free_();
@@ -579,7 +602,8 @@ static int launch_geom_wfs(shwfs_ctx* ctx, GeomParams& gp) {
 		const size_t smem = (size_t)gp.nlayer * nopd * 2 * sizeof(int4);
 		if (smem > 160 * 1024) return fail(ctx, SHWFS_EINVAL, "ray trace: %d layers x %d points too large", gp.nlayer, nopd);
 		if (smem > 48 * 1024) CK(cudaFuncSetAttribute(geom_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-		geom_kernel<<<nblk, 256, smem, ctx->stream>>>(gp, nopd, nitem);
+		const int bps = (nopd * nopd + 255) / 256;  // blocks per subaperture
+		geom_kernel<<<(unsigned)nblk * bps, 256, smem, ctx->stream>>>(gp, nopd, nitem, bps);
 	}
 	CK(cudaGetLastError());
 	return 0;
@@ -827,17 +851,43 @@ static int tc_sm_count(shwfs_ctx* ctx) {
 
 // Per-launch WFS descriptors live in a device ring so that queued launches
 // never see them overwritten.
+static int sync_all_streams(shwfs_ctx* ctx) {
+	CK(cudaStreamSynchronize(ctx->stream));
+	if (ctx->aux) CK(cudaStreamSynchronize(ctx->aux));
+	for (cudaStream_t s : ctx->pstream) CK(cudaStreamSynchronize(s));
+	return 0;
+}
+static const size_t DESC_CACHE_MAX = 64;
+
 static int push_wfsdev(shwfs_ctx* ctx, const std::vector<WfsDev>& wd, const WfsDev** out) {
 	const size_t nw = wd.size();
+	if (ctx->cache_desc) {
+		for (auto& c : ctx->desc_cache)
+			if (c.h.size() == nw && !memcmp(c.h.data(), wd.data(), sizeof(WfsDev) * nw)) {
+				*out = c.d.p;
+				return 0;
+			}
+		if (ctx->capturing) return fail(ctx, SHWFS_ESTATE, "frame graph: descriptors changed since the warm-up frame");
+		if (ctx->desc_cache.size() < DESC_CACHE_MAX) {
+			ctx->desc_cache.emplace_back();
+			auto& c = ctx->desc_cache.back();
+			c.h = wd;
+			int r = dev_upload(ctx, c.d, wd.data(), nw);
+			if (r) return r;
+			*out = c.d.p;
+			return 0;
+		}
+	}
+	if (ctx->capturing) return fail(ctx, SHWFS_ESTATE, "frame graph: no cached descriptors");
 	const size_t need = ctx->wfsdev_h.size() + nw;
 	if (ctx->wfsdev.n < need) {
-		CK(cudaStreamSynchronize(ctx->stream));
+		if (int r = sync_all_streams(ctx)) return r;
 		ctx->wfsdev_h.clear();
 		int r = dev_alloc(ctx, ctx->wfsdev, need < 4096 ? 4096 : need * 2);
 		if (r) return r;
 	}
 	if (ctx->wfsdev_h.size() + nw > ctx->wfsdev.n) {
-		CK(cudaStreamSynchronize(ctx->stream));
+		if (int r = sync_all_streams(ctx)) return r;
 		ctx->wfsdev_h.clear();
 	}
 	const size_t off = ctx->wfsdev_h.size();
@@ -852,8 +902,9 @@ static int push_wfsdev(shwfs_ctx* ctx, const std::vector<WfsDev>& wd, const WfsD
 // the scratch buf (nitem N^2), WFS or uplink mode.
 template <int N>
 static int launch_gen_n(shwfs_ctx* ctx, PowfsState& p, GenParams& G) {
-	const size_t smem = ((size_t)GEN_LINES * (N + 1) + N / 2) * sizeof(float2);
-	const dim3 full(G.nitem, N / GEN_LINES), field(G.nitem, (G.nopd + GEN_LINES - 1) / GEN_LINES);
+	constexpr int L = gen_lines(N);
+	const size_t smem = ((size_t)L * (N + 1) + N / 2) * sizeof(float2);
+	const dim3 full(G.nitem, N / L), field(G.nitem, (G.nopd + L - 1) / L);
 	gen_pass_kernel<N, GEN_FIELD_ROWS><<<field, GEN_THREADS, smem, ctx->stream>>>(G);
 	gen_pass_kernel<N, GEN_PSF_COLS><<<full, GEN_THREADS, smem, ctx->stream>>>(G);
 	gen_pass_kernel<N, GEN_OTF_ROWS><<<full, GEN_THREADS, smem, ctx->stream>>>(G);
@@ -1155,56 +1206,155 @@ int shwfs_addnoise_dev(shwfs_ctx* ctx, float* ints, long n, const float* bkgrnd2
 	return 0;
 }
 
+// The work of one powfs in a frame: ray trace (and uplink), then imaging.
+static int frame_powfs(shwfs_ctx* ctx, int ip, const std::vector<int>& wl, int isim) {
+	PowfsState& p = ctx->powfs[ip];
+	int r;
+	// (a) one ray-trace launch per batch of pupils (WFS + LLT)
+	const int per = p.d.has_llt ? SHWFS_MAX_ENTRIES / 2 : SHWFS_MAX_ENTRIES;
+	for (size_t b = 0; b < wl.size(); b += per) {
+		GeomParams gp;
+		geom_init(ctx, gp);
+		for (size_t k = b; k < wl.size() && k < b + per; k++) {
+			WfsState& w = ctx->wfs[wl[k]];
+			if ((r = add_wfs_entry(ctx, gp, w, isim, w.opd.p))) return r;
+			if (p.d.has_llt && (r = add_llt_entry(ctx, gp, w, isim))) return r;
+		}
+		if ((r = launch_geom(ctx, gp))) return r;
+		if (p.d.has_llt && p.d.notf != 32) {
+			std::vector<int> bw;
+			std::vector<const float*> lo;
+			for (size_t k = b; k < wl.size() && k < b + per; k++) {
+				bw.push_back(wl[k]);
+				lo.push_back(ctx->wfs[wl[k]].lltopd.p);
+			}
+			if ((r = launch_uplink_gen(ctx, p, bw, lo))) return r;
+		}
+	}
+	// (b)-(e)
+	std::vector<const float*> opds;
+	std::vector<const float2*> lotf;
+	std::vector<float*> in, gr;
+	std::vector<int> nz;
+	for (int i : wl) {
+		WfsState& w = ctx->wfs[i];
+		opds.push_back(w.opd.p);
+		lotf.push_back(p.d.has_llt ? w.lotfT.p : nullptr);
+		in.push_back(w.ints.p);
+		gr.push_back(w.grad.p);
+		nz.push_back(w.d.noisy);
+	}
+	return launch_ints(ctx, ip, wl, isim, opds, lotf, in, gr, nz);
+}
+
+static int ensure_branches(shwfs_ctx* ctx) {
+	while (ctx->pstream.size() < ctx->powfs.size()) {
+		cudaStream_t st;
+		cudaEvent_t a, b;
+		CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+		CK(cudaEventCreateWithFlags(&a, cudaEventDisableTiming));
+		CK(cudaEventCreateWithFlags(&b, cudaEventDisableTiming));
+		ctx->pstream.push_back(st);
+		ctx->ev_pfork.push_back(a);
+		ctx->ev_pjoin.push_back(b);
+	}
+	return 0;
+}
+
 int shwfs_frame_queue(shwfs_ctx* ctx, int isim, int iwfs0, int iwfs1) {
 	if (!ctx || iwfs0 < 0 || iwfs1 > (int)ctx->wfs.size() || iwfs0 >= iwfs1)
 		return ctx ? fail(ctx, SHWFS_EINVAL, "frame_queue: bad WFS range") : SHWFS_EINVAL;
 	int r = set_device(ctx);
 	if (r) return r;
+	std::vector<std::vector<int>> wl(ctx->powfs.size());
+	int nbranch = 0;
 	for (size_t ip = 0; ip < ctx->powfs.size(); ip++) {
-		PowfsState& p = ctx->powfs[ip];
-		std::vector<int> wl;
 		for (int i = iwfs0; i < iwfs1; i++)
 			if (ctx->wfs[i].d.ipowfs == (int)ip) {
-				if ((r = check_ready(ctx, p, ctx->wfs[i]))) return r;
-				wl.push_back(i);
+				if ((r = check_ready(ctx, ctx->powfs[ip], ctx->wfs[i]))) return r;
+				wl[ip].push_back(i);
 			}
-		if (wl.empty()) continue;
-		// (a) one ray-trace launch per batch of pupils (WFS + LLT)
-		const int per = p.d.has_llt ? SHWFS_MAX_ENTRIES / 2 : SHWFS_MAX_ENTRIES;
-		for (size_t b = 0; b < wl.size(); b += per) {
-			GeomParams gp;
-			geom_init(ctx, gp);
-			for (size_t k = b; k < wl.size() && k < b + per; k++) {
-				WfsState& w = ctx->wfs[wl[k]];
-				if ((r = add_wfs_entry(ctx, gp, w, isim, w.opd.p))) return r;
-				if (p.d.has_llt && (r = add_llt_entry(ctx, gp, w, isim))) return r;
-			}
-			if ((r = launch_geom(ctx, gp))) return r;
-			if (p.d.has_llt && p.d.notf != 32) {
-				std::vector<int> bw;
-				std::vector<const float*> lo;
-				for (size_t k = b; k < wl.size() && k < b + per; k++) {
-					bw.push_back(wl[k]);
-					lo.push_back(ctx->wfs[wl[k]].lltopd.p);
-				}
-				if ((r = launch_uplink_gen(ctx, p, bw, lo))) return r;
-			}
-		}
-		// (b)-(e)
-		std::vector<const float*> opds;
-		std::vector<const float2*> lotf;
-		std::vector<float*> in, gr;
-		std::vector<int> nz;
-		for (int i : wl) {
-			WfsState& w = ctx->wfs[i];
-			opds.push_back(w.opd.p);
-			lotf.push_back(p.d.has_llt ? w.lotfT.p : nullptr);
-			in.push_back(w.ints.p);
-			gr.push_back(w.grad.p);
-			nz.push_back(w.d.noisy);
-		}
-		if ((r = launch_ints(ctx, (int)ip, wl, isim, opds, lotf, in, gr, nz))) return r;
+		if (!wl[ip].empty()) nbranch++;
 	}
+	ctx->cache_desc = 1;
+	if (nbranch <= 1) {
+		for (size_t ip = 0; ip < ctx->powfs.size() && !r; ip++)
+			if (!wl[ip].empty()) r = frame_powfs(ctx, (int)ip, wl[ip], isim);
+		ctx->cache_desc = 0;
+		return r;
+	}
+	// several powfs: each on its own branch, so the small sensors' chains run
+	// beside the large ones
+	if (!ctx->capturing && (r = ensure_branches(ctx))) {
+		ctx->cache_desc = 0;
+		return r;
+	}
+	if (ctx->pstream.size() < ctx->powfs.size()) {
+		ctx->cache_desc = 0;
+		return fail(ctx, SHWFS_ESTATE, "frame graph: stream branches not created by a warm-up frame");
+	}
+	cudaStream_t main = ctx->stream;
+	CK(cudaEventRecord(ctx->ev_pfork[0], main));
+	for (size_t ip = 0; ip < ctx->powfs.size(); ip++) {
+		if (wl[ip].empty()) continue;
+		CK(cudaStreamWaitEvent(ctx->pstream[ip], ctx->ev_pfork[0], 0));
+		ctx->stream = ctx->pstream[ip];
+		if (!r) r = frame_powfs(ctx, (int)ip, wl[ip], isim);
+		ctx->stream = main;
+		CK(cudaEventRecord(ctx->ev_pjoin[ip], ctx->pstream[ip]));
+		CK(cudaStreamWaitEvent(main, ctx->ev_pjoin[ip], 0));
+	}
+	ctx->cache_desc = 0;
+	return r;
+}
+
+int shwfs_frame_graph(shwfs_ctx* ctx, int isim, int iwfs0, int iwfs1) {
+	if (!ctx || iwfs0 < 0 || iwfs1 > (int)ctx->wfs.size() || iwfs0 >= iwfs1)
+		return ctx ? fail(ctx, SHWFS_EINVAL, "frame_graph: bad WFS range") : SHWFS_EINVAL;
+	int r = set_device(ctx);
+	if (r) return r;
+	if (ctx->profiling) return fail(ctx, SHWFS_ESTATE, "frame_graph: stage profiling must be off");
+	if (!ctx->g_warm || ctx->g_i0 != iwfs0 || ctx->g_i1 != iwfs1) {
+		// warm-up frame: buffers, descriptor cache and stream branches come into being
+		if ((r = shwfs_frame_queue(ctx, isim, iwfs0, iwfs1))) return r;
+		if (ctx->gexec) {
+			CK(cudaGraphExecDestroy(ctx->gexec));
+			ctx->gexec = nullptr;
+		}
+		ctx->g_warm = 1;
+		ctx->g_i0 = iwfs0;
+		ctx->g_i1 = iwfs1;
+		return 0;
+	}
+	cudaGraph_t g = nullptr;
+	CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
+	ctx->capturing = 1;
+	r = shwfs_frame_queue(ctx, isim, iwfs0, iwfs1);
+	ctx->capturing = 0;
+	const cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+	if (r || e != cudaSuccess) {
+		if (g) cudaGraphDestroy(g);
+		ctx->g_warm = 0;
+		return r ? r : fail(ctx, SHWFS_ECUDA, "frame_graph: capture failed: %s", cudaGetErrorString(e));
+	}
+	if (ctx->gexec) {
+		cudaGraphExecUpdateResultInfo info;
+		if (cudaGraphExecUpdate(ctx->gexec, g, &info) != cudaSuccess) {
+			cudaGetLastError();
+			CK(cudaGraphExecDestroy(ctx->gexec));
+			ctx->gexec = nullptr;
+		}
+	}
+	if (!ctx->gexec) {
+		const cudaError_t ei = cudaGraphInstantiate(&ctx->gexec, g, 0);
+		if (ei != cudaSuccess) {
+			cudaGraphDestroy(g);
+			ctx->gexec = nullptr;
+			return fail(ctx, SHWFS_ECUDA, "frame_graph: instantiate: %s", cudaGetErrorString(ei));
+		}
+	}
+	CK(cudaGraphDestroy(g));
+	CK(cudaGraphLaunch(ctx->gexec, ctx->stream));
 	return 0;
 }
 

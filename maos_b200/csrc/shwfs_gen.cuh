@@ -26,19 +26,21 @@
 
 namespace shwfs {
 
-constexpr int GEN_LINES = 16;    // FFT lines per tile
+// FFT lines per tile: 16 (128-byte row segments in the column passes), fewer
+// for the large transforms of the small batches, for more blocks
+__host__ __device__ constexpr int gen_lines(int n) { return n >= 256 ? 4 : n >= 128 ? 8 : 16; }
 constexpr int GEN_THREADS = 256;
 
 enum GenPass { GEN_FIELD_ROWS = 1, GEN_PSF_COLS, GEN_OTF_ROWS, GEN_OTF_COLS, GEN_INV_ROWS, GEN_INV_COLS };
 
 __host__ __device__ constexpr int ilog2c(int n) { return n <= 1 ? 0 : 1 + ilog2c(n / 2); }
 
-// In-place radix-2 FFT of GEN_LINES lines of N points in shared memory, line
+// In-place radix-2 FFT of gen_lines(N) lines of N points in shared memory, line
 // stride N + 1 (bank-conflict free for column tiles), input in bit-reversed
 // order.  tw[k] = exp(-2 pi i k / N), k < N/2; dir -1 forward, +1 inverse.
 template <int N>
 __device__ __forceinline__ void fft_lines(float2* s, const float2* __restrict__ tw, int dir) {
-	constexpr int LOGN = ilog2c(N), LS = N + 1, NB = GEN_LINES * N / 2;
+	constexpr int LOGN = ilog2c(N), LS = N + 1, NB = gen_lines(N) * N / 2;
 #pragma unroll 1
 	for (int st = 0; st < LOGN; st++) {
 		const int half = 1 << st;
@@ -85,7 +87,7 @@ struct GenParams {
 // One pass over one tile (blockIdx.y) of one image (blockIdx.x).
 template <int N, int PASS>
 __global__ void __launch_bounds__(GEN_THREADS) gen_pass_kernel(GenParams G) {
-	constexpr int LS = N + 1;
+	constexpr int LS = N + 1, GEN_LINES = gen_lines(N);
 	constexpr bool ROWS = PASS == GEN_FIELD_ROWS || PASS == GEN_OTF_ROWS || PASS == GEN_INV_ROWS;
 	extern __shared__ float2 gen_s[];
 	float2* tw = gen_s + GEN_LINES * LS;  // N/2 twiddles

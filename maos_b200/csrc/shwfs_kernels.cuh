@@ -314,9 +314,12 @@ __device__ __forceinline__ void psf_to_otf_n32(float2 (&F)[32], float scale, flo
 // direct per-point evaluation forms, so the OPD is the same to the bit.
 // Dynamic shared memory: nlayer * nopd * 2 * 16 bytes.
 //   column entry ix: (jx, jx1, wx, -)      row entry iy: (jy nx, jy1 nx, wy, -)
-__global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomParams P, int nopd, int nitem) {
+// Large pupils (nopd^2 > 256 points) split each subaperture over bps blocks of
+// 256 points: block b covers points [256 (b % bps), +256) of subaperture item
+// b / bps.
+__global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomParams P, int nopd, int nitem, int bps) {
 	extern __shared__ int4 s_tab[];
-	const int item = blockIdx.x;
+	const int item = blockIdx.x / bps, part = blockIdx.x - item * bps;
 	if (item >= nitem) return;
 	int ie = 0;
 	while (ie + 1 < P.nentry && item >= P.e[ie + 1].item0) ie++;
@@ -344,8 +347,8 @@ __global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomP
 		s_tab[k] = make_int4(j * m, j1 * m, __float_as_int(f - fl), 0);
 	}
 	__syncthreads();
-	const int np = nopd * nopd;
-	for (int ip = tid; ip < np; ip += blockDim.x) {
+	const int np = nopd * nopd, p1 = bps == 1 ? np : min(np, 256 * (part + 1));
+	for (int ip = (bps == 1 ? 0 : 256 * part) + tid; ip < p1; ip += blockDim.x) {
 		const int ix = ip % nopd, iy = ip / nopd;
 		float acc = 0.f;
 		for (int l = 0; l < nl; l++) {

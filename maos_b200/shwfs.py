@@ -92,6 +92,7 @@ def _load() -> C.CDLL:
         "shwfs_raytrace_dev": [vp, i, i, vp],
         "shwfs_ints_grad_dev": [vp, i, i, vp, vp, vp, vp, i],
         "shwfs_grad_dev": [vp, i, vp, vp],
+        "shwfs_frame_graph": [vp, i, i, i],
         "shwfs_addnoise_dev": [vp, vp, C.c_long, vp, vp, vp, C.c_double, C.c_double, C.c_double, C.c_double,
                                C.c_uint64, C.c_uint32, C.c_uint32],
         "shwfs_sync": [vp],
@@ -246,6 +247,10 @@ class Context:
     # ---- frames ----
     def frame_queue(self, isim: int, iwfs0: int, iwfs1: int):
         self._check(self._L.shwfs_frame_queue(self._h, isim, iwfs0, iwfs1), "frame_queue")
+
+    def frame_graph(self, isim: int, iwfs0: int, iwfs1: int):
+        """The frame of frame_queue as one CUDA graph (the first call per WFS range runs it plainly)."""
+        self._check(self._L.shwfs_frame_graph(self._h, isim, iwfs0, iwfs1), "frame_graph")
 
     def frame_sync(self, iwfs: int, ipowfs: int, want_ints: bool = False):
         nsa = self.nsa[ipowfs]

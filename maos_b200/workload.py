@@ -85,3 +85,73 @@ def build(cfg: dict, device: int = 0, seed: int = 1, noisy: bool = True, nx: int
               for i, h in enumerate(a["ht"])]
     ctx.atm_set(layers, scr)
     return Workload(cfg=cfg, ctx=ctx, setup=setup, ipowfs=ip, wfs=wl, layers=layers, screens=scr)
+
+
+@dataclass
+class BatchWorkload:
+    """Several WFS types (powfs) of one simulation on one device and one
+    atmosphere: the uneven batch.  ``members`` holds (cfg, setup, ipowfs, wfs)."""
+    ctx: "shwfs.Context"
+    members: list
+    layers: List[dict] = field(default_factory=list)
+    screens: List[np.ndarray] = field(default_factory=list)
+    graph: bool = True
+
+    @property
+    def nwfs(self) -> int:
+        return sum(len(m[3]) for m in self.members)
+
+    @property
+    def images_per_frame(self) -> int:
+        return sum(m[1].nsa * len(m[3]) for m in self.members)
+
+    def frame(self, isim: int):
+        """Queue one frame of every WFS of every member (as one CUDA graph when graph is set)."""
+        if self.graph:
+            self.ctx.frame_graph(isim, 0, self.nwfs)
+        else:
+            self.ctx.frame_queue(isim, 0, self.nwfs)
+
+    def frame_sync(self, want_ints: bool = False):
+        out = []
+        for _, _, ip, wl in self.members:
+            out += [self.ctx.frame_sync(i, ip, want_ints) for i in wl]
+        return out
+
+    def close(self):
+        self.ctx.close()
+        for m in self.members:
+            m[1].close()
+
+
+def build_batch(cfgs, device: int = 0, seed: int = 1, noisy: bool = True, nx: int = None,
+                form: int = shwfs.SHWFS_FORM_FFT, graph: bool = True) -> BatchWorkload:
+    """One context holding every config of ``cfgs`` as its own powfs; the
+    atmosphere (screens, winds, frame period) is that of the first config."""
+    ctx = shwfs.Context(device)
+    ctx.set_form(form)
+    ctx.set_dt(cfgs[0].get("dt", 1.0 / 800))
+    members = []
+    nw = 0
+    for j, cfg in enumerate(cfgs):
+        setup = Setup(cfg)
+        ip = setup.load(ctx)
+        wl = []
+        for k in range(cfg["nwfs"]):
+            i = ctx.wfs_add(ipowfs=ip, thetax=cfg["thetax"][k], thetay=cfg["thetay"][k], hs=cfg["hs"], hc=0.0,
+                            misregx=0.0, misregy=0.0, sigsim=cfg["siglev"], wvlwt=1.0, noisy=1 if noisy else 0)
+            setup.load_wfs(ctx, i)
+            ctx.wfs_seed(i, seed * 1000003 + nw)
+            nw += 1
+            wl.append(i)
+        members.append((cfg, setup, ip, wl))
+    a = cfgs[0]["atm"]
+    n = nx or a["nx"]
+    dx = a["dx"]
+    scr = screens(n, n, dx, a["r0"], a["L0"], a["wt"], seed)
+    vx, vy = wind(cfgs[0], seed)
+    o = -n / 2 * dx
+    layers = [dict(nx=n, ny=n, dx=dx, ox=o, oy=o, ht=float(h), vx=float(vx[i]), vy=float(vy[i]), alpha=1.0)
+              for i, h in enumerate(a["ht"])]
+    ctx.atm_set(layers, scr)
+    return BatchWorkload(ctx=ctx, members=members, layers=layers, screens=scr, graph=graph)

@@ -1,0 +1,48 @@
+"""The uneven batch (LGS FFT 32, NGS FFT 128, tip-tilt FFT 256 on one
+atmosphere) through the CUDA-graph frame: identical to the plain stream
+frame, bit for bit, over several frames (the graph carries each frame's
+parameters), and each sensor type matches its own single-powfs frame."""
+import numpy as np
+import pytest
+
+from tests.conftest import cuda_available
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not cuda_available(), reason="needs a CUDA GPU")]
+
+
+def _frames(graph, isims, noisy):
+    from maos_b200.configs import UNEVEN_BATCH
+    from maos_b200.workload import build_batch
+    wl = build_batch(UNEVEN_BATCH["members"], device=0, seed=6, noisy=noisy, nx=512, graph=graph)
+    out = []
+    for isim in isims:
+        wl.frame(isim)
+        out.append(wl.frame_sync(want_ints=True))
+    wl.close()
+    return out
+
+
+@pytest.mark.parametrize("noisy", [False, True])
+def test_graph_frames_equal_stream_frames(noisy):
+    isims = [0, 1, 2, 5, 9]
+    a = _frames(False, isims, noisy)
+    b = _frames(True, isims, noisy)
+    for fa, fb in zip(a, b):
+        for (ga, ia), (gb, ib) in zip(fa, fb):
+            assert np.array_equal(ga, gb) and np.array_equal(ia, ib)
+    # the frames differ from each other (wind, noise counters)
+    assert not np.array_equal(a[0][0][0], a[-1][0][0])
+
+
+def test_batch_members_match_single_powfs_frames():
+    from maos_b200.configs import UNEVEN_BATCH, NGS30_2X2, TT30
+    from maos_b200.workload import build
+    b = _frames(True, [0, 3], False)[-1]
+    # NGS (index 6) and tip-tilt (7, 8) on the same screens, alone
+    for cfg, idx in ((NGS30_2X2, [6]), (TT30, [7, 8])):
+        wl = build(dict(cfg, atm=UNEVEN_BATCH["members"][0]["atm"]), device=0, seed=6, noisy=False, nx=512)
+        wl.frame(3)
+        single = wl.frame_sync(want_ints=True)
+        wl.close()
+        for k, j in enumerate(idx):
+            assert np.array_equal(single[k][0], b[j][0]) and np.array_equal(single[k][1], b[j][1])
