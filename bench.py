@@ -478,6 +478,52 @@ def run_batch(args, bcfg):
     return 0
 
 
+def run_serving(args):
+    """Serving loop: 32 seeded simulations, Poisson frame requests at a rate sweep."""
+    import torch
+    from maos_b200 import shwfs
+    from maos_b200.serving import Server, draw_sim_cfg, poisson_arrivals
+    ws, rank, local = dist_init()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    nsim = 32
+    cfgs = [draw_sim_cfg(s) for s in range(nsim)]
+    srv = Server(cfgs, device=local, form=shwfs.SHWFS_FORM_FFT, seed=1 + rank)
+    srv.prewarm()
+    clk = ClockSampler(local)
+    clk.start()
+    sweeps = {}
+    rates = [1000.0, 2000.0, 5000.0, 10000.0, 20000.0]
+    for form_name, form in (("fft", shwfs.SHWFS_FORM_FFT), ("tc", shwfs.SHWFS_FORM_TC)):
+        srv.set_form(form)
+        out = []
+        for j, rate in enumerate(rates):
+            n = int(min(max(rate * args.serve_seconds, 200), 20000))
+            arr = poisson_arrivals(rate, n, nsim, seed=100 + j)
+            out.append(srv.run(arr, rate).summary())
+        sweeps[form_name] = out
+    clocks = clk.stop()
+    top = sweeps["fft"][-1]
+    resident = len(srv.sims)
+    footprint = srv.adm.used
+    srv.close()
+    line = {
+        "metric": "subaperture images/s", "value": top["images_per_s"] * ws, "unit": "subap-images/s",
+        "n_gpus": ws, "steps": top["requests"], "warmup": 1, "ms_per_step": top["p50_ms"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "serving_32sims", "sims": [c["name"] for c in cfgs], "resident": resident,
+                   "footprint_bytes": footprint, "rates_req_per_s": rates,
+                   "request": "one frame of every WFS of one simulation, gradients to the host",
+                   "value": "images/s served at the highest rate, FFT form"},
+        "frame_latency_ms": {"p50": top["p50_ms"], "p99": top["p99_ms"]},
+        "serving": sweeps,
+        "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -487,10 +533,16 @@ def main():
     ap.add_argument("--config", default="lgs30_6x60x60_mf")
     ap.add_argument("--form", default="fft", choices=["fft", "tc"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=0.5, help="serving: seconds of requests per rate")
     args = ap.parse_args()
     from maos_b200.configs import CONFIGS, BATCHES
     if args.warmup < 3:
         args.warmup = 3
+    if args.config == "serving_32sims":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no serving loop"}))
+            return 0
+        return run_serving(args)
     if args.config in BATCHES:
         bcfg = BATCHES[args.config]
         if args.impl == "reference":

@@ -918,15 +918,20 @@ static int launch_gen_n(shwfs_ctx* ctx, PowfsState& p, GenParams& G) {
 	return 0;
 }
 
+// twiddles exp(-2 pi i k / N), k < N, of a generic-size powfs
+static int ensure_twiddles(shwfs_ctx* ctx, PowfsState& p) {
+	if (p.gen_tw.p) return 0;
+	const int N = p.d.notf;
+	std::vector<float2> tw(N);  // the passes use the first N/2, the fused 64-point kernel all N
+	for (int k = 0; k < N; k++) tw[k] = make_float2((float)cos(2 * M_PI * k / N), (float)-sin(2 * M_PI * k / N));
+	return dev_upload(ctx, p.gen_tw, tw.data(), tw.size());
+}
+
 static int launch_gen(shwfs_ctx* ctx, PowfsState& p, const WfsDev* wdev, int nw, int nitem, int uplink,
 	DevBuf<float2>& buf, const PowfsDev& P) {
 	const int N = p.d.notf;
 	int r;
-	if (!p.gen_tw.p) {
-		std::vector<float2> tw(N / 2);
-		for (int k = 0; k < N / 2; k++) tw[k] = make_float2((float)cos(2 * M_PI * k / N), (float)-sin(2 * M_PI * k / N));
-		if ((r = dev_upload(ctx, p.gen_tw, tw.data(), tw.size()))) return r;
-	}
+	if ((r = ensure_twiddles(ctx, p))) return r;
 	if (buf.n < (size_t)nitem * N * N) {
 		CK(cudaStreamSynchronize(ctx->stream));
 		if ((r = dev_alloc(ctx, buf, (size_t)nitem * N * N))) return r;
@@ -1028,6 +1033,15 @@ static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist
 	const int nitem = p.d.nsa * nw;
 	const int nblk = (nitem + 3) / 4;
 	const int npix = P.npix;
+	if (p.d.notf == 64 && npix <= 256) {  // fused per image
+		int r = ensure_twiddles(ctx, p);
+		if (r) return r;
+		StageMark mark(ctx, SHWFS_STAGE_INTS);
+		ints_n64_kernel<<<nitem, 256, N64_SMEM_BYTES, ctx->stream>>>(P, wdev, nw, nitem, p.d.nopd,
+			(float)(2.0 / p.d.wvl), p.gen_tw.p);
+		CK(cudaGetLastError());
+		return 0;
+	}
 	if (p.d.notf != 32) {  // generic sizes: FFT passes, then pixels, noise and gradients
 		StageMark mark(ctx, SHWFS_STAGE_INTS);
 		int r = launch_gen(ctx, p, wdev, nw, nitem, 0, p.gen_buf, P);

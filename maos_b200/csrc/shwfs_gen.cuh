@@ -244,4 +244,197 @@ __global__ void gen_pixels_kernel(PowfsDev P, const WfsDev* __restrict__ wfs, in
 			W.grad, P.nsa);
 }
 
+// ---------------------------------------------------------------------------
+// n_f = n_w = 64 fused per image: one block of 256 threads holds the 64x64
+// image in shared memory; every 64-point line transform is 8 x 8: n = 8 n1 +
+// n2, k = k1 + 8 k2, X[k] = sum_n2 w64^(n2 k1) w8^(n2 k2) sum_n1 x[n] w8^(n1 k1),
+// with the 8-point transforms in registers, so each line costs two passes
+// through shared memory.  Form F takes the line in natural order and leaves
+// X[k] at the digit-reversed position r(k) = 8 (k mod 8) + k / 8; form G takes
+// the line in digit-reversed order and leaves it natural.  The chain uses F
+// for the field and the inverse transforms and G for the PSF -> OTF transform,
+// so the OTF is in natural order where the transfer functions multiply it, and
+// the final image sits at digit-reversed rows and columns.
+// ---------------------------------------------------------------------------
+constexpr int N64_LS = 65;  // line stride of the shared image (float2): row, column and
+                            // transfer-function accesses all at the 2-wavefront minimum
+
+__device__ __forceinline__ int digrev8(int k) { return ((k & 7) << 3) | (k >> 3); }
+
+// 8-point DFT in registers, natural order in and out; dir -1 forward, +1 inverse
+__device__ __forceinline__ void dft8(float2 (&a)[8], float dir) {
+	const float h = 0.70710678118654752f;
+	// radix-2 stage on pairs (j, j+4)
+	float2 b[8];
+#pragma unroll
+	for (int j = 0; j < 4; j++) {
+		b[j] = make_float2(a[j].x + a[j + 4].x, a[j].y + a[j + 4].y);
+		b[j + 4] = make_float2(a[j].x - a[j + 4].x, a[j].y - a[j + 4].y);
+	}
+	// twiddles w8^j on b[4..7]: w8 = exp(dir i pi/4)
+	{
+		float2 t = b[5];
+		b[5] = make_float2(h * (t.x - dir * t.y), h * (t.y + dir * t.x));
+		t = b[6];
+		b[6] = make_float2(-dir * t.y, dir * t.x);
+		t = b[7];
+		b[7] = make_float2(h * (-t.x - dir * t.y), h * (-t.y + dir * t.x));
+	}
+	// two 4-point DFTs: (b0..b3) -> even outputs, (b4..b7) -> odd outputs
+#pragma unroll
+	for (int g = 0; g < 2; g++) {
+		const float2 c0 = b[4 * g], c1 = b[4 * g + 1], c2 = b[4 * g + 2], c3 = b[4 * g + 3];
+		const float2 s0 = make_float2(c0.x + c2.x, c0.y + c2.y), d0 = make_float2(c0.x - c2.x, c0.y - c2.y);
+		const float2 s1 = make_float2(c1.x + c3.x, c1.y + c3.y), d1 = make_float2(c1.x - c3.x, c1.y - c3.y);
+		const float2 d1r = make_float2(-dir * d1.y, dir * d1.x);  // d1 * (dir i)
+		a[g] = make_float2(s0.x + s1.x, s0.y + s1.y);                // X[0] / X[1]
+		a[g + 2] = make_float2(d0.x + d1r.x, d0.y + d1r.y);          // X[2] / X[3]
+		a[g + 4] = make_float2(s0.x - s1.x, s0.y - s1.y);            // X[4] / X[5]
+		a[g + 6] = make_float2(d0.x - d1r.x, d0.y - d1r.y);          // X[6] / X[7]
+	}
+}
+
+// One 64-point transform of nlines lines (line L at s + (line0 + L) * ls,
+// element j at + j * es) in form F (digrev_in false) or G (true).  Threads
+// take (line, task) with consecutive lines on consecutive threads when
+// lines_fast (column lines), else consecutive tasks (row lines).
+// tw[k] = exp(-2 pi i k / 64).
+template <bool DIGREV_IN, bool LINES_FAST>
+__device__ __forceinline__ void fft64_lines(float2* s, int ls, int es, int line0, int nlines,
+	const float2* __restrict__ tw, float dir) {
+#pragma unroll
+	for (int step = 0; step < 2; step++) {
+		// F: step 0 gathers 8 i + t and twiddles, step 1 gathers 8 t + i.
+		// G: step 0 gathers 8 t + i and twiddles, step 1 gathers 8 i + t.
+		const bool strided = (step == 0) != DIGREV_IN;
+		const int ntask = nlines * 8;
+		for (int task = threadIdx.x; task < ntask; task += blockDim.x) {
+			int L, t;
+			if (LINES_FAST) {
+				L = task % nlines;
+				t = task / nlines;
+			} else {
+				L = task >> 3;
+				t = task & 7;
+			}
+			float2* line = s + (line0 + L) * ls;
+			float2 a[8];
+#pragma unroll
+			for (int i = 0; i < 8; i++) a[i] = line[(strided ? 8 * i + t : 8 * t + i) * es];
+			dft8(a, dir);
+			if (step == 0) {
+#pragma unroll
+				for (int i = 1; i < 8; i++) {
+					float2 w = tw[(t * i) & 63];
+					w.y *= -dir;  // tw holds exp(-...); dir -1 keeps it, +1 conjugates
+					const float2 v = a[i];
+					a[i] = make_float2(v.x * w.x - v.y * w.y, v.x * w.y + v.y * w.x);
+				}
+			}
+#pragma unroll
+			for (int i = 0; i < 8; i++) line[(strided ? 8 * i + t : 8 * t + i) * es] = a[i];
+		}
+		__syncthreads();
+	}
+}
+
+// (b)-(e) fused for n_f = n_w = 64: one block per work item (item = isa * nw +
+// k as in the other imaging launches).  Dynamic shared memory
+// N64_SMEM_BYTES.  tw64[k] = exp(-2 pi i k / 64), k < 64.
+constexpr int N64_SMEM_BYTES = (64 * N64_LS + 64) * 8 + 256 * 4;
+__global__ void __launch_bounds__(256) ints_n64_kernel(PowfsDev P, const WfsDev* __restrict__ wfs, int nw, int nitem,
+	int nopd, float twoinvwvl, const float2* __restrict__ tw64) {
+	extern __shared__ float2 n64_s[];
+	float2* img = n64_s;
+	float2* tw = n64_s + 64 * N64_LS;
+	float* spix = reinterpret_cast<float*>(tw + 64);
+	const int item = blockIdx.x, tid = threadIdx.x;
+	if (item >= nitem) return;
+	const int isa = item / nw;
+	const WfsDev& W = wfs[item % nw];
+	const int pad = (64 - nopd) / 2, no2 = nopd * nopd;
+	if (tid < 64) tw[tid] = tw64[tid];
+	// (b) field, zero-padded (cembed_wvf, maos/wfsints.c:233)
+	for (int idx = tid; idx < 64 * 64; idx += blockDim.x) img[(idx >> 6) * N64_LS + (idx & 63)] = make_float2(0.f, 0.f);
+	__syncthreads();
+	for (int idx = tid; idx < no2; idx += blockDim.x) {
+		const int y = idx / nopd, x = idx - y * nopd;
+		const float o = __ldg(W.opd + (size_t)isa * no2 + idx), a = __ldg(W.amp + (size_t)isa * no2 + idx);
+		float sn, cs;
+		sincospif(twoinvwvl * o, &sn, &cs);
+		img[(y + pad) * N64_LS + x + pad] = make_float2(a * cs, a * sn);
+	}
+	__syncthreads();
+	// (c) PSF: forward along x on the pupil rows, along y; |.|^2
+	fft64_lines<false, false>(img, N64_LS, 1, pad, nopd, tw, -1.f);
+	fft64_lines<false, true>(img, 1, N64_LS, 0, 64, tw, -1.f);
+	for (int idx = tid; idx < 64 * 64; idx += blockDim.x) {
+		float2* v = img + (idx >> 6) * N64_LS + (idx & 63);
+		*v = make_float2(v->x * v->x + v->y * v->y, 0.f);
+	}
+	__syncthreads();
+	// OTF in natural order: forward along kx, along ky (digit-reversed inputs)
+	fft64_lines<true, false>(img, N64_LS, 1, 0, 64, tw, -1.f);
+	fft64_lines<true, true>(img, 1, N64_LS, 0, 64, tw, -1.f);
+	// x conj(uplink OTF) x ETF / nominal; transfer functions are [fy + 64 fx]
+	{
+		const float2* e1 = P.etfT1 ? P.etfT1 + (size_t)isa * 4096 : nullptr;
+		const float2* e2 = P.etfT2 ? P.etfT2 + (size_t)isa * 4096 : nullptr;
+		const float* nm = P.nominalT ? P.nominalT + (P.nominal_per_sa ? (size_t)isa * 4096 : 0) : nullptr;
+		for (int t = tid; t < 64 * 64; t += blockDim.x) {
+			const int fy = t & 63, fx = t >> 6;
+			float2* v = img + fy * N64_LS + fx;
+			float2 o = *v;
+			if (W.lotfT) o = cmulc(o, __ldg(W.lotfT + t));
+			if (e1) {
+				float2 e = __ldg(e1 + t);
+				if (e2) {
+					const float2 f = __ldg(e2 + t);
+					e = make_float2(e.x * P.etfwt1 + f.x * P.etfwt2, e.y * P.etfwt1 + f.y * P.etfwt2);
+				}
+				o = cmul(o, e);
+			} else if (nm) {
+				const float d = __ldg(nm + t);
+				o = make_float2(o.x * d, o.y * d);
+			}
+			*v = o;
+		}
+	}
+	__syncthreads();
+	// inverse along fx, along fy: the image at digit-reversed rows and columns
+	fft64_lines<false, false>(img, N64_LS, 1, 0, 64, tw, 1.f);
+	fft64_lines<false, true>(img, 1, N64_LS, 0, 64, tw, 1.f);
+	// (d) pixels (bilinear map, real part) and noise, one thread per pixel
+	const int npix = P.npix;
+	const int* sidx = P.simap_idx + (P.simap_per_sa ? (size_t)isa * npix * 4 : 0);
+	const float* swt = P.simap_wt + (P.simap_per_sa ? (size_t)isa * npix * 4 : 0);
+	for (int p = tid; p < npix; p += blockDim.x) {
+		float v = 0.f;
+#pragma unroll
+		for (int c = 0; c < 4; c++) {
+			const int id = __ldg(sidx + 4 * p + c);
+			if (id >= 0) v = fmaf(__ldg(swt + 4 * p + c), img[digrev8(id >> 6) * N64_LS + digrev8(id & 63)].x, v);
+		}
+		v *= W.alpha;
+		if (W.noisy) {
+			PixelRng rng(W.seed, (uint32_t)(isa * npix + p), W.wfs_id, (uint32_t)P.isim);
+			v = poisson_draw(rng, v + P.bkgrnd) + P.rne * rng.normal() - P.bkgrndc;
+		}
+		if (W.ints) W.ints[(size_t)isa * npix + p] = v;
+		spix[p] = v;
+	}
+	__syncthreads();
+	// (e) gradients
+	if (tid < 32 && W.grad) {
+		float pix[8];
+#pragma unroll
+		for (int q = 0; q < 8; q++) {
+			const int p = tid + 32 * q;
+			pix[q] = p < npix ? spix[p] : 0.f;
+		}
+		grad_from_pixels<8>(pix, npix, P.pixpsax, P.pixpsay, P, W.mtche + (size_t)isa * 2 * npix, W.i0sum, isa, tid,
+			W.grad, P.nsa);
+	}
+}
+
 }  // namespace shwfs

@@ -63,7 +63,12 @@ def wind(cfg: dict, seed: int):
 
 def build(cfg: dict, device: int = 0, seed: int = 1, noisy: bool = True, nx: int = None,
           form: int = shwfs.SHWFS_FORM_FFT) -> Workload:
-    setup = Setup(cfg)
+    return build_from_setup(cfg, Setup(cfg), device=device, seed=seed, noisy=noisy, nx=nx, form=form)
+
+
+def build_from_setup(cfg: dict, setup: Setup, device: int = 0, seed: int = 1, noisy: bool = True, nx: int = None,
+                     form: int = shwfs.SHWFS_FORM_FFT) -> Workload:
+    """As build, from a host setup made beforehand (which the workload then owns)."""
     ctx = shwfs.Context(device)
     ctx.set_form(form)
     ctx.set_dt(cfg.get("dt", 1.0 / 800))
