@@ -285,23 +285,13 @@ __device__ __forceinline__ void psf_to_otf_n32(float2 (&F)[32], float scale, flo
 }
 
 // ---------------------------------------------------------------------------
-// (a) ray trace of every pupil of the frame in one launch, and the LGS uplink
-// OTF.  Block b belongs to the entry whose [item0, item0+nsa) holds b; it
-// traces one subaperture's nopd^2 points through every layer.  The start of
-// the subaperture in each screen is formed and wrapped once per layer in FP64
-// (threads l < nlayer), then every point adds its bilinear sample with FP32
-// in-subaperture offsets (< nopd screen pixels).  An LLT block keeps the OPD
-// in shared memory and its first warp turns it into the uplink OTF:
+// (a) ray trace of every pupil of the frame in one launch (geom_kernel), and
+// the LGS uplink OTF of the 32-point path (llt_uplink_kernel): an LLT block
+// keeps its OPD in shared memory and its first warp turns it into
 // lotf = FFT(|FFT(embed(lltamp*exp(i*2*pi*opd/wvl)))|^2 / nlwvf^2), stored
-// transposed (fy fastest).
+// transposed (fy fastest).  Block b of geom_kernel belongs to the entry whose
+// [item0, item0+nsa) holds its subaperture.
 // ---------------------------------------------------------------------------
-// Thread layout: one block of 256 threads per subaperture, one OPD point per
-// thread and pass (points p = threadIdx.x + 256*k), so the 32 lanes of a warp
-// read contiguous runs of a screen row.  The start of the subaperture in each
-// screen is formed and wrapped once per layer in FP64 (threads l < nlayer);
-// the points add their bilinear samples with FP32 in-subaperture offsets
-// (< nopd screen pixels).  A layer whose footprint lies inside the screen
-// skips the periodic-wrap arithmetic.
 // ---- ray trace (a) ----
 // The bilinear coordinates of point (ix, iy) in layer l are separable: the
 // column index and weight depend on ix only, the row on iy only.  Each block
