@@ -602,8 +602,10 @@ static int launch_geom_wfs(shwfs_ctx* ctx, GeomParams& gp) {
 		const size_t smem = (size_t)gp.nlayer * nopd * 2 * sizeof(int4);
 		if (smem > 160 * 1024) return fail(ctx, SHWFS_EINVAL, "ray trace: %d layers x %d points too large", gp.nlayer, nopd);
 		if (smem > 48 * 1024) CK(cudaFuncSetAttribute(geom_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-		const int bps = (nopd * nopd + 255) / 256;  // blocks per subaperture
-		geom_kernel<<<(unsigned)nblk * bps, 256, smem, ctx->stream>>>(gp, nopd, nitem, bps);
+		// 16x16 pupils: 128 threads of 2 points; larger: 256 threads of up to GEOM_PTS
+		const int bd = nopd * nopd <= 256 ? 128 : 256;
+		const int bps = (nopd * nopd + GEOM_PTS * bd - 1) / (GEOM_PTS * bd);  // blocks per subaperture
+		geom_kernel<<<(unsigned)nblk * bps, bd, smem, ctx->stream>>>(gp, nopd, nitem, bps);
 	}
 	CK(cudaGetLastError());
 	return 0;

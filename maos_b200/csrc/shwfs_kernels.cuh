@@ -304,9 +304,11 @@ __device__ __forceinline__ void psf_to_otf_n32(float2 (&F)[32], float scale, flo
 // direct per-point evaluation forms, so the OPD is the same to the bit.
 // Dynamic shared memory: nlayer * nopd * 2 * 16 bytes.
 //   column entry ix: (jx, jx1, wx, -)      row entry iy: (jy nx, jy1 nx, wy, -)
-// Large pupils (nopd^2 > 256 points) split each subaperture over bps blocks of
-// 256 points: block b covers points [256 (b % bps), +256) of subaperture item
-// b / bps.
+// A block of bd threads (128 or 256) traces up to GEOM_PTS * bd points of one
+// subaperture; larger pupils split each subaperture over bps blocks: block b
+// covers points [GEOM_PTS * bd (b % bps), + GEOM_PTS * bd) of subaperture
+// item b / bps.
+constexpr int GEOM_PTS = 4;
 __global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomParams P, int nopd, int nitem, int bps) {
 	extern __shared__ int4 s_tab[];
 	const int item = blockIdx.x / bps, part = blockIdx.x - item * bps;
@@ -337,21 +339,37 @@ __global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomP
 		s_tab[k] = make_int4(j * m, j1 * m, __float_as_int(f - fl), 0);
 	}
 	__syncthreads();
-	const int np = nopd * nopd, p1 = bps == 1 ? np : min(np, 256 * (part + 1));
-	for (int ip = (bps == 1 ? 0 : 256 * part) + tid; ip < p1; ip += blockDim.x) {
-		const int ix = ip % nopd, iy = ip / nopd;
-		float acc = 0.f;
-		for (int l = 0; l < nl; l++) {
-			if (!((E.use >> l) & 1u)) continue;
-			const int4 tx = s_tab[l * 2 * nopd + ix], ty = s_tab[l * 2 * nopd + nopd + iy];
-			const float* __restrict__ sc = P.screen[l];
-			const float m00 = __ldg(sc + (ty.x + tx.x)), m10 = __ldg(sc + (ty.x + tx.y));
-			const float m01 = __ldg(sc + (ty.y + tx.x)), m11 = __ldg(sc + (ty.y + tx.y));
-			const float wx = __int_as_float(tx.z), wy = __int_as_float(ty.z);
-			acc = fmaf(P.alpha[l], (m00 + (m10 - m00) * wx) * (1.f - wy) + (m01 + (m11 - m01) * wx) * wy, acc);
-		}
-		E.opd[(size_t)isa * np + ip] = acc;
+	// up to GEOM_PTS points per thread, layers outermost so that the gathers of the points are in flight
+	// together; every point still sums its layers in order
+	const int bd = blockDim.x;
+	const int np = nopd * nopd, p0 = GEOM_PTS * bd * part, p1 = min(np, p0 + GEOM_PTS * bd);
+	float acc[GEOM_PTS];
+	int ixu[GEOM_PTS], iyu[GEOM_PTS];
+#pragma unroll
+	for (int u = 0; u < GEOM_PTS; u++) {
+		const int ip = p0 + tid + bd * u;
+		acc[u] = 0.f;
+		ixu[u] = ip % nopd;
+		iyu[u] = ip / nopd;
 	}
+	for (int l = 0; l < nl; l++) {
+		if (!((E.use >> l) & 1u)) continue;
+		const float* __restrict__ sc = P.screen[l];
+		const float al = P.alpha[l];
+#pragma unroll
+		for (int u = 0; u < GEOM_PTS; u++) {
+			if (p0 + tid + bd * u < p1) {
+				const int4 tx = s_tab[l * 2 * nopd + ixu[u]], ty = s_tab[l * 2 * nopd + nopd + iyu[u]];
+				const float m00 = __ldg(sc + (ty.x + tx.x)), m10 = __ldg(sc + (ty.x + tx.y));
+				const float m01 = __ldg(sc + (ty.y + tx.x)), m11 = __ldg(sc + (ty.y + tx.y));
+				const float wx = __int_as_float(tx.z), wy = __int_as_float(ty.z);
+				acc[u] = fmaf(al, (m00 + (m10 - m00) * wx) * (1.f - wy) + (m01 + (m11 - m01) * wx) * wy, acc[u]);
+			}
+		}
+	}
+#pragma unroll
+	for (int u = 0; u < GEOM_PTS; u++)
+		if (p0 + tid + bd * u < p1) E.opd[(size_t)isa * np + p0 + tid + bd * u] = acc[u];
 }
 
 // LGS uplink: ray trace of each LLT pupil (one block of 256 threads per
