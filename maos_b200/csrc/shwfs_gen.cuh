@@ -295,9 +295,8 @@ __device__ __forceinline__ void dft8(float2 (&a)[8], float dir) {
 }
 
 // One 64-point transform of nlines lines (line L at s + (line0 + L) * ls,
-// element j at + j * es) in form F (digrev_in false) or G (true).  Threads
-// take (line, task) with consecutive lines on consecutive threads when
-// lines_fast (column lines), else consecutive tasks (row lines).
+// element j at + j * es) in form F (digrev_in false) or G (true); LINES_FAST
+// marks column lines.
 // tw[k] = exp(-2 pi i k / 64).
 template <bool DIGREV_IN, bool LINES_FAST>
 __device__ __forceinline__ void fft64_lines(float2* s, int ls, int es, int line0, int nlines,
@@ -308,9 +307,14 @@ __device__ __forceinline__ void fft64_lines(float2* s, int ls, int es, int line0
 		// G: step 0 gathers 8 t + i and twiddles, step 1 gathers 8 i + t.
 		const bool strided = (step == 0) != DIGREV_IN;
 		const int ntask = nlines * 8;
+		// consecutive threads take consecutive lines for column lines, and for
+		// the gather of 8 consecutive elements of row lines (rows are N64_LS
+		// apart: conflict-free), consecutive tasks for the strided gather of row
+		// lines (consecutive elements)
+		const bool lines_fast = LINES_FAST || !strided;
 		for (int task = threadIdx.x; task < ntask; task += blockDim.x) {
 			int L, t;
-			if (LINES_FAST) {
+			if (lines_fast) {
 				L = task % nlines;
 				t = task / nlines;
 			} else {
