@@ -39,6 +39,8 @@ __device__ __forceinline__ u32x4 philox4x32_10(u32x4 c, uint32_t k0, uint32_t k1
 	}
 	return c;
 }
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 // uniform in [0, 1) with 24-bit resolution
 __device__ __forceinline__ float u01(uint32_t v) { return (v >> 8) * (1.0f / 16777216.0f); }
 // uniform in (0, 1], for logarithms
@@ -525,6 +527,11 @@ __global__ void __launch_bounds__(128, MINB) ints_n32_kernel(PowfsDev P, const W
 	float2* tile = tiles[warp];
 	const size_t off_opd = (size_t)isa * 256;
 	float2 F[32];
+	// the subaperture's ETF (8 KB, read after the first two transforms) into L2 now
+	if (P.etfT1) {
+		prefetch_l2(P.etfT1 + (size_t)isa * 1024 + 32 * lane);
+		prefetch_l2(P.etfT1 + (size_t)isa * 1024 + 32 * lane + 16);
+	}
 	field_fft_n32(W.opd + off_opd, W.amp + off_opd, P.twoinvwvl, tile, lane, F);
 	psf_to_otf_n32(F, 1.f, tile, lane);
 	// lane = fy holds OTF(fx, fy). Uplink OTF (conjugated) and ETF / nominal.

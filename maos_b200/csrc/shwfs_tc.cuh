@@ -224,7 +224,6 @@ __device__ __forceinline__ void split8(const float* x, uint4& hi, uint4& lo) {
 	split_pair(x[4], x[5], hi.z, lo.z);
 	split_pair(x[6], x[7], hi.w, lo.w);
 }
-__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 __device__ __forceinline__ void sts128(unsigned char* base, uint32_t off, const uint4& v) {
 	*reinterpret_cast<uint4*>(base + off) = v;
 }
