@@ -169,6 +169,11 @@ int shwfs_frame_sync(shwfs_ctx* ctx, int iwfs, double* grad, double* ints);
    off.  Replaces the per-WFS gpu_wfsgrad_queue threads of
    cuda/sim/gpu_sim.h:45 for a whole frame. */
 int shwfs_frame_graph(shwfs_ctx* ctx, int isim, int iwfs0, int iwfs1);
+/* Gradients of WFS iwfs0..iwfs1-1 after their frame, one wait for all:
+   grad (host) receives each WFS's 2*nsa values in turn.  The range form of
+   shwfs_frame_sync for the gpu_wfsgrad_sync calls of one step
+   (cuda/sim/gpu_sim.h:46). */
+int shwfs_frame_sync_range(shwfs_ctx* ctx, int iwfs0, int iwfs1, double* grad);
 
 /* ---- stage entry points (device pointers; used by callers that hold the
         OPD already, and by the parity tests) ---- */

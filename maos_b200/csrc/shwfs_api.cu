@@ -1399,6 +1399,29 @@ int shwfs_frame_sync(shwfs_ctx* ctx, int iwfs, double* grad, double* ints) {
 	return 0;
 }
 
+int shwfs_frame_sync_range(shwfs_ctx* ctx, int iwfs0, int iwfs1, double* grad) {
+	if (!ctx || !grad || iwfs0 < 0 || iwfs1 > (int)ctx->wfs.size() || iwfs0 >= iwfs1)
+		return ctx ? fail(ctx, SHWFS_EINVAL, "frame_sync_range: bad arguments") : SHWFS_EINVAL;
+	int r = set_device(ctx);
+	if (r) return r;
+	for (int i = iwfs0; i < iwfs1; i++) {
+		WfsState& w = ctx->wfs[i];
+		const int nsa = ctx->powfs[w.d.ipowfs].d.nsa;
+		CK(cudaMemcpyAsync(w.grad_h, w.grad.p, sizeof(float) * 2 * nsa, cudaMemcpyDeviceToHost, ctx->stream));
+		ctx->d2h_bytes += sizeof(float) * 2 * nsa;
+	}
+	CK(cudaStreamSynchronize(ctx->stream));
+	ctx->wfsdev_h.clear();
+	if ((r = check_errflag(ctx))) return r;
+	for (int i = iwfs0; i < iwfs1; i++) {
+		WfsState& w = ctx->wfs[i];
+		const int n = 2 * ctx->powfs[w.d.ipowfs].d.nsa;
+		for (int k = 0; k < n; k++) grad[k] = w.grad_h[k];
+		grad += n;
+	}
+	return 0;
+}
+
 int shwfs_autotune(shwfs_ctx* ctx, int iwfs0, int iwfs1, int nrep, int* chosen) {
 	if (!ctx || iwfs0 < 0 || iwfs1 > (int)ctx->wfs.size() || iwfs0 >= iwfs1 || nrep <= 0)
 		return ctx ? fail(ctx, SHWFS_EINVAL, "autotune: bad arguments") : SHWFS_EINVAL;

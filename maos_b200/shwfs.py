@@ -93,6 +93,7 @@ def _load() -> C.CDLL:
         "shwfs_ints_grad_dev": [vp, i, i, vp, vp, vp, vp, i],
         "shwfs_grad_dev": [vp, i, vp, vp],
         "shwfs_frame_graph": [vp, i, i, i],
+        "shwfs_frame_sync_range": [vp, i, i, dp],
         "shwfs_addnoise_dev": [vp, vp, C.c_long, vp, vp, vp, C.c_double, C.c_double, C.c_double, C.c_double,
                                C.c_uint64, C.c_uint32, C.c_uint32],
         "shwfs_sync": [vp],
@@ -247,6 +248,14 @@ class Context:
     # ---- frames ----
     def frame_queue(self, isim: int, iwfs0: int, iwfs1: int):
         self._check(self._L.shwfs_frame_queue(self._h, isim, iwfs0, iwfs1), "frame_queue")
+
+    def frame_sync_range(self, iwfs0: int, iwfs1: int, nsa_of):
+        """Gradients of WFS iwfs0..iwfs1-1 after their frame, with one wait;
+        nsa_of(i) gives WFS i's subaperture count.  Returns one array per WFS."""
+        sizes = [2 * nsa_of(i) for i in range(iwfs0, iwfs1)]
+        g = np.zeros(sum(sizes))
+        self._check(self._L.shwfs_frame_sync_range(self._h, iwfs0, iwfs1, _dptr(g)), "frame_sync_range")
+        return np.split(g, np.cumsum(sizes)[:-1])
 
     def frame_graph(self, isim: int, iwfs0: int, iwfs1: int):
         """The frame of frame_queue as one CUDA graph (the first call per WFS range runs it plainly)."""

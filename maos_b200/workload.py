@@ -41,6 +41,8 @@ class Workload:
         self.ctx.frame_queue(isim, self.wfs[0], self.wfs[-1] + 1)
 
     def frame_sync(self, want_ints: bool = False):
+        if not want_ints:  # gradients of every WFS with one wait
+            return self.ctx.frame_sync_range(self.wfs[0], self.wfs[-1] + 1, lambda i: self.setup.nsa)
         return [self.ctx.frame_sync(i, self.ipowfs, want_ints) for i in self.wfs]
 
     def close(self):
