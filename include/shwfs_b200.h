@@ -141,6 +141,17 @@ int shwfs_wfs_add(shwfs_ctx* ctx, const shwfs_wfs_desc* desc, int* iwfs);
    column-major block), i0sum (nsa) and i0sumsum (gpu_wfsgrad_update_ref,
    cuda/sim/wfsinit.cu:107). i0sum may be NULL for CoG. */
 int shwfs_wfs_set_mtche(shwfs_ctx* ctx, int iwfs, const double* mtche, const double* i0sum, double i0sumsum);
+/* The matched filter of WFS iwfs regenerated on the device from the powfs's
+   current amplitude, ETF (with its interpolation weights) or DTF nominal,
+   flat uplink OTF and pixel map, in place of a host-built one (the reference
+   builds it on the host, lib/gensei.c:213-419 and lib/mtch.c:93-335, and
+   copies it with gpu_wfsgrad_update_ref, cuda/sim/gpu_sim.h:42): i0 and its
+   x/y derivatives of a flat wavefront, then the weighted pseudo-inverse with
+   mtchcr's cross-coupling terms (0: none, 1: x and y, 2: x, 3: y), the
+   eigenvalue thresholds of dpinv and the dim-subaperture and
+   noise-equivalent-angle rejections.  i0sum and i0sumsum are set too.
+   16x16 OPD points, FFT 32, one shared pixel map. */
+int shwfs_wfs_update_mtche(shwfs_ctx* ctx, int iwfs, int mtchcr);
 /* Noise seed of one WFS (gpu_wfsgrad_seeding, cuda/sim/wfsinit.cu:532). */
 int shwfs_wfs_seed(shwfs_ctx* ctx, int iwfs, uint64_t seed);
 

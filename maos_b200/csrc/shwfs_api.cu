@@ -18,6 +18,7 @@
 #include "shwfs_kernels.cuh"
 #include "shwfs_tc.cuh"
 #include "shwfs_gen.cuh"
+#include "shwfs_mtch.cuh"
 
 using namespace shwfs;
 
@@ -54,6 +55,9 @@ struct PowfsState {
 	std::vector<double> simap_wt_h;
 	DevBuf<uint4> tc_bmat;            // tensor-core B operands (bf16 images)
 	DevBuf<float2> gen_buf, gen_lbuf, gen_tw;  // generic-size chain: scratch images (WFS, LLT), twiddles
+	DevBuf<float2> lotf_flat;         // uplink OTF of a flat LLT wavefront (matched-filter regeneration)
+	DevBuf<float> mtch_img, zero_opd;  // i0/gx/gy scratch; zeros for flat wavefronts
+	DevBuf<double> mtch_red;          // i0 sum total, max i0 sum (float bits)
 	int tc_ready = 0;
 	std::vector<double> origx_h, origy_h;
 };
@@ -254,6 +258,10 @@ int shwfs_destroy(shwfs_ctx* ctx) {
 		p.gen_buf.free_();
 		p.gen_lbuf.free_();
 		p.gen_tw.free_();
+		p.lotf_flat.free_();
+		p.mtch_img.free_();
+		p.zero_opd.free_();
+		p.mtch_red.free_();
 	}
 	for (auto& c : ctx->desc_cache) c.d.free_();
 	if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
@@ -1397,6 +1405,101 @@ int shwfs_frame_sync(shwfs_ctx* ctx, int iwfs, double* grad, double* ints) {
 	if (ints)
 		for (int i = 0; i < nsa * npix; i++) ints[i] = w->ints_h[i];
 	return 0;
+}
+
+int shwfs_wfs_update_mtche(shwfs_ctx* ctx, int iwfs, int mtchcr) {
+	WfsState* w = get_wfs(ctx, iwfs);
+	if (!w || mtchcr < 0 || mtchcr > 3) return ctx ? fail(ctx, SHWFS_EINVAL, "update_mtche: bad arguments") : SHWFS_EINVAL;
+	int r = set_device(ctx);
+	if (r) return r;
+	PowfsState& p = ctx->powfs[w->d.ipowfs];
+	const shwfs_powfs_desc& d = p.d;
+	const int nsa = d.nsa, npix = d.pixpsax * d.pixpsay;
+	if (!(d.nopd == 16 && d.notf == 32)) return fail(ctx, SHWFS_EINVAL, "update_mtche: needs 16x16 OPD points and FFT 32");
+	if (d.gradtype != SHWFS_GRAD_MF) return fail(ctx, SHWFS_EINVAL, "update_mtche: the powfs uses CoG gradients");
+	if (p.nsimap != 1 || npix > 128) return fail(ctx, SHWFS_EINVAL, "update_mtche: needs one pixel map of at most 128 pixels");
+	if (!p.amp.p || !p.simap_idx.p) return fail(ctx, SHWFS_ESTATE, "update_mtche: geometry or pixel map not set");
+	if (d.has_etf ? !p.etfT[0].p : !p.nominalT.p) return fail(ctx, SHWFS_ESTATE, "update_mtche: ETF / DTF not set");
+	if (!p.zero_opd.p) {
+		std::vector<float> z(256, 0.f);
+		if ((r = dev_upload(ctx, p.zero_opd, z.data(), z.size()))) return r;
+	}
+	if (d.has_llt && !p.lotf_flat.p) {  // flat uplink OTF, as the host setup (lib/gensei.c with lotf)
+		if (!p.lltamp.p) return fail(ctx, SHWFS_ESTATE, "update_mtche: LLT amplitude not set");
+		if ((r = dev_alloc(ctx, p.lotf_flat, (size_t)d.notf * d.notf))) return r;
+		DevBuf<const float*> in;
+		DevBuf<float2*> out;
+		const float* zi = p.zero_opd.p;
+		float2* zo = p.lotf_flat.p;
+		if ((r = dev_upload(ctx, in, &zi, 1)) || (r = dev_upload(ctx, out, &zo, 1))) return r;
+		uplink_otf_n32_kernel<<<1, 128, 0, ctx->stream>>>(in.p, p.lltamp.p, out.p, 1, 0.f,
+			(float)(1.0 / ((double)d.llt_nx * d.embfac * d.llt_nx * d.embfac)));
+		CK(cudaGetLastError());
+		CK(cudaStreamSynchronize(ctx->stream));
+		in.free_();
+		out.free_();
+	}
+	if ((r = dev_alloc(ctx, p.mtch_img, (size_t)nsa * 3 * npix)) || (r = dev_alloc(ctx, p.mtch_red, 2))) return r;
+	if (!w->mtche.p && (r = dev_alloc(ctx, w->mtche, (size_t)nsa * 2 * npix))) return r;
+	if (!w->i0sum.p && (r = dev_alloc(ctx, w->i0sum, (size_t)nsa))) return r;
+	CK(cudaMemsetAsync(p.mtch_red.p, 0, 2 * sizeof(double), ctx->stream));
+	const PowfsDev P = make_powfs_dev(p, 0);
+	MtchParams M;
+	memset(&M, 0, sizeof(M));
+	M.nsa = nsa;
+	M.npix = npix;
+	M.pixpsax = d.pixpsax;
+	M.pixpsay = d.pixpsay;
+	M.nmod = 3;
+	if (mtchcr == 1 || mtchcr == 2) {
+		M.crx = M.nmod;
+		M.nmod += 2;
+	}
+	if (mtchcr == 1 || mtchcr == 3) {
+		M.cry = M.nmod;
+		M.nmod += 2;
+	}
+	M.norm_ints = norm_ints(p, *w);
+	M.dux = (float)(1.0 / (d.wvl / (d.dsa * d.embfac) * d.notf));
+	M.amp = p.amp.p + (p.namp > 1 ? (size_t)w->wfsind * nsa * 256 : 0);
+	M.zero_opd = p.zero_opd.p;
+	M.lotfT = d.has_llt ? p.lotf_flat.p : nullptr;
+	M.etfT1 = P.etfT1;
+	M.etfT2 = P.etfT2;
+	M.etfwt1 = P.etfwt1;
+	M.etfwt2 = P.etfwt2;
+	M.nominalT = P.nominalT;
+	M.nominal_per_sa = P.nominal_per_sa;
+	M.simap_idx = p.simap_idx.p;
+	M.simap_wt = p.simap_wt.p;
+	M.kpx = 1. / d.pixthetax;
+	M.kpy = 1. / d.pixthetay;
+	M.bkgrnd = d.bkgrnd;
+	M.bkgrnd_res = d.bkgrnd - d.bkgrndc;
+	M.rne = d.rne;
+	M.nea2thres = d.pixthetax * d.pixthetax * 100;
+	M.img = p.mtch_img.p;
+	M.i0sum = w->i0sum.p;
+	M.i0sumsum = p.mtch_red.p;
+	M.i0max_bits = reinterpret_cast<unsigned*>(p.mtch_red.p + 1);
+	M.mtche = w->mtche.p;
+	const int nblk = (nsa + 3) / 4;
+	if (npix <= 32) {
+		mtch_images_kernel<1><<<nblk, 128, 0, ctx->stream>>>(M);
+		mtch_filter_kernel<1><<<nblk, 128, 0, ctx->stream>>>(M);
+	} else if (npix <= 64) {
+		mtch_images_kernel<2><<<nblk, 128, 0, ctx->stream>>>(M);
+		mtch_filter_kernel<2><<<nblk, 128, 0, ctx->stream>>>(M);
+	} else {
+		mtch_images_kernel<4><<<nblk, 128, 0, ctx->stream>>>(M);
+		mtch_filter_kernel<4><<<nblk, 128, 0, ctx->stream>>>(M);
+	}
+	CK(cudaGetLastError());
+	double tot = 0;
+	CK(cudaMemcpyAsync(&tot, p.mtch_red.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+	CK(cudaStreamSynchronize(ctx->stream));
+	w->i0sumsum = tot;
+	return check_errflag(ctx);
 }
 
 int shwfs_frame_sync_range(shwfs_ctx* ctx, int iwfs0, int iwfs1, double* grad) {

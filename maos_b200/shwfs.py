@@ -93,6 +93,7 @@ def _load() -> C.CDLL:
         "shwfs_ints_grad_dev": [vp, i, i, vp, vp, vp, vp, i],
         "shwfs_grad_dev": [vp, i, vp, vp],
         "shwfs_frame_graph": [vp, i, i, i],
+        "shwfs_wfs_update_mtche": [vp, i, i],
         "shwfs_frame_sync_range": [vp, i, i, dp],
         "shwfs_addnoise_dev": [vp, vp, C.c_long, vp, vp, vp, C.c_double, C.c_double, C.c_double, C.c_double,
                                C.c_uint64, C.c_uint32, C.c_uint32],
@@ -256,6 +257,10 @@ class Context:
         g = np.zeros(sum(sizes))
         self._check(self._L.shwfs_frame_sync_range(self._h, iwfs0, iwfs1, _dptr(g)), "frame_sync_range")
         return np.split(g, np.cumsum(sizes)[:-1])
+
+    def wfs_update_mtche(self, iwfs: int, mtchcr: int):
+        """Regenerate WFS iwfs's matched filter on the device (shwfs_wfs_update_mtche)."""
+        self._check(self._L.shwfs_wfs_update_mtche(self._h, iwfs, mtchcr), "wfs_update_mtche")
 
     def frame_graph(self, isim: int, iwfs0: int, iwfs1: int):
         """The frame of frame_queue as one CUDA graph (the first call per WFS range runs it plainly)."""
