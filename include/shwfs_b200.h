@@ -43,6 +43,7 @@ typedef struct shwfs_ctx shwfs_ctx;
 /* Gradient algorithms (maos/utils.c:983-1122, cuda/sim/wfsgrad.cu:413-478). */
 #define SHWFS_GRAD_MF 1   /* matched filter, PTYPE_MF */
 #define SHWFS_GRAD_COG 2  /* thresholded centre of gravity, PTYPE_COG */
+#define SHWFS_GRAD_ZTILT 3 /* geometric: z-tilt of the OPD, no imaging (gtype_sim=GTYPE_Z) */
 
 /* Imaging forms. */
 #define SHWFS_FORM_FFT 0  /* FP32 shared-memory/register FFT */
@@ -152,6 +153,17 @@ int shwfs_wfs_set_mtche(shwfs_ctx* ctx, int iwfs, const double* mtche, const dou
    noise-equivalent-angle rejections.  i0sum and i0sumsum are set too.
    16x16 OPD points, FFT 32, one shared pixel map. */
 int shwfs_wfs_update_mtche(shwfs_ctx* ctx, int iwfs, int mtchcr);
+/* ETF time interpolation (maos/wfsints.c:215-223): with ETF slots 0 and 1
+   set and dtrat > 0, frame isim uses ETF0 (1 - w) + ETF1 w with
+   w = (isim mod dtrat) / dtrat; dtrat 0 uses slot 0 alone. */
+int shwfs_powfs_set_etf_dtrat(shwfs_ctx* ctx, int ipowfs, int dtrat);
+/* Geometric (z-tilt) gradients (device, 2*nsa) of WFS iwfs from a device OPD
+   (nsa*nopd^2): cuztilt (cuda/sim/wfsgrad.cu:57-106). */
+int shwfs_grad_ztilt_dev(shwfs_ctx* ctx, int iwfs, const float* opd, float* grad);
+/* Noise of geometric gradients (add_geom_noise_do, cuda/sim/wfsgrad.cu:39-51)
+   for a noisy WFS of a geometric powfs: nea is 3*nsa, the lower Cholesky
+   factor of each subaperture's NEA in radians (xx, yy, xy); null removes it. */
+int shwfs_wfs_set_neasim(shwfs_ctx* ctx, int iwfs, const double* nea);
 /* Noise seed of one WFS (gpu_wfsgrad_seeding, cuda/sim/wfsinit.cu:532). */
 int shwfs_wfs_seed(shwfs_ctx* ctx, int iwfs, uint64_t seed);
 

@@ -47,7 +47,7 @@ struct PowfsState {
 	DevBuf<float> simap_wt;
 	int nsimap = 0;
 	DevBuf<float2> etfT[2];
-	float etfwt[2] = {1.f, 0.f};
+	int etf_dtrat = 0;  // ETF time interpolation period in frames (0: slot 0 alone)
 	DevBuf<float> lltamp;
 	DevBuf<double> lltorig;  // {llt origx, llt origy}
 	int variant = 0;         // imaging-kernel variant chosen by shwfs_autotune
@@ -69,6 +69,7 @@ struct WfsState {
 	double i0sumsum = 0;
 	DevBuf<float> opd, lltopd, ints, grad;
 	DevBuf<float2> lotfT;
+	DevBuf<float> neasim;  // geometric gradient noise: Cholesky factor, 3 nsa
 	uint64_t seed = 1;
 	float* grad_h = nullptr;  // pinned staging
 	float* ints_h = nullptr;
@@ -319,6 +320,21 @@ int shwfs_set_dt(shwfs_ctx* ctx, double dt) {
 
 int shwfs_powfs_add(shwfs_ctx* ctx, const shwfs_powfs_desc* d, int* ipowfs) {
 	if (!ctx || !d || !ipowfs) return SHWFS_EINVAL;
+	if (d->gradtype == SHWFS_GRAD_ZTILT) {
+		// geometric sensor: ray trace and z-tilt only, no imaging
+		if (d->nsa <= 0 || d->nopd <= 0 || d->nopd > 128)
+			return fail(ctx, SHWFS_EINVAL, "powfs: geometric sensor needs nsa > 0 and 0 < nopd <= 128");
+		if (d->has_llt) return fail(ctx, SHWFS_EINVAL, "powfs: geometric sensor has no LLT uplink");
+		int r = set_device(ctx);
+		if (r) return r;
+		ctx->powfs.emplace_back();
+		shwfs_powfs_desc& g = ctx->powfs.back().d;
+		g = *d;
+		g.pixpsax = g.pixpsay = 0;  // no detector
+		g.has_etf = 0;
+		*ipowfs = (int)ctx->powfs.size() - 1;
+		return 0;
+	}
 	if (d->nsa <= 0 || d->nopd <= 0 || d->embfac <= 0 || d->notf <= 0 || d->pixpsax <= 0 || d->pixpsay <= 0)
 		return fail(ctx, SHWFS_EINVAL, "powfs: sizes must be positive");
 	const int nw = d->nopd * d->embfac;
@@ -331,7 +347,7 @@ int shwfs_powfs_add(shwfs_ctx* ctx, const shwfs_powfs_desc* d, int* ipowfs) {
 	if (d->pixpsax * d->pixpsay > (n32 ? 128 : 256))
 		return fail(ctx, SHWFS_EINVAL, "powfs: at most %d pixels per subaperture", n32 ? 128 : 256);
 	if (d->gradtype != SHWFS_GRAD_MF && d->gradtype != SHWFS_GRAD_COG)
-		return fail(ctx, SHWFS_EINVAL, "powfs: gradtype must be SHWFS_GRAD_MF or SHWFS_GRAD_COG");
+		return fail(ctx, SHWFS_EINVAL, "powfs: gradtype must be SHWFS_GRAD_MF, SHWFS_GRAD_COG or SHWFS_GRAD_ZTILT");
 	if (d->sigmatch < 0 || d->sigmatch > 2) return fail(ctx, SHWFS_EINVAL, "powfs: sigmatch must be 0, 1 or 2");
 	if (d->has_llt && d->llt_nx != d->nopd)
 		return fail(ctx, SHWFS_EINVAL, "powfs: LLT pupil sampling (%d) must equal the subaperture's (%d)", d->llt_nx, d->nopd);
@@ -467,7 +483,7 @@ int shwfs_wfs_add(shwfs_ctx* ctx, const shwfs_wfs_desc* d, int* iwfs) {
 		if ((r = dev_alloc(ctx, w.lotfT, (size_t)p->d.notf * p->d.notf))) return r;
 	}
 	CK(cudaMallocHost(&w.grad_h, sizeof(float) * 2 * nsa));
-	CK(cudaMallocHost(&w.ints_h, sizeof(float) * nsa * npix));
+	if (npix > 0) CK(cudaMallocHost(&w.ints_h, sizeof(float) * nsa * npix));
 	CK(cudaStreamSynchronize(ctx->stream));
 	*iwfs = (int)ctx->wfs.size() - 1;
 	return 0;
@@ -656,9 +672,15 @@ static PowfsDev make_powfs_dev(const PowfsState& p, int isim) {
 	P.pixpsay = p.d.pixpsay;
 	P.npix = p.d.pixpsax * p.d.pixpsay;
 	P.etfT1 = p.d.has_etf ? p.etfT[0].p : nullptr;
-	P.etfT2 = (p.d.has_etf && p.etfT[1].p) ? p.etfT[1].p : nullptr;
-	P.etfwt1 = p.etfwt[0];
-	P.etfwt2 = p.etfwt[1];
+	// ETF time interpolation (maos/wfsints.c:215-223, cuda/sim/wfsints.cu:362-370)
+	P.etfT2 = (p.d.has_etf && p.etfT[1].p && p.etf_dtrat > 0) ? p.etfT[1].p : nullptr;
+	P.etfwt1 = 1.f;
+	P.etfwt2 = 0.f;
+	if (P.etfT2) {
+		const double wt2 = (double)(isim % p.etf_dtrat) / (double)p.etf_dtrat;
+		P.etfwt2 = (float)wt2;
+		P.etfwt1 = (float)(1. - wt2);
+	}
 	P.nominalT = p.d.has_etf ? nullptr : p.nominalT.p;
 	P.nominal_per_sa = p.nnominal > 1;
 	P.simap_idx = p.simap_idx.p;
@@ -684,6 +706,7 @@ static PowfsDev make_powfs_dev(const PowfsState& p, int isim) {
 
 static int check_ready(shwfs_ctx* ctx, const PowfsState& p, const WfsState& w) {
 	if (!p.amp.p || !p.origx.p) return fail(ctx, SHWFS_ESTATE, "powfs geometry not set");
+	if (p.d.gradtype == SHWFS_GRAD_ZTILT) return 0;
 	if (!p.simap_idx.p) return fail(ctx, SHWFS_ESTATE, "pixel sampling map not set");
 	if (p.d.has_etf && !p.etfT[0].p) return fail(ctx, SHWFS_ESTATE, "ETF not set");
 	if (!p.d.has_etf && !p.nominalT.p) return fail(ctx, SHWFS_ESTATE, "DTF nominal not set");
@@ -1001,6 +1024,7 @@ static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist
 	PowfsState& p = ctx->powfs[ipowfs];
 	const int nw = (int)wlist.size();
 	if (nw == 0) return 0;
+	if (p.d.gradtype == SHWFS_GRAD_ZTILT) return fail(ctx, SHWFS_EINVAL, "geometric sensor: no imaging");
 	if (ctx->form == SHWFS_FORM_TC && nw > TC_MAX_WFS) {
 		// the tensor-core launch holds at most TC_MAX_WFS WFS descriptors in shared memory
 		for (int k0 = 0; k0 < nw; k0 += TC_MAX_WFS) {
@@ -1200,6 +1224,7 @@ int shwfs_grad_dev(shwfs_ctx* ctx, int iwfs, const float* ints, float* grad) {
 	int r = set_device(ctx);
 	if (r) return r;
 	PowfsState& p = ctx->powfs[w->d.ipowfs];
+	if (p.d.gradtype == SHWFS_GRAD_ZTILT) return fail(ctx, SHWFS_EINVAL, "grad: geometric sensor has no pixels");
 	if (p.d.gradtype == SHWFS_GRAD_MF && !w->mtche.p) return fail(ctx, SHWFS_ESTATE, "matched filter not set");
 	if (p.d.sigmatch == 2) return fail(ctx, SHWFS_EINVAL, "sigmatch=2 is not supported by this build");
 	PowfsDev P = make_powfs_dev(p, 0);
@@ -1230,10 +1255,40 @@ int shwfs_addnoise_dev(shwfs_ctx* ctx, float* ints, long n, const float* bkgrnd2
 	return 0;
 }
 
+// Geometric gradients of one WFS from its OPD (one warp per subaperture).
+static int launch_ztilt(shwfs_ctx* ctx, WfsState& w, const float* opd, float* grad, bool noisy, int isim) {
+	PowfsState& p = ctx->powfs[w.d.ipowfs];
+	const int nsa = p.d.nsa;
+	const float* amp = p.amp.p + (p.namp > 1 ? (size_t)w.wfsind * nsa * p.d.nopd * p.d.nopd : 0);
+	{
+		StageMark m(ctx, SHWFS_STAGE_POST);
+		ztilt_kernel<<<(nsa + 7) / 8, 256, 0, ctx->stream>>>(opd, amp, p.origx.p, p.origy.p, nsa, p.d.nopd, p.d.dx,
+			grad, noisy ? w.neasim.p : nullptr, w.seed, (uint32_t)(&w - ctx->wfs.data()), (uint32_t)isim);
+	}
+	CK(cudaGetLastError());
+	return 0;
+}
+
 // The work of one powfs in a frame: ray trace (and uplink), then imaging.
 static int frame_powfs(shwfs_ctx* ctx, int ip, const std::vector<int>& wl, int isim) {
 	PowfsState& p = ctx->powfs[ip];
 	int r;
+	if (p.d.gradtype == SHWFS_GRAD_ZTILT) {
+		for (size_t b = 0; b < wl.size(); b += SHWFS_MAX_ENTRIES) {
+			GeomParams gp;
+			geom_init(ctx, gp);
+			for (size_t k = b; k < wl.size() && k < b + SHWFS_MAX_ENTRIES; k++) {
+				WfsState& w = ctx->wfs[wl[k]];
+				if ((r = add_wfs_entry(ctx, gp, w, isim, w.opd.p))) return r;
+			}
+			if ((r = launch_geom(ctx, gp))) return r;
+		}
+		for (int i : wl) {
+			WfsState& w = ctx->wfs[i];
+			if ((r = launch_ztilt(ctx, w, w.opd.p, w.grad.p, w.d.noisy && w.neasim.p, isim))) return r;
+		}
+		return 0;
+	}
 	// (a) one ray-trace launch per batch of pupils (WFS + LLT)
 	const int per = p.d.has_llt ? SHWFS_MAX_ENTRIES / 2 : SHWFS_MAX_ENTRIES;
 	for (size_t b = 0; b < wl.size(); b += per) {
@@ -1389,6 +1444,7 @@ int shwfs_frame_sync(shwfs_ctx* ctx, int iwfs, double* grad, double* ints) {
 	if (r) return r;
 	PowfsState& p = ctx->powfs[w->d.ipowfs];
 	const int nsa = p.d.nsa, npix = p.d.pixpsax * p.d.pixpsay;
+	if (ints && p.d.gradtype == SHWFS_GRAD_ZTILT) return fail(ctx, SHWFS_EINVAL, "frame_sync: geometric sensor has no pixels");
 	if (grad) {
 		CK(cudaMemcpyAsync(w->grad_h, w->grad.p, sizeof(float) * 2 * nsa, cudaMemcpyDeviceToHost, ctx->stream));
 		ctx->d2h_bytes += sizeof(float) * 2 * nsa;
@@ -1500,6 +1556,36 @@ int shwfs_wfs_update_mtche(shwfs_ctx* ctx, int iwfs, int mtchcr) {
 	CK(cudaStreamSynchronize(ctx->stream));
 	w->i0sumsum = tot;
 	return check_errflag(ctx);
+}
+
+int shwfs_powfs_set_etf_dtrat(shwfs_ctx* ctx, int ipowfs, int dtrat) {
+	PowfsState* p = get_powfs(ctx, ipowfs);
+	if (!p || dtrat < 0) return ctx ? fail(ctx, SHWFS_EINVAL, "set_etf_dtrat: bad arguments") : SHWFS_EINVAL;
+	if (dtrat > 0 && !p->d.has_etf) return fail(ctx, SHWFS_EINVAL, "set_etf_dtrat: the powfs has no ETF");
+	p->etf_dtrat = dtrat;
+	return 0;
+}
+
+int shwfs_wfs_set_neasim(shwfs_ctx* ctx, int iwfs, const double* nea) {
+	WfsState* w = get_wfs(ctx, iwfs);
+	if (!w) return ctx ? fail(ctx, SHWFS_EINVAL, "set_neasim: unknown wfs %d", iwfs) : SHWFS_EINVAL;
+	int r = set_device(ctx);
+	if (r) return r;
+	if (!nea) {
+		w->neasim.free_();
+		return 0;
+	}
+	return dev_upload_f(ctx, w->neasim, nea, (size_t)3 * ctx->powfs[w->d.ipowfs].d.nsa);
+}
+
+int shwfs_grad_ztilt_dev(shwfs_ctx* ctx, int iwfs, const float* opd, float* grad) {
+	WfsState* w = get_wfs(ctx, iwfs);
+	if (!w || !opd || !grad) return ctx ? fail(ctx, SHWFS_EINVAL, "grad_ztilt: bad arguments") : SHWFS_EINVAL;
+	int r = set_device(ctx);
+	if (r) return r;
+	const PowfsState& p = ctx->powfs[w->d.ipowfs];
+	if (!p.amp.p || !p.origx.p) return fail(ctx, SHWFS_ESTATE, "powfs geometry not set");
+	return launch_ztilt(ctx, *w, opd, grad, false, 0);
 }
 
 int shwfs_frame_sync_range(shwfs_ctx* ctx, int iwfs0, int iwfs1, double* grad) {
@@ -1670,6 +1756,7 @@ int shwfs_frame_noalloc(shwfs_ctx* ctx, int iwfs, int isim, float* ints, float* 
 	WfsState* w = get_wfs(ctx, iwfs);
 	if (!w || (!ints && !grad)) return ctx ? fail(ctx, SHWFS_EINVAL, "frame_noalloc: bad arguments") : SHWFS_EINVAL;
 	PowfsState& p = ctx->powfs[w->d.ipowfs];
+	if (p.d.gradtype == SHWFS_GRAD_ZTILT) return fail(ctx, SHWFS_EINVAL, "frame_noalloc: geometric sensor");
 	if (p.d.nsa > SHWFS_NOALLOC_MAX_NSA)
 		return fail(ctx, SHWFS_EINVAL, "frame_noalloc: %d subapertures exceed the allocation-free maximum of %d",
 			p.d.nsa, SHWFS_NOALLOC_MAX_NSA);

@@ -653,6 +653,64 @@ __global__ void noise_grad_kernel(PowfsDev P, const WfsDev* __restrict__ wfs, in
 			lane, W.grad, P.nsa);
 }
 
+// Geometric gradients (z-tilt): the amplitude-weighted least-squares plane
+// of each subaperture's OPD, as cuztilt_do (cuda/sim/wfsgrad.cu:57-106) with
+// the inverse moment matrix of pts_mcc_ptt (math/loc.c:612-650) formed here:
+// g = [(b0, b1, b2) . imcc(:, 1), (b0, b1, b2) . imcc(:, 2)], b = (sum a o,
+// sum a o x, sum a o y), imcc = inv(sum a [1 x y]'[1 x y]), x = origx + ix dx.
+// One warp per subaperture, FP64 sums.  With nea (3 nsa: the lower Cholesky
+// factor per subaperture, xx, yy, xy) the noise of add_geom_noise_do
+// (cuda/sim/wfsgrad.cu:39-51) is added: gx += n1 nea_xx, gy += n2 nea_yy +
+// n1 nea_xy, n1 and n2 standard normals from the Philox stream (seed,
+// 2^31 + isa, wfs, frame).
+__global__ void ztilt_kernel(const float* __restrict__ opd, const float* __restrict__ amp,
+	const double* __restrict__ origx, const double* __restrict__ origy, int nsa, int nopd, double dx,
+	float* __restrict__ grad, const float* __restrict__ nea, uint64_t seed, uint32_t wfs_id, uint32_t frame) {
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int isa = blockIdx.x * (blockDim.x >> 5) + warp;
+	if (isa >= nsa) return;
+	const int np = nopd * nopd;
+	const double ox = origx[isa], oy = origy[isa];
+	double m[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // a00 a01 a02 a11 a12 a22 b0 b1 b2
+	for (int ip = lane; ip < np; ip += 32) {
+		const double x = ox + (ip % nopd) * dx, y = oy + (ip / nopd) * dx;
+		const double a = amp[(size_t)isa * np + ip], ao = a * (double)opd[(size_t)isa * np + ip];
+		m[0] += a;
+		m[1] += a * x;
+		m[2] += a * y;
+		m[3] += a * x * x;
+		m[4] += a * x * y;
+		m[5] += a * y * y;
+		m[6] += ao;
+		m[7] += ao * x;
+		m[8] += ao * y;
+	}
+#pragma unroll
+	for (int k = 0; k < 9; k++)
+#pragma unroll
+		for (int off = 16; off > 0; off >>= 1) m[k] += __shfl_xor_sync(0xffffffffu, m[k], off);
+	if (lane == 0) {
+		const double a00 = m[0], a01 = m[1], a02 = m[2], a11 = m[3], a12 = m[4], a22 = m[5];
+		// inverse of the symmetric 3x3 by cofactors
+		const double c00 = a11 * a22 - a12 * a12, c01 = a02 * a12 - a01 * a22, c02 = a01 * a12 - a02 * a11;
+		const double c11 = a00 * a22 - a02 * a02, c12 = a01 * a02 - a00 * a12, c22 = a00 * a11 - a01 * a01;
+		const double det = a00 * c00 + a01 * c01 + a02 * c02;
+		float gx = 0.f, gy = 0.f;
+		if (det != 0) {
+			gx = (float)((m[6] * c01 + m[7] * c11 + m[8] * c12) / det);
+			gy = (float)((m[6] * c02 + m[7] * c12 + m[8] * c22) / det);
+		}
+		if (nea) {
+			PixelRng rng(seed, 0x80000000u + (uint32_t)isa, wfs_id, frame);
+			const float n1 = rng.normal(), n2 = rng.normal();
+			gx = fmaf(n1, nea[isa], gx);
+			gy = fmaf(n2, nea[isa + nsa], fmaf(n1, nea[isa + 2 * nsa], gy));
+		}
+		grad[isa] = gx;
+		grad[isa + nsa] = gy;
+	}
+}
+
 // (e) alone: one warp per subaperture from stored intensities.
 template <int NPQ>
 __global__ void grad_kernel(PowfsDev P, const float* __restrict__ ints, const float* __restrict__ mtche,

@@ -22,6 +22,7 @@ LIB_PATH = os.path.join(HERE, "libshwfs_b200.so")
 
 SHWFS_GRAD_MF = 1
 SHWFS_GRAD_COG = 2
+SHWFS_GRAD_ZTILT = 3
 SHWFS_FORM_FFT = 0
 SHWFS_FORM_TC = 1
 
@@ -104,6 +105,9 @@ def _load() -> C.CDLL:
         "shwfs_autotune": [vp, i, i, i, ip],
         "shwfs_set_variant": [vp, i, i],
         "shwfs_frame_noalloc": [vp, i, i, vp, vp],
+        "shwfs_powfs_set_etf_dtrat": [vp, i, i],
+        "shwfs_grad_ztilt_dev": [vp, i, vp, vp],
+        "shwfs_wfs_set_neasim": [vp, i, dp],
     }
     for name, args in sig.items():
         f = getattr(lib, name)
@@ -215,6 +219,11 @@ class Context:
         a = np.ascontiguousarray(etf, dtype=np.complex128).view(np.float64)
         self._check(self._L.shwfs_powfs_set_etf(self._h, ipowfs, _dptr(a), slot), "powfs_set_etf")
 
+    def powfs_set_etf_dtrat(self, ipowfs, dtrat: int):
+        """ETF time interpolation: frame isim blends slots 0 and 1 with weight
+        (isim mod dtrat) / dtrat on slot 1 (0 turns it off)."""
+        self._check(self._L.shwfs_powfs_set_etf_dtrat(self._h, ipowfs, int(dtrat)), "powfs_set_etf_dtrat")
+
     def powfs_set_lltamp(self, ipowfs, lltamp):
         a = _f64(lltamp)
         self._check(self._L.shwfs_powfs_set_lltamp(self._h, ipowfs, _dptr(a)), "powfs_set_lltamp")
@@ -229,6 +238,12 @@ class Context:
         m = _f64(mtche) if mtche is not None else None
         s = _f64(i0sum) if i0sum is not None else None
         self._check(self._L.shwfs_wfs_set_mtche(self._h, iwfs, _dptr(m), _dptr(s), float(i0sumsum)), "wfs_set_mtche")
+
+    def wfs_set_neasim(self, iwfs, nea):
+        """Geometric-gradient noise of WFS iwfs: (3, nsa) or 3*nsa Cholesky
+        factor (xx, yy, xy) in radians; None removes it."""
+        a = _f64(nea) if nea is not None else None
+        self._check(self._L.shwfs_wfs_set_neasim(self._h, iwfs, _dptr(a)), "wfs_set_neasim")
 
     def wfs_seed(self, iwfs, seed):
         self._check(self._L.shwfs_wfs_seed(self._h, iwfs, int(seed) & 0xFFFFFFFFFFFFFFFF), "wfs_seed")
@@ -284,6 +299,10 @@ class Context:
         """One frame of WFS iwfs that allocates no device memory (scratch in a
         static device array); ints/grad are caller-owned device tensors."""
         self._check(self._L.shwfs_frame_noalloc(self._h, iwfs, isim, _devptr(ints), _devptr(grad)), "frame_noalloc")
+
+    def grad_ztilt_dev(self, iwfs, opd, grad):
+        """Geometric z-tilt gradients (2*nsa, device) of a device OPD (nsa*nopd^2)."""
+        self._check(self._L.shwfs_grad_ztilt_dev(self._h, iwfs, _devptr(opd), _devptr(grad)), "grad_ztilt_dev")
 
     def grad_dev(self, iwfs, ints, grad):
         self._check(self._L.shwfs_grad_dev(self._h, iwfs, _devptr(ints), _devptr(grad)), "grad_dev")

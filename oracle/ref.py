@@ -139,6 +139,27 @@ class RefPowfs:
             out[isa] = buf[0::2] + 1j * buf[1::2]
         return out
 
+    def setup_etf2(self, deltah: float, coldtrat: int):
+        """Second ETF of the time interpolation (sodium focus at hs + deltah)
+        and its period in frames."""
+        lib().oref_setup_etf2(C.c_double(deltah), C.c_int(coldtrat))
+
+    def etf2(self):
+        n2 = self.notf ** 2
+        out = np.zeros((self.nsa, n2), dtype=np.complex128)
+        buf = np.zeros(2 * n2)
+        for isa in range(self.nsa):
+            lib().oref_get_etf2(C.c_int(isa), _p(buf))
+            out[isa] = buf[0::2] + 1j * buf[1::2]
+        return out
+
+    def ztilt(self, opd):
+        """Geometric z-tilt gradients (2 nsa) of an OPD (nsa nopd^2)."""
+        g = np.zeros(2 * self.nsa)
+        opd = np.ascontiguousarray(opd, dtype=np.float64)
+        lib().oref_ztilt(_p(opd), _p(g))
+        return g
+
     def srot(self):
         a = np.zeros(self.nsa); lib().oref_get_srot(_p(a)); return a
 

@@ -360,6 +360,8 @@ void oref_rand_stream(unsigned int seed, long n, double* u, double* g, long* poi
 /* The reference's multithreaded CPU frame for one WFS, as the MAOS time step
    runs it: wfsints over thread_prep(0,nsa,NTHREAD) (maos/sim_utils.c:1072-1079),
    then addnoise per subaperture and shwfs_grad.  Returns seconds spent. */
+/* frame index passed to wfsints (ETF time interpolation, maos/wfsints.c:215-223) */
+static int g_frame_isim=0;
 double oref_frame_mt(int iwfs, const double* opd, const double* lltopd, double* ints, double* grad,
 	unsigned int seed, int noisy){
 	const long nsa=g_powfs[0].saloc->nloc;
@@ -382,6 +384,7 @@ double oref_frame_mt(int iwfs, const double* opd, const double* lltopd, double* 
 	data.opd=dopd;
 	data.lltopd=dllt;
 	data.iwfs=iwfs;
+	data.isim=g_frame_isim;
 	thread_t* thd=thread_prep(0, nsa, NTHREAD, wfsints, &data);
 	CALL_THREAD(thd, 1);
 	free(thd);
@@ -489,8 +492,39 @@ double oref_frame_full_mt(int iwfs, int isim, double dt, double* ints, double* g
 		}
 	}
 	double t1=omp_get_wtime();
+	g_frame_isim=isim;
 	double t=oref_frame_mt(iwfs, P(opd), lltopd?P(lltopd):NULL, ints, grad, seed, noisy);
+	g_frame_isim=0;
 	dfree(opd);
 	dfree(lltopd);
 	return (t1-t0)+t;
+}
+
+/* The second ETF of the time interpolation: the reference's own
+   setup_shwfs_etf in mode 2 (maos/powfs.c:1157-1175) for the sodium layer
+   focused at hs + deltah, and the interpolation period coldtrat
+   (maos/wfsints.c:215-223). */
+void oref_setup_etf2(double deltah, int coldtrat){
+	setup_shwfs_etf(g_powfs, g_parms, 0, 2, 0, deltah, 0);
+	g_parms->powfs[0].llt->coldtrat=coldtrat;
+}
+void oref_get_etf2(int isa, double* out){
+	cmat* e=P(g_powfs[0].etfsim2[0].etf, isa, 0);
+	copy_vec(out, (double*)P(e), 2*PN(e));
+}
+
+/* Geometric z-tilt gradients (2*nsa) of an OPD (nsa*nopd^2) over the
+   powfs's subapertures: the reference's pts_mcc_ptt and dcellinvspd_each
+   (maos/powfs.c:633-645) and pts_ztilt (math/loc.c:839-885). */
+void oref_ztilt(const double* opd, double* grad){
+	const long nsa=g_powfs[0].saloc->nloc;
+	const double* amp=P(P(g_powfs[0].amp, 0));
+	dcell* mcc=pts_mcc_ptt(g_powfs[0].pts, amp);
+	dcell* imcc=dcellinvspd_each(mcc);
+	dmat* g=dnew(2*nsa, 1);
+	pts_ztilt(&g, g_powfs[0].pts, imcc, amp, opd);
+	copy_vec(grad, P(g), 2*nsa);
+	dfree(g);
+	dcellfree(imcc);
+	dcellfree(mcc);
 }

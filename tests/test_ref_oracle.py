@@ -30,3 +30,36 @@ def test_reference_setup_lgs30(ref_lib):
     assert ref.llt_nx == 16
     m = ref.mtche()
     assert m.shape == (2820, 72) and np.isfinite(m).all()
+
+
+def _tilt_opd(r, a, b):
+    """OPD a x + b y + c over every subaperture's points (nsa nopd^2, x fastest)."""
+    ox, oy = r.ptsorig()
+    dx = r.ptsdx()
+    i = np.arange(r.nopd)
+    x = ox[:, None, None] + dx * i[None, None, :]
+    y = oy[:, None, None] + dx * i[None, :, None]
+    return (a * x + b * y + 3e-7 + 0 * x).ravel()
+
+
+def test_reference_ztilt_known_answer(ref_lib):
+    """pts_ztilt of a plane recovers its slope in every lit subaperture and
+    ignores piston (the weighted least-squares fit is exact for a plane)."""
+    from maos_b200.configs import NGS8
+    r = ref_lib.RefPowfs(NGS8)
+    a, b = 2.5e-6, -1.25e-6
+    g = r.ztilt(_tilt_opd(r, a, b))
+    assert np.allclose(g[:r.nsa], a, rtol=1e-9, atol=0)
+    assert np.allclose(g[r.nsa:], b, rtol=1e-9, atol=0)
+
+
+def test_reference_second_etf(ref_lib):
+    """The second ETF slot: same focus gives the first ETF, another focus a different one."""
+    from maos_b200.configs import LGS30
+    r = ref_lib.RefPowfs(LGS30)
+    e1 = r.etf()
+    r.setup_etf2(0.0, 4)
+    assert np.array_equal(r.etf2(), e1)
+    r.setup_etf2(2000.0, 4)
+    e2 = r.etf2()
+    assert np.abs(e2 - e1).max() > 1e-3 * np.abs(e1).max()
