@@ -44,6 +44,7 @@ typedef struct shwfs_ctx shwfs_ctx;
 #define SHWFS_GRAD_MF 1   /* matched filter, PTYPE_MF */
 #define SHWFS_GRAD_COG 2  /* thresholded centre of gravity, PTYPE_COG */
 #define SHWFS_GRAD_ZTILT 3 /* geometric: z-tilt of the OPD, no imaging (gtype_sim=GTYPE_Z) */
+#define SHWFS_GRAD_GTILT 4 /* geometric: averaged gradient GS0*OPD, no imaging (gtype_sim=GTYPE_G) */
 
 /* Imaging forms. */
 #define SHWFS_FORM_FFT 0  /* FP32 shared-memory/register FFT */
@@ -164,6 +165,14 @@ int shwfs_grad_ztilt_dev(shwfs_ctx* ctx, int iwfs, const float* opd, float* grad
    for a noisy WFS of a geometric powfs: nea is 3*nsa, the lower Cholesky
    factor of each subaperture's NEA in radians (xx, yy, xy); null removes it. */
 int shwfs_wfs_set_neasim(shwfs_ctx* ctx, int iwfs, const double* nea);
+/* G-tilt operator of a geometric powfs (powfs.GS0, maos/powfs.c:607-632, made
+   by mkg, lib/mkg.c:471): a MAOS sparse matrix (CSC, spint = int) of 2*nsa
+   rows and nsa*nopd^2 columns; iamp selects the matrix of WFS wfsind = iamp
+   when the powfs has one amplitude per WFS (else 0). */
+int shwfs_powfs_set_gs0(shwfs_ctx* ctx, int ipowfs, int iamp, long nrow, long ncol, const int* pp,
+	const int* pi, const double* px);
+/* G-tilt gradients (device, 2*nsa) of WFS iwfs from a device OPD. */
+int shwfs_grad_gtilt_dev(shwfs_ctx* ctx, int iwfs, const float* opd, float* grad);
 /* Noise seed of one WFS (gpu_wfsgrad_seeding, cuda/sim/wfsinit.cu:532). */
 int shwfs_wfs_seed(shwfs_ctx* ctx, int iwfs, uint64_t seed);
 

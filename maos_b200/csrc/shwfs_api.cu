@@ -35,6 +35,9 @@ struct DevBuf {
 	}
 };
 
+// geometric sensors: ray trace and gradients of the OPD, no imaging
+static inline bool is_geom(int gradtype) { return gradtype == SHWFS_GRAD_ZTILT || gradtype == SHWFS_GRAD_GTILT; }
+
 struct PowfsState {
 	shwfs_powfs_desc d;
 	DevBuf<double> origx, origy;
@@ -60,6 +63,8 @@ struct PowfsState {
 	DevBuf<double> mtch_red;          // i0 sum total, max i0 sum (float bits)
 	int tc_ready = 0;
 	std::vector<double> origx_h, origy_h;
+	std::vector<DevBuf<int>> gs0_ptr, gs0_col;  // G-tilt operators in CSR, one per amplitude
+	std::vector<DevBuf<float>> gs0_val;
 };
 
 struct WfsState {
@@ -263,6 +268,9 @@ int shwfs_destroy(shwfs_ctx* ctx) {
 		p.mtch_img.free_();
 		p.zero_opd.free_();
 		p.mtch_red.free_();
+		for (auto& b : p.gs0_ptr) b.free_();
+		for (auto& b : p.gs0_col) b.free_();
+		for (auto& b : p.gs0_val) b.free_();
 	}
 	for (auto& c : ctx->desc_cache) c.d.free_();
 	if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
@@ -280,6 +288,7 @@ int shwfs_destroy(shwfs_ctx* ctx) {
 		w.ints.free_();
 		w.grad.free_();
 		w.lotfT.free_();
+		w.neasim.free_();
 		if (w.grad_h) cudaFreeHost(w.grad_h);
 		if (w.ints_h) cudaFreeHost(w.ints_h);
 	}
@@ -320,7 +329,7 @@ int shwfs_set_dt(shwfs_ctx* ctx, double dt) {
 
 int shwfs_powfs_add(shwfs_ctx* ctx, const shwfs_powfs_desc* d, int* ipowfs) {
 	if (!ctx || !d || !ipowfs) return SHWFS_EINVAL;
-	if (d->gradtype == SHWFS_GRAD_ZTILT) {
+	if (is_geom(d->gradtype)) {
 		// geometric sensor: ray trace and z-tilt only, no imaging
 		if (d->nsa <= 0 || d->nopd <= 0 || d->nopd > 128)
 			return fail(ctx, SHWFS_EINVAL, "powfs: geometric sensor needs nsa > 0 and 0 < nopd <= 128");
@@ -347,7 +356,7 @@ int shwfs_powfs_add(shwfs_ctx* ctx, const shwfs_powfs_desc* d, int* ipowfs) {
 	if (d->pixpsax * d->pixpsay > (n32 ? 128 : 256))
 		return fail(ctx, SHWFS_EINVAL, "powfs: at most %d pixels per subaperture", n32 ? 128 : 256);
 	if (d->gradtype != SHWFS_GRAD_MF && d->gradtype != SHWFS_GRAD_COG)
-		return fail(ctx, SHWFS_EINVAL, "powfs: gradtype must be SHWFS_GRAD_MF, SHWFS_GRAD_COG or SHWFS_GRAD_ZTILT");
+		return fail(ctx, SHWFS_EINVAL, "powfs: gradtype must be SHWFS_GRAD_MF, SHWFS_GRAD_COG, SHWFS_GRAD_ZTILT or SHWFS_GRAD_GTILT");
 	if (d->sigmatch < 0 || d->sigmatch > 2) return fail(ctx, SHWFS_EINVAL, "powfs: sigmatch must be 0, 1 or 2");
 	if (d->has_llt && d->llt_nx != d->nopd)
 		return fail(ctx, SHWFS_EINVAL, "powfs: LLT pupil sampling (%d) must equal the subaperture's (%d)", d->llt_nx, d->nopd);
@@ -706,7 +715,11 @@ static PowfsDev make_powfs_dev(const PowfsState& p, int isim) {
 
 static int check_ready(shwfs_ctx* ctx, const PowfsState& p, const WfsState& w) {
 	if (!p.amp.p || !p.origx.p) return fail(ctx, SHWFS_ESTATE, "powfs geometry not set");
-	if (p.d.gradtype == SHWFS_GRAD_ZTILT) return 0;
+	if (p.d.gradtype == SHWFS_GRAD_GTILT) {
+		const size_t m = p.namp > 1 ? (size_t)w.wfsind : 0;
+		if (m >= p.gs0_ptr.size() || !p.gs0_ptr[m].p) return fail(ctx, SHWFS_ESTATE, "G-tilt operator GS0 not set");
+	}
+	if (is_geom(p.d.gradtype)) return 0;
 	if (!p.simap_idx.p) return fail(ctx, SHWFS_ESTATE, "pixel sampling map not set");
 	if (p.d.has_etf && !p.etfT[0].p) return fail(ctx, SHWFS_ESTATE, "ETF not set");
 	if (!p.d.has_etf && !p.nominalT.p) return fail(ctx, SHWFS_ESTATE, "DTF nominal not set");
@@ -1024,7 +1037,7 @@ static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist
 	PowfsState& p = ctx->powfs[ipowfs];
 	const int nw = (int)wlist.size();
 	if (nw == 0) return 0;
-	if (p.d.gradtype == SHWFS_GRAD_ZTILT) return fail(ctx, SHWFS_EINVAL, "geometric sensor: no imaging");
+	if (is_geom(p.d.gradtype)) return fail(ctx, SHWFS_EINVAL, "geometric sensor: no imaging");
 	if (ctx->form == SHWFS_FORM_TC && nw > TC_MAX_WFS) {
 		// the tensor-core launch holds at most TC_MAX_WFS WFS descriptors in shared memory
 		for (int k0 = 0; k0 < nw; k0 += TC_MAX_WFS) {
@@ -1224,7 +1237,7 @@ int shwfs_grad_dev(shwfs_ctx* ctx, int iwfs, const float* ints, float* grad) {
 	int r = set_device(ctx);
 	if (r) return r;
 	PowfsState& p = ctx->powfs[w->d.ipowfs];
-	if (p.d.gradtype == SHWFS_GRAD_ZTILT) return fail(ctx, SHWFS_EINVAL, "grad: geometric sensor has no pixels");
+	if (is_geom(p.d.gradtype)) return fail(ctx, SHWFS_EINVAL, "grad: geometric sensor has no pixels");
 	if (p.d.gradtype == SHWFS_GRAD_MF && !w->mtche.p) return fail(ctx, SHWFS_ESTATE, "matched filter not set");
 	if (p.d.sigmatch == 2) return fail(ctx, SHWFS_EINVAL, "sigmatch=2 is not supported by this build");
 	PowfsDev P = make_powfs_dev(p, 0);
@@ -1255,15 +1268,24 @@ int shwfs_addnoise_dev(shwfs_ctx* ctx, float* ints, long n, const float* bkgrnd2
 	return 0;
 }
 
-// Geometric gradients of one WFS from its OPD (one warp per subaperture).
-static int launch_ztilt(shwfs_ctx* ctx, WfsState& w, const float* opd, float* grad, bool noisy, int isim) {
+// Geometric gradients of one WFS from its OPD (one warp per subaperture):
+// z-tilt, or G-tilt with the WFS's GS0.
+static int launch_geom_grad(shwfs_ctx* ctx, WfsState& w, const float* opd, float* grad, bool noisy, int isim) {
 	PowfsState& p = ctx->powfs[w.d.ipowfs];
 	const int nsa = p.d.nsa;
-	const float* amp = p.amp.p + (p.namp > 1 ? (size_t)w.wfsind * nsa * p.d.nopd * p.d.nopd : 0);
-	{
-		StageMark m(ctx, SHWFS_STAGE_POST);
+	const float* nea = noisy ? w.neasim.p : nullptr;
+	const uint32_t wid = (uint32_t)(&w - ctx->wfs.data());
+	if (p.d.gradtype == SHWFS_GRAD_GTILT) {
+		const size_t m = p.namp > 1 ? (size_t)w.wfsind : 0;
+		if (m >= p.gs0_ptr.size() || !p.gs0_ptr[m].p) return fail(ctx, SHWFS_ESTATE, "G-tilt operator GS0 not set");
+		StageMark mk(ctx, SHWFS_STAGE_POST);
+		gtilt_kernel<<<(nsa + 7) / 8, 256, 0, ctx->stream>>>(p.gs0_ptr[m].p, p.gs0_col[m].p, p.gs0_val[m].p, nsa, opd,
+			grad, nea, w.seed, wid, (uint32_t)isim);
+	} else {
+		const float* amp = p.amp.p + (p.namp > 1 ? (size_t)w.wfsind * nsa * p.d.nopd * p.d.nopd : 0);
+		StageMark mk(ctx, SHWFS_STAGE_POST);
 		ztilt_kernel<<<(nsa + 7) / 8, 256, 0, ctx->stream>>>(opd, amp, p.origx.p, p.origy.p, nsa, p.d.nopd, p.d.dx,
-			grad, noisy ? w.neasim.p : nullptr, w.seed, (uint32_t)(&w - ctx->wfs.data()), (uint32_t)isim);
+			grad, nea, w.seed, wid, (uint32_t)isim);
 	}
 	CK(cudaGetLastError());
 	return 0;
@@ -1273,7 +1295,7 @@ static int launch_ztilt(shwfs_ctx* ctx, WfsState& w, const float* opd, float* gr
 static int frame_powfs(shwfs_ctx* ctx, int ip, const std::vector<int>& wl, int isim) {
 	PowfsState& p = ctx->powfs[ip];
 	int r;
-	if (p.d.gradtype == SHWFS_GRAD_ZTILT) {
+	if (is_geom(p.d.gradtype)) {
 		for (size_t b = 0; b < wl.size(); b += SHWFS_MAX_ENTRIES) {
 			GeomParams gp;
 			geom_init(ctx, gp);
@@ -1285,7 +1307,7 @@ static int frame_powfs(shwfs_ctx* ctx, int ip, const std::vector<int>& wl, int i
 		}
 		for (int i : wl) {
 			WfsState& w = ctx->wfs[i];
-			if ((r = launch_ztilt(ctx, w, w.opd.p, w.grad.p, w.d.noisy && w.neasim.p, isim))) return r;
+			if ((r = launch_geom_grad(ctx, w, w.opd.p, w.grad.p, w.d.noisy && w.neasim.p, isim))) return r;
 		}
 		return 0;
 	}
@@ -1444,7 +1466,7 @@ int shwfs_frame_sync(shwfs_ctx* ctx, int iwfs, double* grad, double* ints) {
 	if (r) return r;
 	PowfsState& p = ctx->powfs[w->d.ipowfs];
 	const int nsa = p.d.nsa, npix = p.d.pixpsax * p.d.pixpsay;
-	if (ints && p.d.gradtype == SHWFS_GRAD_ZTILT) return fail(ctx, SHWFS_EINVAL, "frame_sync: geometric sensor has no pixels");
+	if (ints && is_geom(p.d.gradtype)) return fail(ctx, SHWFS_EINVAL, "frame_sync: geometric sensor has no pixels");
 	if (grad) {
 		CK(cudaMemcpyAsync(w->grad_h, w->grad.p, sizeof(float) * 2 * nsa, cudaMemcpyDeviceToHost, ctx->stream));
 		ctx->d2h_bytes += sizeof(float) * 2 * nsa;
@@ -1585,7 +1607,64 @@ int shwfs_grad_ztilt_dev(shwfs_ctx* ctx, int iwfs, const float* opd, float* grad
 	if (r) return r;
 	const PowfsState& p = ctx->powfs[w->d.ipowfs];
 	if (!p.amp.p || !p.origx.p) return fail(ctx, SHWFS_ESTATE, "powfs geometry not set");
-	return launch_ztilt(ctx, *w, opd, grad, false, 0);
+	// the z-tilt fit on any powfs's geometry
+	const int nsa = p.d.nsa;
+	const float* amp = p.amp.p + (p.namp > 1 ? (size_t)w->wfsind * nsa * p.d.nopd * p.d.nopd : 0);
+	ztilt_kernel<<<(nsa + 7) / 8, 256, 0, ctx->stream>>>(opd, amp, p.origx.p, p.origy.p, nsa, p.d.nopd, p.d.dx, grad,
+		nullptr, 0, 0, 0);
+	CK(cudaGetLastError());
+	return 0;
+}
+
+int shwfs_grad_gtilt_dev(shwfs_ctx* ctx, int iwfs, const float* opd, float* grad) {
+	WfsState* w = get_wfs(ctx, iwfs);
+	if (!w || !opd || !grad) return ctx ? fail(ctx, SHWFS_EINVAL, "grad_gtilt: bad arguments") : SHWFS_EINVAL;
+	int r = set_device(ctx);
+	if (r) return r;
+	if (ctx->powfs[w->d.ipowfs].d.gradtype != SHWFS_GRAD_GTILT)
+		return fail(ctx, SHWFS_EINVAL, "grad_gtilt: the powfs is not a G-tilt sensor");
+	return launch_geom_grad(ctx, *w, opd, grad, false, 0);
+}
+
+int shwfs_powfs_set_gs0(shwfs_ctx* ctx, int ipowfs, int iamp, long nrow, long ncol, const int* pp, const int* pi,
+	const double* px) {
+	PowfsState* p = get_powfs(ctx, ipowfs);
+	if (!p || iamp < 0 || iamp > 1023 || !pp || (pp[ncol] > 0 && (!pi || !px)))
+		return ctx ? fail(ctx, SHWFS_EINVAL, "set_gs0: bad arguments") : SHWFS_EINVAL;
+	const long nsa = p->d.nsa, nloc = (long)nsa * p->d.nopd * p->d.nopd;
+	if (nrow != 2 * nsa || ncol != nloc)
+		return fail(ctx, SHWFS_EINVAL, "set_gs0: GS0 is %ldx%ld, needs %ldx%ld", nrow, ncol, 2 * nsa, nloc);
+	// CSC (MAOS dsp) -> CSR, checking every index
+	const long nnz = pp[ncol];
+	if (pp[0] != 0 || nnz < 0 || nnz > 0x7fffffffL) return fail(ctx, SHWFS_EINVAL, "set_gs0: bad column pointers");
+	std::vector<int> rp(nrow + 1, 0), ci(nnz);
+	std::vector<double> v(nnz);
+	for (long c = 0; c < ncol; c++) {
+		if (pp[c + 1] < pp[c] || pp[c + 1] > nnz) return fail(ctx, SHWFS_EINVAL, "set_gs0: bad column pointers");
+		for (long k = pp[c]; k < pp[c + 1]; k++) {
+			if (pi[k] < 0 || pi[k] >= nrow) return fail(ctx, SHWFS_EINVAL, "set_gs0: row index out of range");
+			rp[pi[k] + 1]++;
+		}
+	}
+	for (long i = 0; i < nrow; i++) rp[i + 1] += rp[i];
+	std::vector<int> fill(rp.begin(), rp.end() - 1);
+	for (long c = 0; c < ncol; c++)
+		for (long k = pp[c]; k < pp[c + 1]; k++) {
+			const int at = fill[pi[k]]++;
+			ci[at] = (int)c;
+			v[at] = px[k];
+		}
+	int r = set_device(ctx);
+	if (r) return r;
+	if ((size_t)iamp >= p->gs0_ptr.size()) {
+		p->gs0_ptr.resize(iamp + 1);
+		p->gs0_col.resize(iamp + 1);
+		p->gs0_val.resize(iamp + 1);
+	}
+	if ((r = dev_upload(ctx, p->gs0_ptr[iamp], rp.data(), rp.size()))) return r;
+	if (nnz == 0) return 0;
+	if ((r = dev_upload(ctx, p->gs0_col[iamp], ci.data(), ci.size()))) return r;
+	return dev_upload_f(ctx, p->gs0_val[iamp], v.data(), v.size());
 }
 
 int shwfs_frame_sync_range(shwfs_ctx* ctx, int iwfs0, int iwfs1, double* grad) {
@@ -1756,7 +1835,7 @@ int shwfs_frame_noalloc(shwfs_ctx* ctx, int iwfs, int isim, float* ints, float* 
 	WfsState* w = get_wfs(ctx, iwfs);
 	if (!w || (!ints && !grad)) return ctx ? fail(ctx, SHWFS_EINVAL, "frame_noalloc: bad arguments") : SHWFS_EINVAL;
 	PowfsState& p = ctx->powfs[w->d.ipowfs];
-	if (p.d.gradtype == SHWFS_GRAD_ZTILT) return fail(ctx, SHWFS_EINVAL, "frame_noalloc: geometric sensor");
+	if (is_geom(p.d.gradtype)) return fail(ctx, SHWFS_EINVAL, "frame_noalloc: geometric sensor");
 	if (p.d.nsa > SHWFS_NOALLOC_MAX_NSA)
 		return fail(ctx, SHWFS_EINVAL, "frame_noalloc: %d subapertures exceed the allocation-free maximum of %d",
 			p.d.nsa, SHWFS_NOALLOC_MAX_NSA);

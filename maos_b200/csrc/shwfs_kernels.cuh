@@ -653,16 +653,25 @@ __global__ void noise_grad_kernel(PowfsDev P, const WfsDev* __restrict__ wfs, in
 			lane, W.grad, P.nsa);
 }
 
+// Noise of geometric gradients, add_geom_noise_do (cuda/sim/wfsgrad.cu:39-51):
+// nea holds per subaperture the lower Cholesky factor (xx, yy, xy) of the
+// gradient noise covariance; gx += n1 nea_xx, gy += n2 nea_yy + n1 nea_xy,
+// n1 and n2 standard normals from the Philox stream (seed, 2^31 + isa, wfs,
+// frame).
+__device__ __forceinline__ void geom_noise(float& gx, float& gy, int isa, int nsa, const float* __restrict__ nea,
+	uint64_t seed, uint32_t wfs_id, uint32_t frame) {
+	PixelRng rng(seed, 0x80000000u + (uint32_t)isa, wfs_id, frame);
+	const float n1 = rng.normal(), n2 = rng.normal();
+	gx = fmaf(n1, nea[isa], gx);
+	gy = fmaf(n2, nea[isa + nsa], fmaf(n1, nea[isa + 2 * nsa], gy));
+}
+
 // Geometric gradients (z-tilt): the amplitude-weighted least-squares plane
 // of each subaperture's OPD, as cuztilt_do (cuda/sim/wfsgrad.cu:57-106) with
 // the inverse moment matrix of pts_mcc_ptt (math/loc.c:612-650) formed here:
 // g = [(b0, b1, b2) . imcc(:, 1), (b0, b1, b2) . imcc(:, 2)], b = (sum a o,
 // sum a o x, sum a o y), imcc = inv(sum a [1 x y]'[1 x y]), x = origx + ix dx.
-// One warp per subaperture, FP64 sums.  With nea (3 nsa: the lower Cholesky
-// factor per subaperture, xx, yy, xy) the noise of add_geom_noise_do
-// (cuda/sim/wfsgrad.cu:39-51) is added: gx += n1 nea_xx, gy += n2 nea_yy +
-// n1 nea_xy, n1 and n2 standard normals from the Philox stream (seed,
-// 2^31 + isa, wfs, frame).
+// One warp per subaperture, FP64 sums; with nea, geom_noise is added.
 __global__ void ztilt_kernel(const float* __restrict__ opd, const float* __restrict__ amp,
 	const double* __restrict__ origx, const double* __restrict__ origy, int nsa, int nopd, double dx,
 	float* __restrict__ grad, const float* __restrict__ nea, uint64_t seed, uint32_t wfs_id, uint32_t frame) {
@@ -700,12 +709,34 @@ __global__ void ztilt_kernel(const float* __restrict__ opd, const float* __restr
 			gx = (float)((m[6] * c01 + m[7] * c11 + m[8] * c12) / det);
 			gy = (float)((m[6] * c02 + m[7] * c12 + m[8] * c22) / det);
 		}
-		if (nea) {
-			PixelRng rng(seed, 0x80000000u + (uint32_t)isa, wfs_id, frame);
-			const float n1 = rng.normal(), n2 = rng.normal();
-			gx = fmaf(n1, nea[isa], gx);
-			gy = fmaf(n2, nea[isa + nsa], fmaf(n1, nea[isa + 2 * nsa], gy));
-		}
+		if (nea) geom_noise(gx, gy, isa, nsa, nea, seed, wfs_id, frame);
+		grad[isa] = gx;
+		grad[isa + nsa] = gy;
+	}
+}
+
+// Geometric gradients (G-tilt): grad = GS0 opd, GS0 the averaged-gradient
+// operator of mkg (lib/mkg.c:471-477) held in CSR (2 nsa rows, nsa nopd^2
+// columns), as cuspmul in cuda/sim/wfsgrad.cu:649.  One warp per
+// subaperture (rows isa and isa + nsa), FP64 sums; noise as ztilt_kernel.
+__global__ void gtilt_kernel(const int* __restrict__ rowptr, const int* __restrict__ col,
+	const float* __restrict__ val, int nsa, const float* __restrict__ opd, float* __restrict__ grad,
+	const float* __restrict__ nea, uint64_t seed, uint32_t wfs_id, uint32_t frame) {
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int isa = blockIdx.x * (blockDim.x >> 5) + warp;
+	if (isa >= nsa) return;
+	double sx = 0, sy = 0;
+	for (int k = rowptr[isa] + lane, e = rowptr[isa + 1]; k < e; k += 32) sx += (double)val[k] * opd[col[k]];
+	for (int k = rowptr[isa + nsa] + lane, e = rowptr[isa + nsa + 1]; k < e; k += 32)
+		sy += (double)val[k] * opd[col[k]];
+#pragma unroll
+	for (int off = 16; off > 0; off >>= 1) {
+		sx += __shfl_xor_sync(0xffffffffu, sx, off);
+		sy += __shfl_xor_sync(0xffffffffu, sy, off);
+	}
+	if (lane == 0) {
+		float gx = (float)sx, gy = (float)sy;
+		if (nea) geom_noise(gx, gy, isa, nsa, nea, seed, wfs_id, frame);
 		grad[isa] = gx;
 		grad[isa + nsa] = gy;
 	}

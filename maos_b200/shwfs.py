@@ -23,6 +23,7 @@ LIB_PATH = os.path.join(HERE, "libshwfs_b200.so")
 SHWFS_GRAD_MF = 1
 SHWFS_GRAD_COG = 2
 SHWFS_GRAD_ZTILT = 3
+SHWFS_GRAD_GTILT = 4
 SHWFS_FORM_FFT = 0
 SHWFS_FORM_TC = 1
 
@@ -108,6 +109,8 @@ def _load() -> C.CDLL:
         "shwfs_powfs_set_etf_dtrat": [vp, i, i],
         "shwfs_grad_ztilt_dev": [vp, i, vp, vp],
         "shwfs_wfs_set_neasim": [vp, i, dp],
+        "shwfs_powfs_set_gs0": [vp, i, i, C.c_long, C.c_long, ip, ip, dp],
+        "shwfs_grad_gtilt_dev": [vp, i, vp, vp],
     }
     for name, args in sig.items():
         f = getattr(lib, name)
@@ -224,6 +227,15 @@ class Context:
         (isim mod dtrat) / dtrat on slot 1 (0 turns it off)."""
         self._check(self._L.shwfs_powfs_set_etf_dtrat(self._h, ipowfs, int(dtrat)), "powfs_set_etf_dtrat")
 
+    def powfs_set_gs0(self, ipowfs, nrow, ncol, pp, pi, px, iamp=0):
+        """G-tilt operator (MAOS CSC: column pointers pp, row indices pi, values px)."""
+        a = np.ascontiguousarray(pp, dtype=np.int32)
+        b = np.ascontiguousarray(pi, dtype=np.int32)
+        v = _f64(px)
+        ipt = C.POINTER(C.c_int)
+        self._check(self._L.shwfs_powfs_set_gs0(self._h, ipowfs, iamp, nrow, ncol, a.ctypes.data_as(ipt),
+                                                b.ctypes.data_as(ipt), _dptr(v)), "powfs_set_gs0")
+
     def powfs_set_lltamp(self, ipowfs, lltamp):
         a = _f64(lltamp)
         self._check(self._L.shwfs_powfs_set_lltamp(self._h, ipowfs, _dptr(a)), "powfs_set_lltamp")
@@ -303,6 +315,10 @@ class Context:
     def grad_ztilt_dev(self, iwfs, opd, grad):
         """Geometric z-tilt gradients (2*nsa, device) of a device OPD (nsa*nopd^2)."""
         self._check(self._L.shwfs_grad_ztilt_dev(self._h, iwfs, _devptr(opd), _devptr(grad)), "grad_ztilt_dev")
+
+    def grad_gtilt_dev(self, iwfs, opd, grad):
+        """G-tilt gradients GS0 opd (2*nsa, device) of a device OPD."""
+        self._check(self._L.shwfs_grad_gtilt_dev(self._h, iwfs, _devptr(opd), _devptr(grad)), "grad_gtilt_dev")
 
     def grad_dev(self, iwfs, ints, grad):
         self._check(self._L.shwfs_grad_dev(self._h, iwfs, _devptr(ints), _devptr(grad)), "grad_dev")

@@ -160,6 +160,27 @@ class RefPowfs:
         lib().oref_ztilt(_p(opd), _p(g))
         return g
 
+    def gs0(self):
+        """The G-tilt operator as MAOS CSC arrays: (nrow, ncol, pp, pi, px)."""
+        L = lib()
+        L.oref_gs0_nnz.restype = C.c_long
+        nnz = L.oref_gs0_nnz()
+        ncol = self.nsa * self.nopd ** 2
+        pp = np.zeros(ncol + 1, dtype=np.int32)
+        pi = np.zeros(nnz, dtype=np.int32)
+        px = np.zeros(nnz)
+        nr, nc = C.c_long(), C.c_long()
+        L.oref_get_gs0(C.byref(nr), C.byref(nc), _p(pp), _p(pi), _p(px))
+        assert nc.value == ncol
+        return nr.value, nc.value, pp, pi, px
+
+    def gtilt(self, opd):
+        """G-tilt gradients GS0 opd (2 nsa)."""
+        g = np.zeros(2 * self.nsa)
+        opd = np.ascontiguousarray(opd, dtype=np.float64)
+        lib().oref_gtilt(_p(opd), _p(g))
+        return g
+
     def srot(self):
         a = np.zeros(self.nsa); lib().oref_get_srot(_p(a)); return a
 

@@ -59,6 +59,7 @@ typedef struct oref_cfg_t{
 }oref_cfg_t;
 
 static parms_t* g_parms=NULL;
+static dsp* g_gs0=NULL;  /* G-tilt operator of the current powfs, made on first use */
 static powfs_t* g_powfs=NULL;
 static dmat* g_wvl=NULL;
 
@@ -71,6 +72,8 @@ static lmat* lvec(long n, long start){
 /* Builds parms_t/powfs_t for one powfs with cfg->nwfs WFS and runs the
    reference's SH setup. Returns the number of valid subapertures. */
 int oref_setup(const oref_cfg_t* c){
+	dspfree(g_gs0);
+	g_gs0=NULL;
 	if(!global) global=mycalloc(1, global_t);
 	NTHREAD=c->nthread>0?c->nthread:1;
 	omp_set_num_threads(NTHREAD);
@@ -527,4 +530,31 @@ void oref_ztilt(const double* opd, double* grad){
 	dfree(g);
 	dcellfree(imcc);
 	dcellfree(mcc);
+}
+
+/* The G-tilt operator GS0 of the powfs as maos/powfs.c:619-626 makes it:
+   mkg (lib/mkg.c:471) on the WFS OPD grid with the amplitude, subaperture
+   list, saa and saat; CSC export and GS0*opd by the reference's dspmm. */
+static void gs0_make(void){
+	if(g_gs0) return;
+	g_gs0=mkg(g_powfs[0].loc, g_powfs[0].loc, P(g_powfs[0].amp, 0), g_powfs[0].saloc, P(g_powfs[0].saa, 0),
+		g_parms->powfs[0].saat, 1, 0, 0, 1);
+}
+long oref_gs0_nnz(void){ gs0_make(); return (long)g_gs0->pp[g_gs0->ny]; }
+void oref_get_gs0(long* nrow, long* ncol, int* pp, int* pi, double* px){
+	gs0_make();
+	*nrow=g_gs0->nx;
+	*ncol=g_gs0->ny;
+	const long nnz=g_gs0->pp[g_gs0->ny];
+	for(long i=0; i<=g_gs0->ny; i++) pp[i]=(int)g_gs0->pp[i];
+	for(long i=0; i<nnz; i++){ pi[i]=(int)g_gs0->pi[i]; px[i]=g_gs0->px[i]; }
+}
+void oref_gtilt(const double* opd, double* grad){
+	gs0_make();
+	dmat* o=dnew_do(g_gs0->ny, 1, (double*)opd, 0);
+	dmat* g=dnew(g_gs0->nx, 1);
+	dspmm(&g, g_gs0, o, "nn", 1);
+	copy_vec(grad, P(g), g_gs0->nx);
+	dfree(g);
+	dfree(o);
 }

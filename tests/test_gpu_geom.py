@@ -3,8 +3,10 @@ the reference's own CPU code (oracle/_ref):
 
 - z-tilt of a device OPD against pts_mcc_ptt / dcellinvspd_each / pts_ztilt
   (maos/powfs.c:633-645, math/loc.c:839-885) on the same OPD;
-- a full frame of a geometric sensor (ray trace + z-tilt) against the
-  reference's prop + pts_ztilt on the same screens;
+- G-tilt of a device OPD against the reference's mkg operator GS0
+  (lib/mkg.c:471, maos/powfs.c:619-626) applied by its dspmm;
+- full frames of geometric sensors (ray trace + z-tilt or G-tilt) against
+  the reference's prop + pts_ztilt / GS0 on the same screens;
 - the noise of geometric gradients (add_geom_noise_do,
   cuda/sim/wfsgrad.cu:39-51): sample covariance against L L^T;
 - LGS frames with two ETFs interpolated in time (maos/wfsints.c:215-223)
@@ -21,19 +23,23 @@ from tests.conftest import cuda_available
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not cuda_available(), reason="needs a CUDA GPU")]
 
 
-def _geom_ctx(ref_lib, cfg, thetas, noisy=0, nx=512, seed=3):
-    """A context with one geometric powfs of the reference's geometry and a
-    WFS per direction, under the turbulence of the workload builder."""
+def _geom_ctx(ref_lib, cfg, thetas, noisy=0, nx=512, seed=3, gradtype=None):
+    """A context with one geometric powfs of the reference's geometry (and,
+    for G-tilt, its GS0) and a WFS per direction, under the turbulence of the
+    workload builder."""
     from maos_b200 import shwfs
     from maos_b200.workload import build
     wl = build(cfg, device=0, seed=seed, noisy=False, nx=nx)  # for its screens and layers
     r = ref_lib.RefPowfs(cfg)
     ctx = shwfs.Context(0)
     ctx.set_dt(cfg["dt"])
+    gt = shwfs.SHWFS_GRAD_ZTILT if gradtype is None else gradtype
     ip = ctx.powfs_add(nsa=r.nsa, nopd=r.nopd, embfac=1, notf=0, pixpsax=0, pixpsay=0, dsa=cfg["dsa"],
-                       dx=r.ptsdx(), hs=cfg["hs"], areascale=1.0, wvl=cfg["wvl"], gradtype=shwfs.SHWFS_GRAD_ZTILT)
+                       dx=r.ptsdx(), hs=cfg["hs"], areascale=1.0, wvl=cfg["wvl"], gradtype=gt)
     ox, oy = r.ptsorig()
     ctx.powfs_set_geom(ip, ox, oy, r.amp())
+    if gt == shwfs.SHWFS_GRAD_GTILT:
+        ctx.powfs_set_gs0(ip, *r.gs0())
     ws = []
     for k, (tx, ty) in enumerate(thetas):
         i = ctx.wfs_add(ipowfs=ip, thetax=tx, thetay=ty, hs=cfg["hs"], hc=0.0, misregx=0.0, misregy=0.0,
@@ -65,11 +71,30 @@ def test_ztilt_dev_matches_reference(ref_lib):
     wl.close()
 
 
+def test_gtilt_dev_matches_reference(ref_lib):
+    import torch
+    from maos_b200 import shwfs
+    from maos_b200.configs import NGS8
+    ctx, ip, ws, wl, r = _geom_ctx(ref_lib, NGS8, [(0.0, 0.0)], gradtype=shwfs.SHWFS_GRAD_GTILT)
+    opd = torch.zeros(r.nsa * r.nopd ** 2, dtype=torch.float32, device="cuda")
+    grad = torch.zeros(2 * r.nsa, dtype=torch.float32, device="cuda")
+    ctx.raytrace_dev(ws[0], 17, opd)
+    ctx.grad_gtilt_dev(ws[0], opd, grad)
+    ctx.sync()
+    g_ref = r.gtilt(opd.double().cpu().numpy())
+    assert _rel(grad.double().cpu().numpy(), g_ref) <= 1e-5
+    ctx.close()
+    wl.close()
+
+
 @pytest.mark.parametrize("isim", [0, 41])
-def test_geometric_frame_matches_reference(ref_lib, isim):
+@pytest.mark.parametrize("kind", ["ztilt", "gtilt"])
+def test_geometric_frame_matches_reference(ref_lib, isim, kind):
+    from maos_b200 import shwfs
     from maos_b200.configs import NGS8
     thetas = [(NGS8["thetax"][0], NGS8["thetay"][0]), (3e-5, -2e-5)]
-    ctx, ip, ws, wl, r = _geom_ctx(ref_lib, NGS8, thetas)
+    gt = shwfs.SHWFS_GRAD_ZTILT if kind == "ztilt" else shwfs.SHWFS_GRAD_GTILT
+    ctx, ip, ws, wl, r = _geom_ctx(ref_lib, NGS8, thetas, gradtype=gt)
     ctx.frame_queue(isim, ws[0], ws[-1] + 1)
     out = ctx.frame_sync_range(ws[0], ws[-1] + 1, lambda i: r.nsa)
     dt = NGS8["dt"]
@@ -78,7 +103,7 @@ def test_geometric_frame_matches_reference(ref_lib, isim):
         for L, scr in zip(wl.layers, wl.screens):
             r.prop_layer(scr, L["dx"], L["ox"], L["oy"], L["ht"], tx, ty, NGS8["hs"], -L["vx"] * dt * isim,
                          -L["vy"] * dt * isim, opd=opd_ref)
-        g_ref = r.ztilt(opd_ref)
+        g_ref = r.ztilt(opd_ref) if kind == "ztilt" else r.gtilt(opd_ref)
         assert _rel(out[k], g_ref) <= 1e-4, (k, _rel(out[k], g_ref))
     with pytest.raises(Exception):
         ctx.frame_sync(ws[0], ip, want_ints=True)  # no pixels on a geometric sensor

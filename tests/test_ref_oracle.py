@@ -53,6 +53,18 @@ def test_reference_ztilt_known_answer(ref_lib):
     assert np.allclose(g[r.nsa:], b, rtol=1e-9, atol=0)
 
 
+def test_reference_gtilt_known_answer(ref_lib):
+    """GS0 (mkg) applied to a plane gives its slope in every subaperture."""
+    from maos_b200.configs import NGS8
+    r = ref_lib.RefPowfs(NGS8)
+    nrow, ncol, pp, pi, px = r.gs0()
+    assert (nrow, ncol) == (2 * r.nsa, r.nsa * r.nopd ** 2) and pp[-1] == len(px)
+    a, b = 2.5e-6, -1.25e-6
+    g = r.gtilt(_tilt_opd(r, a, b))
+    assert np.allclose(g[:r.nsa], a, rtol=1e-9, atol=0)
+    assert np.allclose(g[r.nsa:], b, rtol=1e-9, atol=0)
+
+
 def test_reference_second_etf(ref_lib):
     """The second ETF slot: same focus gives the first ETF, another focus a different one."""
     from maos_b200.configs import LGS30
