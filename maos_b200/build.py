@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libshwfs_b200.so")
 SOURCES = [os.path.join(HERE, "csrc", "shwfs_api.cu")]
-HOST_SOURCES = [os.path.join(HERE, "csrc", "host", f) for f in ("hmath.c", "setup.c")]
+HOST_SOURCES = [os.path.join(HERE, "csrc", "host", f) for f in ("hmath.c", "setup.c", "binio.c")]
 OBJDIR = os.path.join(HERE, "_build")
 
 
@@ -57,7 +57,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         subprocess.run([os.environ.get("CC", "gcc"), "-std=gnu11", "-O2", "-fPIC", "-Wall", "-Wno-unused-function",
                         "-c", src, "-o", obj], check=True)
         objs.append(obj)
-    cmd = [nvcc(), *NVCC_FLAGS, *SOURCES, *objs, "-o", LIB]
+    cmd = [nvcc(), *NVCC_FLAGS, *SOURCES, *objs, "-lz", "-o", LIB]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd), file=sys.stderr)

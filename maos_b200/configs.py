@@ -101,7 +101,16 @@ LGS8_N64 = dict(
     atm=dict(LGS30["atm"], nx=512, dx=1.0 / 64),
 )
 
-CONFIGS = {c["name"]: c for c in (NGS8, LGS30, LGS30_N64, NGS30_2X2, TT30, LGS8_N64)}
+# The LGS30 sensor (16x16 OPD points, FFT 32, 6x6 pixels, matched filter) on
+# an 8 m telescope with 16x16 subapertures: a parity-test case small enough
+# for committed fixtures.
+LGS8_N32 = dict(
+    LGS30, name="lgs8_2x16x16_mf",
+    D=8.0, Din=1.2, order=16, llt_ox=4.0, nwfs=2, thetax=[10.0 * AS2RAD, -10.0 * AS2RAD], thetay=[0.0, 5.0 * AS2RAD],
+    atm=dict(LGS30["atm"], nx=512),
+)
+
+CONFIGS = {c["name"]: c for c in (NGS8, LGS30, LGS30_N64, NGS30_2X2, TT30, LGS8_N64, LGS8_N32)}
 
 # The uneven batch: six LGS of LGS30 (FFT 32), the 2x2 NGS (FFT 128) and the
 # two tip-tilt sensors (FFT 256) in one frame, on the LGS30 atmosphere.

@@ -558,3 +558,55 @@ void oref_gtilt(const double* opd, double* grad){
 	dfree(g);
 	dfree(o);
 }
+
+/* The reference's own .bin writer and reader (writebin, math/cell.c:330-337;
+   dread/readbin, math/cell.c:545-559) on plain arrays, to check the
+   product's format code byte for byte and to write golden fixtures. */
+void oref_writebin_d(const char* fn, const double* p, long nx, long ny, const char* keywords){
+	dmat* a=dnew(nx, ny);
+	copy_vec(P(a), p, nx*ny);
+	if(keywords) a->keywords=strdup(keywords);
+	writebin(a, "%s", fn);
+	dfree(a);
+}
+void oref_writebin_f(const char* fn, const float* p, long nx, long ny, const char* keywords){
+	smat* a=snew(nx, ny);
+	memcpy(P(a), p, sizeof(float)*nx*ny);
+	if(keywords) a->keywords=strdup(keywords);
+	writebin(a, "%s", fn);
+	sfree(a);
+}
+void oref_writebin_c(const char* fn, const double* p, long nx, long ny){
+	cmat* a=cnew(nx, ny);
+	memcpy(P(a), p, sizeof(double)*2*nx*ny);
+	writebin(a, "%s", fn);
+	cfree(a);
+}
+/* A cell of n members, member i of nx[i] x ny[i] doubles (0 x 0 = empty). */
+void oref_writebin_dcell(const char* fn, int n, const long* nx, const long* ny, const double* const* p,
+	const char* keywords){
+	dcell* c=dcellnew(n, 1);
+	for(int i=0; i<n; i++){
+		if(nx[i]*ny[i]>0){
+			P(c, i)=dnew(nx[i], ny[i]);
+			copy_vec(P(P(c, i)), p[i], nx[i]*ny[i]);
+		}
+	}
+	if(keywords) c->keywords=strdup(keywords);
+	writebin(c, "%s", fn);
+	dcellfree(c);
+}
+void oref_writebin_gs0(const char* fn){
+	gs0_make();
+	writebin(g_gs0, "%s", fn);
+}
+/* dread of a file: returns nx*ny (copied up to nmax), dimensions in *nx, *ny. */
+long oref_readbin_d(const char* fn, double* out, long nmax, long* nx, long* ny){
+	dmat* a=dread("%s", fn);
+	if(!a){ *nx=*ny=0; return 0; }
+	*nx=a->nx; *ny=a->ny;
+	long n=a->nx*a->ny;
+	copy_vec(out, P(a), n<nmax?n:nmax);
+	dfree(a);
+	return n;
+}
