@@ -96,6 +96,17 @@ int shwfs_setup_load_wfs(const shwfs_setup* s, shwfs_ctx* ctx, int iwfs);
 int shwfs_screens_vonkarman(double* const* out, int nlayer, long nx, long ny, double dx, double r0, double L0,
 	const double* wt, uint32_t seed);
 
+/* Science aperture of an annulus (D, Din) sampled at dx, as setup_aper
+   builds it without loaded locs, amplitude map or pupil mask
+   (maos/aper.c:45-110): create_metapupil with one guard point and
+   loc_from_map (math/map.c:131-239, math/loc.c:448-492), mkamp's
+   area-weighted annulus (loc_circle_add, math/loc.c:942-986), loc_reduce of
+   each row's leading and trailing points below EPS (math/loc.c:1048-1128)
+   and the amplitude normalised to sum 1.  With locx == NULL only *nloc is
+   set; otherwise locx, locy, amp receive *nloc values (row by row, x
+   fastest). */
+int shwfs_aper_build(double D, double Din, double dx, long* nloc, double* locx, double* locy, double* amp);
+
 #ifdef __cplusplus
 }
 #endif

@@ -817,3 +817,102 @@ int shwfs_screens_vonkarman(double* const* out, int nlayer, long nx, long ny, do
 	free(p2);
 	return 0;
 }
+
+/* ---- science aperture: maos/aper.c:45-110 for an annulus ---- */
+
+/* X(circle) (math/matmath.c:476-516) on an nx x ny map of spacing dx with
+   centre (cx, cy) in map coordinates, val 1: the bilinear-weighted coverage
+   of each point, kept as the mask (coverage > 1e-15) create_metapupil uses. */
+static int circle_mask_pt(int ix, int iy, double cx, double cy, double dx, double r) {
+	const int nres = 10;
+	const double res = 2. / nres, res2 = res * res, resm = (nres - 1) * 0.5;
+	const double r2 = r * r;
+	const double r2l = r > 1.5 ? ((r - 1.5) * (r - 1.5)) : 0;
+	const double r2u = (r + 2.5) * (r + 2.5);
+	const double r2y = (iy * dx - cy) * (iy * dx - cy);
+	const double r2r = (ix * dx - cx) * (ix * dx - cx) + r2y;
+	double v = 0;
+	if (r2r < r2l) {
+		v = 1;
+	} else if (r2r < r2u) {
+		double tot = 0.;
+		for (int jy = 0; jy < nres; jy++) {
+			const double iiy = iy + (jy - resm) * res;
+			const double rr2y = (iiy * dx - cy) * (iiy * dx - cy);
+			const double wty = 1. - fabs(iy - iiy);
+			for (int jx = 0; jx < nres; jx++) {
+				const double iix = ix + (jx - resm) * res;
+				const double rr2r = (iix * dx - cx) * (iix * dx - cx) + rr2y;
+				const double wtx = 1. - fabs(ix - iix);
+				if (rr2r < r2) tot += res2 * wty * wtx;
+			}
+		}
+		v = tot;
+	}
+	return v > 1.e-15;
+}
+
+int shwfs_aper_build(double D, double Din, double dx, long* nloc, double* locx, double* locy, double* amp) {
+	if (!nloc || !(D > 0) || !(dx > 0) || Din < 0 || Din >= D) return SHWFS_EINVAL;
+	const double R = D / 2, guard = dx;
+	// create_metapupil (math/map.c:144-182) with ht0 = 0, offset 0, no padding
+	const double minx = -R - guard, maxx = R + guard;
+	const double ox = floor(minx / dx) * dx;
+	const long nx = (long)ceil((maxx - ox) / dx) + 1;
+	const double oy = floor(minx / dx) * dx;
+	const long ny = (long)ceil((maxx - oy) / dx) + 1;
+	if (nx > 100000) return SHWFS_EINVAL;
+	const long cap = locx ? *nloc : 0;
+	double* row = (double*)malloc(sizeof(double) * nx);
+	double* ax = locx ? (double*)malloc(sizeof(double) * (cap > 0 ? cap : 1)) : NULL;
+	if (!row || (locx && !ax)) {
+		free(row);
+		free(ax);
+		return SHWFS_ENOMEM;
+	}
+	long count = 0;
+	for (long iy = 0; iy < ny; iy++) {
+		// loc_from_map: the row from its first to its last masked point
+		long i0 = -1, i1 = -1;
+		for (long ix = 0; ix < nx && i0 < 0; ix++)
+			if (circle_mask_pt((int)ix, (int)iy, -ox, -oy, dx, R)) i0 = ix;
+		for (long ix = nx - 1; ix > -1 && i1 < 0; ix--)
+			if (circle_mask_pt((int)ix, (int)iy, -ox, -oy, dx, R)) i1 = ix;
+		if (i0 < 0) continue;
+		// mkamp: loc_circle_add of the annulus; loc_reduce (cont = 1) drops
+		// the row's leading and trailing points below EPS
+		long j0 = -1, j1 = -1;
+		for (long ix = i0; ix <= i1; ix++) {
+			const double x = ix * dx + ox, y = iy * dx + oy;
+			double a = circle_add_pt(x, y, dx, R, 1);
+			if (Din > 0) a += circle_add_pt(x, y, dx, Din * 0.5, -1);
+			row[ix] = a;
+			if (a >= 1.e-15) {
+				if (j0 < 0) j0 = ix;
+				j1 = ix;
+			}
+		}
+		if (j0 < 0) continue;
+		for (long ix = j0; ix <= j1; ix++, count++) {
+			if (!locx) continue;
+			if (count >= cap) {
+				free(row);
+				free(ax);
+				return SHWFS_EINVAL;
+			}
+			locx[count] = ix * dx + ox;
+			locy[count] = iy * dx + oy;
+			ax[count] = row[ix];
+		}
+	}
+	if (locx) {
+		double sum = 0;  // dnormalize_sum: scale by 1 / (sequential sum)
+		for (long i = 0; i < count; i++) sum += ax[i];
+		const double w = 1. / sum;
+		for (long i = 0; i < count; i++) amp[i] = ax[i] * w;
+	}
+	free(row);
+	free(ax);
+	*nloc = count;
+	return 0;
+}

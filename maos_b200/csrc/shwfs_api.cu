@@ -87,6 +87,8 @@ struct LayerState {
 
 }  // namespace
 
+struct EvlState;  // science-path evaluation (shwfs_evl_host.cuh)
+
 struct shwfs_ctx {
 	int device = 0;
 	cudaStream_t stream = nullptr;
@@ -127,7 +129,9 @@ struct shwfs_ctx {
 		cudaEvent_t a, b;
 	};
 	std::vector<Mark> marks;
+	EvlState* evl = nullptr;
 };
+static void evl_free(shwfs_ctx* ctx);
 
 static cudaEvent_t ev_get(shwfs_ctx* ctx) {
 	if (!ctx->ev_pool.empty()) {
@@ -272,6 +276,7 @@ int shwfs_destroy(shwfs_ctx* ctx) {
 		for (auto& b : p.gs0_col) b.free_();
 		for (auto& b : p.gs0_val) b.free_();
 	}
+	evl_free(ctx);
 	for (auto& c : ctx->desc_cache) c.d.free_();
 	if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
 	for (size_t i = 0; i < ctx->pstream.size(); i++) {
@@ -1902,3 +1907,5 @@ int shwfs_frame_noalloc(shwfs_ctx* ctx, int iwfs, int isim, float* ints, float* 
 }
 
 }  // extern "C"
+
+#include "shwfs_evl_host.cuh"

@@ -59,6 +59,8 @@ def _lib():
         L.shwfs_setup_load_wfs.argtypes = [vp, vp, i]
         L.shwfs_screens_vonkarman.argtypes = [C.POINTER(dp), i, C.c_long, C.c_long, C.c_double, C.c_double, C.c_double,
                                              dp, C.c_uint32]
+        L.shwfs_aper_build.argtypes = [C.c_double, C.c_double, C.c_double, C.POINTER(C.c_long), dp, dp, dp]
+        L.shwfs_aper_build.restype = i
         _bound = True
     return L
 
@@ -158,3 +160,17 @@ def screens(nx: int, ny: int, dx: float, r0: float, L0: float, wt: Sequence[floa
     if rc != 0:
         raise shwfs.ShwfsError("screen generation failed")
     return outs
+
+
+def aperture(D: float, Din: float, dx: float):
+    """Science aperture of an annulus sampled at dx (shwfs_aper_build): (locx,
+    locy, amp) with the amplitude normalised to sum 1."""
+    L = _lib()
+    n = C.c_long()
+    if L.shwfs_aper_build(D, Din, dx, C.byref(n), None, None, None) != 0:
+        raise shwfs.ShwfsError("aperture: bad arguments")
+    x, y, a = np.zeros(n.value), np.zeros(n.value), np.zeros(n.value)
+    dp = C.POINTER(C.c_double)
+    if L.shwfs_aper_build(D, Din, dx, C.byref(n), x.ctypes.data_as(dp), y.ctypes.data_as(dp), a.ctypes.data_as(dp)):
+        raise shwfs.ShwfsError("aperture: build failed")
+    return x, y, a

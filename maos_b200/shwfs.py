@@ -12,6 +12,7 @@ module fails.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 from typing import Optional, Sequence
 
@@ -110,6 +111,14 @@ def _load() -> C.CDLL:
         "shwfs_grad_ztilt_dev": [vp, i, vp, vp],
         "shwfs_wfs_set_neasim": [vp, i, dp],
         "shwfs_powfs_set_gs0": [vp, i, i, C.c_long, C.c_long, ip, ip, dp],
+        "shwfs_evl_set_aper": [vp, C.c_long, dp, dp, C.c_double, dp],
+        "shwfs_evl_add_dir": [vp, C.c_double, C.c_double, C.c_double, ip],
+        "shwfs_evl_set_psf": [vp, i, dp, ip, ip, i],
+        "shwfs_evl_queue": [vp, i, i],
+        "shwfs_evl_sync": [vp, dp, dp],
+        "shwfs_evl_psf_get": [vp, i, i, dp, C.POINTER(C.c_long)],
+        "shwfs_evl_psf_reset": [vp],
+        "shwfs_evl_opd_dev": [vp, i, vp],
         "shwfs_grad_gtilt_dev": [vp, i, vp, vp],
     }
     for name, args in sig.items():
@@ -329,6 +338,53 @@ class Context:
         self._check(self._L.shwfs_addnoise_dev(self._h, _devptr(ints), ints.numel(), _devptr(bkgrnd2),
                                                _devptr(bkgrnd2c), _devptr(qe), bkgrnd, bkgrndc, rne, excess,
                                                seed, stream, frame), "addnoise_dev")
+
+    # ---- science path (include/shwfs_evl.h) ----
+    def evl_set_aper(self, locx, locy, dx, amp):
+        x, y, a = _f64(locx), _f64(locy), _f64(amp)
+        self._check(self._L.shwfs_evl_set_aper(self._h, len(x), _dptr(x), _dptr(y), float(dx), _dptr(a)),
+                    "evl_set_aper")
+        self._evl_n = 0
+
+    def evl_add_dir(self, thetax, thetay, hs=math.inf) -> int:
+        out = C.c_int()
+        self._check(self._L.shwfs_evl_add_dir(self._h, float(thetax), float(thetay), float(hs), C.byref(out)),
+                    "evl_add_dir")
+        self._evl_n = out.value + 1
+        return out.value
+
+    def evl_set_psf(self, wvl, nembed, psfsize=None, pttr=False):
+        w = _f64(wvl)
+        n = np.ascontiguousarray(nembed, dtype=np.int32)
+        p = np.ascontiguousarray(psfsize if psfsize is not None else [0] * len(w), dtype=np.int32)
+        ipt = C.POINTER(C.c_int)
+        self._check(self._L.shwfs_evl_set_psf(self._h, len(w), _dptr(w), n.ctypes.data_as(ipt), p.ctypes.data_as(ipt),
+                                              1 if pttr else 0), "evl_set_psf")
+        self._evl_psfsize = [int(q if q > 0 else m) for q, m in zip(p, n)]
+
+    def evl_queue(self, isim: int, do_psf: bool = False):
+        self._check(self._L.shwfs_evl_queue(self._h, int(isim), 1 if do_psf else 0), "evl_queue")
+
+    def evl_sync(self):
+        """(wfe, coeff), each (nevl, 3): {PR, TT, PTTR} and {piston, tip, tilt}."""
+        n = getattr(self, "_evl_n", 0)
+        wfe, coeff = np.zeros(3 * n), np.zeros(3 * n)
+        self._check(self._L.shwfs_evl_sync(self._h, _dptr(wfe), _dptr(coeff)), "evl_sync")
+        return wfe.reshape(n, 3), coeff.reshape(n, 3)
+
+    def evl_psf(self, ievl: int, iwvl: int):
+        """(psf (psfsize, psfsize) with psf[ix, iy], number of frames summed)."""
+        n = self._evl_psfsize[iwvl]
+        out = np.zeros(n * n)
+        nf = C.c_long()
+        self._check(self._L.shwfs_evl_psf_get(self._h, ievl, iwvl, _dptr(out), C.byref(nf)), "evl_psf_get")
+        return out.reshape(n, n, order="F"), nf.value
+
+    def evl_psf_reset(self):
+        self._check(self._L.shwfs_evl_psf_reset(self._h), "evl_psf_reset")
+
+    def evl_opd_dev(self, ievl: int, opd):
+        self._check(self._L.shwfs_evl_opd_dev(self._h, ievl, _devptr(opd)), "evl_opd_dev")
 
     def sync(self):
         self._check(self._L.shwfs_sync(self._h), "sync")

@@ -295,3 +295,40 @@ def genatm_simple(r0, L0, slope, dx, n, seed):
     lib().oref_genatm_simple(C.c_double(r0), C.c_double(L0), C.c_double(slope), C.c_double(dx), C.c_long(n),
                              C.c_uint(seed), _p(out))
     return out.reshape(n, n)
+
+
+class RefEvl:
+    """The reference's science aperture and open-loop evaluation (setup_aper
+    for an annulus; prop onto aper->locs, loc_calc_ptt, locfft_psf)."""
+
+    def __init__(self, D, Din, dx, wvl=(), nembed=()):
+        L = lib()
+        L.oref_evl_setup.restype = C.c_long
+        w = np.ascontiguousarray(wvl, dtype=np.float64)
+        n = np.ascontiguousarray(nembed, dtype=np.int64)
+        self.nwvl = len(w)
+        self.nloc = L.oref_evl_setup(C.c_double(D), C.c_double(Din), C.c_double(dx), C.c_int(self.nwvl), _p(w), _p(n))
+        self.dx = dx
+
+    def aper(self):
+        x, y, a = np.zeros(self.nloc), np.zeros(self.nloc), np.zeros(self.nloc)
+        lib().oref_evl_get_aper(_p(x), _p(y), _p(a))
+        return x, y, a
+
+    def frame(self, thetax, thetay, hs, isim, dt, pttr=0, psfsize=None):
+        """(opd, wfe[3], coeff[3], [psf per wavelength] or None)"""
+        opd, wfe, coeff = np.zeros(self.nloc), np.zeros(3), np.zeros(3)
+        psf = None
+        ps = None
+        if psfsize is not None:
+            ps = np.ascontiguousarray(psfsize, dtype=np.int64)
+            psf = np.zeros(int(np.sum(ps.astype(np.int64) ** 2)))
+        lib().oref_evl_frame(C.c_double(thetax), C.c_double(thetay), C.c_double(hs), C.c_int(isim), C.c_double(dt),
+                             C.c_int(pttr), C.c_int(self.nwvl), _p(ps), _p(opd), _p(wfe), _p(coeff), _p(psf))
+        out = None
+        if psf is not None:
+            out, off = [], 0
+            for n in ps:
+                out.append(psf[off:off + n * n].reshape(n, n, order="F"))
+                off += n * n
+        return opd, wfe, coeff, out

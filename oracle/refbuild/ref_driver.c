@@ -610,3 +610,76 @@ long oref_readbin_d(const char* fn, double* out, long nmax, long* nx, long* ny){
 	dfree(a);
 	return n;
 }
+
+/* Science aperture and open-loop evaluation by the reference's own code:
+   setup_aper (maos/aper.c:32-150) for an annulus (no loaded locs, amplitude
+   map, pupil mask or distortion), then per frame the atmosphere traced onto
+   aper->locs as perfevl_ievl does (prop with the locs' column statistics,
+   maos/sim_utils.c:729-743 and maos/perfevl.c:146-166), loc_calc_ptt
+   (math/loc.c:653-709) and, for the PSF, loc_sub_ptt when pttr and
+   locfft_psf followed by |.|^2 (maos/perfevl.c:206-226). */
+static loc_t* g_elocs=NULL;
+static dmat* g_eamp=NULL;
+static dmat* g_emcc=NULL;
+static dmat* g_eimcc=NULL;
+static real g_eipcc=0;
+static locfft_t* g_elocfft=NULL;
+long oref_evl_setup(double D, double Din, double dx, int nwvl, const double* wvl, const long* nembed){
+	if(g_elocfft){ locfft_free(g_elocfft); g_elocfft=NULL; }
+	locfree(g_elocs); dfree(g_eamp); dfree(g_emcc); dfree(g_eimcc);
+	map_t* smap=NULL;
+	create_metapupil(&smap, 0, 0, NULL, D, 0, dx, dx, 0, dx, 0, 0, 0, 0);
+	g_elocs=loc_from_map(smap, 0);
+	mapfree(smap);
+	g_eamp=mkamp(g_elocs, NULL, 0, 0, D, Din);
+	loc_reduce(g_elocs, g_eamp, EPS, 1, NULL);
+	loc_create_stat(g_elocs);
+	dnormalize_sum(g_eamp, 1);
+	g_emcc=loc_mcc_ptt(g_elocs, P(g_eamp));
+	g_eipcc=1./P(g_emcc, 0);
+	g_eimcc=dinvspd(g_emcc);
+	if(nwvl>0){
+		dmat* w=dnew(nwvl, 1);
+		lmat* fs=lnew(nwvl, 1);
+		for(int i=0; i<nwvl; i++){ P(w, i)=wvl[i]; P(fs, i)=nembed[i]; }
+		g_elocfft=locfft_init(g_elocs, g_eamp, w, fs, 2, 0);
+		dfree(w);
+		lfree(fs);
+	}
+	return g_elocs->nloc;
+}
+void oref_evl_get_aper(double* locx, double* locy, double* amp){
+	copy_vec(locx, g_elocs->locx, g_elocs->nloc);
+	copy_vec(locy, g_elocs->locy, g_elocs->nloc);
+	copy_vec(amp, P(g_eamp), g_elocs->nloc);
+}
+/* One frame of direction (thetax, thetay, hs): opd (nloc), wfe {PR, TT,
+   PTTR}, coeff {p, tip, tilt}, and per wavelength the psfsize^2 |PSF|^2
+   (column-major, concatenated), when psf is not NULL. */
+void oref_evl_frame(double thetax, double thetay, double hs, int isim, double dt, int pttr, int nwvl,
+	const long* psfsize, double* opd, double* wfe, double* coeff, double* psf){
+	dmat* o=dnew(g_elocs->nloc, 1);
+	for(int ips=0; ips<g_natm; ips++){
+		prop(&(propdata_t){.mapin=g_atm[ips], .ostat=g_elocs->stat, .phiout=P(o), .alpha=1, .hs=hs,
+			.thetax=thetax, .thetay=thetay, .shiftx=-g_atm[ips]->vx*isim*dt, .shifty=-g_atm[ips]->vy*isim*dt,
+			.wrap=1});
+	}
+	copy_vec(opd, P(o), g_elocs->nloc);
+	loc_calc_ptt(wfe, coeff, g_elocs, g_eipcc, g_eimcc, P(g_eamp), P(o));
+	if(psf && g_elocfft){
+		if(pttr) loc_sub_ptt(o, coeff, g_elocs);
+		lmat* ps=lnew(nwvl, 1);
+		for(int i=0; i<nwvl; i++) P(ps, i)=psfsize[i];
+		ccell* psf2s=NULL;
+		locfft_psf(&psf2s, g_elocfft, o, ps, 0);
+		long off=0;
+		for(int i=0; i<nwvl; i++){
+			cmat* c=P(psf2s, i);
+			for(long k=0; k<PN(c); k++) psf[off+k]=creal(P(c, k)*conj(P(c, k)));
+			off+=PN(c);
+		}
+		ccellfree(psf2s);
+		lfree(ps);
+	}
+	dfree(o);
+}
