@@ -524,6 +524,195 @@ def run_serving(args):
     return 0
 
 
+def _science_ctx(scfg, device, seed):
+    import torch  # noqa: F401
+    from maos_b200 import shwfs
+    from maos_b200.setup import aperture, screens
+    from maos_b200.workload import wind
+    x, y, a = aperture(scfg["D"], scfg["Din"], scfg["dx"])
+    ctx = shwfs.Context(device)
+    ctx.set_dt(scfg["dt"])
+    at = scfg["atm"]
+    n = at["nx"]
+    scr = screens(n, n, at["dx"], at["r0"], at["L0"], at["wt"], seed)
+    vx, vy = wind(scfg, seed)
+    o = -n / 2 * at["dx"]
+    layers = [dict(nx=n, ny=n, dx=at["dx"], ox=o, oy=o, ht=float(h), vx=float(vx[i]), vy=float(vy[i]), alpha=1.0)
+              for i, h in enumerate(at["ht"])]
+    ctx.atm_set(layers, scr)
+    ctx.evl_set_aper(x, y, scfg["dx"], a)
+    for d in scfg["dirs"]:
+        ctx.evl_add_dir(*d)
+    ctx.evl_set_psf(scfg["wvl"], scfg["nembed"], scfg["psfsize"], pttr=scfg["pttr"])
+    # points traced per direction: the 16x16 tiles that hold aperture points
+    X = np.rint((x - x.min()) / scfg["dx"]).astype(np.int64)
+    Y = np.rint((y - y.min()) / scfg["dx"]).astype(np.int64)
+    ntx = (X.max() + 16) // 16
+    traced = 256 * len(np.unique((Y // 16) * ntx + X // 16))
+    return ctx, len(x), layers, scr, traced
+
+
+def science_flops(scfg, nX):
+    """Nominal FFT flops of one direction-frame's PSFs: per wavelength nY rows
+    and psfsize columns of N-point transforms (5 N log2 N each)."""
+    tot = 0.0
+    for N, ps in zip(scfg["nembed"], scfg["psfsize"]):
+        tot += (nX + ps) * 5 * N * math.log2(N)
+    return tot
+
+
+def science_cpu(scfg, layers, scr, seconds=20.0, max_frames=4):
+    from oracle import ref
+    e = ref.RefEvl(scfg["D"], scfg["Din"], scfg["dx"], wvl=scfg["wvl"], nembed=scfg["nembed"])
+    ref.atm_set(scr, layers)
+    t, n = 0.0, 0
+    while t < seconds and n < max_frames:
+        d = scfg["dirs"][n % len(scfg["dirs"])]
+        t0 = time.perf_counter()
+        e.frame(d[0], d[1], d[2], n, scfg["dt"], pttr=scfg["pttr"], psfsize=scfg["psfsize"])
+        t += time.perf_counter() - t0
+        n += 1
+    nw = len(scfg["wvl"])
+    return n / t, n, min(nw, os.cpu_count() or 1)
+
+
+def run_science(args, scfg):
+    """Science path: every direction of a frame (ray trace, WFE, PSFs)."""
+    import torch
+    ws, rank, local = dist_init()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        from maos_b200.setup import screens
+        from maos_b200.workload import wind
+        at = scfg["atm"]
+        n = at["nx"]
+        scr = screens(n, n, at["dx"], at["r0"], at["L0"], at["wt"], 1)
+        vx, vy = wind(scfg, 1)
+        o = -n / 2 * at["dx"]
+        layers = [dict(nx=n, ny=n, dx=at["dx"], ox=o, oy=o, ht=float(h), vx=float(vx[i]), vy=float(vy[i]))
+                  for i, h in enumerate(at["ht"])]
+        v, nfr, cores = science_cpu(scfg, layers, scr, seconds=30.0, max_frames=max(args.steps, 1))
+        sample = (f"{nfr} direction-frames of {scfg['name']}: prop of 7 layers onto aper->locs, loc_calc_ptt, "
+                  f"locfft_psf at 3 wavelengths (reference C, FFT stand-in for FFTW)")
+        print(json.dumps({"impl": "reference", "metric": "science direction-frames/s", "value": v,
+                          "unit": "direction-frames/s", "n_gpus": args.gpus, "steps": nfr, "warmup": 0,
+                          "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                          "config": {"workload": scfg["name"], "step": "one direction-frame (reference CPU path)"},
+                          "cpu_baseline": {"value": v, "unit": "direction-frames/s", "cores": cores,
+                                           "kind": "reference", "sample": sample},
+                          "e2e": {"value": v, "unit": "direction-frames/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}))
+        return 0
+    ctx, nloc, layers, scr, npts_traced = _science_ctx(scfg, local, 1 + rank)
+    nevl = len(scfg["dirs"])
+    ext = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    isim = 0
+    for _ in range(args.warmup):
+        ctx.evl_queue(isim, do_psf=True)
+        ctx.evl_sync()
+        isim += 1
+    barrier(ws, dev)
+    clk = ClockSampler(local)
+    clk.start()
+    time.sleep(0.5)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with torch.cuda.stream(ext):
+        for k in range(args.steps):
+            flush.zero_()
+            starts[k].record(ext)
+            ctx.evl_queue(isim, do_psf=True)
+            ends[k].record(ext)
+            isim += 1
+    ctx.sync()
+    torch.cuda.synchronize(dev)
+    clocks = clk.stop()
+    step_ms = [s_.elapsed_time(e_) for s_, e_ in zip(starts, ends)]
+    tot_ms = allreduce_max(sum(step_ms), ws, dev)
+    value = nevl * args.steps * ws / (tot_ms * 1e-3)
+    ctx.profile_enable(True)
+    nprof = min(args.steps, 10)
+    with torch.cuda.stream(ext):
+        for k in range(nprof):
+            flush.zero_()
+            ctx.evl_queue(isim, do_psf=True)
+            isim += 1
+    ctx.sync()
+    stages = ctx.profile_read()
+    ctx.profile_enable(False)
+    launches_per_step = sum(n for _, n in stages.values()) / nprof
+    ctx.copy_counters()
+    e2e_s = 0.0
+    for k in range(args.steps):
+        with torch.cuda.stream(ext):
+            flush.zero_()
+        ctx.sync()
+        t0 = time.perf_counter()
+        ctx.evl_queue(isim, do_psf=True)
+        ctx.evl_sync()
+        e2e_s += time.perf_counter() - t0
+        isim += 1
+    h2d, d2h = ctx.copy_counters()
+    e2e_s = allreduce_max(e2e_s, ws, dev)
+    e2e = nevl * args.steps * ws / e2e_s
+    st = {k: dict(ms_per_launch=(ms / n if n else 0.0), launches_per_step=n / nprof, ms_per_step=ms / nprof)
+          for k, (ms, n) in stages.items()}
+    hbm, bf16, src = _peaks()
+    src_note = f"{src} (MEASURED_PEAKS.json)" if src == "measured" else "fallback"
+    nlayer = len(scfg["atm"]["ht"])
+    ray_bytes = nevl * npts_traced * (nlayer * 4 + 4)
+    ray_ms = st["raytrace"]["ms_per_launch"]
+    ray_gbs = ray_bytes / (ray_ms * 1e-3) / 1e9 if ray_ms else 0.0
+    psf_ms = st["ints"]["ms_per_step"]
+    nX = int(round(scfg["D"] / scfg["dx"])) + 3
+    psf_flops = nevl * science_flops(scfg, nX)
+    fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12
+    psf_tf = psf_flops / (psf_ms * 1e-3) / 1e12 if psf_ms else 0.0
+    roofline = {"kernel": "geom_kernel (aperture ray trace)", "bound": "hbm", "achieved": ray_gbs, "peak": hbm,
+                "unit": "GB/s", "frac": ray_gbs / hbm, "peak_source": src_note + " hbm_gbs", "traffic": None,
+                "algorithmic_bytes_per_launch": ray_bytes,
+                "psf": {"kernels": "evl_psf_rows_kernel + evl_psf_cols_kernel", "achieved": psf_tf,
+                        "peak": fp32_peak, "unit": "TFLOP/s", "frac": psf_tf / fp32_peak,
+                        "flops_per_step": psf_flops,
+                        "note": "nominal FFT flops (5 N log2 N per transform, pruned rows and columns) vs "
+                                "nominal FP32 CUDA-core peak"}}
+    line = {
+        "metric": "science direction-frames/s", "value": value, "unit": "direction-frames/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": scfg["name"], "directions": nevl, "aperture_points": nloc,
+                   "wavelengths": scfg["wvl"], "psf_grid": scfg["nembed"], "psf_size": scfg["psfsize"],
+                   "layers": nlayer, "screen": f"{scfg['atm']['nx']}^2 FP32",
+                   "l2": "flushed (256 MiB write) before every timed step", "parallelism": f"replicas x{ws}"},
+        "stages": st,
+        "gpu_launches": int(round(launches_per_step * args.steps)),
+        "e2e": {"value": e2e, "unit": "direction-frames/s", "h2d_bytes_per_step": h2d // args.steps,
+                "d2h_bytes_per_step": d2h // args.steps},
+        "roofline": roofline,
+        "clocks": clocks,
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            v, nfr, cores = science_cpu(scfg, layers, scr)
+            line["cpu_baseline"] = {"value": v, "unit": "direction-frames/s", "cores": cores, "kind": "reference",
+                                    "sample": f"{nfr} direction-frames: prop onto aper->locs, loc_calc_ptt, "
+                                              f"locfft_psf at 3 wavelengths (reference C, FFT stand-in)"}
+        except Exception as e:
+            line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+    if rank == 0:
+        print(json.dumps(line))
+    ctx.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -535,9 +724,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=0.5, help="serving: seconds of requests per rate")
     args = ap.parse_args()
-    from maos_b200.configs import CONFIGS, BATCHES
+    from maos_b200.configs import CONFIGS, BATCHES, SCIENCE
     if args.warmup < 3:
         args.warmup = 3
+    if args.config in SCIENCE:
+        return run_science(args, SCIENCE[args.config])
     if args.config == "serving_32sims":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no serving loop"}))

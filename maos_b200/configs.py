@@ -112,6 +112,19 @@ LGS8_N32 = dict(
 
 CONFIGS = {c["name"]: c for c in (NGS8, LGS30, LGS30_N64, NGS30_2X2, TT30, LGS8_N64, LGS8_N32)}
 
+# Science path: the 30 m aperture sampled at 1/64 m (the reference's default
+# evl.dx = atm.dx), 9 directions on a 3x3 grid over a 30" field, PSFs at J, H
+# and K (evl.wvl) on a 4096-point grid cropped to 1024 pixels, on the
+# 7-layer atmosphere of the stress configuration (4096^2 screens at 1/64 m).
+SCIENCE30 = dict(
+    name="science_30m_9dir",
+    D=30.0, Din=3.6, dx=1.0 / 64,
+    dirs=[(x * AS2RAD, y * AS2RAD, math.inf) for y in (-15.0, 0.0, 15.0) for x in (-15.0, 0.0, 15.0)],
+    wvl=[1.25e-6, 1.65e-6, 2.2e-6], nembed=[4096, 4096, 4096], psfsize=[1024, 1024, 1024], pttr=0,
+    atm=LGS30_N64["atm"], dt=1.0 / 800,
+)
+SCIENCE = {SCIENCE30["name"]: SCIENCE30}
+
 # The uneven batch: six LGS of LGS30 (FFT 32), the 2x2 NGS (FFT 128) and the
 # two tip-tilt sensors (FFT 256) in one frame, on the LGS30 atmosphere.
 UNEVEN_BATCH = dict(name="uneven_batch_lgs6_ngs1_tt2", members=[LGS30, NGS30_2X2, TT30])

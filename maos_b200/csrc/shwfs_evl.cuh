@@ -10,6 +10,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include "shwfs_gen.cuh"
 
 namespace shwfs {
 
@@ -74,48 +75,124 @@ __global__ void evl_coeff_kernel(const double* __restrict__ sums, const double* 
 	for (int i = 0; i < 3; i++) coeff[e * 3 + i] = imcc[i] * c[0] + imcc[3 + i] * c[1] + imcc[6 + i] * c[2];
 }
 
-// Radix-2 decimation-in-time FFT, forward (exp(-i), FFTW sign -1,
-// unnormalised), of `rows` sequences of N points held in shared memory in
-// bit-reversed order; output in natural order.  tw[k] = exp(-2 pi i k / N),
-// k < N/2.
+// Shared-memory rows of N points hold one pad element after every 16
+// (evl_pad), so that the strided stores of the first Stockham passes fall on
+// distinct banks.
 template <int N>
-__device__ __forceinline__ void evl_fft_smem(float2* buf, int rows, const float2* __restrict__ tw) {
-	const int nb = rows * (N / 2);
-	for (int half = 1; half < N; half <<= 1) {
-		const int tstride = N / (2 * half);
-		for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-			const int r = b / (N / 2), q = b - r * (N / 2);
-			const int grp = q / half, pos = q - grp * half;
-			const int i = r * N + grp * 2 * half + pos, j = i + half;
-			const float2 w = __ldg(tw + pos * tstride);
-			const float2 u = buf[i], v = buf[j];
-			const float2 t = make_float2(w.x * v.x - w.y * v.y, w.x * v.y + w.y * v.x);
-			buf[i] = make_float2(u.x + t.x, u.y + t.y);
-			buf[j] = make_float2(u.x - t.x, u.y - t.y);
-		}
-		__syncthreads();
+__host__ __device__ constexpr int evl_row_len() { return N + N / 16; }
+__device__ __forceinline__ int evl_pad(int i) { return i + (i >> 4); }
+
+// Forward FFT (exp(-i), FFTW sign -1, unnormalised) of ROWS sequences of N
+// points in shared memory, natural order in and out, by a block of
+// EVL_THREADS threads: Stockham passes of radix 8 (and one of radix 2 or 4
+// when log2 N is not a multiple of 3).  A radix-R pass reads the R points
+// j + k N/R of group j into registers, applies the twiddles w^((j mod Ns) k)
+// of the Ns*R-point stage and an R-point DFT, and writes them to
+// (j / Ns) Ns R + (j mod Ns) + k Ns.  Each thread holds all its groups of a
+// pass, so one barrier between the loads and the stores makes the pass in
+// place.  tw[m] = exp(-2 pi i m / N), m < N.
+constexpr int EVL_THREADS = 512;
+
+template <int R>
+__device__ __forceinline__ void evl_dft_small(float2 (&v)[R]) {
+	if constexpr (R == 8) {
+		dft8(v, -1.f);
+	} else if constexpr (R == 4) {
+		const float2 s0 = make_float2(v[0].x + v[2].x, v[0].y + v[2].y), d0 = make_float2(v[0].x - v[2].x, v[0].y - v[2].y);
+		const float2 s1 = make_float2(v[1].x + v[3].x, v[1].y + v[3].y), d1 = make_float2(v[1].x - v[3].x, v[1].y - v[3].y);
+		const float2 d1r = make_float2(d1.y, -d1.x);  // d1 * (-i)
+		v[0] = make_float2(s0.x + s1.x, s0.y + s1.y);
+		v[1] = make_float2(d0.x + d1r.x, d0.y + d1r.y);
+		v[2] = make_float2(s0.x - s1.x, s0.y - s1.y);
+		v[3] = make_float2(d0.x - d1r.x, d0.y - d1r.y);
+	} else {
+		static_assert(R == 2, "radix 2, 4 or 8");
+		const float2 a = v[0], b = v[1];
+		v[0] = make_float2(a.x + b.x, a.y + b.y);
+		v[1] = make_float2(a.x - b.x, a.y - b.y);
 	}
 }
 
-template <int N>
-__device__ __forceinline__ int evl_brev(int i) {
-	return (int)(__brev((unsigned)i) >> (33 - __ffs(N)));
+template <int N, int R, int ROWS>
+__device__ __forceinline__ void evl_stockham_pass(float2* buf, int Ns, const float2* __restrict__ tw) {
+	constexpr int NG = N / R;  // groups per row
+	constexpr int NGT = ROWS * NG;
+	constexpr int GPT = (NGT + EVL_THREADS - 1) / EVL_THREADS;
+	float2 v[GPT][R];
+#pragma unroll
+	for (int g = 0; g < GPT; g++) {
+		const int gi = threadIdx.x + g * EVL_THREADS;
+		if (gi < NGT) {
+			const int row = gi / NG, j = gi - row * NG;
+			const float2* x = buf + row * evl_row_len<N>();
+			const int jm = j % Ns, tstep = jm * (N / (Ns * R));
+#pragma unroll
+			for (int k = 0; k < R; k++) v[g][k] = x[evl_pad(j + k * NG)];
+			if (jm) {
+				// w^k for k < R from w, w^2 and w^4 of the table (two roundings at most)
+				float2 w[R];
+				w[1] = __ldg(tw + tstep);
+				if constexpr (R >= 4) {
+					w[2] = __ldg(tw + 2 * tstep);
+					w[3] = cmul(w[1], w[2]);
+				}
+				if constexpr (R == 8) {
+					w[4] = __ldg(tw + 4 * tstep);
+					w[5] = cmul(w[1], w[4]);
+					w[6] = cmul(w[2], w[4]);
+					w[7] = cmul(w[3], w[4]);
+				}
+#pragma unroll
+				for (int k = 1; k < R; k++) v[g][k] = cmul(v[g][k], w[k]);
+			}
+			evl_dft_small<R>(v[g]);
+		}
+	}
+	__syncthreads();
+#pragma unroll
+	for (int g = 0; g < GPT; g++) {
+		const int gi = threadIdx.x + g * EVL_THREADS;
+		if (gi < NGT) {
+			const int row = gi / NG, j = gi - row * NG;
+			float2* y = buf + row * evl_row_len<N>();
+			const int jm = j % Ns, base = (j / Ns) * Ns * R + jm;
+#pragma unroll
+			for (int k = 0; k < R; k++) y[evl_pad(base + k * Ns)] = v[g][k];
+		}
+	}
+	__syncthreads();
+}
+
+template <int N, int ROWS>
+__device__ __forceinline__ void evl_fft_smem(float2* buf, const float2* __restrict__ tw) {
+	constexpr int L = (N >= 4096) ? 12 : (N >= 2048) ? 11 : (N >= 1024) ? 10 : (N >= 512) ? 9 : (N >= 256) ? 8
+		: (N >= 128) ? 7 : 6;
+	static_assert((1 << L) == N, "N must be a power of two in [64, 4096]");
+	int Ns = 1;
+#pragma unroll
+	for (int p = 0; p < L / 3; p++) {
+		evl_stockham_pass<N, 8, ROWS>(buf, Ns, tw);
+		Ns *= 8;
+	}
+	if constexpr (L % 3 == 2) evl_stockham_pass<N, 4, ROWS>(buf, Ns, tw);
+	if constexpr (L % 3 == 1) evl_stockham_pass<N, 2, ROWS>(buf, Ns, tw);
 }
 
 // (3) PSF, first dimension (locfft_psf, lib/locfft.c:150-159): R raster
-// rows per block, each embedded at column X + offx of an N-point row as
+// rows per block (512 threads), each embedded at column X + offx of an N-point row as
 // amp * exp(i k (OPD - PTT)), transformed along x; the 2h columns the crop
 // keeps are written to T (per direction, crop column ax major, row Y
 // fastest).  Crop column ax takes frequency kx = ax < h ? N - h + ax : ax - h
 // (the corner-to-centre copy).  Grid (ceil(nY / R), nevl).
 template <int N, int R>
-__global__ void __launch_bounds__(512) evl_psf_rows_kernel(EvlRaster Ra, const float* __restrict__ opd,
+__global__ void __launch_bounds__(EVL_THREADS) evl_psf_rows_kernel(EvlRaster Ra, const float* __restrict__ opd,
 	const double* __restrict__ coeff, int pttr, float kwvl, int offx, int h, const float2* __restrict__ tw,
 	float2* __restrict__ T, int nYp) {
 	extern __shared__ float2 s_row[];
 	const int e = blockIdx.y, Y0 = blockIdx.x * R;
 	const float* o = opd + (size_t)e * Ra.nslot * 256;
-	for (int i = threadIdx.x; i < R * N; i += blockDim.x) s_row[i] = make_float2(0.f, 0.f);
+	constexpr int LN = evl_row_len<N>();
+	for (int i = threadIdx.x; i < R * LN; i += blockDim.x) s_row[i] = make_float2(0.f, 0.f);
 	__syncthreads();
 	double c0 = 0, c1 = 0, c2 = 0;
 	if (pttr) {
@@ -135,17 +212,17 @@ __global__ void __launch_bounds__(512) evl_psf_rows_kernel(EvlRaster Ra, const f
 		if (pttr) v = (float)((double)v - (c0 + c1 * (Ra.ox + X * Ra.dx) + c2 * (Ra.oy + Y * Ra.dx)));
 		float sn, cs;
 		sincosf(kwvl * v, &sn, &cs);
-		s_row[r * N + evl_brev<N>(X + offx)] = make_float2(a * cs, a * sn);
+		s_row[r * LN + evl_pad(X + offx)] = make_float2(a * cs, a * sn);
 	}
 	__syncthreads();
-	evl_fft_smem<N>(s_row, R, tw);
+	evl_fft_smem<N, R>(s_row, tw);
 	const int ncol = 2 * h;
 	float2* Te = T + (size_t)e * ncol * nYp;
 	for (int idx = threadIdx.x; idx < R * ncol; idx += blockDim.x) {
 		const int ax = idx / R, r = idx - ax * R, Y = Y0 + r;
 		if (Y >= Ra.nY) continue;
 		const int kx = ax < h ? N - h + ax : ax - h;
-		Te[(size_t)ax * nYp + Y] = s_row[r * N + kx];
+		Te[(size_t)ax * nYp + Y] = s_row[r * LN + evl_pad(kx)];
 	}
 }
 
@@ -154,20 +231,20 @@ __global__ void __launch_bounds__(512) evl_psf_rows_kernel(EvlRaster Ra, const f
 // transformed along y, |.|^2 of the 2h kept frequencies added to the sum
 // psf (per direction, ax major, ay fastest).
 template <int N>
-__global__ void __launch_bounds__(512) evl_psf_cols_kernel(const float2* __restrict__ T, int nY, int nYp, int offy,
+__global__ void __launch_bounds__(EVL_THREADS) evl_psf_cols_kernel(const float2* __restrict__ T, int nY, int nYp, int offy,
 	int h, const float2* __restrict__ tw, float* __restrict__ psf) {
 	extern __shared__ float2 s_col[];
 	const int ax = blockIdx.x, e = blockIdx.y, ncol = 2 * h;
 	const float2* Tc = T + ((size_t)e * ncol + ax) * nYp;
-	for (int i = threadIdx.x; i < N; i += blockDim.x) s_col[i] = make_float2(0.f, 0.f);
+	for (int i = threadIdx.x; i < evl_row_len<N>(); i += blockDim.x) s_col[i] = make_float2(0.f, 0.f);
 	__syncthreads();
-	for (int Y = threadIdx.x; Y < nY; Y += blockDim.x) s_col[evl_brev<N>(Y + offy)] = Tc[Y];
+	for (int Y = threadIdx.x; Y < nY; Y += blockDim.x) s_col[evl_pad(Y + offy)] = Tc[Y];
 	__syncthreads();
-	evl_fft_smem<N>(s_col, 1, tw);
+	evl_fft_smem<N, 1>(s_col, tw);
 	float* P = psf + ((size_t)e * ncol + ax) * ncol;
 	for (int ay = threadIdx.x; ay < ncol; ay += blockDim.x) {
 		const int ky = ay < h ? N - h + ay : ay - h;
-		const float2 v = s_col[ky];
+		const float2 v = s_col[evl_pad(ky)];
 		P[ay] += v.x * v.x + v.y * v.y;
 	}
 }

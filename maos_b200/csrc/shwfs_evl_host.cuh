@@ -7,7 +7,7 @@
 struct EvlPsf {
 	int N = 0, psfsize = 0, h = 0, offx = 0, offy = 0;
 	double wvl = 0;
-	DevBuf<float2> tw;   // exp(-2 pi i k / N), k < N/2
+	DevBuf<float2> tw;   // exp(-2 pi i k / N), k < N
 	DevBuf<float> psf;   // nevl * psfsize^2 sums, crop column major
 };
 
@@ -209,8 +209,8 @@ int shwfs_evl_set_psf(shwfs_ctx* ctx, int nwvl, const double* wvl, const int* ne
 		v[w].offx = offx;
 		v[w].offy = offy;
 		v[w].wvl = wvl[w];
-		std::vector<float2> tw(N / 2);
-		for (int k = 0; k < N / 2; k++) {
+		std::vector<float2> tw(N);
+		for (int k = 0; k < N; k++) {
 			const double a = -2.0 * M_PI * k / N;
 			tw[k] = make_float2((float)cos(a), (float)sin(a));
 		}
@@ -240,16 +240,16 @@ int shwfs_evl_psf_reset(shwfs_ctx* ctx) {
 
 template <int N>
 static int evl_launch_psf(shwfs_ctx* ctx, EvlState& E, EvlPsf& P, int nevl) {
-	constexpr int R = N >= 4096 ? 2 : (N >= 2048 ? 4 : 8);
-	const size_t smem_r = (size_t)R * N * sizeof(float2), smem_c = (size_t)N * sizeof(float2);
+	constexpr int R = 8192 / N;  // rows per block: 1024 radix-8 groups, two per thread
+	const size_t smem_r = (size_t)R * evl_row_len<N>() * sizeof(float2), smem_c = (size_t)evl_row_len<N>() * sizeof(float2);
 	if (smem_r > 48 * 1024)
 		CK(cudaFuncSetAttribute(evl_psf_rows_kernel<N, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_r));
 	const EvlRaster Ra = evl_raster(E);
 	const float kwvl = (float)(2.0 * M_PI / P.wvl);
-	evl_psf_rows_kernel<N, R><<<dim3((E.nY + R - 1) / R, nevl), 512, smem_r, ctx->stream>>>(
+	evl_psf_rows_kernel<N, R><<<dim3((E.nY + R - 1) / R, nevl), EVL_THREADS, smem_r, ctx->stream>>>(
 		Ra, E.opd.p, E.coeff.p, E.pttr, kwvl, P.offx, P.h, P.tw.p, E.T.p, E.nY);
 	CK(cudaGetLastError());
-	evl_psf_cols_kernel<N><<<dim3(2 * P.h, nevl), 512, smem_c, ctx->stream>>>(E.T.p, E.nY, E.nY, P.offy, P.h, P.tw.p,
+	evl_psf_cols_kernel<N><<<dim3(2 * P.h, nevl), EVL_THREADS, smem_c, ctx->stream>>>(E.T.p, E.nY, E.nY, P.offy, P.h, P.tw.p,
 		P.psf.p);
 	CK(cudaGetLastError());
 	return 0;

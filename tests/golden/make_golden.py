@@ -16,7 +16,10 @@ written by the reference's own .bin writer (writebin, math/cell.c:330-337):
   lib/mtch.c: a cell of nsa members of 2 x npix) and i0sum (i0sumsum in the
   header);
 - geometric z-tilt (pts_ztilt, math/loc.c) and G-tilt gradients (GS0 opd,
-  GS0 from mkg, lib/mkg.c) of the NGS OPD, and GS0 itself (gzip stream).
+  GS0 from mkg, lib/mkg.c) of the NGS OPD, and GS0 itself (gzip stream);
+- the science path of a 4 m annulus (setup_aper, maos/aper.c): the OPD of
+  two directions on aper->locs, their PR/TT/PTTR and piston/tip/tilt
+  (loc_calc_ptt, math/loc.c) and PSF (locfft_psf, lib/locfft.c, |.|^2).
 
 Needs the reference tree (it builds the oracle); the fixtures it writes
 travel with the repository.  Run from the repository root:
@@ -26,6 +29,7 @@ from __future__ import annotations
 
 import ctypes as C
 import gzip
+import math
 import os
 import sys
 
@@ -91,8 +95,33 @@ def write_f(L, fn, a, kw=None):
                       kw.encode() if kw else None)
 
 
+# Science path: aperture (D, Din, dx), PSF (wavelength, grid, crop), pttr,
+# directions (thetax, thetay, hs), frame index, screen size and seed.
+EVL_CASE = dict(name="evl4", D=4.0, Din=0.5, dx=1.0 / 16, wvl=[1.65e-6], nembed=[256], psfsize=[64], pttr=1,
+                dirs=[(0.0, 0.0, math.inf), (10.0 * math.pi / 648000, -5.0 * math.pi / 648000, 90e3)],
+                isim=9, nx=512, seed=14, cfg=LGS8_N32)
+
+
+def write_evl(L):
+    c = EVL_CASE
+    scr, lay = layers_of(c["cfg"], c["nx"], c["seed"])
+    ref.atm_set(scr, lay)
+    e = ref.RefEvl(c["D"], c["Din"], c["dx"], wvl=c["wvl"], nembed=c["nembed"])
+    kw = (f"D={c['D']}\nDin={c['Din']}\ndx={c['dx']!r}\nwvl={c['wvl'][0]!r}\nnembed={c['nembed'][0]}\n"
+          f"psfsize={c['psfsize'][0]}\npttr={c['pttr']}\nisim={c['isim']}\nscreen_config={c['cfg']['name']}\n"
+          f"screen_nx={c['nx']}\nscreen_seed={c['seed']}\nndir={len(c['dirs'])}")
+    for k, (tx, ty, hs) in enumerate(c["dirs"]):
+        opd, wfe, coeff, psf = e.frame(tx, ty, hs, c["isim"], c["cfg"]["dt"], pttr=c["pttr"], psfsize=c["psfsize"])
+        p = lambda what: os.path.join(HERE, f"{c['name']}_dir{k}_{what}.bin")  # noqa: E731
+        write_d(L, p("opd"), opd, len(opd), 1, kw=kw + f"\nthetax={tx!r}\nthetay={ty!r}\nhs={hs!r}")
+        write_d(L, p("wfe"), np.concatenate([wfe, coeff]), 6, 1)
+        write_d(L, p("psf"), psf[0].ravel(order="F"), c["psfsize"][0], c["psfsize"][0])
+    print(c["name"], "nloc", e.nloc)
+
+
 def main():
     L = ref.lib()
+    write_evl(L)
     for name, cfg, iwfs, isim, nx, seed in CASES:
         r = ref.RefPowfs(cfg)
         scr, lay = layers_of(cfg, nx, seed)

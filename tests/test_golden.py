@@ -104,3 +104,24 @@ def test_gtilt_fixture_is_gs0_times_opd():
     opd = golden("ngs8", "opd").ravel().astype(np.float64)
     gg = golden("ngs8", "gtilt").ravel()
     assert np.abs(gs0 @ opd - gg).max() <= 1e-12 * np.abs(gg).max()
+
+
+def evl_meta():
+    _, kw = golden("evl4_dir0", "opd", keywords=True)
+    return dict(line.split("=", 1) for line in kw.splitlines())
+
+
+def test_evl_fixtures_reproduced_by_reference(ref_lib):
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    c = mg.EVL_CASE
+    scr, lay = mg.layers_of(c["cfg"], c["nx"], c["seed"])
+    ref_lib.atm_set(scr, lay)
+    e = ref_lib.RefEvl(c["D"], c["Din"], c["dx"], wvl=c["wvl"], nembed=c["nembed"])
+    for k, (tx, ty, hs) in enumerate(c["dirs"]):
+        opd, wfe, coeff, psf = e.frame(tx, ty, hs, c["isim"], c["cfg"]["dt"], pttr=c["pttr"], psfsize=c["psfsize"])
+        assert np.array_equal(opd, golden(f"evl4_dir{k}", "opd").ravel())
+        assert np.array_equal(np.concatenate([wfe, coeff]), golden(f"evl4_dir{k}", "wfe").ravel())
+        assert np.array_equal(psf[0], golden(f"evl4_dir{k}", "psf"))

@@ -92,3 +92,52 @@ def test_geometric_gradients_match_golden():
         assert e <= 1e-5, (what, e)
     ctx.close()
     s.close()
+
+
+def test_science_path_matches_golden():
+    """The science path on the fixture's aperture (the product's builder,
+    bit-exact with the reference's) and screens (the product's generator,
+    bit-exact too): OPD within 1e-5 of its peak, PR/TT/PTTR within 1e-4
+    relative, the PSF within 2e-5 of its peak."""
+    import math
+    import torch
+    from maos_b200 import shwfs
+    from maos_b200.configs import CONFIGS
+    from maos_b200.setup import aperture, screens
+    from maos_b200.workload import wind
+    from tests.test_golden import evl_meta
+    m = evl_meta()
+    D, Din, dx = float(m["D"]), float(m["Din"]), float(m["dx"])
+    cfg = CONFIGS[m["screen_config"]]
+    nx, seed = int(m["screen_nx"]), int(m["screen_seed"])
+    at = cfg["atm"]
+    scr = screens(nx, nx, at["dx"], at["r0"], at["L0"], at["wt"], seed)
+    vx, vy = wind(cfg, seed)
+    o = -nx / 2 * at["dx"]
+    layers = [dict(nx=nx, ny=nx, dx=at["dx"], ox=o, oy=o, ht=float(h), vx=float(vx[i]), vy=float(vy[i]), alpha=1.0)
+              for i, h in enumerate(at["ht"])]
+    x, y, a = aperture(D, Din, dx)
+    ctx = shwfs.Context(0)
+    ctx.set_dt(cfg["dt"])
+    ctx.atm_set(layers, scr)
+    ctx.evl_set_aper(x, y, dx, a)
+    ndir = int(m["ndir"])
+    for k in range(ndir):
+        _, kw = golden(f"evl4_dir{k}", "opd", keywords=True)
+        d = dict(line.split("=", 1) for line in kw.splitlines())
+        ctx.evl_add_dir(float(d["thetax"]), float(d["thetay"]), float(d["hs"]))
+    ctx.evl_set_psf([float(m["wvl"])], [int(m["nembed"])], [int(m["psfsize"])], pttr=int(m["pttr"]))
+    ctx.evl_queue(int(m["isim"]), do_psf=True)
+    wfe, coeff = ctx.evl_sync()
+    for k in range(ndir):
+        opd = torch.zeros(len(x), dtype=torch.float32, device="cuda")
+        ctx.evl_opd_dev(k, opd)
+        ctx.sync()
+        o_ref = golden(f"evl4_dir{k}", "opd").ravel()
+        assert np.abs(opd.double().cpu().numpy() - o_ref).max() <= 1e-5 * np.abs(o_ref).max()
+        w_ref = golden(f"evl4_dir{k}", "wfe").ravel()
+        assert np.all(np.abs(wfe[k] - w_ref[:3]) <= 1e-4 * np.abs(w_ref[:3])), (k, wfe[k], w_ref[:3])
+        p, nf = ctx.evl_psf(k, 0)
+        p_ref = golden(f"evl4_dir{k}", "psf")
+        assert nf == 1 and np.abs(p - p_ref).max() <= 2e-5 * p_ref.max()
+    ctx.close()
