@@ -640,9 +640,11 @@ static int launch_geom_wfs(shwfs_ctx* ctx, GeomParams& gp) {
 		const size_t smem = (size_t)gp.nlayer * nopd * 2 * sizeof(int4);
 		if (smem > 160 * 1024) return fail(ctx, SHWFS_EINVAL, "ray trace: %d layers x %d points too large", gp.nlayer, nopd);
 		if (smem > 48 * 1024) CK(cudaFuncSetAttribute(geom_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-		// 16x16 pupils: 128 threads of 2 points; larger: 256 threads of up to GEOM_PTS
-		const int bd = nopd * nopd <= 256 ? 128 : 256;
-		const int bps = (nopd * nopd + GEOM_PTS * bd - 1) / (GEOM_PTS * bd);  // blocks per subaperture
+		// GEOM_PTS points per thread with no idle slot where the pupil allows it:
+		// 16x16 pupils 64 threads, 32x32 256, larger ones split over blocks of 256
+		const int np = nopd * nopd;
+		const int bd = std::min(256, std::max(32, ((np + GEOM_PTS - 1) / GEOM_PTS + 31) / 32 * 32));
+		const int bps = (np + GEOM_PTS * bd - 1) / (GEOM_PTS * bd);  // blocks per subaperture
 		geom_kernel<<<(unsigned)nblk * bps, bd, smem, ctx->stream>>>(gp, nopd, nitem, bps);
 	}
 	CK(cudaGetLastError());

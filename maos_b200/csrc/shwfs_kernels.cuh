@@ -306,8 +306,10 @@ __device__ __forceinline__ void psf_to_otf_n32(float2 (&F)[32], float scale, flo
 // direct per-point evaluation forms, so the OPD is the same to the bit.
 // Dynamic shared memory: nlayer * nopd * 2 * 16 bytes.
 //   column entry ix: (jx, jx1, wx, -)      row entry iy: (jy nx, jy1 nx, wy, -)
-// A block of bd threads (128 or 256) traces up to GEOM_PTS * bd points of one
-// subaperture; larger pupils split each subaperture over bps blocks: block b
+// A block of bd threads (a multiple of 32, at most 256, chosen so that
+// GEOM_PTS * bd covers a pupil with no idle slot where it can) traces up to
+// GEOM_PTS * bd points of one subaperture; larger pupils split each
+// subaperture over bps blocks: block b
 // covers points [GEOM_PTS * bd (b % bps), + GEOM_PTS * bd) of subaperture
 // item b / bps.
 constexpr int GEOM_PTS = 4;
