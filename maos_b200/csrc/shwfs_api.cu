@@ -7,6 +7,7 @@
 // layouts; the ETF, DTF nominal and uplink OTF are stored transposed
 // (fy fastest) so that the imaging kernel reads them coalesced.
 #include <cuda_runtime.h>
+#include <emmintrin.h>
 #include <math.h>
 #include <stdarg.h>
 #include <stdio.h>
@@ -76,6 +77,7 @@ struct WfsState {
 	DevBuf<float2> lotfT;
 	DevBuf<float> neasim;  // geometric gradient noise: Cholesky factor, 3 nsa
 	uint64_t seed = 1;
+	int garena = -1;          // gradient arena chunk holding grad and grad_h (shwfs_ctx::garena)
 	float* grad_h = nullptr;  // pinned staging
 	float* ints_h = nullptr;
 };
@@ -120,6 +122,16 @@ struct shwfs_ctx {
 	DevBuf<const float*> llt_in;
 	DevBuf<float2*> llt_out;
 	DevBuf<int> errflag;                 // bounded device waits record expiry here
+	int* errflag_h = nullptr;            // pinned copy read by the frame syncs
+	// gradients of the WFS in consecutive slices of a few chunks (device and
+	// pinned host at the same offsets), so that a range of WFS crosses to the
+	// host in one copy
+	struct GradArena {
+		DevBuf<float> d;
+		float* h = nullptr;
+		size_t cap = 0, used = 0;
+	};
+	std::vector<GradArena> garena;
 	uint64_t h2d_bytes = 0, d2h_bytes = 0;
 	// stage timing
 	int profiling = 0;
@@ -204,6 +216,18 @@ static int dev_upload_f(shwfs_ctx* ctx, DevBuf<float>& b, const double* h, size_
 	std::vector<float> t(n);
 	for (size_t i = 0; i < n; i++) t[i] = (float)h[i];
 	return dev_upload(ctx, b, t.data(), n);
+}
+
+// FP32 -> FP64 copy of host results (gradients, intensities) with SSE2
+// conversions, four values per step.
+static void f32_to_f64(const float* __restrict__ src, double* __restrict__ dst, size_t n) {
+	size_t k = 0;
+	for (; k + 4 <= n; k += 4) {
+		const __m128 v = _mm_loadu_ps(src + k);
+		_mm_storeu_pd(dst + k, _mm_cvtps_pd(v));
+		_mm_storeu_pd(dst + k + 2, _mm_cvtps_pd(_mm_movehl_ps(v, v)));
+	}
+	for (; k < n; k++) dst[k] = src[k];
 }
 
 static int check_errflag(shwfs_ctx* ctx) {
@@ -291,12 +315,19 @@ int shwfs_destroy(shwfs_ctx* ctx) {
 		w.opd.free_();
 		w.lltopd.free_();
 		w.ints.free_();
-		w.grad.free_();
+		if (w.garena < 0) {
+			w.grad.free_();
+			if (w.grad_h) cudaFreeHost(w.grad_h);
+		}
 		w.lotfT.free_();
 		w.neasim.free_();
-		if (w.grad_h) cudaFreeHost(w.grad_h);
 		if (w.ints_h) cudaFreeHost(w.ints_h);
 	}
+	for (auto& g : ctx->garena) {
+		g.d.free_();
+		if (g.h) cudaFreeHost(g.h);
+	}
+	if (ctx->errflag_h) cudaFreeHost(ctx->errflag_h);
 	for (auto& l : ctx->atm) l.screen.free_();
 	for (auto& m : ctx->marks) {
 		cudaEventDestroy(m.a);
@@ -490,13 +521,27 @@ int shwfs_wfs_add(shwfs_ctx* ctx, const shwfs_wfs_desc* d, int* iwfs) {
 	const int nsa = p->d.nsa, npix = p->d.pixpsax * p->d.pixpsay;
 	if ((r = dev_alloc(ctx, w.opd, (size_t)nsa * p->d.nopd * p->d.nopd))) return r;
 	if ((r = dev_alloc(ctx, w.ints, (size_t)nsa * npix))) return r;
-	if ((r = dev_alloc(ctx, w.grad, (size_t)2 * nsa))) return r;
+	{
+		const size_t need = (size_t)2 * nsa;
+		if (ctx->garena.empty() || ctx->garena.back().used + need > ctx->garena.back().cap) {
+			ctx->garena.emplace_back();
+			auto& g = ctx->garena.back();
+			g.cap = std::max((size_t)1 << 18, need);
+			if ((r = dev_alloc(ctx, g.d, g.cap))) return r;
+			CK(cudaMallocHost(&g.h, sizeof(float) * g.cap));
+		}
+		auto& g = ctx->garena.back();
+		w.garena = (int)ctx->garena.size() - 1;
+		w.grad.p = g.d.p + g.used;
+		w.grad.n = need;
+		w.grad_h = g.h + g.used;
+		g.used += need;
+	}
 	CK(cudaMemsetAsync(w.grad.p, 0, sizeof(float) * 2 * nsa, ctx->stream));
 	if (p->d.has_llt) {
 		if ((r = dev_alloc(ctx, w.lltopd, (size_t)p->d.llt_nx * p->d.llt_nx))) return r;
 		if ((r = dev_alloc(ctx, w.lotfT, (size_t)p->d.notf * p->d.notf))) return r;
 	}
-	CK(cudaMallocHost(&w.grad_h, sizeof(float) * 2 * nsa));
 	if (npix > 0) CK(cudaMallocHost(&w.ints_h, sizeof(float) * nsa * npix));
 	CK(cudaStreamSynchronize(ctx->stream));
 	*iwfs = (int)ctx->wfs.size() - 1;
@@ -1482,13 +1527,18 @@ int shwfs_frame_sync(shwfs_ctx* ctx, int iwfs, double* grad, double* ints) {
 		CK(cudaMemcpyAsync(w->ints_h, w->ints.p, sizeof(float) * nsa * npix, cudaMemcpyDeviceToHost, ctx->stream));
 		ctx->d2h_bytes += sizeof(float) * nsa * npix;
 	}
+	if (ctx->errflag.p) {
+		if (!ctx->errflag_h) CK(cudaMallocHost(&ctx->errflag_h, sizeof(int)));
+		CK(cudaMemcpyAsync(ctx->errflag_h, ctx->errflag.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+	}
 	CK(cudaStreamSynchronize(ctx->stream));
 	ctx->wfsdev_h.clear();
-	if ((r = check_errflag(ctx))) return r;
-	if (grad)
-		for (int i = 0; i < 2 * nsa; i++) grad[i] = w->grad_h[i];
-	if (ints)
-		for (int i = 0; i < nsa * npix; i++) ints[i] = w->ints_h[i];
+	if (ctx->errflag.p && *ctx->errflag_h) {
+		CK(cudaMemset(ctx->errflag.p, 0, sizeof(int)));
+		return fail(ctx, SHWFS_ETIMEOUT, "a bounded tensor-core wait expired in the imaging kernel");
+	}
+	if (grad) f32_to_f64(w->grad_h, grad, (size_t)2 * nsa);
+	if (ints) f32_to_f64(w->ints_h, ints, (size_t)nsa * npix);
 	return 0;
 }
 
@@ -1679,19 +1729,32 @@ int shwfs_frame_sync_range(shwfs_ctx* ctx, int iwfs0, int iwfs1, double* grad) {
 		return ctx ? fail(ctx, SHWFS_EINVAL, "frame_sync_range: bad arguments") : SHWFS_EINVAL;
 	int r = set_device(ctx);
 	if (r) return r;
-	for (int i = iwfs0; i < iwfs1; i++) {
-		WfsState& w = ctx->wfs[i];
-		const int nsa = ctx->powfs[w.d.ipowfs].d.nsa;
-		CK(cudaMemcpyAsync(w.grad_h, w.grad.p, sizeof(float) * 2 * nsa, cudaMemcpyDeviceToHost, ctx->stream));
-		ctx->d2h_bytes += sizeof(float) * 2 * nsa;
+	// one copy per run of WFS whose gradients are consecutive in an arena chunk
+	for (int i = iwfs0; i < iwfs1;) {
+		const WfsState& w0 = ctx->wfs[i];
+		size_t n = w0.grad.n;
+		int j = i + 1;
+		while (j < iwfs1 && w0.garena >= 0 && ctx->wfs[j].garena == w0.garena && ctx->wfs[j].grad.p == w0.grad.p + n) {
+			n += ctx->wfs[j].grad.n;
+			j++;
+		}
+		CK(cudaMemcpyAsync(w0.grad_h, w0.grad.p, sizeof(float) * n, cudaMemcpyDeviceToHost, ctx->stream));
+		ctx->d2h_bytes += sizeof(float) * n;
+		i = j;
+	}
+	if (ctx->errflag.p) {
+		if (!ctx->errflag_h) CK(cudaMallocHost(&ctx->errflag_h, sizeof(int)));
+		CK(cudaMemcpyAsync(ctx->errflag_h, ctx->errflag.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
 	}
 	CK(cudaStreamSynchronize(ctx->stream));
 	ctx->wfsdev_h.clear();
-	if ((r = check_errflag(ctx))) return r;
+	if (ctx->errflag.p && *ctx->errflag_h) {
+		CK(cudaMemset(ctx->errflag.p, 0, sizeof(int)));
+		return fail(ctx, SHWFS_ETIMEOUT, "a bounded tensor-core wait expired in the imaging kernel");
+	}
 	for (int i = iwfs0; i < iwfs1; i++) {
-		WfsState& w = ctx->wfs[i];
-		const int n = 2 * ctx->powfs[w.d.ipowfs].d.nsa;
-		for (int k = 0; k < n; k++) grad[k] = w.grad_h[k];
+		const size_t n = ctx->wfs[i].grad.n;
+		f32_to_f64(ctx->wfs[i].grad_h, grad, n);
 		grad += n;
 	}
 	return 0;

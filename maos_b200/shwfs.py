@@ -11,9 +11,11 @@ module fails.
 """
 from __future__ import annotations
 
+import atexit
 import ctypes as C
 import math
 import os
+import weakref
 from typing import Optional, Sequence
 
 import numpy as np
@@ -163,6 +165,20 @@ def _devptr(t) -> Optional[int]:
     return int(t.data_ptr())
 
 
+_live = weakref.WeakSet()
+
+
+@atexit.register
+def _close_all():
+    """Close the contexts still open when the interpreter exits, while the
+    CUDA runtime is still up (its own exit handlers run after Python's)."""
+    for ctx in list(_live):
+        try:
+            ctx.close()
+        except Exception:
+            pass
+
+
 class Context:
     """One device context: static powfs/WFS data, screens and frame buffers."""
 
@@ -175,6 +191,7 @@ class Context:
         self._h = h
         self.npix = {}
         self.nsa = {}
+        _live.add(self)
 
     def _check(self, rc: int, what: str):
         if rc != 0:
