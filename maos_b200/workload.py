@@ -120,6 +120,14 @@ class BatchWorkload:
             self.ctx.frame_queue(isim, 0, self.nwfs)
 
     def frame_sync(self, want_ints: bool = False):
+        """Gradients of every WFS (with intensities when want_ints); without
+        intensities, one wait and one copy for the whole frame."""
+        if not want_ints:
+            nsa = {}
+            for _, setup, _, wl in self.members:
+                for i in wl:
+                    nsa[i] = setup.nsa
+            return self.ctx.frame_sync_range(0, self.nwfs, lambda i: nsa[i])
         out = []
         for _, _, ip, wl in self.members:
             out += [self.ctx.frame_sync(i, ip, want_ints) for i in wl]

@@ -46,3 +46,19 @@ def test_batch_members_match_single_powfs_frames():
         wl.close()
         for k, j in enumerate(idx):
             assert np.array_equal(single[k][0], b[j][0]) and np.array_equal(single[k][1], b[j][1])
+
+
+def test_range_sync_equals_per_wfs_sync():
+    """One range sync of the whole batch frame returns every WFS's gradients
+    as the per-WFS syncs do."""
+    from maos_b200.configs import UNEVEN_BATCH
+    from maos_b200.workload import build_batch
+    wl = build_batch(UNEVEN_BATCH["members"], device=0, seed=6, noisy=True, nx=512, graph=True)
+    wl.frame(4)
+    a = wl.frame_sync()                      # one range call
+    wl.frame(4)
+    b = [g for g, _ in wl.frame_sync(want_ints=True)]  # per-WFS calls
+    wl.close()
+    assert len(a) == len(b) == 9
+    for ga, gb in zip(a, b):
+        assert np.array_equal(ga, gb)
