@@ -101,33 +101,18 @@ class ClockSampler:
 
 
 def dist_init():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if ws > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=None)
-    return ws, rank, local
+    from maos_b200 import replicas
+    return replicas.init("nccl")
 
 
 def allreduce_max(x: float, ws: int, device) -> float:
-    if ws == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device=device)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from maos_b200 import replicas
+    return replicas.max_over_ranks(x, ws, device)
 
 
 def barrier(ws: int, device):
-    if ws > 1:
-        import torch
-        import torch.distributed as dist
-        dist.barrier(device_ids=[device.index])
-        torch.cuda.synchronize(device)
+    from maos_b200 import replicas
+    replicas.barrier(ws, device)
 
 
 # ---------------------------------------------------------------------------
