@@ -158,6 +158,10 @@ int shwfs_wfs_update_mtche(shwfs_ctx* ctx, int iwfs, int mtchcr);
    set and dtrat > 0, frame isim uses ETF0 (1 - w) + ETF1 w with
    w = (isim mod dtrat) / dtrat; dtrat 0 uses slot 0 alone. */
 int shwfs_powfs_set_etf_dtrat(shwfs_ctx* ctx, int ipowfs, int dtrat);
+/* powfs.saasum (maos/powfs.c:227-230), the divisor of the CoG signal level
+   under sigmatch 2 (maos/utils.c:1033-1035); shwfs_powfs_set_geom sets it to
+   the sum of the saa it is given. */
+int shwfs_powfs_set_saasum(shwfs_ctx* ctx, int ipowfs, double saasum);
 /* Geometric (z-tilt) gradients (device, 2*nsa) of WFS iwfs from a device OPD
    (nsa*nopd^2): cuztilt (cuda/sim/wfsgrad.cu:57-106). */
 int shwfs_grad_ztilt_dev(shwfs_ctx* ctx, int iwfs, const float* opd, float* grad);

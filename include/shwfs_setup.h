@@ -59,6 +59,8 @@ double shwfs_setup_dx(const shwfs_setup* s);
 double shwfs_setup_areascale(const shwfs_setup* s);
 double shwfs_setup_dtheta(const shwfs_setup* s);
 double shwfs_setup_i0sumsum(const shwfs_setup* s);
+/* powfs.saasum as the reference forms it (maos/powfs.c:227-230). */
+double shwfs_setup_saasum(const shwfs_setup* s);
 
 /* Array getters (sizes in brackets); return SHWFS_EINVAL if the array does not exist. */
 #define SHWFS_SETUP_SALOCX 1  /* [nsa] subaperture lower-left corner x */

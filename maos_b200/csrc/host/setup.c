@@ -19,6 +19,7 @@ struct shwfs_setup {
 	char err[256];
 	int nsa, nopd, notf, pixpsax, pixpsay, npix, llt_nx;
 	double dx, areascale, dtheta, i0sumsum;
+	double saasum;     /* powfs.saasum as the reference forms it (see setup_geom) */
 	double *salocx, *salocy, *origx, *origy, *amp, *saa;
 	double* nominal;   /* notf^2 */
 	int* simap_idx;    /* npix*4 */
@@ -194,6 +195,11 @@ static int setup_geom(shwfs_setup* s) {
 	}
 	free(gi);
 	free(gj);
+	/* powfs.saasum (maos/powfs.c:227-230) is summed before saa is cut to the
+	   kept subapertures: over all candidates after the compaction, the
+	   entries past the kept ones included */
+	s->saasum = 0;
+	for (long isa = 0; isa < count; isa++) s->saasum += saa[isa];
 	if (nsa == 0) {
 		free(sx); free(sy); free(amp); free(saa);
 		return serr(s, "no subaperture above the area threshold");
@@ -689,6 +695,7 @@ double shwfs_setup_dx(const shwfs_setup* s) { return s->dx; }
 double shwfs_setup_areascale(const shwfs_setup* s) { return s->areascale; }
 double shwfs_setup_dtheta(const shwfs_setup* s) { return s->dtheta; }
 double shwfs_setup_i0sumsum(const shwfs_setup* s) { return s->i0sumsum; }
+double shwfs_setup_saasum(const shwfs_setup* s) { return s->saasum; }
 
 int shwfs_setup_get(const shwfs_setup* s, int what, double* out) {
 	if (!s || !out) return SHWFS_EINVAL;
@@ -761,6 +768,7 @@ int shwfs_setup_load(const shwfs_setup* s, shwfs_ctx* ctx, int* ipowfs) {
 	int r = shwfs_powfs_add(ctx, &d, ipowfs);
 	if (r) return r;
 	if ((r = shwfs_powfs_set_geom(ctx, *ipowfs, s->origx, s->origy, s->amp, 1, s->saa))) return r;
+	if ((r = shwfs_powfs_set_saasum(ctx, *ipowfs, s->saasum))) return r;
 	if ((r = shwfs_powfs_set_simap(ctx, *ipowfs, s->simap_idx, s->simap_wt, 1))) return r;
 	if (c->has_llt) {
 		if ((r = shwfs_powfs_set_etf(ctx, *ipowfs, (const double*)s->etf, 0))) return r;

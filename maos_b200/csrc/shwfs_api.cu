@@ -45,6 +45,7 @@ struct PowfsState {
 	DevBuf<float> amp;  // namp*nsa*nopd^2
 	int namp = 0;
 	DevBuf<float> saa;
+	double saasum = 0;  // sum of saa (sigmatch 2 CoG signal level, powfs.saasum)
 	DevBuf<float> nominalT;
 	int nnominal = 0;
 	DevBuf<int> simap_idx;
@@ -76,6 +77,7 @@ struct WfsState {
 	DevBuf<float> opd, lltopd, ints, grad;
 	DevBuf<float2> lotfT;
 	DevBuf<float> neasim;  // geometric gradient noise: Cholesky factor, 3 nsa
+	DevBuf<double> i1sum;  // sigmatch 2: total intensity of the frame
 	uint64_t seed = 1;
 	int garena = -1;          // gradient arena chunk holding grad and grad_h (shwfs_ctx::garena)
 	float* grad_h = nullptr;  // pinned staging
@@ -142,6 +144,7 @@ struct shwfs_ctx {
 	};
 	std::vector<Mark> marks;
 	EvlState* evl = nullptr;
+	int sig2_inner = 0;        // launch_ints_sig2 is running the imaging part
 };
 static void evl_free(shwfs_ctx* ctx);
 
@@ -321,6 +324,7 @@ int shwfs_destroy(shwfs_ctx* ctx) {
 		}
 		w.lotfT.free_();
 		w.neasim.free_();
+		w.i1sum.free_();
 		if (w.ints_h) cudaFreeHost(w.ints_h);
 	}
 	for (auto& g : ctx->garena) {
@@ -429,8 +433,11 @@ int shwfs_powfs_set_geom(shwfs_ctx* ctx, int ipowfs, const double* origx, const 
 	if ((r = dev_upload(ctx, p->origy, origy, nsa))) return r;
 	if ((r = dev_upload_f(ctx, p->amp, amp, (size_t)namp * nsa * n2))) return r;
 	p->namp = namp;
+	p->saasum = nsa;
 	if (saa) {
 		if ((r = dev_upload_f(ctx, p->saa, saa, nsa))) return r;
+		p->saasum = 0;
+		for (int i = 0; i < nsa; i++) p->saasum += saa[i];
 	}
 	return 0;
 }
@@ -778,7 +785,8 @@ static int check_ready(shwfs_ctx* ctx, const PowfsState& p, const WfsState& w) {
 	if (p.d.has_llt && !p.lltamp.p) return fail(ctx, SHWFS_ESTATE, "LLT amplitude not set");
 	if (p.d.gradtype == SHWFS_GRAD_MF && !w.mtche.p) return fail(ctx, SHWFS_ESTATE, "matched filter not set");
 	if (p.d.gradtype == SHWFS_GRAD_MF && p.d.sigmatch == 1 && !w.i0sum.p) return fail(ctx, SHWFS_ESTATE, "i0sum not set");
-	if (p.d.sigmatch == 2) return fail(ctx, SHWFS_EINVAL, "sigmatch=2 is not supported by this build");
+	if (p.d.gradtype == SHWFS_GRAD_MF && p.d.sigmatch == 2 && !(w.i0sumsum > 0))
+		return fail(ctx, SHWFS_ESTATE, "sigmatch 2: i0sumsum not set");
 	return 0;
 }
 
@@ -1083,6 +1091,9 @@ static int launch_uplink_gen(shwfs_ctx* ctx, PowfsState& p, const std::vector<in
 }
 
 // (b)-(e) for a set of WFS of one powfs sharing the launch.
+static int launch_ints_sig2(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist, int isim,
+	const std::vector<const float*>& opds, const std::vector<const float2*>& lotfs, const std::vector<float*>& ints,
+	const std::vector<float*>& grads, const std::vector<int>& noisy);
 static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist, int isim,
 	const std::vector<const float*>& opds, const std::vector<const float2*>& lotfs, const std::vector<float*>& ints,
 	const std::vector<float*>& grads, const std::vector<int>& noisy) {
@@ -1090,6 +1101,8 @@ static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist
 	const int nw = (int)wlist.size();
 	if (nw == 0) return 0;
 	if (is_geom(p.d.gradtype)) return fail(ctx, SHWFS_EINVAL, "geometric sensor: no imaging");
+	if (p.d.sigmatch == 2 && !ctx->sig2_inner)
+		return launch_ints_sig2(ctx, ipowfs, wlist, isim, opds, lotfs, ints, grads, noisy);
 	if (ctx->form == SHWFS_FORM_TC && nw > TC_MAX_WFS) {
 		// the tensor-core launch holds at most TC_MAX_WFS WFS descriptors in shared memory
 		for (int k0 = 0; k0 < nw; k0 += TC_MAX_WFS) {
@@ -1249,6 +1262,66 @@ static int launch_uplink(shwfs_ctx* ctx, const std::vector<int>& wlist, const st
 	return 0;
 }
 
+// Imaging of a sigmatch-2 powfs (normalisation by the frame's total
+// intensity, maos/utils.c:1013-1036): intensities with noise first, then the
+// total of each WFS (ints_sum_kernel), then the gradients (grad_sig2_kernel).
+static int launch_ints_sig2(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist, int isim,
+	const std::vector<const float*>& opds, const std::vector<const float2*>& lotfs, const std::vector<float*>& ints,
+	const std::vector<float*>& grads, const std::vector<int>& noisy) {
+	PowfsState& p = ctx->powfs[ipowfs];
+	const int nw = (int)wlist.size();
+	std::vector<float*> in(ints), none(nw, nullptr);
+	for (int k = 0; k < nw; k++) {
+		WfsState& w = ctx->wfs[wlist[k]];
+		if (!in[k]) in[k] = w.ints.p;
+		if (!in[k]) return fail(ctx, SHWFS_ESTATE, "sigmatch 2: WFS %d has no intensity buffer", wlist[k]);
+		int r = dev_alloc(ctx, w.i1sum, 1);
+		if (r) return r;
+	}
+	ctx->sig2_inner = 1;
+	int r = launch_ints(ctx, ipowfs, wlist, isim, opds, lotfs, in, none, noisy);
+	ctx->sig2_inner = 0;
+	if (r) return r;
+	const PowfsDev P = make_powfs_dev(p, isim);
+	const long n = (long)p.d.nsa * P.npix;
+	for (int k0 = 0; k0 < nw; k0 += GEOM_SUM_MAX) {
+		SumParams S;
+		memset(&S, 0, sizeof(S));
+		S.nw = std::min(GEOM_SUM_MAX, nw - k0);
+		S.n = n;
+		for (int k = 0; k < S.nw; k++) {
+			WfsState& w = ctx->wfs[wlist[k0 + k]];
+			CK(cudaMemsetAsync(w.i1sum.p, 0, sizeof(double), ctx->stream));
+			S.ints[k] = in[k0 + k];
+			S.sum[k] = w.i1sum.p;
+		}
+		const int nblk = (int)std::min((n + 255) / 256, (long)64);
+		StageMark m(ctx, SHWFS_STAGE_POST);
+		ints_sum_kernel<<<dim3(nblk, S.nw), 256, 0, ctx->stream>>>(S);
+		CK(cudaGetLastError());
+	}
+	for (int k = 0; k < nw; k++) {
+		if (!grads[k]) continue;
+		WfsState& w = ctx->wfs[wlist[k]];
+		const int nblk = (p.d.nsa + 3) / 4;
+		StageMark m(ctx, SHWFS_STAGE_POST);
+		if (P.npix <= 32)
+			grad_sig2_kernel<1><<<nblk, 128, 0, ctx->stream>>>(P, in[k], w.mtche.p, w.i0sum.p, grads[k], w.i1sum.p,
+				w.i0sumsum, p.saasum);
+		else if (P.npix <= 64)
+			grad_sig2_kernel<2><<<nblk, 128, 0, ctx->stream>>>(P, in[k], w.mtche.p, w.i0sum.p, grads[k], w.i1sum.p,
+				w.i0sumsum, p.saasum);
+		else if (P.npix <= 128)
+			grad_sig2_kernel<4><<<nblk, 128, 0, ctx->stream>>>(P, in[k], w.mtche.p, w.i0sum.p, grads[k], w.i1sum.p,
+				w.i0sumsum, p.saasum);
+		else
+			grad_sig2_kernel<8><<<nblk, 128, 0, ctx->stream>>>(P, in[k], w.mtche.p, w.i0sum.p, grads[k], w.i1sum.p,
+				w.i0sumsum, p.saasum);
+		CK(cudaGetLastError());
+	}
+	return 0;
+}
+
 extern "C" {
 
 int shwfs_raytrace_dev(shwfs_ctx* ctx, int iwfs, int isim, float* opd) {
@@ -1291,9 +1364,32 @@ int shwfs_grad_dev(shwfs_ctx* ctx, int iwfs, const float* ints, float* grad) {
 	PowfsState& p = ctx->powfs[w->d.ipowfs];
 	if (is_geom(p.d.gradtype)) return fail(ctx, SHWFS_EINVAL, "grad: geometric sensor has no pixels");
 	if (p.d.gradtype == SHWFS_GRAD_MF && !w->mtche.p) return fail(ctx, SHWFS_ESTATE, "matched filter not set");
-	if (p.d.sigmatch == 2) return fail(ctx, SHWFS_EINVAL, "sigmatch=2 is not supported by this build");
 	PowfsDev P = make_powfs_dev(p, 0);
 	const int nblk = (p.d.nsa + 3) / 4;
+	if (p.d.sigmatch == 2) {
+		// the total intensity of the given frame first (maos/utils.c:1022-1026)
+		if (p.d.gradtype == SHWFS_GRAD_MF && !(w->i0sumsum > 0)) return fail(ctx, SHWFS_ESTATE, "sigmatch 2: i0sumsum not set");
+		if ((r = dev_alloc(ctx, w->i1sum, 1))) return r;
+		CK(cudaMemsetAsync(w->i1sum.p, 0, sizeof(double), ctx->stream));
+		SumParams S;
+		memset(&S, 0, sizeof(S));
+		S.nw = 1;
+		S.n = (long)p.d.nsa * P.npix;
+		S.ints[0] = ints;
+		S.sum[0] = w->i1sum.p;
+		ints_sum_kernel<<<dim3((unsigned)std::min((S.n + 255) / 256, 64L), 1), 256, 0, ctx->stream>>>(S);
+		CK(cudaGetLastError());
+		if (P.npix <= 32)
+			grad_sig2_kernel<1><<<nblk, 128, 0, ctx->stream>>>(P, ints, w->mtche.p, w->i0sum.p, grad, w->i1sum.p, w->i0sumsum, p.saasum);
+		else if (P.npix <= 64)
+			grad_sig2_kernel<2><<<nblk, 128, 0, ctx->stream>>>(P, ints, w->mtche.p, w->i0sum.p, grad, w->i1sum.p, w->i0sumsum, p.saasum);
+		else if (P.npix <= 128)
+			grad_sig2_kernel<4><<<nblk, 128, 0, ctx->stream>>>(P, ints, w->mtche.p, w->i0sum.p, grad, w->i1sum.p, w->i0sumsum, p.saasum);
+		else
+			grad_sig2_kernel<8><<<nblk, 128, 0, ctx->stream>>>(P, ints, w->mtche.p, w->i0sum.p, grad, w->i1sum.p, w->i0sumsum, p.saasum);
+		CK(cudaGetLastError());
+		return 0;
+	}
 	if (P.npix <= 32)
 		grad_kernel<1><<<nblk, 128, 0, ctx->stream>>>(P, ints, w->mtche.p, w->i0sum.p, grad);
 	else if (P.npix <= 64)
@@ -1645,6 +1741,13 @@ int shwfs_powfs_set_etf_dtrat(shwfs_ctx* ctx, int ipowfs, int dtrat) {
 	return 0;
 }
 
+int shwfs_powfs_set_saasum(shwfs_ctx* ctx, int ipowfs, double saasum) {
+	PowfsState* p = get_powfs(ctx, ipowfs);
+	if (!p || !(saasum > 0)) return ctx ? fail(ctx, SHWFS_EINVAL, "set_saasum: bad arguments") : SHWFS_EINVAL;
+	p->saasum = saasum;
+	return 0;
+}
+
 int shwfs_wfs_set_neasim(shwfs_ctx* ctx, int iwfs, const double* nea) {
 	WfsState* w = get_wfs(ctx, iwfs);
 	if (!w) return ctx ? fail(ctx, SHWFS_EINVAL, "set_neasim: unknown wfs %d", iwfs) : SHWFS_EINVAL;
@@ -1906,6 +2009,7 @@ int shwfs_frame_noalloc(shwfs_ctx* ctx, int iwfs, int isim, float* ints, float* 
 	if (!w || (!ints && !grad)) return ctx ? fail(ctx, SHWFS_EINVAL, "frame_noalloc: bad arguments") : SHWFS_EINVAL;
 	PowfsState& p = ctx->powfs[w->d.ipowfs];
 	if (is_geom(p.d.gradtype)) return fail(ctx, SHWFS_EINVAL, "frame_noalloc: geometric sensor");
+	if (p.d.sigmatch == 2) return fail(ctx, SHWFS_EINVAL, "frame_noalloc: sigmatch 2 needs the frame path");
 	if (p.d.nsa > SHWFS_NOALLOC_MAX_NSA)
 		return fail(ctx, SHWFS_EINVAL, "frame_noalloc: %d subapertures exceed the allocation-free maximum of %d",
 			p.d.nsa, SHWFS_NOALLOC_MAX_NSA);

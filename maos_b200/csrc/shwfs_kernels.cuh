@@ -132,6 +132,7 @@ __device__ __forceinline__ float poisson_draw(PixelRng& rng, float xm) {
 // ---------------------------------------------------------------------------
 #define SHWFS_MAX_LAYERS 16
 #define SHWFS_MAX_ENTRIES 16
+#define GEOM_SUM_MAX 32
 
 // One pupil to ray trace in a frame: the subapertures of a WFS, or the LLT
 // pupil of an LGS (one "subaperture"), with the per-layer geometry of
@@ -441,9 +442,12 @@ __global__ void uplink_otf_n32_kernel(const float* const* lltopd, const float* l
 // Lane holds pixels p = lane + 32*q.  Sums in FP64.
 // ---------------------------------------------------------------------------
 template <int NPQ>
+// s2 serves sigmatch 2 (normalisation by the whole frame's intensity,
+// maos/utils.c:1013-1036): the matched filter's scale i0sumg / i1sum, or the
+// CoG's signal level i1sum / saasum; unused otherwise.
 __device__ __forceinline__ void grad_from_pixels(const float (&pix)[NPQ], int npix, int pixpsax, int pixpsay,
 	const PowfsDev& P, const float* __restrict__ mtche, const float* __restrict__ i0sum, int isa, int lane,
-	float* __restrict__ grad, int nsa) {
+	float* __restrict__ grad, int nsa, double s2 = 0) {
 	if (P.saa && P.saa[isa] < P.saat) return;  // maos/utils.c:1041: vignetted, left unchanged
 	double gx = 0, gy = 0;
 	if (P.gradtype == 1) {
@@ -469,6 +473,8 @@ __device__ __forceinline__ void grad_from_pixels(const float (&pix)[NPQ], int np
 		if (P.sigmatch == 1) {
 			scale = (double)i0sum[isa] / si;
 			if (scale <= 0 || scale > 10 || !isfinite(scale)) scale = 1;
+		} else if (P.sigmatch == 2) {
+			scale = s2;
 		}
 		gx = sx * scale;
 		gy = sy * scale;
@@ -497,7 +503,7 @@ __device__ __forceinline__ void grad_from_pixels(const float (&pix)[NPQ], int np
 		if (P.sigmatch == 0) {
 			flux = i0sum ? (double)i0sum[isa] : (double)P.sigtot * (P.saa ? P.saa[isa] : 1.f);
 		} else if (P.sigmatch == 2) {
-			flux = (double)P.sigtot * (P.saa ? P.saa[isa] : 1.f);
+			flux = s2 * (P.saa ? P.saa[isa] : 1.f);
 		}
 		if (flux != 0) sum = flux;
 		if (sum > (double)P.cogthres) {
@@ -759,6 +765,51 @@ __global__ void grad_kernel(PowfsDev P, const float* __restrict__ ints, const fl
 	}
 	grad_from_pixels<NPQ>(pix, P.npix, P.pixpsax, P.pixpsay, P, mtche ? mtche + (size_t)isa * 2 * P.npix : nullptr,
 		i0sum, isa, lane, grad, P.nsa);
+}
+
+// sigmatch 2: the total intensity of each WFS of a launch (i1sum,
+// maos/utils.c:1022-1026), FP64; grid (blocks, nw), sums zeroed before.
+struct SumParams {
+	int nw;
+	long n;                          // intensities per WFS
+	const float* ints[GEOM_SUM_MAX];
+	double* sum[GEOM_SUM_MAX];
+};
+__global__ void ints_sum_kernel(const __grid_constant__ SumParams S) {
+	const int k = blockIdx.y;
+	const float* x = S.ints[k];
+	double t = 0;
+	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < S.n; i += (long)gridDim.x * blockDim.x) t += x[i];
+#pragma unroll
+	for (int off = 16; off > 0; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
+	__shared__ double red[32];
+	if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double u = 0;
+		for (int w = 0; w < (int)(blockDim.x >> 5); w++) u += red[w];
+		atomicAdd(S.sum[k], u);
+	}
+}
+
+// sigmatch 2 gradients of one WFS from its stored intensities once i1sum is
+// known: s2 = i0sumg / i1sum (matched filter) or i1sum / saasum (CoG).
+template <int NPQ>
+__global__ void grad_sig2_kernel(PowfsDev P, const float* __restrict__ ints, const float* __restrict__ mtche,
+	const float* __restrict__ i0sum, float* __restrict__ grad, const double* __restrict__ i1sum, double i0sumg,
+	double saasum) {
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int isa = blockIdx.x * (blockDim.x >> 5) + warp;
+	if (isa >= P.nsa) return;
+	const double s2 = P.gradtype == 1 ? i0sumg / *i1sum : *i1sum / saasum;
+	float pix[NPQ];
+#pragma unroll
+	for (int q = 0; q < NPQ; q++) {
+		const int p = lane + 32 * q;
+		pix[q] = p < P.npix ? ints[(size_t)isa * P.npix + p] : 0.f;
+	}
+	grad_from_pixels<NPQ>(pix, P.npix, P.pixpsax, P.pixpsay, P, mtche ? mtche + (size_t)isa * 2 * P.npix : nullptr,
+		i0sum, isa, lane, grad, P.nsa, s2);
 }
 
 // Photon and read noise on n intensities in place, the rule of addnoise

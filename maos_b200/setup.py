@@ -49,7 +49,7 @@ def _lib():
             f = getattr(L, f"shwfs_setup_{n}")
             f.argtypes = [vp]
             f.restype = i
-        for n in ("dx", "areascale", "dtheta", "i0sumsum"):
+        for n in ("dx", "areascale", "dtheta", "i0sumsum", "saasum"):
             f = getattr(L, f"shwfs_setup_{n}")
             f.argtypes = [vp]
             f.restype = C.c_double
@@ -103,6 +103,7 @@ class Setup:
         self.areascale = L.shwfs_setup_areascale(h)
         self.dtheta = L.shwfs_setup_dtheta(h)
         self.i0sumsum = L.shwfs_setup_i0sumsum(h)
+        self.saasum = L.shwfs_setup_saasum(h)
 
     def close(self):
         if getattr(self, "_h", None):

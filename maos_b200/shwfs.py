@@ -110,6 +110,7 @@ def _load() -> C.CDLL:
         "shwfs_set_variant": [vp, i, i],
         "shwfs_frame_noalloc": [vp, i, i, vp, vp],
         "shwfs_powfs_set_etf_dtrat": [vp, i, i],
+        "shwfs_powfs_set_saasum": [vp, i, C.c_double],
         "shwfs_grad_ztilt_dev": [vp, i, vp, vp],
         "shwfs_wfs_set_neasim": [vp, i, dp],
         "shwfs_powfs_set_gs0": [vp, i, i, C.c_long, C.c_long, ip, ip, dp],
@@ -261,6 +262,10 @@ class Context:
         ipt = C.POINTER(C.c_int)
         self._check(self._L.shwfs_powfs_set_gs0(self._h, ipowfs, iamp, nrow, ncol, a.ctypes.data_as(ipt),
                                                 b.ctypes.data_as(ipt), _dptr(v)), "powfs_set_gs0")
+
+    def powfs_set_saasum(self, ipowfs, saasum: float):
+        """powfs.saasum for sigmatch 2 CoG (default: the sum of saa)."""
+        self._check(self._L.shwfs_powfs_set_saasum(self._h, ipowfs, float(saasum)), "powfs_set_saasum")
 
     def powfs_set_lltamp(self, ipowfs, lltamp):
         a = _f64(lltamp)

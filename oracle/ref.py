@@ -49,7 +49,7 @@ def lib():
         for name in ("oref_nsa", "oref_nopd", "oref_notf", "oref_pixpsax", "oref_pixpsay", "oref_llt_nx", "oref_setup"):
             getattr(L, name).restype = C.c_int
         for name in ("oref_areascale", "oref_dtheta", "oref_get_ptsdx", "oref_get_i0sumsum", "oref_frame_mt",
-                     "oref_frame_full_mt"):
+                     "oref_frame_full_mt", "oref_get_saasum"):
             getattr(L, name).restype = C.c_double
         _lib = L
     return _lib
@@ -114,6 +114,9 @@ class RefPowfs:
         a = np.zeros(self.nsa * self.nopd ** 2)
         lib().oref_get_amp(_p(a))
         return a
+
+    def saasum(self) -> float:
+        return lib().oref_get_saasum()
 
     def saa(self):
         a = np.zeros(self.nsa)

@@ -220,6 +220,7 @@ void oref_get_ptsorig(double* x, double* y){
 double oref_get_ptsdx(void){ return g_powfs[0].pts->dx; }
 void oref_get_amp(double* amp){ dmat* a=P(g_powfs[0].amp, 0); copy_vec(amp, P(a), PN(a)); }
 void oref_get_saa(double* saa){ dmat* a=P(g_powfs[0].saa, 0); copy_vec(saa, P(a), PN(a)); }
+double oref_get_saasum(void){ return P(g_powfs[0].saasum, 0); }
 /* nominal DTF (treated, peak in corner with chess pattern) for subaperture isa */
 void oref_get_nominal(int isa, double* out){
 	dcell* nom=g_powfs[0].dtf[0].nominal;

@@ -32,6 +32,7 @@ def context_from_ref(ref, cfg, nwfs=1, noisy=0, device=0):
     ip = ctx.powfs_add(**powfs_desc_from_ref(ref, cfg))
     ox, oy = ref.ptsorig()
     ctx.powfs_set_geom(ip, ox, oy, ref.amp(), ref.saa())
+    ctx.powfs_set_saasum(ip, ref.saasum())
     idx, wt = si_to_taps(ref.si_dense(0))
     ctx.powfs_set_simap(ip, idx, wt)
     if cfg.get("has_llt"):

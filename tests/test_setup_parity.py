@@ -24,6 +24,7 @@ def test_geometry_bit_exact(ref_lib, cfg):
     assert np.array_equal(ox, s.get("origx")) and np.array_equal(oy, s.get("origy"))
     assert np.array_equal(r.amp(), s.get("amp"))
     assert np.array_equal(r.saa(), s.get("saa"))
+    assert s.saasum == r.saasum()  # powfs.saasum, summed as the reference does
 
 
 @pytest.mark.parametrize("cfg", [NGS8, LGS30, LGS8_N64, NGS30_2X2, TT30], ids=lambda c: c["name"])
