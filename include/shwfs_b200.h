@@ -162,6 +162,12 @@ int shwfs_powfs_set_etf_dtrat(shwfs_ctx* ctx, int ipowfs, int dtrat);
    under sigmatch 2 (maos/utils.c:1033-1035); shwfs_powfs_set_geom sets it to
    the sum of the saa it is given. */
 int shwfs_powfs_set_saasum(shwfs_ctx* ctx, int ipowfs, double saasum);
+/* Frames integrated per output frame (powfs.dtrat): the intensities of
+   frames isim with isim mod dtrat = 0 .. dtrat-1 add up in each WFS's
+   intensity buffer, and on the last one (isim + 1 a multiple of dtrat) the
+   noise is drawn on the sum and the gradients are formed; other frames leave
+   the gradients as they were.  1 (the default) forms every frame. */
+int shwfs_powfs_set_dtrat(shwfs_ctx* ctx, int ipowfs, int dtrat);
 /* Geometric (z-tilt) gradients (device, 2*nsa) of WFS iwfs from a device OPD
    (nsa*nopd^2): cuztilt (cuda/sim/wfsgrad.cu:57-106). */
 int shwfs_grad_ztilt_dev(shwfs_ctx* ctx, int iwfs, const float* opd, float* grad);

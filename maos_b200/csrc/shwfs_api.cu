@@ -53,6 +53,7 @@ struct PowfsState {
 	int nsimap = 0;
 	DevBuf<float2> etfT[2];
 	int etf_dtrat = 0;  // ETF time interpolation period in frames (0: slot 0 alone)
+	int dtrat = 1;      // frames integrated per output frame (powfs.dtrat)
 	DevBuf<float> lltamp;
 	DevBuf<double> lltorig;  // {llt origx, llt origy}
 	int variant = 0;         // imaging-kernel variant chosen by shwfs_autotune
@@ -145,6 +146,7 @@ struct shwfs_ctx {
 	std::vector<Mark> marks;
 	EvlState* evl = nullptr;
 	int sig2_inner = 0;        // launch_ints_sig2 is running the imaging part
+	int dtrat_inner = 0;       // launch_ints_dtrat is running the imaging part
 };
 static void evl_free(shwfs_ctx* ctx);
 
@@ -769,6 +771,7 @@ static PowfsDev make_powfs_dev(const PowfsState& p, int isim) {
 	P.bkgrndc = (float)p.d.bkgrndc;
 	P.isim = isim;
 	P.lltnorm = (float)(1.0 / ((double)p.d.llt_nx * p.d.embfac * p.d.llt_nx * p.d.embfac));
+	P.accum = p.dtrat > 1 && isim % p.dtrat != 0;
 	return P;
 }
 
@@ -1094,6 +1097,9 @@ static int launch_uplink_gen(shwfs_ctx* ctx, PowfsState& p, const std::vector<in
 static int launch_ints_sig2(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist, int isim,
 	const std::vector<const float*>& opds, const std::vector<const float2*>& lotfs, const std::vector<float*>& ints,
 	const std::vector<float*>& grads, const std::vector<int>& noisy);
+static int launch_ints_dtrat(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist, int isim,
+	const std::vector<const float*>& opds, const std::vector<const float2*>& lotfs, const std::vector<float*>& ints,
+	const std::vector<float*>& grads, const std::vector<int>& noisy);
 static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist, int isim,
 	const std::vector<const float*>& opds, const std::vector<const float2*>& lotfs, const std::vector<float*>& ints,
 	const std::vector<float*>& grads, const std::vector<int>& noisy) {
@@ -1101,6 +1107,8 @@ static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist
 	const int nw = (int)wlist.size();
 	if (nw == 0) return 0;
 	if (is_geom(p.d.gradtype)) return fail(ctx, SHWFS_EINVAL, "geometric sensor: no imaging");
+	if (p.dtrat > 1 && !ctx->dtrat_inner)
+		return launch_ints_dtrat(ctx, ipowfs, wlist, isim, opds, lotfs, ints, grads, noisy);
 	if (p.d.sigmatch == 2 && !ctx->sig2_inner)
 		return launch_ints_sig2(ctx, ipowfs, wlist, isim, opds, lotfs, ints, grads, noisy);
 	if (ctx->form == SHWFS_FORM_TC && nw > TC_MAX_WFS) {
@@ -1259,6 +1267,41 @@ static int launch_uplink(shwfs_ctx* ctx, const std::vector<int>& wlist, const st
 			twoinvwvl, lltnorm);
 	}
 	CK(cudaGetLastError());
+	return 0;
+}
+
+// Imaging of a powfs that integrates dtrat frames per output frame
+// (powfs.dtrat, maos/wfsgrad.c: intensities accumulate in wfsints and noise
+// and gradients are formed on the frame with (isim + 1) % dtrat == 0): each
+// WFS's intensity buffer holds the sum; the first frame of a period starts
+// it, the others add to it, and the last adds noise and forms the gradients.
+static int launch_ints_dtrat(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist, int isim,
+	const std::vector<const float*>& opds, const std::vector<const float2*>& lotfs, const std::vector<float*>& ints,
+	const std::vector<float*>& grads, const std::vector<int>& noisy) {
+	PowfsState& p = ctx->powfs[ipowfs];
+	const int nw = (int)wlist.size();
+	if (isim < 0) return fail(ctx, SHWFS_EINVAL, "dtrat: negative frame index");
+	const bool out = (isim + 1) % p.dtrat == 0;
+	std::vector<float*> acc(nw), gr(nw, nullptr);
+	std::vector<int> nz(nw, 0);
+	for (int k = 0; k < nw; k++) {
+		WfsState& w = ctx->wfs[wlist[k]];
+		if (!w.ints.p) return fail(ctx, SHWFS_ESTATE, "dtrat: WFS %d has no intensity buffer", wlist[k]);
+		acc[k] = w.ints.p;
+		if (out) {
+			gr[k] = grads[k];
+			nz[k] = noisy[k];
+		}
+	}
+	ctx->dtrat_inner = 1;
+	int r = launch_ints(ctx, ipowfs, wlist, isim, opds, lotfs, acc, gr, nz);
+	ctx->dtrat_inner = 0;
+	if (r) return r;
+	if (out)
+		for (int k = 0; k < nw; k++)
+			if (ints[k] && ints[k] != acc[k])
+				CK(cudaMemcpyAsync(ints[k], acc[k], sizeof(float) * p.d.nsa * p.d.pixpsax * p.d.pixpsay,
+					cudaMemcpyDeviceToDevice, ctx->stream));
 	return 0;
 }
 
@@ -1741,6 +1784,15 @@ int shwfs_powfs_set_etf_dtrat(shwfs_ctx* ctx, int ipowfs, int dtrat) {
 	return 0;
 }
 
+int shwfs_powfs_set_dtrat(shwfs_ctx* ctx, int ipowfs, int dtrat) {
+	PowfsState* p = get_powfs(ctx, ipowfs);
+	if (!p || dtrat < 1 || dtrat > 100000) return ctx ? fail(ctx, SHWFS_EINVAL, "set_dtrat: bad arguments") : SHWFS_EINVAL;
+	if (is_geom(p->d.gradtype) && dtrat > 1) return fail(ctx, SHWFS_EINVAL, "set_dtrat: geometric sensors form every frame");
+	if (p->d.sigmatch == 2 && dtrat > 1) return fail(ctx, SHWFS_EINVAL, "set_dtrat: sigmatch 2 with dtrat > 1 is not supported");
+	p->dtrat = dtrat;
+	return 0;
+}
+
 int shwfs_powfs_set_saasum(shwfs_ctx* ctx, int ipowfs, double saasum) {
 	PowfsState* p = get_powfs(ctx, ipowfs);
 	if (!p || !(saasum > 0)) return ctx ? fail(ctx, SHWFS_EINVAL, "set_saasum: bad arguments") : SHWFS_EINVAL;
@@ -2010,6 +2062,7 @@ int shwfs_frame_noalloc(shwfs_ctx* ctx, int iwfs, int isim, float* ints, float* 
 	PowfsState& p = ctx->powfs[w->d.ipowfs];
 	if (is_geom(p.d.gradtype)) return fail(ctx, SHWFS_EINVAL, "frame_noalloc: geometric sensor");
 	if (p.d.sigmatch == 2) return fail(ctx, SHWFS_EINVAL, "frame_noalloc: sigmatch 2 needs the frame path");
+	if (p.dtrat > 1) return fail(ctx, SHWFS_EINVAL, "frame_noalloc: dtrat > 1 needs the frame path");
 	if (p.d.nsa > SHWFS_NOALLOC_MAX_NSA)
 		return fail(ctx, SHWFS_EINVAL, "frame_noalloc: %d subapertures exceed the allocation-free maximum of %d",
 			p.d.nsa, SHWFS_NOALLOC_MAX_NSA);

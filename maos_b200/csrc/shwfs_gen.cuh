@@ -219,6 +219,7 @@ __global__ void gen_pixels_kernel(PowfsDev P, const WfsDev* __restrict__ wfs, in
 				if (id >= 0) v = fmaf(__ldg(swt + 4 * p + c), im[id].x, v);
 			}
 			v *= W.alpha;
+			if (P.accum) v += W.ints[(size_t)isa * npix + p];  // dtrat > 1: the frames so far
 		}
 		pix[q] = v;
 	}
@@ -420,6 +421,7 @@ __global__ void __launch_bounds__(256) ints_n64_kernel(PowfsDev P, const WfsDev*
 			if (id >= 0) v = fmaf(__ldg(swt + 4 * p + c), img[digrev8(id >> 6) * N64_LS + digrev8(id & 63)].x, v);
 		}
 		v *= W.alpha;
+		if (P.accum) v += W.ints[(size_t)isa * npix + p];  // dtrat > 1: the frames so far
 		if (W.noisy) {
 			PixelRng rng(W.seed, (uint32_t)(isa * npix + p), W.wfs_id, (uint32_t)P.isim);
 			v = poisson_draw(rng, v + P.bkgrnd) + P.rne * rng.normal() - P.bkgrndc;

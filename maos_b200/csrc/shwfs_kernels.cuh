@@ -192,6 +192,7 @@ struct PowfsDev {
 	float rne, bkgrnd, bkgrndc;
 	int isim;
 	float lltnorm;         // 1/nlwvf^2 for the uplink PSF
+	int accum;             // dtrat > 1: add this frame's intensities to the stored ones (maos/wfsints.c)
 };
 
 // ---------------------------------------------------------------------------
@@ -598,6 +599,7 @@ __global__ void __launch_bounds__(128, MINB) ints_n32_kernel(PowfsDev P, const W
 				if (id >= 0) v = fmaf(__ldg(swt + 4 * p + c), psf[id], v);
 			}
 			v *= W.alpha;
+			if (P.accum) v += W.ints[(size_t)isa * npix + p];  // dtrat > 1: the frames so far
 		}
 		pix[q] = v;
 	}

@@ -561,7 +561,7 @@ __global__ void __launch_bounds__(TC_THREADS, TC_CTAS_PER_SM) ints_tc_kernel(Pow
 				const float alpha = W.alpha;
 #pragma unroll
 				for (int ix = 0; ix < 8; ix++)
-					if (ix < npx) o[ix] = v[ix] * alpha;
+					if (ix < npx) o[ix] = P.accum ? o[ix] + v[ix] * alpha : v[ix] * alpha;
 			}
 		}
 	}

@@ -111,6 +111,7 @@ def _load() -> C.CDLL:
         "shwfs_frame_noalloc": [vp, i, i, vp, vp],
         "shwfs_powfs_set_etf_dtrat": [vp, i, i],
         "shwfs_powfs_set_saasum": [vp, i, C.c_double],
+        "shwfs_powfs_set_dtrat": [vp, i, i],
         "shwfs_grad_ztilt_dev": [vp, i, vp, vp],
         "shwfs_wfs_set_neasim": [vp, i, dp],
         "shwfs_powfs_set_gs0": [vp, i, i, C.c_long, C.c_long, ip, ip, dp],
@@ -262,6 +263,10 @@ class Context:
         ipt = C.POINTER(C.c_int)
         self._check(self._L.shwfs_powfs_set_gs0(self._h, ipowfs, iamp, nrow, ncol, a.ctypes.data_as(ipt),
                                                 b.ctypes.data_as(ipt), _dptr(v)), "powfs_set_gs0")
+
+    def powfs_set_dtrat(self, ipowfs, dtrat: int):
+        """Frames integrated per output frame (noise and gradients on the last)."""
+        self._check(self._L.shwfs_powfs_set_dtrat(self._h, ipowfs, int(dtrat)), "powfs_set_dtrat")
 
     def powfs_set_saasum(self, ipowfs, saasum: float):
         """powfs.saasum for sigmatch 2 CoG (default: the sum of saa)."""
