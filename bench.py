@@ -308,6 +308,8 @@ def run_b200(args, cfg):
         roofline = {"kernel": "ints_n32_kernel (fused imaging, noise, gradients)", "bound": "hbm",
                     "achieved": ints_gbs, "peak": hbm, "unit": "GB/s", "frac": ints_gbs / hbm,
                     "peak_source": src_note + " hbm_gbs", "traffic": traffic,
+                    "note": "the kernel moves its algorithmic bytes at this rate but is bound by FP32 issue "
+                            "(ncu: issue active 61 %, HBM 5 %); compute gives its FFT flop rate",
                     "algorithmic_bytes_per_launch": ints_bytes,
                     "compute": {"achieved": ints_tf, "peak": fp32_peak, "unit": "TFLOP/s",
                                 "frac": ints_tf / fp32_peak,
