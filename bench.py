@@ -305,11 +305,18 @@ def run_b200(args, cfg):
                     "post": {"kernel": "noise_grad_kernel", "ms_per_launch": post_ms},
                     "raytrace": raytrace}
     else:
-        roofline = {"kernel": "ints_n32_kernel (fused imaging, noise, gradients)", "bound": "hbm",
+        if wl.setup.notf == 64:
+            kname = "ints_n64_kernel (fused imaging, noise, gradients; half-spectrum transforms)"
+            knote = ("the kernel moves its algorithmic bytes at this rate but is bound by shared-memory traffic "
+                     "and issue (ncu: issue active 66 %, L1/shared 73 %, HBM 3 %); compute gives its FFT flop rate")
+        else:
+            kname = "ints_n32_kernel (fused imaging, noise, gradients)"
+            knote = ("the kernel moves its algorithmic bytes at this rate but is bound by FP32 issue "
+                     "(ncu: issue active 61 %, HBM 5 %); compute gives its FFT flop rate")
+        roofline = {"kernel": kname, "bound": "hbm",
                     "achieved": ints_gbs, "peak": hbm, "unit": "GB/s", "frac": ints_gbs / hbm,
                     "peak_source": src_note + " hbm_gbs", "traffic": traffic,
-                    "note": "the kernel moves its algorithmic bytes at this rate but is bound by FP32 issue "
-                            "(ncu: issue active 61 %, HBM 5 %); compute gives its FFT flop rate",
+                    "note": knote,
                     "algorithmic_bytes_per_launch": ints_bytes,
                     "compute": {"achieved": ints_tf, "peak": fp32_peak, "unit": "TFLOP/s",
                                 "frac": ints_tf / fp32_peak,

@@ -1157,8 +1157,9 @@ static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist
 		int r = ensure_twiddles(ctx, p);
 		if (r) return r;
 		StageMark mark(ctx, SHWFS_STAGE_INTS);
-		ints_n64_kernel<<<nitem, 256, N64_SMEM_BYTES, ctx->stream>>>(P, wdev, nw, nitem, p.d.nopd,
-			(float)(2.0 / p.d.wvl), p.gen_tw.p);
+		auto kern = p.d.nopd == 32 ? ints_n64_kernel<32> : ints_n64_kernel<0>;
+		kern<<<nitem, N64_THREADS, N64_SMEM_BYTES, ctx->stream>>>(P, wdev, nw, nitem, p.d.nopd, (float)(2.0 / p.d.wvl),
+			p.gen_tw.p);
 		CK(cudaGetLastError());
 		return 0;
 	}

@@ -295,29 +295,37 @@ __device__ __forceinline__ void dft8(float2 (&a)[8], float dir) {
 	}
 }
 
-// One 64-point transform of nlines lines (line L at s + (line0 + L) * ls,
-// element j at + j * es) in form F (digrev_in false) or G (true); LINES_FAST
-// marks column lines.
+// One 64-point transform of NLINES lines (nlines when NLINES is 0) of the
+// 64 x N64_LS shared image: rows (line L at s + (line0 + L) * N64_LS, element
+// j at + j) or columns (COLS: line L at s + line0 + L, element j at + j *
+// N64_LS), in form F (DIGREV_IN false) or G (true), DIR -1 forward, +1
+// inverse.  In form F the input elements outside [lo, hi) are taken as zero
+// and not read (a zero-padded field needs no zero fill).  Called by all
+// N64_THREADS threads of the block.
 // tw[k] = exp(-2 pi i k / 64).
-template <bool DIGREV_IN, bool LINES_FAST>
-__device__ __forceinline__ void fft64_lines(float2* s, int ls, int es, int line0, int nlines,
-	const float2* __restrict__ tw, float dir) {
+constexpr int N64_THREADS = 256;
+template <bool DIGREV_IN, bool COLS, int NLINES, int DIR>
+__device__ __forceinline__ void fft64_lines(float2* s, int line0, const float2* __restrict__ tw, int nlines = NLINES,
+	int lo = 0, int hi = 64) {
+	constexpr int ls = COLS ? 1 : N64_LS, es = COLS ? N64_LS : 1;
+	constexpr float dir = (float)DIR;
+	const unsigned nl = NLINES > 0 ? (unsigned)NLINES : (unsigned)nlines;
 #pragma unroll
 	for (int step = 0; step < 2; step++) {
 		// F: step 0 gathers 8 i + t and twiddles, step 1 gathers 8 t + i.
 		// G: step 0 gathers 8 t + i and twiddles, step 1 gathers 8 i + t.
 		const bool strided = (step == 0) != DIGREV_IN;
-		const int ntask = nlines * 8;
+		const unsigned ntask = nl * 8;
 		// consecutive threads take consecutive lines for column lines, and for
 		// the gather of 8 consecutive elements of row lines (rows are N64_LS
 		// apart: conflict-free), consecutive tasks for the strided gather of row
 		// lines (consecutive elements)
-		const bool lines_fast = LINES_FAST || !strided;
-		for (int task = threadIdx.x; task < ntask; task += blockDim.x) {
-			int L, t;
+		const bool lines_fast = COLS || !strided;
+		for (unsigned task = threadIdx.x; task < ntask; task += N64_THREADS) {
+			unsigned L, t;
 			if (lines_fast) {
-				L = task % nlines;
-				t = task / nlines;
+				L = task % nl;
+				t = task / nl;
 			} else {
 				L = task >> 3;
 				t = task & 7;
@@ -325,19 +333,25 @@ __device__ __forceinline__ void fft64_lines(float2* s, int ls, int es, int line0
 			float2* line = s + (line0 + L) * ls;
 			float2 a[8];
 #pragma unroll
-			for (int i = 0; i < 8; i++) a[i] = line[(strided ? 8 * i + t : 8 * t + i) * es];
+			for (int i = 0; i < 8; i++) {
+				const int j = strided ? 8 * i + (int)t : 8 * (int)t + i;
+				if (!DIGREV_IN && step == 0)
+					a[i] = (j >= lo && j < hi) ? line[j * es] : make_float2(0.f, 0.f);
+				else
+					a[i] = line[j * es];
+			}
 			dft8(a, dir);
 			if (step == 0) {
 #pragma unroll
 				for (int i = 1; i < 8; i++) {
-					float2 w = tw[(t * i) & 63];
+					float2 w = tw[(t * i) & 63u];
 					w.y *= -dir;  // tw holds exp(-...); dir -1 keeps it, +1 conjugates
 					const float2 v = a[i];
 					a[i] = make_float2(v.x * w.x - v.y * w.y, v.x * w.y + v.y * w.x);
 				}
 			}
 #pragma unroll
-			for (int i = 0; i < 8; i++) line[(strided ? 8 * i + t : 8 * t + i) * es] = a[i];
+			for (int i = 0; i < 8; i++) line[(strided ? 8 * i + (int)t : 8 * (int)t + i) * es] = a[i];
 		}
 		__syncthreads();
 	}
@@ -347,8 +361,11 @@ __device__ __forceinline__ void fft64_lines(float2* s, int ls, int es, int line0
 // k as in the other imaging launches).  Dynamic shared memory
 // N64_SMEM_BYTES.  tw64[k] = exp(-2 pi i k / 64), k < 64.
 constexpr int N64_SMEM_BYTES = (64 * N64_LS + 64) * 8 + 256 * 4;
-__global__ void __launch_bounds__(256) ints_n64_kernel(PowfsDev P, const WfsDev* __restrict__ wfs, int nw, int nitem,
-	int nopd, float twoinvwvl, const float2* __restrict__ tw64) {
+// NOPD > 0 fixes the pupil size at compile time (nopd is then ignored).
+template <int NOPD>
+__global__ void __launch_bounds__(N64_THREADS, 6) ints_n64_kernel(PowfsDev P, const WfsDev* __restrict__ wfs, int nw,
+	int nitem, int nopd_rt, float twoinvwvl, const float2* __restrict__ tw64) {
+	const int nopd = NOPD > 0 ? NOPD : nopd_rt;
 	extern __shared__ float2 n64_s[];
 	float2* img = n64_s;
 	float2* tw = n64_s + 64 * N64_LS;
@@ -359,10 +376,9 @@ __global__ void __launch_bounds__(256) ints_n64_kernel(PowfsDev P, const WfsDev*
 	const WfsDev& W = wfs[item % nw];
 	const int pad = (64 - nopd) / 2, no2 = nopd * nopd;
 	if (tid < 64) tw[tid] = tw64[tid];
-	// (b) field, zero-padded (cembed_wvf, maos/wfsints.c:233)
-	for (int idx = tid; idx < 64 * 64; idx += blockDim.x) img[(idx >> 6) * N64_LS + (idx & 63)] = make_float2(0.f, 0.f);
-	__syncthreads();
-	for (int idx = tid; idx < no2; idx += blockDim.x) {
+	// (b) field, zero-padded (cembed_wvf, maos/wfsints.c:233): only the pupil
+	// square is written; the first transforms read nothing outside it
+	for (int idx = tid; idx < no2; idx += N64_THREADS) {
 		const int y = idx / nopd, x = idx - y * nopd;
 		const float o = __ldg(W.opd + (size_t)isa * no2 + idx), a = __ldg(W.amp + (size_t)isa * no2 + idx);
 		float sn, cs;
@@ -370,27 +386,52 @@ __global__ void __launch_bounds__(256) ints_n64_kernel(PowfsDev P, const WfsDev*
 		img[(y + pad) * N64_LS + x + pad] = make_float2(a * cs, a * sn);
 	}
 	__syncthreads();
-	// (c) PSF: forward along x on the pupil rows, along y; |.|^2
-	fft64_lines<false, false>(img, N64_LS, 1, pad, nopd, tw, -1.f);
-	fft64_lines<false, true>(img, 1, N64_LS, 0, 64, tw, -1.f);
-	for (int idx = tid; idx < 64 * 64; idx += blockDim.x) {
+	// (c) PSF: forward along x on the pupil rows, along y
+	fft64_lines<false, false, NOPD, -1>(img, pad, tw, nopd, pad, pad + nopd);
+	fft64_lines<false, true, 64, -1>(img, 0, tw, 64, pad, pad + nopd);
+	// |.|^2, two real PSF rows per complex row: row r <- (PSF row r) + i (PSF row r + 32)
+	for (int idx = tid; idx < 32 * 64; idx += N64_THREADS) {
 		float2* v = img + (idx >> 6) * N64_LS + (idx & 63);
-		*v = make_float2(v->x * v->x + v->y * v->y, 0.f);
+		const float2 a = v[0], b = v[32 * N64_LS];
+		v[0] = make_float2(a.x * a.x + a.y * a.y, b.x * b.x + b.y * b.y);
 	}
 	__syncthreads();
-	// OTF in natural order: forward along kx, along ky (digit-reversed inputs)
-	fft64_lines<true, false>(img, N64_LS, 1, 0, 64, tw, -1.f);
-	fft64_lines<true, true>(img, 1, N64_LS, 0, 64, tw, -1.f);
-	// x conj(uplink OTF) x ETF / nominal; transfer functions are [fy + 64 fx]
+	// OTF, half spectrum kx = 0..32 (the PSF is real, so OTF(-k) = conj OTF(k)):
+	// forward along kx on the 32 packed rows (digit-reversed inputs)
+	fft64_lines<true, false, 32, -1>(img, 0, tw);
+	// unpack the pairs: row r's spectrum Z = H_r + i H_{r+32}, H_r(kx) = (Z(kx) +
+	// conj Z(-kx)) / 2, H_{r+32}(kx) = (Z(kx) - conj Z(-kx)) / 2i.  H(0) and
+	// H(32) are real, so column 0 carries H(0) + i H(32) and column 32 is free.
+	for (int idx = tid; idx < 32 * 32; idx += N64_THREADS) {
+		const int r = idx >> 5, kx = idx & 31;
+		float2* row = img + r * N64_LS;
+		const float2 z = row[kx], zm = row[kx ? 64 - kx : 32];
+		if (kx) {
+			row[kx] = make_float2(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y));
+			row[32 * N64_LS + kx] = make_float2(0.5f * (z.y + zm.y), 0.5f * (zm.x - z.x));
+		} else {
+			row[0] = make_float2(z.x, zm.x);
+			row[32 * N64_LS] = make_float2(z.y, zm.y);
+		}
+	}
+	__syncthreads();
+	// forward along ky on columns 0..31 (digit-reversed inputs): natural OTF
+	fft64_lines<true, true, 32, -1>(img, 0, tw);
+	// x conj(uplink OTF) x ETF / nominal; transfer functions are [fy + 64 fx].
+	// The image is the real part of the inverse transform, which is the inverse
+	// of OTF x (TF(k) + conj TF(-k)) / 2 over the half spectrum.  Column 0 holds
+	// Y = O(.,0) + i O(.,32) with O(.,0), O(.,32) the transforms of real
+	// columns; the products for kx = 0 and 32 go to column 32 as X(.,0) + i X(.,32).
 	{
 		const float2* e1 = P.etfT1 ? P.etfT1 + (size_t)isa * 4096 : nullptr;
 		const float2* e2 = P.etfT2 ? P.etfT2 + (size_t)isa * 4096 : nullptr;
 		const float* nm = P.nominalT ? P.nominalT + (P.nominal_per_sa ? (size_t)isa * 4096 : 0) : nullptr;
-		for (int t = tid; t < 64 * 64; t += blockDim.x) {
-			const int fy = t & 63, fx = t >> 6;
-			float2* v = img + fy * N64_LS + fx;
-			float2 o = *v;
-			if (W.lotfT) o = cmulc(o, __ldg(W.lotfT + t));
+		auto tf = [&](int t) -> float2 {
+			float2 o = make_float2(1.f, 0.f);
+			if (W.lotfT) {
+				const float2 l = __ldg(W.lotfT + t);
+				o = make_float2(l.x, -l.y);
+			}
 			if (e1) {
 				float2 e = __ldg(e1 + t);
 				if (e2) {
@@ -402,23 +443,64 @@ __global__ void __launch_bounds__(256) ints_n64_kernel(PowfsDev P, const WfsDev*
 				const float d = __ldg(nm + t);
 				o = make_float2(o.x * d, o.y * d);
 			}
-			*v = o;
+			return o;
+		};
+		// (TF(t) + conj TF(tm)) / 2
+		auto tfh = [&](int t, int tm) -> float2 {
+			const float2 a = tf(t), b = tf(tm);
+			return make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));
+		};
+		for (int t = tid; t < 64 * 32; t += N64_THREADS) {
+			const int fy = t & 63, fx = t >> 6, my = (64 - fy) & 63;
+			if (fx) {
+				float2* v = img + fy * N64_LS + fx;
+				*v = cmul(*v, tfh(t, my + 64 * (64 - fx)));
+			} else {
+				const float2 y = img[fy * N64_LS], ym = img[my * N64_LS];
+				const float2 o0 = make_float2(0.5f * (y.x + ym.x), 0.5f * (y.y - ym.y));
+				const float2 o32 = make_float2(0.5f * (y.y + ym.y), 0.5f * (ym.x - y.x));
+				const float2 x0 = cmul(o0, tfh(fy, my)), x32 = cmul(o32, tfh(fy + 64 * 32, my + 64 * 32));
+				img[fy * N64_LS + 32] = make_float2(x0.x - x32.y, x0.y + x32.x);
+			}
 		}
 	}
 	__syncthreads();
-	// inverse along fx, along fy: the image at digit-reversed rows and columns
-	fft64_lines<false, false>(img, N64_LS, 1, 0, 64, tw, 1.f);
-	fft64_lines<false, true>(img, 1, N64_LS, 0, 64, tw, 1.f);
-	// (d) pixels (bilinear map, real part) and noise, one thread per pixel
+	// inverse along fy on columns 1..32: G(y, kx) at digit-reversed rows, column
+	// 32 holding G(., 0) + i G(., 32) (both real)
+	fft64_lines<false, true, 32, 1>(img, 1, tw);
+	// two real image rows per complex row: row r <- a + i b over the full kx
+	// range, a and b the Hermitian extensions of rows r and r + 32
+	for (int idx = tid; idx < 32 * 32; idx += N64_THREADS) {
+		const int r = idx >> 5, kx = idx & 31;
+		float2* row = img + r * N64_LS;
+		if (kx) {
+			const float2 a = row[kx], b = row[32 * N64_LS + kx];
+			row[kx] = make_float2(a.x - b.y, a.y + b.x);
+			row[64 - kx] = make_float2(a.x + b.y, b.x - a.y);
+		} else {
+			const float2 a = row[32], b = row[32 * N64_LS + 32];
+			row[0] = make_float2(a.x, b.x);
+			row[32] = make_float2(a.y, b.y);
+		}
+	}
+	__syncthreads();
+	// inverse along fx on the 32 packed rows: image row s (digit-reversed) is the
+	// real part of row s for s < 32, the imaginary part of row s - 32 otherwise
+	fft64_lines<false, false, 32, 1>(img, 0, tw);
+	// (d) pixels (bilinear map) and noise, one thread per pixel
 	const int npix = P.npix;
 	const int* sidx = P.simap_idx + (P.simap_per_sa ? (size_t)isa * npix * 4 : 0);
 	const float* swt = P.simap_wt + (P.simap_per_sa ? (size_t)isa * npix * 4 : 0);
-	for (int p = tid; p < npix; p += blockDim.x) {
+	for (int p = tid; p < npix; p += N64_THREADS) {
 		float v = 0.f;
 #pragma unroll
 		for (int c = 0; c < 4; c++) {
 			const int id = __ldg(sidx + 4 * p + c);
-			if (id >= 0) v = fmaf(__ldg(swt + 4 * p + c), img[digrev8(id >> 6) * N64_LS + digrev8(id & 63)].x, v);
+			if (id >= 0) {
+				const int sr = digrev8(id >> 6);
+				const float2 q = img[(sr & 31) * N64_LS + digrev8(id & 63)];
+				v = fmaf(__ldg(swt + 4 * p + c), sr < 32 ? q.x : q.y, v);
+			}
 		}
 		v *= W.alpha;
 		if (P.accum) v += W.ints[(size_t)isa * npix + p];  // dtrat > 1: the frames so far
