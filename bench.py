@@ -256,8 +256,10 @@ def run_b200(args, cfg):
     ctx.profile_enable(False)
     launches_per_step = sum(n for _, n in stages.values()) / nprof
 
-    # end to end through the C ABI: queue + sync with host gradients each step
+    # end to end through the C ABI: queue + sync with host gradients each step,
+    # into one host buffer the loop owns (as a C caller passes its own)
     ctx.copy_counters()
+    gbuf = np.empty(sum(2 * ctx.wfs_nsa[i] for i in wl.wfs))
     e2e_s = 0.0
     for k in range(args.steps):
         with torch.cuda.stream(ext):
@@ -265,7 +267,7 @@ def run_b200(args, cfg):
         ctx.sync()
         t0 = time.perf_counter()
         wl.frame(isim)
-        wl.frame_sync()
+        wl.frame_sync(out=gbuf)
         e2e_s += time.perf_counter() - t0
         isim += 1
     h2d, d2h = ctx.copy_counters()
@@ -413,8 +415,9 @@ def run_batch(args, bcfg):
     launches_per_step = sum(n for _, n in stages.values()) / nprof
     st = {k: dict(ms_per_launch=(ms / n if n else 0.0), launches_per_step=n / nprof, ms_per_step=ms / nprof)
           for k, (ms, n) in stages.items()}
-    # end to end: graph frame + host gradients of every WFS
+    # end to end: graph frame + host gradients of every WFS into one host buffer
     ctx.copy_counters()
+    gbuf = np.empty(sum(2 * ctx.wfs_nsa[i] for i in range(wl.nwfs)))
     e2e_s = 0.0
     for k in range(args.steps):
         with torch.cuda.stream(ext):
@@ -422,7 +425,7 @@ def run_batch(args, bcfg):
         ctx.sync()
         t0 = time.perf_counter()
         wl.frame(isim)
-        wl.frame_sync()
+        wl.frame_sync(out=gbuf)
         e2e_s += time.perf_counter() - t0
         isim += 1
     h2d, d2h = ctx.copy_counters()

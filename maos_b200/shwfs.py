@@ -193,6 +193,7 @@ class Context:
         self._h = h
         self.npix = {}
         self.nsa = {}
+        self.wfs_nsa = {}  # iwfs -> subapertures of its powfs
         _live.add(self)
 
     def _check(self, rc: int, what: str):
@@ -280,6 +281,7 @@ class Context:
         d = WfsDesc(**kw)
         out = C.c_int()
         self._check(self._L.shwfs_wfs_add(self._h, C.byref(d), C.byref(out)), "wfs_add")
+        self.wfs_nsa[out.value] = self.nsa.get(d.ipowfs, 0)
         return out.value
 
     def wfs_set_mtche(self, iwfs, mtche, i0sum=None, i0sumsum=0.0):
@@ -313,10 +315,24 @@ class Context:
     def frame_queue(self, isim: int, iwfs0: int, iwfs1: int):
         self._check(self._L.shwfs_frame_queue(self._h, isim, iwfs0, iwfs1), "frame_queue")
 
-    def frame_sync_range(self, iwfs0: int, iwfs1: int, nsa_of):
-        """Gradients of WFS iwfs0..iwfs1-1 after their frame, with one wait;
-        nsa_of(i) gives WFS i's subaperture count.  Returns one array per WFS."""
-        sizes = [2 * nsa_of(i) for i in range(iwfs0, iwfs1)]
+    def frame_sync_range(self, iwfs0: int, iwfs1: int, nsa_of=None, out: Optional[np.ndarray] = None):
+        """Gradients of WFS iwfs0..iwfs1-1 after their frame, with one wait.
+
+        With ``out`` (a C-contiguous float64 array of at least the range's
+        2 nsa values per WFS, in WFS order) they are written there and ``out``
+        is returned: a caller that consumes each frame before the next reuses
+        one buffer, as a C caller does.  Otherwise one new array per WFS is
+        returned (nsa_of(i), if given, is WFS i's subaperture count)."""
+        if out is not None:
+            n = 0
+            for i in range(iwfs0, iwfs1):
+                n += 2 * self.wfs_nsa[i]
+            if out.dtype != np.float64 or not out.flags.c_contiguous or out.size < n:
+                raise ValueError(f"frame_sync_range: out must be a C-contiguous float64 array of >= {n} values")
+            self._check(self._L.shwfs_frame_sync_range(self._h, iwfs0, iwfs1, _dptr(out)), "frame_sync_range")
+            return out
+        f = nsa_of if nsa_of is not None else self.wfs_nsa.__getitem__
+        sizes = [2 * f(i) for i in range(iwfs0, iwfs1)]
         g = np.zeros(sum(sizes))
         self._check(self._L.shwfs_frame_sync_range(self._h, iwfs0, iwfs1, _dptr(g)), "frame_sync_range")
         return np.split(g, np.cumsum(sizes)[:-1])

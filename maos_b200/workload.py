@@ -40,9 +40,12 @@ class Workload:
         """Queue one frame of every WFS (asynchronous)."""
         self.ctx.frame_queue(isim, self.wfs[0], self.wfs[-1] + 1)
 
-    def frame_sync(self, want_ints: bool = False):
-        if not want_ints:  # gradients of every WFS with one wait
-            return self.ctx.frame_sync_range(self.wfs[0], self.wfs[-1] + 1, lambda i: self.setup.nsa)
+    def frame_sync(self, want_ints: bool = False, out=None):
+        """Gradients of every WFS with one wait (one array per WFS, or all of
+        them written into ``out``: see Context.frame_sync_range); with
+        want_ints, (gradients, intensities) per WFS."""
+        if not want_ints:
+            return self.ctx.frame_sync_range(self.wfs[0], self.wfs[-1] + 1, out=out)
         return [self.ctx.frame_sync(i, self.ipowfs, want_ints) for i in self.wfs]
 
     def close(self):
@@ -119,15 +122,12 @@ class BatchWorkload:
         else:
             self.ctx.frame_queue(isim, 0, self.nwfs)
 
-    def frame_sync(self, want_ints: bool = False):
+    def frame_sync(self, want_ints: bool = False, out=None):
         """Gradients of every WFS (with intensities when want_ints); without
-        intensities, one wait and one copy for the whole frame."""
+        intensities, one wait and one copy for the whole frame, into ``out``
+        when given (see Context.frame_sync_range)."""
         if not want_ints:
-            nsa = {}
-            for _, setup, _, wl in self.members:
-                for i in wl:
-                    nsa[i] = setup.nsa
-            return self.ctx.frame_sync_range(0, self.nwfs, lambda i: nsa[i])
+            return self.ctx.frame_sync_range(0, self.nwfs, out=out)
         out = []
         for _, _, ip, wl in self.members:
             out += [self.ctx.frame_sync(i, ip, want_ints) for i in wl]

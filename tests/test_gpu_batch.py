@@ -62,3 +62,25 @@ def test_range_sync_equals_per_wfs_sync():
     assert len(a) == len(b) == 9
     for ga, gb in zip(a, b):
         assert np.array_equal(ga, gb)
+
+
+def test_range_sync_into_caller_buffer():
+    """The range sync into a caller-owned buffer writes the same gradients as
+    the per-WFS arrays, in WFS order, and refuses a buffer that is too small
+    or not float64."""
+    import pytest
+    from maos_b200.configs import UNEVEN_BATCH
+    from maos_b200.workload import build_batch
+    wl = build_batch(UNEVEN_BATCH["members"], device=0, seed=6, noisy=True, nx=512, graph=True)
+    wl.frame(4)
+    a = wl.frame_sync()
+    n = sum(len(g) for g in a)
+    buf = np.full(n, np.nan)
+    wl.frame(4)
+    assert wl.frame_sync(out=buf) is buf
+    assert np.array_equal(buf, np.concatenate(a))
+    with pytest.raises(ValueError):
+        wl.frame_sync(out=np.empty(n - 1))
+    with pytest.raises(ValueError):
+        wl.frame_sync(out=np.empty(n, dtype=np.float32))
+    wl.close()
