@@ -255,8 +255,9 @@ int shwfs_profile_read(shwfs_ctx* ctx, double* ms, int* launches);
 
 /* ---- tuning ---- */
 #define SHWFS_NVARIANT 3 /* imaging-kernel variants: register cap for 4, 5 or 6 blocks per SM */
-/* Times every imaging-kernel variant on nrep frames of WFS [iwfs0, iwfs1)
-   (their powfs) and keeps the fastest; *chosen receives its index. */
+/* Times every imaging-kernel variant on nrep whole frames of WFS
+   [iwfs0, iwfs1) (their powfs; device time of the frame on the context's
+   stream) and keeps the fastest; *chosen receives its index. */
 int shwfs_autotune(shwfs_ctx* ctx, int iwfs0, int iwfs1, int nrep, int* chosen);
 /* Selects an imaging-kernel variant explicitly. */
 int shwfs_set_variant(shwfs_ctx* ctx, int ipowfs, int variant);

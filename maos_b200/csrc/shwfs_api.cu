@@ -1218,8 +1218,8 @@ static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist
 		return 0;
 	}
 	StageMark mark(ctx, SHWFS_STAGE_INTS);
-	auto go = [&](auto kern) { kern<<<nblk, 128, 0, ctx->stream>>>(P, wdev, nw, nitem); };
 	const int v = p.variant;
+	auto go = [&](auto kern) { kern<<<nblk, 128, 0, ctx->stream>>>(P, wdev, nw, nitem); };
 	if (npix <= 32) {
 		if (v == 1) go(ints_n32_kernel<1, 5>);
 		else if (v == 2) go(ints_n32_kernel<1, 6>);
@@ -1923,28 +1923,36 @@ int shwfs_autotune(shwfs_ctx* ctx, int iwfs0, int iwfs1, int nrep, int* chosen) 
 	if (r) return r;
 	const int ipowfs = ctx->wfs[iwfs0].d.ipowfs;
 	PowfsState& p = ctx->powfs[ipowfs];
-	const int saved = ctx->profiling;
-	ctx->profiling = 1;
+	// whole frames on the device: the variants differ in which launches a frame has
+	cudaEvent_t e0 = nullptr, e1 = nullptr;
+	CK(cudaEventCreate(&e0));
+	if (cudaEventCreate(&e1) != cudaSuccess) {
+		cudaEventDestroy(e0);
+		return fail(ctx, SHWFS_ECUDA, "autotune: cudaEventCreate failed");
+	}
 	double best = 1e300;
 	int bestv = 0;
-	double ms[SHWFS_NSTAGE];
-	int n[SHWFS_NSTAGE];
-	if ((r = shwfs_profile_read(ctx, ms, n))) return r;  // drain
-	for (int v = 0; v < SHWFS_NVARIANT; v++) {
+	for (int v = 0; v < SHWFS_NVARIANT && !r; v++) {
 		p.variant = v;
-		if ((r = shwfs_frame_queue(ctx, 0, iwfs0, iwfs1))) return r;  // warm
-		if ((r = shwfs_profile_read(ctx, ms, n))) return r;
-		for (int k = 0; k < nrep; k++)
-			if ((r = shwfs_frame_queue(ctx, k, iwfs0, iwfs1))) return r;
-		if ((r = shwfs_profile_read(ctx, ms, n))) return r;
-		const double t = ms[SHWFS_STAGE_INTS] / (n[SHWFS_STAGE_INTS] ? n[SHWFS_STAGE_INTS] : 1);
-		if (t < best) {
-			best = t;
+		if ((r = shwfs_frame_queue(ctx, 0, iwfs0, iwfs1))) break;  // warm
+		if (cudaEventRecord(e0, ctx->stream) != cudaSuccess) { r = fail(ctx, SHWFS_ECUDA, "autotune: event record failed"); break; }
+		for (int k = 0; k < nrep && !r; k++) r = shwfs_frame_queue(ctx, k, iwfs0, iwfs1);
+		if (r) break;
+		float ms = 0.f;
+		if (cudaEventRecord(e1, ctx->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+			cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+			r = fail(ctx, SHWFS_ECUDA, "autotune: event timing failed");
+			break;
+		}
+		if (ms < best) {
+			best = ms;
 			bestv = v;
 		}
 	}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	if (r) return r;
 	p.variant = bestv;
-	ctx->profiling = saved;
 	if (chosen) *chosen = bestv;
 	return 0;
 }

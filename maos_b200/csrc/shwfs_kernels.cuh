@@ -203,19 +203,14 @@ constexpr int LD = 33;  // padded leading dimension of the warp tile (float2)
 
 // Field of a 16x16 OPD patch embedded at offset 8 in 32x32, then the 2-D
 // forward FFT, pruned to the 16 non-zero rows and columns.  On return lane l
-// holds F(kx=l, ky=0..31).  opd/amp are the subaperture's 256 values
-// (x fastest); tile is the warp's 32x33 float2 scratch.
-__device__ __forceinline__ void field_fft_n32(const float* opd, const float* __restrict__ amp,
-	float twoinvwvl, float2* tile, int lane, float2 (&F)[32]) {
-	// (b) field. lane holds elements e = j*32 + lane: ix = lane&15, iy = 2j + lane/16
-	float o[8], a[8];
+// holds F(kx=l, ky=0..31).  The lane brings the OPD and amplitude of elements
+// e = j*32 + lane (ix = lane&15, iy = 2j + lane/16) in o[j], a[j]; tile is
+// the warp's 32x33 float2 scratch.
+__device__ __forceinline__ void field_fft_n32_regs(const float (&o)[8], const float (&a)[8], float twoinvwvl,
+	float2* tile, int lane, float2 (&F)[32]) {
 	float s = 0.f;
 #pragma unroll
-	for (int j = 0; j < 8; j++) {
-		o[j] = opd[j * 32 + lane];
-		a[j] = amp[j * 32 + lane];
-		s += o[j];
-	}
+	for (int j = 0; j < 8; j++) s += o[j];
 	// remove the subaperture piston before forming the phase: a constant phase
 	// factor cancels in |FFT|^2, and it keeps the FP32 phase small
 #pragma unroll
@@ -273,6 +268,19 @@ __device__ __forceinline__ void field_fft_n32(const float* opd, const float* __r
 	}
 }
 
+// The same with the subaperture's 256 OPD and amplitude values (x fastest)
+// read from memory.
+__device__ __forceinline__ void field_fft_n32(const float* opd, const float* __restrict__ amp,
+	float twoinvwvl, float2* tile, int lane, float2 (&F)[32]) {
+	float o[8], a[8];
+#pragma unroll
+	for (int j = 0; j < 8; j++) {
+		o[j] = opd[j * 32 + lane];
+		a[j] = amp[j * 32 + lane];
+	}
+	field_fft_n32_regs(o, a, twoinvwvl, tile, lane, F);
+}
+
 // |F|^2 then the forward 2-D FFT of the real PSF. Input: lane = kx holds
 // F(kx, ky=0..31).  Output: lane = fy holds OTF(fx=0..31, fy=lane).
 __device__ __forceinline__ void psf_to_otf_n32(float2 (&F)[32], float scale, float2* tile, int lane) {
@@ -315,6 +323,39 @@ __device__ __forceinline__ void psf_to_otf_n32(float2 (&F)[32], float scale, flo
 // covers points [GEOM_PTS * bd (b % bps), + GEOM_PTS * bd) of subaperture
 // item b / bps.
 constexpr int GEOM_PTS = 4;
+
+// The footprint origin of subaperture isa of entry E in layer l along x (isy
+// false) or y, in FP64 from the subaperture origin: first screen index j0 and
+// FP32 fraction f0, wrapped into the screen (prop_grid_pts,
+// lib/accphi_grid_do.c:424-434, wrap=1).
+__device__ __forceinline__ void geom_origin(const GeomParams& P, const GeomEntry& E, int isa, int l, bool isy, int& j0,
+	float& f0) {
+	const int n = isy ? P.ny[l] : P.nx[l];
+	double x0 = (isy ? E.origy[isa] : E.origx[isa]) * E.sx[l] + (isy ? E.dispy[l] : E.dispx[l]);
+	if (!isfinite(x0) || !isfinite((isy ? E.origx[isa] : E.origy[isa]) * E.sx[l] + (isy ? E.dispx[l] : E.dispy[l])))
+		x0 = 0;
+	x0 -= floor(x0 / n) * n;
+	j0 = (int)floor(x0);
+	f0 = (float)(x0 - j0);
+	if (j0 >= n) j0 -= n;
+}
+// Point i of a line from its origin (j0, f0) at FP32 step `step` (OPD
+// sampling x scale / screen sampling): screen index j, wrapped neighbour j1,
+// bilinear weight w.
+__device__ __forceinline__ void geom_point(int j0, float f0, int i, float step, int n, int& j, int& j1, float& w) {
+	const float f = f0 + i * step;
+	const float fl = floorf(f);
+	j = j0 + (int)fl;
+	while (j >= n) j -= n;
+	j1 = j == n - 1 ? 0 : j + 1;
+	w = f - fl;
+}
+// acc + al * bilinear(m00, m10, m01, m11; wx, wy)
+__device__ __forceinline__ float geom_bilerp(float al, float m00, float m10, float m01, float m11, float wx, float wy,
+	float acc) {
+	return fmaf(al, (m00 + (m10 - m00) * wx) * (1.f - wy) + (m01 + (m11 - m01) * wx) * wy, acc);
+}
+
 __global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomParams P, int nopd, int nitem, int bps) {
 	extern __shared__ int4 s_tab[];
 	const int item = blockIdx.x / bps, part = blockIdx.x - item * bps;
@@ -329,20 +370,12 @@ __global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomP
 		const bool isy = r >= nopd;
 		const int i = isy ? r - nopd : r;
 		const int n = isy ? P.ny[l] : P.nx[l];
-		double x0 = (isy ? E.origy[isa] : E.origx[isa]) * E.sx[l] + (isy ? E.dispy[l] : E.dispx[l]);
-		if (!isfinite(x0) || !isfinite((isy ? E.origx[isa] : E.origy[isa]) * E.sx[l] + (isy ? E.dispx[l] : E.dispy[l])))
-			x0 = 0;
-		x0 -= floor(x0 / n) * n;
-		int j0 = (int)floor(x0);
-		const float f0 = (float)(x0 - j0);
-		if (j0 >= n) j0 -= n;
-		const float f = f0 + i * (float)(E.dx * E.sx[l]);
-		const float fl = floorf(f);
-		int j = j0 + (int)fl;
-		while (j >= n) j -= n;
-		const int j1 = j == n - 1 ? 0 : j + 1;
+		int j0, j, j1;
+		float f0, w;
+		geom_origin(P, E, isa, l, isy, j0, f0);
+		geom_point(j0, f0, i, (float)(E.dx * E.sx[l]), n, j, j1, w);
 		const int m = isy ? P.nx[l] : 1;
-		s_tab[k] = make_int4(j * m, j1 * m, __float_as_int(f - fl), 0);
+		s_tab[k] = make_int4(j * m, j1 * m, __float_as_int(w), 0);
 	}
 	__syncthreads();
 	// up to GEOM_PTS points per thread, layers outermost so that the gathers of the points are in flight
@@ -368,8 +401,7 @@ __global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomP
 				const int4 tx = s_tab[l * 2 * nopd + ixu[u]], ty = s_tab[l * 2 * nopd + nopd + iyu[u]];
 				const float m00 = __ldg(sc + (ty.x + tx.x)), m10 = __ldg(sc + (ty.x + tx.y));
 				const float m01 = __ldg(sc + (ty.y + tx.x)), m11 = __ldg(sc + (ty.y + tx.y));
-				const float wx = __int_as_float(tx.z), wy = __int_as_float(ty.z);
-				acc[u] = fmaf(al, (m00 + (m10 - m00) * wx) * (1.f - wy) + (m01 + (m11 - m01) * wx) * wy, acc[u]);
+				acc[u] = geom_bilerp(al, m00, m10, m01, m11, __int_as_float(tx.z), __int_as_float(ty.z), acc[u]);
 			}
 		}
 	}
@@ -522,26 +554,11 @@ __device__ __forceinline__ void grad_from_pixels(const float (&pix)[NPQ], int np
 // (b)-(e) fused, n_opd=16, n_w=n_f=32.  Work item w -> (isa = w / nw, wfs =
 // wlist[w % nw]) so the WFS that share a subaperture's ETF run together.
 // ---------------------------------------------------------------------------
-// NPQ: pixel slots per lane, ceil(npix/32).  MINB: resident blocks per SM the
-// register allocation must allow (occupancy/spill trade-off, picked by the
-// autotuner).
-template <int NPQ, int MINB>
-__global__ void __launch_bounds__(128, MINB) ints_n32_kernel(PowfsDev P, const WfsDev* __restrict__ wfs, int nw, int nitem) {
-	__shared__ float2 tiles[4][32 * LD];
-	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	const int item = blockIdx.x * 4 + warp;
-	if (item >= nitem) return;
-	const int isa = item / nw;
-	const WfsDev W = wfs[item % nw];
-	float2* tile = tiles[warp];
-	const size_t off_opd = (size_t)isa * 256;
-	float2 F[32];
-	// the subaperture's ETF (8 KB, read after the first two transforms) into L2 now
-	if (P.etfT1) {
-		prefetch_l2(P.etfT1 + (size_t)isa * 1024 + 32 * lane);
-		prefetch_l2(P.etfT1 + (size_t)isa * 1024 + 32 * lane + 16);
-	}
-	field_fft_n32(W.opd + off_opd, W.amp + off_opd, P.twoinvwvl, tile, lane, F);
+// (c)-(e) of one subaperture image after its field transform: F from
+// field_fft_n32 (lane = kx holds F(kx, ky=0..31)); tile is the warp's scratch.
+template <int NPQ>
+__device__ __forceinline__ void ints_n32_tail(const PowfsDev& P, const WfsDev& W, int isa, int lane, float2* tile,
+	float2 (&F)[32]) {
 	psf_to_otf_n32(F, 1.f, tile, lane);
 	// lane = fy holds OTF(fx, fy). Uplink OTF (conjugated) and ETF / nominal.
 	if (W.lotfT) {
@@ -627,6 +644,29 @@ __global__ void __launch_bounds__(128, MINB) ints_n32_kernel(PowfsDev P, const W
 		grad_from_pixels<NPQ>(pix, npix, P.pixpsax, P.pixpsay, P, W.mtche + (size_t)isa * 2 * npix,
 			W.i0sum, isa, lane, W.grad, P.nsa);
 	}
+}
+
+// NPQ: pixel slots per lane, ceil(npix/32).  MINB: resident blocks per SM the
+// register allocation must allow (occupancy/spill trade-off, picked by the
+// autotuner).
+template <int NPQ, int MINB>
+__global__ void __launch_bounds__(128, MINB) ints_n32_kernel(PowfsDev P, const WfsDev* __restrict__ wfs, int nw, int nitem) {
+	__shared__ float2 tiles[4][32 * LD];
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int item = blockIdx.x * 4 + warp;
+	if (item >= nitem) return;
+	const int isa = item / nw;
+	const WfsDev W = wfs[item % nw];
+	float2* tile = tiles[warp];
+	const size_t off_opd = (size_t)isa * 256;
+	float2 F[32];
+	// the subaperture's ETF (8 KB, read after the first two transforms) into L2 now
+	if (P.etfT1) {
+		prefetch_l2(P.etfT1 + (size_t)isa * 1024 + 32 * lane);
+		prefetch_l2(P.etfT1 + (size_t)isa * 1024 + 32 * lane + 16);
+	}
+	field_fft_n32(W.opd + off_opd, W.amp + off_opd, P.twoinvwvl, tile, lane, F);
+	ints_n32_tail<NPQ>(P, W, isa, lane, tile, F);
 }
 
 // (d)-(e) after an imaging kernel that stored noise-free intensities (the
