@@ -113,8 +113,13 @@ __device__ __forceinline__ void evl_dft_small(float2 (&v)[R]) {
 	}
 }
 
-template <int N, int R, int ROWS>
-__device__ __forceinline__ void evl_stockham_pass(float2* buf, int Ns, const float2* __restrict__ tw) {
+// FIRST: the pass reads only row elements in [lo, hi) and takes the others
+// as zero, so the rows need no zero fill.  LAST: the pass hands each output
+// (row, index, value) to epi instead of storing it, so a crop reads no
+// shared memory afterwards.
+template <int N, int R, int ROWS, bool FIRST, bool LAST, class Epi>
+__device__ __forceinline__ void evl_stockham_pass(float2* buf, int Ns, const float2* __restrict__ tw, int lo, int hi,
+	Epi& epi) {
 	constexpr int NG = N / R;  // groups per row
 	constexpr int NGT = ROWS * NG;
 	constexpr int GPT = (NGT + EVL_THREADS - 1) / EVL_THREADS;
@@ -127,7 +132,13 @@ __device__ __forceinline__ void evl_stockham_pass(float2* buf, int Ns, const flo
 			const float2* x = buf + row * evl_row_len<N>();
 			const int jm = j % Ns, tstep = jm * (N / (Ns * R));
 #pragma unroll
-			for (int k = 0; k < R; k++) v[g][k] = x[evl_pad(j + k * NG)];
+			for (int k = 0; k < R; k++) {
+				const int xi = j + k * NG;
+				if (FIRST)
+					v[g][k] = (xi >= lo && xi < hi) ? x[evl_pad(xi)] : make_float2(0.f, 0.f);
+				else
+					v[g][k] = x[evl_pad(xi)];
+			}
 			if (jm) {
 				// w^k for k < R from w, w^2 and w^4 of the table (two roundings at most)
 				float2 w[R];
@@ -148,42 +159,72 @@ __device__ __forceinline__ void evl_stockham_pass(float2* buf, int Ns, const flo
 			evl_dft_small<R>(v[g]);
 		}
 	}
-	__syncthreads();
+	if constexpr (LAST) {
 #pragma unroll
-	for (int g = 0; g < GPT; g++) {
-		const int gi = threadIdx.x + g * EVL_THREADS;
-		if (gi < NGT) {
-			const int row = gi / NG, j = gi - row * NG;
-			float2* y = buf + row * evl_row_len<N>();
-			const int jm = j % Ns, base = (j / Ns) * Ns * R + jm;
+		for (int g = 0; g < GPT; g++) {
+			const int gi = threadIdx.x + g * EVL_THREADS;
+			if (gi < NGT) {
+				const int row = gi / NG, j = gi - row * NG;
+				const int jm = j % Ns, base = (j / Ns) * Ns * R + jm;
 #pragma unroll
-			for (int k = 0; k < R; k++) y[evl_pad(base + k * Ns)] = v[g][k];
+				for (int k = 0; k < R; k++) epi(row, base + k * Ns, v[g][k]);
+			}
 		}
+	} else {
+		__syncthreads();
+#pragma unroll
+		for (int g = 0; g < GPT; g++) {
+			const int gi = threadIdx.x + g * EVL_THREADS;
+			if (gi < NGT) {
+				const int row = gi / NG, j = gi - row * NG;
+				float2* y = buf + row * evl_row_len<N>();
+				const int jm = j % Ns, base = (j / Ns) * Ns * R + jm;
+#pragma unroll
+				for (int k = 0; k < R; k++) y[evl_pad(base + k * Ns)] = v[g][k];
+			}
+		}
+		__syncthreads();
 	}
-	__syncthreads();
 }
 
-template <int N, int ROWS>
-__device__ __forceinline__ void evl_fft_smem(float2* buf, const float2* __restrict__ tw) {
-	constexpr int L = (N >= 4096) ? 12 : (N >= 2048) ? 11 : (N >= 1024) ? 10 : (N >= 512) ? 9 : (N >= 256) ? 8
-		: (N >= 128) ? 7 : 6;
-	static_assert((1 << L) == N, "N must be a power of two in [64, 4096]");
-	int Ns = 1;
-#pragma unroll
-	for (int p = 0; p < L / 3; p++) {
-		evl_stockham_pass<N, 8, ROWS>(buf, Ns, tw);
-		Ns *= 8;
-	}
-	if constexpr (L % 3 == 2) evl_stockham_pass<N, 4, ROWS>(buf, Ns, tw);
-	if constexpr (L % 3 == 1) evl_stockham_pass<N, 2, ROWS>(buf, Ns, tw);
+template <int N>
+__host__ __device__ constexpr int evl_log2() {
+	return (N >= 4096) ? 12 : (N >= 2048) ? 11 : (N >= 1024) ? 10 : (N >= 512) ? 9 : (N >= 256) ? 8 : (N >= 128) ? 7 : 6;
+}
+
+// Pass P of the transform and the passes after it: log2(N)/3 radix-8
+// passes, then one radix-4 or radix-2 pass when log2 N is not a multiple of 3.
+template <int N, int ROWS, int P, class Epi>
+__device__ __forceinline__ void evl_fft_passes(float2* buf, int Ns, const float2* __restrict__ tw, int lo, int hi,
+	Epi& epi) {
+	constexpr int L = evl_log2<N>();
+	constexpr int NP8 = L / 3;
+	constexpr int NPASS = NP8 + (L % 3 ? 1 : 0);
+	constexpr int RP = P < NP8 ? 8 : (L % 3 == 2 ? 4 : 2);
+	evl_stockham_pass<N, RP, ROWS, P == 0, P == NPASS - 1>(buf, Ns, tw, lo, hi, epi);
+	if constexpr (P + 1 < NPASS) evl_fft_passes<N, ROWS, P + 1>(buf, Ns * RP, tw, lo, hi, epi);
+}
+
+// Forward transform of ROWS rows whose elements outside [lo, hi) are zero
+// (not read); output (row, k, X[k]) goes to epi.
+template <int N, int ROWS, class Epi>
+__device__ __forceinline__ void evl_fft_smem(float2* buf, const float2* __restrict__ tw, int lo, int hi, Epi& epi) {
+	static_assert((1 << evl_log2<N>()) == N, "N must be a power of two in [64, 4096]");
+	evl_fft_passes<N, ROWS, 0>(buf, 1, tw, lo, hi, epi);
+}
+
+// Column of the corner-to-centre crop that frequency k lands in (the crop
+// keeps kx = ax < h ? N - h + ax : ax - h), or -1.
+template <int N>
+__device__ __forceinline__ int evl_crop_index(int k, int h) {
+	return k < h ? k + h : (k >= N - h ? k - (N - h) : -1);
 }
 
 // (3) PSF, first dimension (locfft_psf, lib/locfft.c:150-159): R raster
 // rows per block (512 threads), each embedded at column X + offx of an N-point row as
 // amp * exp(i k (OPD - PTT)), transformed along x; the 2h columns the crop
 // keeps are written to T (per direction, crop column ax major, row Y
-// fastest).  Crop column ax takes frequency kx = ax < h ? N - h + ax : ax - h
-// (the corner-to-centre copy).  Grid (ceil(nY / R), nevl).
+// fastest) straight from the last pass.  Grid (ceil(nY / R), nevl).
 template <int N, int R>
 __global__ void __launch_bounds__(EVL_THREADS) evl_psf_rows_kernel(EvlRaster Ra, const float* __restrict__ opd,
 	const double* __restrict__ coeff, int pttr, float kwvl, int offx, int h, const float2* __restrict__ tw,
@@ -192,61 +233,80 @@ __global__ void __launch_bounds__(EVL_THREADS) evl_psf_rows_kernel(EvlRaster Ra,
 	const int e = blockIdx.y, Y0 = blockIdx.x * R;
 	const float* o = opd + (size_t)e * Ra.nslot * 256;
 	constexpr int LN = evl_row_len<N>();
-	for (int i = threadIdx.x; i < R * LN; i += blockDim.x) s_row[i] = make_float2(0.f, 0.f);
-	__syncthreads();
 	double c0 = 0, c1 = 0, c2 = 0;
 	if (pttr) {
 		c0 = coeff[e * 3];
 		c1 = coeff[e * 3 + 1];
 		c2 = coeff[e * 3 + 2];
 	}
-	for (int idx = threadIdx.x; idx < R * Ra.nX; idx += blockDim.x) {
-		const int r = idx / Ra.nX, X = idx - r * Ra.nX, Y = Y0 + r;
-		if (Y >= Ra.nY) continue;
-		const int slot = Ra.tile_slot[(Y >> 4) * Ra.ntx + (X >> 4)];
-		if (slot < 0) continue;
-		const int p = slot * 256 + (Y & 15) * 16 + (X & 15);
-		const float a = Ra.amp[p];
-		if (a == 0.f) continue;
-		float v = o[p];
-		if (pttr) v = (float)((double)v - (c0 + c1 * (Ra.ox + X * Ra.dx) + c2 * (Ra.oy + Y * Ra.dx)));
-		float sn, cs;
-		sincosf(kwvl * v, &sn, &cs);
-		s_row[r * LN + evl_pad(X + offx)] = make_float2(a * cs, a * sn);
+	// the field on columns [offx, offx + nX) of every row (zero where the
+	// aperture has no point); four elements per thread in flight
+	const int nX = Ra.nX, total = R * nX;
+	constexpr int U = 4;
+	for (int b0 = threadIdx.x; b0 < total; b0 += U * EVL_THREADS) {
+		int pp[U];
+#pragma unroll
+		for (int u = 0; u < U; u++) {
+			const int idx = b0 + u * EVL_THREADS;
+			pp[u] = -1;
+			if (idx < total) {
+				const int r = idx / nX, X = idx - r * nX, Y = Y0 + r;
+				if (Y < Ra.nY) {
+					const int slot = Ra.tile_slot[(Y >> 4) * Ra.ntx + (X >> 4)];
+					if (slot >= 0) pp[u] = slot * 256 + (Y & 15) * 16 + (X & 15);
+				}
+			}
+		}
+		float av[U], ov[U];
+#pragma unroll
+		for (int u = 0; u < U; u++) {
+			av[u] = pp[u] >= 0 ? Ra.amp[pp[u]] : 0.f;
+			ov[u] = pp[u] >= 0 ? o[pp[u]] : 0.f;
+		}
+#pragma unroll
+		for (int u = 0; u < U; u++) {
+			const int idx = b0 + u * EVL_THREADS;
+			if (idx < total) {
+				const int r = idx / nX, X = idx - r * nX, Y = Y0 + r;
+				float2 val = make_float2(0.f, 0.f);
+				if (av[u] != 0.f) {
+					float v = ov[u];
+					if (pttr) v = (float)((double)v - (c0 + c1 * (Ra.ox + X * Ra.dx) + c2 * (Ra.oy + Y * Ra.dx)));
+					float sn, cs;
+					sincosf(kwvl * v, &sn, &cs);
+					val = make_float2(av[u] * cs, av[u] * sn);
+				}
+				s_row[r * LN + evl_pad(X + offx)] = val;
+			}
+		}
 	}
 	__syncthreads();
-	evl_fft_smem<N, R>(s_row, tw);
-	const int ncol = 2 * h;
-	float2* Te = T + (size_t)e * ncol * nYp;
-	for (int idx = threadIdx.x; idx < R * ncol; idx += blockDim.x) {
-		const int ax = idx / R, r = idx - ax * R, Y = Y0 + r;
-		if (Y >= Ra.nY) continue;
-		const int kx = ax < h ? N - h + ax : ax - h;
-		Te[(size_t)ax * nYp + Y] = s_row[r * LN + evl_pad(kx)];
-	}
+	float2* Te = T + (size_t)e * (2 * h) * nYp;
+	auto crop = [&](int r, int kx, float2 v) {
+		const int ax = evl_crop_index<N>(kx, h), Y = Y0 + r;
+		if (ax >= 0 && Y < Ra.nY) Te[(size_t)ax * nYp + Y] = v;
+	};
+	evl_fft_smem<N, R>(s_row, tw, offx, offx + nX, crop);
 }
 
 // (4) PSF, second dimension: one block per kept column ax and direction;
 // rows Y of T placed at Y + offy of an N-point column (zero elsewhere),
 // transformed along y, |.|^2 of the 2h kept frequencies added to the sum
-// psf (per direction, ax major, ay fastest).
+// psf (per direction, ax major, ay fastest) straight from the last pass.
 template <int N>
 __global__ void __launch_bounds__(EVL_THREADS) evl_psf_cols_kernel(const float2* __restrict__ T, int nY, int nYp, int offy,
 	int h, const float2* __restrict__ tw, float* __restrict__ psf) {
 	extern __shared__ float2 s_col[];
 	const int ax = blockIdx.x, e = blockIdx.y, ncol = 2 * h;
 	const float2* Tc = T + ((size_t)e * ncol + ax) * nYp;
-	for (int i = threadIdx.x; i < evl_row_len<N>(); i += blockDim.x) s_col[i] = make_float2(0.f, 0.f);
-	__syncthreads();
 	for (int Y = threadIdx.x; Y < nY; Y += blockDim.x) s_col[evl_pad(Y + offy)] = Tc[Y];
 	__syncthreads();
-	evl_fft_smem<N, 1>(s_col, tw);
 	float* P = psf + ((size_t)e * ncol + ax) * ncol;
-	for (int ay = threadIdx.x; ay < ncol; ay += blockDim.x) {
-		const int ky = ay < h ? N - h + ay : ay - h;
-		const float2 v = s_col[evl_pad(ky)];
-		P[ay] += v.x * v.x + v.y * v.y;
-	}
+	auto acc = [&](int, int ky, float2 v) {
+		const int ay = evl_crop_index<N>(ky, h);
+		if (ay >= 0) P[ay] += v.x * v.x + v.y * v.y;
+	};
+	evl_fft_smem<N, 1>(s_col, tw, offy, offy + nY, acc);
 }
 
 // (5) OPD of one direction in aperture order.
