@@ -117,9 +117,8 @@ __device__ __forceinline__ void evl_dft_small(float2 (&v)[R]) {
 // as zero, so the rows need no zero fill.  LAST: the pass hands each output
 // (row, index, value) to epi instead of storing it, so a crop reads no
 // shared memory afterwards.
-template <int N, int R, int ROWS, bool FIRST, bool LAST, class Epi>
-__device__ __forceinline__ void evl_stockham_pass(float2* buf, int Ns, const float2* __restrict__ tw, int lo, int hi,
-	Epi& epi) {
+template <int N, int R, int ROWS, int Ns, bool FIRST, bool LAST, class Epi>
+__device__ __forceinline__ void evl_stockham_pass(float2* buf, const float2* __restrict__ tw, int lo, int hi, Epi& epi) {
 	constexpr int NG = N / R;  // groups per row
 	constexpr int NGT = ROWS * NG;
 	constexpr int GPT = (NGT + EVL_THREADS - 1) / EVL_THREADS;
@@ -194,15 +193,14 @@ __host__ __device__ constexpr int evl_log2() {
 
 // Pass P of the transform and the passes after it: log2(N)/3 radix-8
 // passes, then one radix-4 or radix-2 pass when log2 N is not a multiple of 3.
-template <int N, int ROWS, int P, class Epi>
-__device__ __forceinline__ void evl_fft_passes(float2* buf, int Ns, const float2* __restrict__ tw, int lo, int hi,
-	Epi& epi) {
+template <int N, int ROWS, int P, int Ns, class Epi>
+__device__ __forceinline__ void evl_fft_passes(float2* buf, const float2* __restrict__ tw, int lo, int hi, Epi& epi) {
 	constexpr int L = evl_log2<N>();
 	constexpr int NP8 = L / 3;
 	constexpr int NPASS = NP8 + (L % 3 ? 1 : 0);
 	constexpr int RP = P < NP8 ? 8 : (L % 3 == 2 ? 4 : 2);
-	evl_stockham_pass<N, RP, ROWS, P == 0, P == NPASS - 1>(buf, Ns, tw, lo, hi, epi);
-	if constexpr (P + 1 < NPASS) evl_fft_passes<N, ROWS, P + 1>(buf, Ns * RP, tw, lo, hi, epi);
+	evl_stockham_pass<N, RP, ROWS, Ns, P == 0, P == NPASS - 1>(buf, tw, lo, hi, epi);
+	if constexpr (P + 1 < NPASS) evl_fft_passes<N, ROWS, P + 1, Ns * RP>(buf, tw, lo, hi, epi);
 }
 
 // Forward transform of ROWS rows whose elements outside [lo, hi) are zero
@@ -210,7 +208,7 @@ __device__ __forceinline__ void evl_fft_passes(float2* buf, int Ns, const float2
 template <int N, int ROWS, class Epi>
 __device__ __forceinline__ void evl_fft_smem(float2* buf, const float2* __restrict__ tw, int lo, int hi, Epi& epi) {
 	static_assert((1 << evl_log2<N>()) == N, "N must be a power of two in [64, 4096]");
-	evl_fft_passes<N, ROWS, 0>(buf, 1, tw, lo, hi, epi);
+	evl_fft_passes<N, ROWS, 0, 1>(buf, tw, lo, hi, epi);
 }
 
 // Column of the corner-to-centre crop that frequency k lands in (the crop
@@ -222,12 +220,12 @@ __device__ __forceinline__ int evl_crop_index(int k, int h) {
 
 // (3) PSF, first dimension (locfft_psf, lib/locfft.c:150-159): R raster
 // rows per block (512 threads), each embedded at column X + offx of an N-point row as
-// amp * exp(i k (OPD - PTT)), transformed along x; the 2h columns the crop
+// amp * exp(i 2 pi (OPD - PTT) / wvl), transformed along x; the 2h columns the crop
 // keeps are written to T (per direction, crop column ax major, row Y
 // fastest) straight from the last pass.  Grid (ceil(nY / R), nevl).
 template <int N, int R>
-__global__ void __launch_bounds__(EVL_THREADS) evl_psf_rows_kernel(EvlRaster Ra, const float* __restrict__ opd,
-	const double* __restrict__ coeff, int pttr, float kwvl, int offx, int h, const float2* __restrict__ tw,
+__global__ void __launch_bounds__(EVL_THREADS, 2) evl_psf_rows_kernel(EvlRaster Ra, const float* __restrict__ opd,
+	const double* __restrict__ coeff, int pttr, float twoinvwvl, int offx, int h, const float2* __restrict__ tw,
 	float2* __restrict__ T, int nYp) {
 	extern __shared__ float2 s_row[];
 	const int e = blockIdx.y, Y0 = blockIdx.x * R;
@@ -240,43 +238,50 @@ __global__ void __launch_bounds__(EVL_THREADS) evl_psf_rows_kernel(EvlRaster Ra,
 		c2 = coeff[e * 3 + 2];
 	}
 	// the field on columns [offx, offx + nX) of every row (zero where the
-	// aperture has no point); four elements per thread in flight
-	const int nX = Ra.nX, total = R * nX;
+	// aperture has no point); U elements of a row per thread in flight
+	const int nX = Ra.nX;
 	constexpr int U = 4;
-	for (int b0 = threadIdx.x; b0 < total; b0 += U * EVL_THREADS) {
-		int pp[U];
+#pragma unroll 1
+	for (int r = 0; r < R; r++) {
+		const int Y = Y0 + r;
+		float2* srow = s_row + r * LN;
+		if (Y >= Ra.nY) {
+			for (int X = threadIdx.x; X < nX; X += EVL_THREADS) srow[evl_pad(X + offx)] = make_float2(0.f, 0.f);
+			continue;
+		}
+		const int* trow = Ra.tile_slot + (Y >> 4) * Ra.ntx;
+		const int py = (Y & 15) * 16;
+		for (int X0 = threadIdx.x; X0 < nX; X0 += U * EVL_THREADS) {
+			int pp[U];
 #pragma unroll
-		for (int u = 0; u < U; u++) {
-			const int idx = b0 + u * EVL_THREADS;
-			pp[u] = -1;
-			if (idx < total) {
-				const int r = idx / nX, X = idx - r * nX, Y = Y0 + r;
-				if (Y < Ra.nY) {
-					const int slot = Ra.tile_slot[(Y >> 4) * Ra.ntx + (X >> 4)];
-					if (slot >= 0) pp[u] = slot * 256 + (Y & 15) * 16 + (X & 15);
+			for (int u = 0; u < U; u++) {
+				const int X = X0 + u * EVL_THREADS;
+				pp[u] = -1;
+				if (X < nX) {
+					const int slot = trow[X >> 4];
+					if (slot >= 0) pp[u] = slot * 256 + py + (X & 15);
 				}
 			}
-		}
-		float av[U], ov[U];
+			float av[U], ov[U];
 #pragma unroll
-		for (int u = 0; u < U; u++) {
-			av[u] = pp[u] >= 0 ? Ra.amp[pp[u]] : 0.f;
-			ov[u] = pp[u] >= 0 ? o[pp[u]] : 0.f;
-		}
+			for (int u = 0; u < U; u++) {
+				av[u] = pp[u] >= 0 ? Ra.amp[pp[u]] : 0.f;
+				ov[u] = pp[u] >= 0 ? o[pp[u]] : 0.f;
+			}
 #pragma unroll
-		for (int u = 0; u < U; u++) {
-			const int idx = b0 + u * EVL_THREADS;
-			if (idx < total) {
-				const int r = idx / nX, X = idx - r * nX, Y = Y0 + r;
-				float2 val = make_float2(0.f, 0.f);
-				if (av[u] != 0.f) {
-					float v = ov[u];
-					if (pttr) v = (float)((double)v - (c0 + c1 * (Ra.ox + X * Ra.dx) + c2 * (Ra.oy + Y * Ra.dx)));
-					float sn, cs;
-					sincosf(kwvl * v, &sn, &cs);
-					val = make_float2(av[u] * cs, av[u] * sn);
+			for (int u = 0; u < U; u++) {
+				const int X = X0 + u * EVL_THREADS;
+				if (X < nX) {
+					float2 val = make_float2(0.f, 0.f);
+					if (av[u] != 0.f) {
+						float v = ov[u];
+						if (pttr) v = (float)((double)v - (c0 + c1 * (Ra.ox + X * Ra.dx) + c2 * (Ra.oy + Y * Ra.dx)));
+						float sn, cs;
+						sincospif(twoinvwvl * v, &sn, &cs);  // exp(i 2 pi v / wvl)
+						val = make_float2(av[u] * cs, av[u] * sn);
+					}
+					srow[evl_pad(X + offx)] = val;
 				}
-				s_row[r * LN + evl_pad(X + offx)] = val;
 			}
 		}
 	}
@@ -299,7 +304,8 @@ __global__ void __launch_bounds__(EVL_THREADS) evl_psf_cols_kernel(const float2*
 	extern __shared__ float2 s_col[];
 	const int ax = blockIdx.x, e = blockIdx.y, ncol = 2 * h;
 	const float2* Tc = T + ((size_t)e * ncol + ax) * nYp;
-	for (int Y = threadIdx.x; Y < nY; Y += blockDim.x) s_col[evl_pad(Y + offy)] = Tc[Y];
+#pragma unroll 4
+	for (int Y = threadIdx.x; Y < nY; Y += EVL_THREADS) s_col[evl_pad(Y + offy)] = __ldg(Tc + Y);
 	__syncthreads();
 	float* P = psf + ((size_t)e * ncol + ax) * ncol;
 	auto acc = [&](int, int ky, float2 v) {

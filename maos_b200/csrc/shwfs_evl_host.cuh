@@ -245,9 +245,9 @@ static int evl_launch_psf(shwfs_ctx* ctx, EvlState& E, EvlPsf& P, int nevl) {
 	if (smem_r > 48 * 1024)
 		CK(cudaFuncSetAttribute(evl_psf_rows_kernel<N, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_r));
 	const EvlRaster Ra = evl_raster(E);
-	const float kwvl = (float)(2.0 * M_PI / P.wvl);
+	const float twoinvwvl = (float)(2.0 / P.wvl);
 	evl_psf_rows_kernel<N, R><<<dim3((E.nY + R - 1) / R, nevl), EVL_THREADS, smem_r, ctx->stream>>>(
-		Ra, E.opd.p, E.coeff.p, E.pttr, kwvl, P.offx, P.h, P.tw.p, E.T.p, E.nY);
+		Ra, E.opd.p, E.coeff.p, E.pttr, twoinvwvl, P.offx, P.h, P.tw.p, E.T.p, E.nY);
 	CK(cudaGetLastError());
 	evl_psf_cols_kernel<N><<<dim3(2 * P.h, nevl), EVL_THREADS, smem_c, ctx->stream>>>(E.T.p, E.nY, E.nY, P.offy, P.h, P.tw.p,
 		P.psf.p);
