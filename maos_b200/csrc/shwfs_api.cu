@@ -679,6 +679,8 @@ static int launch_geom_wfs(shwfs_ctx* ctx, GeomParams& gp) {
 	const int nopd = gp.nentry ? gp.e[0].nopd : 0;
 	for (int i = 0; i < gp.nentry; i++) {
 		if (gp.e[i].nopd != nopd) return fail(ctx, SHWFS_EINVAL, "ray trace: pupils of one launch need the same sampling");
+		if (gp.interleave && gp.e[i].nsa != gp.e[0].nsa)
+			return fail(ctx, SHWFS_EINVAL, "ray trace: interleaved pupils need the same number of subapertures");
 		gp.e[i].item0 = nitem;
 		nitem += gp.e[i].nsa;
 	}

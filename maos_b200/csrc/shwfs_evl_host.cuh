@@ -284,6 +284,7 @@ int shwfs_evl_queue(shwfs_ctx* ctx, int isim, int do_psf) {
 					 E.nslot, 16, E.dx, E.opd.p + per * e)))
 				return r;
 		}
+		gp.interleave = 1;  // the directions of a tile together: the screens' rows are fetched once for all
 		if ((r = launch_geom(ctx, gp))) return r;
 	}
 	// (b) WFE sums (calc_ptt, cuda/sim/perfevl.cu:46-102)

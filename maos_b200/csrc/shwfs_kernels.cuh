@@ -155,6 +155,7 @@ struct GeomEntry {
 };
 struct GeomParams {
 	int nentry, nlayer;
+	int interleave;  // items are (subaperture, entry) pairs, entry fastest (all entries have the same nsa)
 	const float* screen[SHWFS_MAX_LAYERS];
 	int nx[SHWFS_MAX_LAYERS], ny[SHWFS_MAX_LAYERS];
 	float alpha[SHWFS_MAX_LAYERS];
@@ -301,8 +302,9 @@ __device__ __forceinline__ void psf_to_otf_n32(float2 (&F)[32], float scale, flo
 // the LGS uplink OTF of the 32-point path (llt_uplink_kernel): an LLT block
 // keeps its OPD in shared memory and its first warp turns it into
 // lotf = FFT(|FFT(embed(lltamp*exp(i*2*pi*opd/wvl)))|^2 / nlwvf^2), stored
-// transposed (fy fastest).  Block b of geom_kernel belongs to the entry whose
-// [item0, item0+nsa) holds its subaperture.
+// transposed (fy fastest).  Item b of geom_kernel belongs to the entry whose
+// [item0, item0+nsa) holds it, or, when the launch is interleaved, to entry
+// b % nentry at subaperture b / nentry.
 // ---------------------------------------------------------------------------
 // ---- ray trace (a) ----
 // The bilinear coordinates of point (ix, iy) in layer l are separable: the
@@ -360,10 +362,15 @@ __global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomP
 	extern __shared__ int4 s_tab[];
 	const int item = blockIdx.x / bps, part = blockIdx.x - item * bps;
 	if (item >= nitem) return;
-	int ie = 0;
-	while (ie + 1 < P.nentry && item >= P.e[ie + 1].item0) ie++;
+	int ie = 0, isa;
+	if (P.interleave) {  // the entries' footprints of one subaperture run together and share L2
+		ie = item % P.nentry;
+		isa = item / P.nentry;
+	} else {
+		while (ie + 1 < P.nentry && item >= P.e[ie + 1].item0) ie++;
+		isa = item - P.e[ie].item0;
+	}
 	const GeomEntry& E = P.e[ie];
-	const int isa = item - E.item0;
 	const int tid = threadIdx.x, nl = P.nlayer;
 	for (int k = tid; k < nl * 2 * nopd; k += blockDim.x) {
 		const int l = k / (2 * nopd), r = k - l * 2 * nopd;
