@@ -281,7 +281,7 @@ def run_b200(args, cfg):
     st = {k: dict(ms_per_launch=(ms / n if n else 0.0), launches_per_step=n / nprof, ms_per_step=ms / nprof)
           for k, (ms, n) in stages.items()}
     ints_ms = st["ints"]["ms_per_launch"]
-    ray_ms = st["raytrace"]["ms_per_launch"]
+    ray_ms = st["raytrace"]["ms_per_step"]  # the WFS pupils, plus any LLT pupils traced in a second launch
     ints_gbs = ints_bytes / (ints_ms * 1e-3) / 1e9 if ints_ms else 0.0
     ray_gbs = ray_bytes / (ray_ms * 1e-3) / 1e9 if ray_ms else 0.0
     flops = fft_flops_per_image(wl.setup.notf) * units_per_step
@@ -663,7 +663,7 @@ def run_science(args, scfg):
     src_note = f"{src} (MEASURED_PEAKS.json)" if src == "measured" else "fallback"
     nlayer = len(scfg["atm"]["ht"])
     ray_bytes = nevl * npts_traced * (nlayer * 4 + 4)
-    ray_ms = st["raytrace"]["ms_per_launch"]
+    ray_ms = st["raytrace"]["ms_per_step"]
     ray_gbs = ray_bytes / (ray_ms * 1e-3) / 1e9 if ray_ms else 0.0
     psf_ms = st["ints"]["ms_per_step"]
     nX = int(round(scfg["D"] / scfg["dx"])) + 3

@@ -598,7 +598,7 @@ int shwfs_atm_set(shwfs_ctx* ctx, int nlayer, const shwfs_layer_desc* layers, co
 
 // ---- frame machinery ----
 
-static int launch_geom_wfs(shwfs_ctx* ctx, GeomParams& gp);
+static int launch_geom_wfs(shwfs_ctx* ctx, GeomParams& gp, bool split = true);
 
 // Appends one pupil to a batched ray-trace launch: per-layer geometry of
 // prop_range (lib/accphi.c:223-244) and prop_grid_pts
@@ -674,7 +674,46 @@ static int launch_geom(shwfs_ctx* ctx, GeomParams& all) {
 }
 
 
-static int launch_geom_wfs(shwfs_ctx* ctx, GeomParams& gp) {
+static int l2_bytes(shwfs_ctx* ctx) {
+	static int l2[64] = {0};
+	if (ctx->device < 64 && l2[ctx->device]) return l2[ctx->device];
+	int v = 0;
+	cudaDeviceGetAttribute(&v, cudaDevAttrL2CacheSize, ctx->device);
+	if (v <= 0) v = 126 << 20;
+	if (ctx->device < 64) l2[ctx->device] = v;
+	return v;
+}
+
+// split: when the launch's screens exceed L2, the pupils of the largest size
+// are traced interleaved (each screen row their footprints share is fetched
+// from DRAM once while in L2) and any other pupils in a second launch.  With
+// the screens in L2, the order as listed keeps each block's neighbours on the
+// same footprint, which measured faster.
+static int launch_geom_wfs(shwfs_ctx* ctx, GeomParams& gp, bool split) {
+	if (split && !gp.interleave && gp.nentry >= 2) {
+		double screen = 0;
+		for (int l = 0; l < gp.nlayer; l++) screen += 4.0 * gp.nx[l] * gp.ny[l];
+		int nmax = 0, nbig = 0;
+		for (int i = 0; i < gp.nentry; i++) nmax = std::max(nmax, gp.e[i].nsa);
+		for (int i = 0; i < gp.nentry; i++) nbig += gp.e[i].nsa == nmax;
+		if (screen > l2_bytes(ctx) && nbig >= 2) {
+			if (nbig == gp.nentry) {
+				gp.interleave = 1;
+			} else {
+				GeomParams big, rest;
+				memcpy(&big, &gp, sizeof(GeomParams));
+				memcpy(&rest, &gp, sizeof(GeomParams));
+				big.nentry = rest.nentry = 0;
+				for (int i = 0; i < gp.nentry; i++) {
+					if (gp.e[i].nsa == nmax) big.e[big.nentry++] = gp.e[i];
+					else rest.e[rest.nentry++] = gp.e[i];
+				}
+				big.interleave = 1;
+				int r = launch_geom_wfs(ctx, big, false);
+				return r ? r : launch_geom_wfs(ctx, rest, false);
+			}
+		}
+	}
 	int nitem = 0;
 	const int nopd = gp.nentry ? gp.e[0].nopd : 0;
 	for (int i = 0; i < gp.nentry; i++) {
