@@ -24,23 +24,33 @@ struct EvlRaster {
 
 // (1) loc_calc_ptt_stride (math/loc.c:653-704) sums over the aperture, per
 // direction: s = {sum a o^2, sum a o, sum a o x, sum a o y}, FP64; grid
-// (blocks, nevl), 256 threads; sums zeroed before the launch.
+// (ceil(nslot / EVL_SUM_TILES), nevl), 256 threads (one point of a tile
+// each), EVL_SUM_TILES tiles per block with all their loads in flight; sums
+// zeroed before the launch.
+constexpr int EVL_SUM_TILES = 8;
 __global__ void __launch_bounds__(256) evl_sums_kernel(EvlRaster R, const float* __restrict__ opd, double* sums) {
-	const int e = blockIdx.y;
-	const long n = (long)R.nslot * 256;
-	const float* o = opd + (size_t)e * n;
+	const int e = blockIdx.y, p = threadIdx.x;
+	const float* o = opd + (size_t)e * R.nslot * 256;
+	const int slot0 = blockIdx.x * EVL_SUM_TILES;
+	float av[EVL_SUM_TILES], ov[EVL_SUM_TILES];
+#pragma unroll
+	for (int k = 0; k < EVL_SUM_TILES; k++) {
+		const int slot = slot0 + k;
+		const size_t i = (size_t)slot * 256 + p;
+		av[k] = slot < R.nslot ? __ldg(R.amp + i) : 0.f;
+		ov[k] = slot < R.nslot ? __ldg(o + i) : 0.f;
+	}
 	double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-		const float a = R.amp[i];
-		if (a == 0.f) continue;
-		const int slot = (int)(i >> 8), p = (int)(i & 255);
-		const int tile = R.slot_tile[slot];
+#pragma unroll
+	for (int k = 0; k < EVL_SUM_TILES; k++) {
+		if (av[k] == 0.f) continue;
+		const int tile = R.slot_tile[slot0 + k];
 		const int X = (tile % R.ntx) * 16 + (p & 15), Y = (tile / R.ntx) * 16 + (p >> 4);
-		const double v = o[i], av = (double)a * v;
-		s0 += av * v;
-		s1 += av;
-		s2 += av * (R.ox + X * R.dx);
-		s3 += av * (R.oy + Y * R.dx);
+		const double v = ov[k], a = (double)av[k] * v;
+		s0 += a * v;
+		s1 += a;
+		s2 += a * (R.ox + X * R.dx);
+		s3 += a * (R.oy + Y * R.dx);
 	}
 	__shared__ double red[4][8];
 #pragma unroll

@@ -291,8 +291,8 @@ int shwfs_evl_queue(shwfs_ctx* ctx, int isim, int do_psf) {
 	CK(cudaMemsetAsync(E.sums.p, 0, sizeof(double) * 4 * nevl, ctx->stream));
 	{
 		StageMark m(ctx, SHWFS_STAGE_POST);
-		const long nblk = std::min((long)((per + 255) / 256), (long)tc_sm_count(ctx) * 4);
-		evl_sums_kernel<<<dim3((unsigned)nblk, nevl), 256, 0, ctx->stream>>>(evl_raster(E), E.opd.p, E.sums.p);
+		const unsigned nblk = (unsigned)((E.nslot + EVL_SUM_TILES - 1) / EVL_SUM_TILES);
+		evl_sums_kernel<<<dim3(nblk, nevl), 256, 0, ctx->stream>>>(evl_raster(E), E.opd.p, E.sums.p);
 		CK(cudaGetLastError());
 	}
 	// (c) PSF sums (psfcomp_r, cuda/sim/perfevl.cu:255-300)
