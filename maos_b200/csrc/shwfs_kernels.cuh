@@ -372,15 +372,27 @@ __global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomP
 	}
 	const GeomEntry& E = P.e[ie];
 	const int tid = threadIdx.x, nl = P.nlayer;
+	// the footprint origin of each (layer, axis) once, in FP64; then the
+	// entries of the nopd points of each line from it in FP32
+	__shared__ int s_j0[2 * SHWFS_MAX_LAYERS];
+	__shared__ float s_f0[2 * SHWFS_MAX_LAYERS], s_step[SHWFS_MAX_LAYERS];
+	if (tid < 2 * nl) {
+		int j0;
+		float f0;
+		geom_origin(P, E, isa, tid >> 1, tid & 1, j0, f0);
+		s_j0[tid] = j0;
+		s_f0[tid] = f0;
+		if (!(tid & 1)) s_step[tid >> 1] = (float)(E.dx * E.sx[tid >> 1]);
+	}
+	__syncthreads();
 	for (int k = tid; k < nl * 2 * nopd; k += blockDim.x) {
 		const int l = k / (2 * nopd), r = k - l * 2 * nopd;
 		const bool isy = r >= nopd;
 		const int i = isy ? r - nopd : r;
 		const int n = isy ? P.ny[l] : P.nx[l];
-		int j0, j, j1;
-		float f0, w;
-		geom_origin(P, E, isa, l, isy, j0, f0);
-		geom_point(j0, f0, i, (float)(E.dx * E.sx[l]), n, j, j1, w);
+		int j, j1;
+		float w;
+		geom_point(s_j0[2 * l + isy], s_f0[2 * l + isy], i, s_step[l], n, j, j1, w);
 		const int m = isy ? P.nx[l] : 1;
 		s_tab[k] = make_int4(j * m, j1 * m, __float_as_int(w), 0);
 	}
