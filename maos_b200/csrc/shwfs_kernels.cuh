@@ -435,21 +435,37 @@ __global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomP
 __global__ void __launch_bounds__(256) llt_uplink_kernel(const __grid_constant__ GeomParams P) {
 	__shared__ float s_opd[256];
 	__shared__ float2 s_tile[32 * LD];
+	__shared__ int s_i0[SHWFS_MAX_LAYERS][2];
+	__shared__ float s_f0[SHWFS_MAX_LAYERS][3];  // x fraction, y fraction, step
 	const GeomEntry& E = P.e[blockIdx.x];
 	const int ip = threadIdx.x;
 	const int ix = ip & 15, iy = ip >> 4;
-	float acc = 0.f;
-	for (int l = 0; l < P.nlayer; l++) {
-		if (!((E.use >> l) & 1u)) continue;
-		const int nx = P.nx[l], ny = P.ny[l];
+	// the pupil's FP64 origin in each layer once (thread l), -1 where it is not finite
+	if (ip < P.nlayer) {
+		const int l = ip, nx = P.nx[l], ny = P.ny[l];
 		double x0 = E.origx[0] * E.sx[l] + E.dispx[l];
 		double y0 = E.origy[0] * E.sx[l] + E.dispy[l];
-		if (!isfinite(x0) || !isfinite(y0)) continue;
-		x0 -= floor(x0 / nx) * nx;
-		y0 -= floor(y0 / ny) * ny;
-		const int ix0 = (int)floor(x0), iy0 = (int)floor(y0);
-		const float step = (float)(E.dx * E.sx[l]);
-		const float xf = (float)(x0 - ix0) + ix * step, yf = (float)(y0 - iy0) + iy * step;
+		if (!isfinite(x0) || !isfinite(y0)) {
+			s_i0[l][0] = -1;
+		} else {
+			x0 -= floor(x0 / nx) * nx;
+			y0 -= floor(y0 / ny) * ny;
+			const int ix0 = (int)floor(x0), iy0 = (int)floor(y0);
+			s_i0[l][0] = ix0;
+			s_i0[l][1] = iy0;
+			s_f0[l][0] = (float)(x0 - ix0);
+			s_f0[l][1] = (float)(y0 - iy0);
+			s_f0[l][2] = (float)(E.dx * E.sx[l]);
+		}
+	}
+	__syncthreads();
+	float acc = 0.f;
+	for (int l = 0; l < P.nlayer; l++) {
+		if (!((E.use >> l) & 1u) || s_i0[l][0] < 0) continue;
+		const int nx = P.nx[l], ny = P.ny[l];
+		const int ix0 = s_i0[l][0], iy0 = s_i0[l][1];
+		const float step = s_f0[l][2];
+		const float xf = s_f0[l][0] + ix * step, yf = s_f0[l][1] + iy * step;
 		const float flx = floorf(xf), fly = floorf(yf);
 		int jx = ix0 + (int)flx, jy = iy0 + (int)fly;
 		const float wx = xf - flx, wy = yf - fly;
