@@ -261,6 +261,15 @@ int shwfs_profile_read(shwfs_ctx* ctx, double* ms, int* launches);
 int shwfs_autotune(shwfs_ctx* ctx, int iwfs0, int iwfs1, int nrep, int* chosen);
 /* Selects an imaging-kernel variant explicitly. */
 int shwfs_set_variant(shwfs_ctx* ctx, int ipowfs, int variant);
+/* Order of the pupils in a ray-trace launch.  AUTO interleaves pupils of the
+   same size (subaperture-major, pupil fastest) when the screens exceed L2,
+   so that a screen row their footprints share is fetched once, and keeps
+   the listed order otherwise; LISTED and INTERLEAVED force one order.  The
+   OPD is the same in every order. */
+#define SHWFS_TRACE_AUTO 0
+#define SHWFS_TRACE_LISTED 1
+#define SHWFS_TRACE_INTERLEAVED 2
+int shwfs_set_trace_order(shwfs_ctx* ctx, int order);
 
 /* Bytes the context has copied host->device and device->host on the frame
    path (descriptor tables, gradients, intensities) since the previous call;

@@ -138,6 +138,7 @@ struct shwfs_ctx {
 	uint64_t h2d_bytes = 0, d2h_bytes = 0;
 	// stage timing
 	int profiling = 0;
+	int trace_order = SHWFS_TRACE_AUTO;  // pupil order of ray-trace launches
 	std::vector<cudaEvent_t> ev_pool;
 	struct Mark {
 		int stage;
@@ -690,13 +691,15 @@ static int l2_bytes(shwfs_ctx* ctx) {
 // the screens in L2, the order as listed keeps each block's neighbours on the
 // same footprint, which measured faster.
 static int launch_geom_wfs(shwfs_ctx* ctx, GeomParams& gp, bool split) {
-	if (split && !gp.interleave && gp.nentry >= 2) {
+	if (ctx->trace_order == SHWFS_TRACE_LISTED) gp.interleave = 0;
+	if (split && !gp.interleave && gp.nentry >= 2 && ctx->trace_order != SHWFS_TRACE_LISTED) {
 		double screen = 0;
 		for (int l = 0; l < gp.nlayer; l++) screen += 4.0 * gp.nx[l] * gp.ny[l];
 		int nmax = 0, nbig = 0;
 		for (int i = 0; i < gp.nentry; i++) nmax = std::max(nmax, gp.e[i].nsa);
 		for (int i = 0; i < gp.nentry; i++) nbig += gp.e[i].nsa == nmax;
-		if (screen > l2_bytes(ctx) && nbig >= 2) {
+		const bool want = ctx->trace_order == SHWFS_TRACE_INTERLEAVED || screen > l2_bytes(ctx);
+		if (want && nbig >= 2) {
 			if (nbig == gp.nentry) {
 				gp.interleave = 1;
 			} else {
@@ -1995,6 +1998,14 @@ int shwfs_autotune(shwfs_ctx* ctx, int iwfs0, int iwfs1, int nrep, int* chosen) 
 	if (r) return r;
 	p.variant = bestv;
 	if (chosen) *chosen = bestv;
+	return 0;
+}
+
+int shwfs_set_trace_order(shwfs_ctx* ctx, int order) {
+	if (!ctx) return SHWFS_EINVAL;
+	if (order < SHWFS_TRACE_AUTO || order > SHWFS_TRACE_INTERLEAVED)
+		return fail(ctx, SHWFS_EINVAL, "set_trace_order: order %d is not AUTO, LISTED or INTERLEAVED", order);
+	ctx->trace_order = order;
 	return 0;
 }
 

@@ -284,7 +284,8 @@ int shwfs_evl_queue(shwfs_ctx* ctx, int isim, int do_psf) {
 					 E.nslot, 16, E.dx, E.opd.p + per * e)))
 				return r;
 		}
-		gp.interleave = 1;  // the directions of a tile together: the screens' rows are fetched once for all
+		// the directions of a tile together: the screens' rows are fetched once for all
+		gp.interleave = ctx->trace_order != SHWFS_TRACE_LISTED;
 		if ((r = launch_geom(ctx, gp))) return r;
 	}
 	// (b) WFE sums (calc_ptt, cuda/sim/perfevl.cu:46-102)

@@ -29,6 +29,9 @@ SHWFS_GRAD_ZTILT = 3
 SHWFS_GRAD_GTILT = 4
 SHWFS_FORM_FFT = 0
 SHWFS_FORM_TC = 1
+SHWFS_TRACE_AUTO = 0
+SHWFS_TRACE_LISTED = 1
+SHWFS_TRACE_INTERLEAVED = 2
 
 
 class ShwfsError(RuntimeError):
@@ -108,6 +111,7 @@ def _load() -> C.CDLL:
         "shwfs_copy_counters": [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)],
         "shwfs_autotune": [vp, i, i, i, ip],
         "shwfs_set_variant": [vp, i, i],
+        "shwfs_set_trace_order": [vp, i],
         "shwfs_frame_noalloc": [vp, i, i, vp, vp],
         "shwfs_powfs_set_etf_dtrat": [vp, i, i],
         "shwfs_powfs_set_saasum": [vp, i, C.c_double],
@@ -446,6 +450,10 @@ class Context:
 
     def set_variant(self, ipowfs: int, variant: int):
         self._check(self._L.shwfs_set_variant(self._h, ipowfs, variant), "set_variant")
+
+    def set_trace_order(self, order: int):
+        """Pupil order of ray-trace launches (SHWFS_TRACE_AUTO, _LISTED, _INTERLEAVED)."""
+        self._check(self._L.shwfs_set_trace_order(self._h, order), "set_trace_order")
 
     STAGES = ("raytrace", "uplink", "ints", "post")
 
