@@ -234,7 +234,7 @@ __device__ __forceinline__ int evl_crop_index(int k, int h) {
 // keeps are written to T (per direction, crop column ax major, row Y
 // fastest) straight from the last pass.  Grid (ceil(nY / R), nevl).
 template <int N, int R>
-__global__ void __launch_bounds__(EVL_THREADS, 2) evl_psf_rows_kernel(EvlRaster Ra, const float* __restrict__ opd,
+__global__ void __launch_bounds__(EVL_THREADS, 4) evl_psf_rows_kernel(EvlRaster Ra, const float* __restrict__ opd,
 	const double* __restrict__ coeff, int pttr, float twoinvwvl, int offx, int h, const float2* __restrict__ tw,
 	float2* __restrict__ T, int nYp) {
 	extern __shared__ float2 s_row[];
@@ -309,7 +309,7 @@ __global__ void __launch_bounds__(EVL_THREADS, 2) evl_psf_rows_kernel(EvlRaster 
 // transformed along y, |.|^2 of the 2h kept frequencies added to the sum
 // psf (per direction, ax major, ay fastest) straight from the last pass.
 template <int N>
-__global__ void __launch_bounds__(EVL_THREADS) evl_psf_cols_kernel(const float2* __restrict__ T, int nY, int nYp, int offy,
+__global__ void __launch_bounds__(EVL_THREADS, 4) evl_psf_cols_kernel(const float2* __restrict__ T, int nY, int nYp, int offy,
 	int h, const float2* __restrict__ tw, float* __restrict__ psf) {
 	extern __shared__ float2 s_col[];
 	const int ax = blockIdx.x, e = blockIdx.y, ncol = 2 * h;

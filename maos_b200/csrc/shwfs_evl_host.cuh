@@ -240,7 +240,7 @@ int shwfs_evl_psf_reset(shwfs_ctx* ctx) {
 
 template <int N>
 static int evl_launch_psf(shwfs_ctx* ctx, EvlState& E, EvlPsf& P, int nevl) {
-	constexpr int R = 8192 / N;  // rows per block: 1024 radix-8 groups, two per thread
+	constexpr int R = 4096 / N;  // rows per block: 512 radix-8 groups, one per thread
 	const size_t smem_r = (size_t)R * evl_row_len<N>() * sizeof(float2), smem_c = (size_t)evl_row_len<N>() * sizeof(float2);
 	if (smem_r > 48 * 1024)
 		CK(cudaFuncSetAttribute(evl_psf_rows_kernel<N, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_r));
