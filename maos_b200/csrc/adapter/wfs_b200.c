@@ -1,0 +1,210 @@
+/*
+ * Adapter from MAOS's GPU wavefront-sensor seam to libshwfs_b200.
+ *
+ * This file belongs in the MAOS tree (beside cuda/sim/wfsgrad.cu) and is compiled against
+ * the headers under maos/ and linked with -lshwfs_b200. It defines the C-linkage functions that the simulator
+ * calls when gpu.wfs is set (cuda/sim/gpu_sim.h:39-49; selected in maos/sim_utils.c:1497-1504),
+ * so maos.c's time loop is unchanged:
+ *
+ *   gpu_wfsgrad_init        cuda/sim/wfsinit.cu:159   powfs and WFS descriptors, geometry,
+ *                                                     pixel maps, DTF/ETF, LLT, matched filters
+ *   gpu_wfsgrad_update_etf  cuda/sim/wfsinit.cu:32    etfsim / etfsim2 slots, interpolation period
+ *   gpu_wfsgrad_update_ref  cuda/sim/wfsinit.cu:107   matched filters and i0 sums
+ *   gpu_wfsgrad_seeding     cuda/sim/wfsinit.cu:532   one lrand() per WFS
+ *   gpu_atm2gpu             cuda/sim/atm.cu:106       turbulence screens
+ *   gpu_wfsgrad_queue       cuda/sim/wfsgrad.cu:483   queue the frame of info->start..end
+ *   gpu_wfsgrad_sync        cuda/sim/wfsgrad.cu:747   gradients into simu->gradcl
+ *   gpu_wfs_init_sim, gpu_save_pistat, gpu_wfssurf2gpu: no device state to reset, and the
+ *                           pistat diagnostics and NCPA surfaces are not on this path.
+ *
+ * The reference aborts on errors (error()); a nonzero status from the library is reported the
+ * same way, with the library's message. One context serves every WFS. The simulator queues and
+ * syncs WFS from several host threads at once, and calls on one context must not overlap, so
+ * every call goes through one mutex.
+ */
+#include <pthread.h>
+#include <string.h>
+#include "gpu_sim.h"
+#include "shwfs_b200.h"
+
+static shwfs_ctx* g_ctx;
+static int g_ipowfs[64];   /* MAOS ipowfs -> context powfs */
+static pthread_mutex_t g_lock=PTHREAD_MUTEX_INITIALIZER;
+
+static void chk(int rc, const char* what){
+	if(rc) error("shwfs %s: %s\n", what, shwfs_last_error(g_ctx));
+}
+
+/* dtf.si (npix x notf^2, CSC, bilinear: at most four entries per pixel row) -> 4-tap map */
+static void si_taps(const dsp* si, int* idx, double* wt){
+	const long npix=si->nx;
+	for(long i=0; i<npix*4; i++){ idx[i]=-1; wt[i]=0; }
+	int* k=mycalloc(npix, int);
+	for(long ic=0; ic<si->ny; ic++){
+		for(long j=si->pp[ic]; j<si->pp[ic+1]; j++){
+			const long p=si->pi[j];
+			if(k[p]>=4) error("shwfs: pixel %ld has more than four taps\n", p);
+			idx[4*p+k[p]]=(int)ic; wt[4*p+k[p]]=si->px[j]; k[p]++;
+		}
+	}
+	free(k);
+}
+
+/* etf.etf is a cell of nsa (x 1 or x nllt) notf x notf complex arrays; pack the first LLT's
+   column subaperture-major, as shwfs_powfs_set_etf takes it. */
+static void set_etf(const powfs_t* p, int ip, const etf_t* etf, int slot){
+	const long nsa=p->saloc->nloc, n2=(long)p->notfx*p->notfy;
+	cmat* e=cnew(n2, nsa);
+	for(long isa=0; isa<nsa; isa++) memcpy(PCOL(e, isa), P(P(etf->etf, isa, 0)), sizeof(comp)*n2);
+	chk(shwfs_powfs_set_etf(g_ctx, g_ipowfs[ip], (const double*)P(e), slot), "set_etf");
+	cfree(e);
+}
+
+/* intstat->mtche is nsa x nwfs cells of 2 x npix; pack the WFS's column subaperture-major. */
+static void set_mtche(const parms_t* parms, const powfs_t* p, int ip, int iwfs){
+	const intstat_t* st=p->intstat;
+	if(!st || !st->mtche) return;
+	const long wfsind=P(parms->powfs[ip].wfsind, iwfs);
+	const long nsa=p->saloc->nloc, npix=(long)p->pixpsax*p->pixpsay;
+	const long icol=NY(st->mtche)>1?wfsind:0;
+	dmat* mt=dnew(2*npix, nsa);
+	for(long isa=0; isa<nsa; isa++) memcpy(PCOL(mt, isa), P(P(st->mtche, isa, icol)), sizeof(real)*2*npix);
+	const long ii0=NY(st->i0sum)>1?wfsind:0;
+	chk(shwfs_wfs_set_mtche(g_ctx, iwfs, P(mt), PCOL(st->i0sum, ii0), P(st->i0sumsum, ii0)), "set_mtche");
+	dfree(mt);
+}
+
+void gpu_wfsgrad_init(const parms_t* parms, const powfs_t* powfs){
+	pthread_mutex_lock(&g_lock);
+	chk(shwfs_create(&g_ctx, 0), "create");
+	if(parms->npowfs>64) error("shwfs: at most 64 powfs\n");
+	for(int ip=0; ip<parms->npowfs; ip++){
+		const powfs_t* p=&powfs[ip];
+		const powfs_cfg_t* pc=&parms->powfs[ip];
+		const int llt=p->llt!=NULL;
+		shwfs_powfs_desc d={
+			.nsa=(int)p->saloc->nloc, .nopd=(int)p->pts->nxsa, .embfac=pc->embfac,
+			.notf=p->notfx, .pixpsax=p->pixpsax, .pixpsay=p->pixpsay,
+			.pixthetax=pc->radpixtheta, .pixthetay=pc->pixtheta,
+			.wvl=P(pc->wvl, 0), .dsa=p->pts->dsa, .dx=p->pts->dx,
+			.areascale=p->areascale, .hs=pc->hs,
+			.has_etf=llt, .has_llt=llt, .llt_nx=llt?(int)p->llt->pts->nxsa:0,
+			.llt_ox=llt?P(pc->llt->ox, 0):0, .llt_oy=llt?P(pc->llt->oy, 0):0,
+			.llt_origx=llt?p->llt->pts->origx[0]:0, .llt_origy=llt?p->llt->pts->origy[0]:0,
+			.gradtype=pc->phytype_sim, .sigmatch=pc->sigmatch,
+			.cogthres=pc->cogthres, .cogoff=pc->cogoff, .rne=pc->rne,
+			.bkgrnd=pc->bkgrnd*pc->dtrat, .bkgrndc=pc->bkgrnd*pc->dtrat*pc->bkgrndc,
+			.saat=pc->saat, .sigtot_cog=pc->siglev*pc->dtrat};
+		chk(shwfs_powfs_add(g_ctx, &d, &g_ipowfs[ip]), "powfs_add");
+		chk(shwfs_powfs_set_geom(g_ctx, g_ipowfs[ip], p->pts->origx, p->pts->origy,
+			P(P(p->amp, 0)), (int)PN(P(p->amp, 0)), P(P(p->saa, 0))), "set_geom");
+		chk(shwfs_powfs_set_saasum(g_ctx, g_ipowfs[ip], P(p->saasum, 0)), "set_saasum");
+		const long npix=(long)p->pixpsax*p->pixpsay;
+		int* idx=mymalloc(npix*4, int);
+		double* wt=mymalloc(npix*4, double);
+		si_taps(P(p->dtf[0].si, 0), idx, wt);
+		chk(shwfs_powfs_set_simap(g_ctx, g_ipowfs[ip], idx, wt, 1), "set_simap");
+		free(idx); free(wt);
+		if(llt){
+			set_etf(p, ip, &p->etfsim[0], 0);
+			chk(shwfs_powfs_set_lltamp(g_ctx, g_ipowfs[ip], P(p->llt->amp)), "set_lltamp");
+		}else{
+			/* nominal is real-valued in MAOS's FFT layout; one shared by every subaperture */
+			chk(shwfs_powfs_set_nominal(g_ctx, g_ipowfs[ip], P(P(p->dtf[0].nominal, 0)), 1), "set_nominal");
+		}
+		if(pc->dtrat>1) chk(shwfs_powfs_set_dtrat(g_ctx, g_ipowfs[ip], pc->dtrat), "set_dtrat");
+	}
+	for(int iwfs=0; iwfs<parms->nwfs; iwfs++){
+		const int ip=parms->wfs[iwfs].powfs;
+		const wfs_cfg_t* wc=&parms->wfs[iwfs];
+		shwfs_wfs_desc w={.ipowfs=g_ipowfs[ip], .thetax=wc->thetax, .thetay=wc->thetay,
+			.hs=wc->hs, .hc=wc->hc, .misregx=wc->misregx, .misregy=wc->misregy,
+			.sigsim=wc->sigsim, .wvlwt=P(wc->wvlwts, 0), .noisy=parms->powfs[ip].noisy};
+		int i;
+		chk(shwfs_wfs_add(g_ctx, &w, &i), "wfs_add");
+		if(i!=iwfs) error("shwfs: WFS %d registered as %d\n", iwfs, i);
+		set_mtche(parms, &powfs[ip], ip, iwfs);
+	}
+	chk(shwfs_set_dt(g_ctx, parms->sim.dt), "set_dt");
+	pthread_mutex_unlock(&g_lock);
+}
+
+void gpu_wfs_init_sim(const parms_t* parms, powfs_t* powfs){
+	(void)parms; (void)powfs; /* intensities and gradients are formed afresh each frame */
+}
+
+void gpu_wfsgrad_update_etf(const parms_t* parms, const powfs_t* powfs, int ipowfs){
+	const powfs_t* p=&powfs[ipowfs];
+	if(!p->llt) return;
+	pthread_mutex_lock(&g_lock);
+	set_etf(p, ipowfs, &p->etfsim[0], 0);
+	if(p->etfsim2){
+		set_etf(p, ipowfs, &p->etfsim2[0], 1);
+		const int dtrat=parms->powfs[ipowfs].llt->coldtrat>0?parms->powfs[ipowfs].llt->coldtrat
+			:parms->powfs[ipowfs].zoomdtrat;
+		chk(shwfs_powfs_set_etf_dtrat(g_ctx, g_ipowfs[ipowfs], dtrat), "set_etf_dtrat");
+	}
+	pthread_mutex_unlock(&g_lock);
+}
+
+void gpu_wfsgrad_update_ref(const parms_t* parms, const powfs_t* powfs, int ipowfs){
+	pthread_mutex_lock(&g_lock);
+	for(int jwfs=0; jwfs<parms->powfs[ipowfs].nwfs; jwfs++){
+		const int iwfs=P(parms->powfs[ipowfs].wfs, jwfs);
+		set_mtche(parms, &powfs[ipowfs], ipowfs, iwfs);
+	}
+	pthread_mutex_unlock(&g_lock);
+}
+
+void gpu_wfsgrad_seeding(const parms_t* parms, const powfs_t* powfs, rand_t* rstat){
+	(void)powfs;
+	pthread_mutex_lock(&g_lock);
+	for(int iwfs=0; iwfs<parms->nwfs; iwfs++) chk(shwfs_wfs_seed(g_ctx, iwfs, lrand(rstat)), "seed");
+	pthread_mutex_unlock(&g_lock);
+}
+
+void gpu_atm2gpu(const mapcell* atm, const dmat* atmscale, const parms_t* parms, int iseed, int isim){
+	(void)parms; (void)iseed; (void)isim;
+	/* atmscale (atm.r0evolve) scales the screens frame by frame (cuda/sim/accphi.cu:155-156);
+	   the library's layer weights are fixed per screen set. */
+	if(atmscale) error("shwfs: atm.r0evolve (a per-frame atmscale) is not supported\n");
+	const int n=(int)PN(atm);
+	shwfs_layer_desc* L=mycalloc(n, shwfs_layer_desc);
+	const double** s=mycalloc(n, const double*);
+	for(int i=0; i<n; i++){
+		const map_t* m=P(atm, i);
+		L[i]=(shwfs_layer_desc){.nx=m->nx, .ny=m->ny, .dx=m->dx, .ox=m->ox, .oy=m->oy,
+			.ht=m->ht, .vx=m->vx, .vy=m->vy, .alpha=1};
+		s[i]=P(m);
+	}
+	pthread_mutex_lock(&g_lock);
+	chk(shwfs_atm_set(g_ctx, n, L, s), "atm_set");
+	pthread_mutex_unlock(&g_lock);
+	free(L); free(s);
+}
+
+void* gpu_wfsgrad_queue(thread_t* info){
+	sim_t* simu=(sim_t*)info->data;
+	pthread_mutex_lock(&g_lock);
+	for(int iwfs=info->start; iwfs<info->end; iwfs++)
+		chk(shwfs_frame_queue(g_ctx, simu->wfsisim, iwfs, iwfs+1), "frame_queue");
+	pthread_mutex_unlock(&g_lock);
+	return NULL;
+}
+
+void gpu_wfsgrad_sync(sim_t* simu, int iwfs){
+	const int ip=simu->parms->wfs[iwfs].powfs;
+	dmat** pg=&P(simu->gradcl, iwfs);
+	if(!*pg) *pg=dnew(simu->powfs[ip].saloc->nloc*2, 1);
+	pthread_mutex_lock(&g_lock);
+	chk(shwfs_frame_sync(g_ctx, iwfs, P(*pg), NULL), "frame_sync");
+	pthread_mutex_unlock(&g_lock);
+}
+
+void gpu_save_pistat(sim_t* simu){
+	(void)simu; /* pistat diagnostics are not formed on this path */
+}
+
+void gpu_wfssurf2gpu(const parms_t* parms, powfs_t* powfs){
+	(void)parms; (void)powfs; /* NCPA surfaces are not on this path */
+}
