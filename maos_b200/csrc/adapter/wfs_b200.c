@@ -76,6 +76,10 @@ static void set_mtche(const parms_t* parms, const powfs_t* p, int ip, int iwfs){
 
 void gpu_wfsgrad_init(const parms_t* parms, const powfs_t* powfs){
 	pthread_mutex_lock(&g_lock);
+	if(g_ctx){ /* a new simulation in the same process */
+		shwfs_destroy(g_ctx);
+		g_ctx=NULL;
+	}
 	chk(shwfs_create(&g_ctx, 0), "create");
 	if(parms->npowfs>64) error("shwfs: at most 64 powfs\n");
 	for(int ip=0; ip<parms->npowfs; ip++){
@@ -97,7 +101,7 @@ void gpu_wfsgrad_init(const parms_t* parms, const powfs_t* powfs){
 			.saat=pc->saat, .sigtot_cog=pc->siglev*pc->dtrat};
 		chk(shwfs_powfs_add(g_ctx, &d, &g_ipowfs[ip]), "powfs_add");
 		chk(shwfs_powfs_set_geom(g_ctx, g_ipowfs[ip], p->pts->origx, p->pts->origy,
-			P(P(p->amp, 0)), (int)PN(P(p->amp, 0)), P(P(p->saa, 0))), "set_geom");
+			P(P(p->amp, 0)), 1, P(P(p->saa, 0))), "set_geom"); /* one amplitude map for every WFS */
 		chk(shwfs_powfs_set_saasum(g_ctx, g_ipowfs[ip], P(p->saasum, 0)), "set_saasum");
 		const long npix=(long)p->pixpsax*p->pixpsay;
 		int* idx=mymalloc(npix*4, int);

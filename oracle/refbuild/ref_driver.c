@@ -198,6 +198,10 @@ int oref_setup(const oref_cfg_t* c){
 }
 
 int oref_nsa(void){ return (int)g_powfs[0].saloc->nloc; }
+/* The structures built by oref_setup and oref_atm_set, for the driver of the MAOS-side adapter
+   (adapter_driver.c), which hands them to MAOS's GPU seam as the simulator does. */
+parms_t* oref_parms(void){ return g_parms; }
+powfs_t* oref_powfs(void){ return g_powfs; }
 int oref_nopd(void){ return (int)g_powfs[0].pts->nxsa; }
 int oref_notf(void){ return g_powfs[0].notfx; }
 int oref_pixpsax(void){ return g_powfs[0].pixpsax; }
@@ -451,6 +455,7 @@ void oref_atm_set(int nlayer, const double* const* screens, const long* nx, cons
 		m->ox=ox[i]; m->oy=oy[i]; m->ht=ht[i]; m->vx=vx[i]; m->vy=vy[i];
 	}
 }
+map_t** oref_atm(int* nlayer){ *nlayer=g_natm; return g_atm; }
 
 /* One complete WFS frame of the reference CPU path at step isim, as
    wfsgrad_iwfs runs it (maos/wfsgrad.c:170-194, 330-473): the ray trace of

@@ -1,0 +1,65 @@
+"""The MAOS-side adapter, run as the simulator runs it, against the reference's CPU frame.
+
+`oracle/_ref/libmaosadapter.so` holds the adapter (`maos_b200/csrc/adapter/wfs_b200.c`, the ten
+`gpu_*` functions of `cuda/sim/gpu_sim.h` over `libshwfs_b200.so`) and a driver that calls
+`gpu_wfsgrad_init`, `gpu_atm2gpu`, `gpu_wfsgrad_queue` and `gpu_wfsgrad_sync` on the `parms_t`,
+`powfs_t` and screens that the reference's own setup built. Every static array the library gets
+(subaperture origins, amplitude, pixel map from `dtf.si`, nominal DTF, ETF, LLT amplitude,
+matched filter, i0 sums) is the one the adapter reads from the reference's structures. The
+gradients that come back in `simu->gradcl` must match the reference's own CPU frame on the same
+screens within 1e-4 relative (max |dg| / max |g|), as the library's direct frames do.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from tests.conftest import cuda_available
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not cuda_available(), reason="needs a CUDA GPU")]
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ADAPTER_LIB = os.path.join(ROOT, "oracle", "_ref", "libmaosadapter.so")
+
+
+def _adapter(ref_lib):
+    if not os.path.exists(ADAPTER_LIB):
+        pytest.skip("oracle/_ref/libmaosadapter.so is not built (make -C oracle adapter)")
+    ref_lib.lib()  # the reference's C, which the adapter library links to, loads first
+    L = C.CDLL(ADAPTER_LIB)
+    L.oadp_init.restype = C.c_int
+    L.oadp_init.argtypes = [C.c_int, C.c_double]
+    L.oadp_frame.restype = C.c_int
+    L.oadp_frame.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double)]
+    return L
+
+
+def _screens(cfg):
+    from maos_b200.workload import build
+    wl = build(cfg, device=0, seed=3, noisy=False, nx=512)
+    screens, layers = wl.screens, wl.layers
+    wl.close()
+    return screens, layers
+
+
+@pytest.mark.parametrize("cfg_name,isims,wfs", [("NGS8", (5, 6), (0,)), ("LGS30", (0, 37), (0, 3))])
+def test_adapter_frames_match_reference(ref_lib, cfg_name, isims, wfs):
+    from maos_b200 import configs
+    from tests.helpers import grad_rel_err
+    cfg = getattr(configs, cfg_name)
+    screens, layers = _screens(cfg)
+    r = ref_lib.RefPowfs(cfg)
+    ref_lib.atm_set(screens, layers)
+    A = _adapter(ref_lib)
+    nwfs = A.oadp_init(0, cfg["dt"])
+    assert nwfs == len(cfg["thetax"])
+    g = np.zeros(nwfs * 2 * r.nsa)
+    for isim in isims:
+        assert A.oadp_frame(isim, 0, nwfs, g.ctypes.data_as(C.POINTER(C.c_double))) == 0
+        for k in wfs:
+            _, g_ref, _ = ref_lib.frame_full_mt(r, k, isim, cfg["dt"], noisy=False)
+            gk = g[k * 2 * r.nsa:(k + 1) * 2 * r.nsa]
+            assert np.isfinite(gk).all()
+            err = grad_rel_err(gk, g_ref)
+            assert err <= 1e-4, (cfg_name, isim, k, err)
