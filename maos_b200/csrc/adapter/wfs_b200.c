@@ -144,7 +144,8 @@ void gpu_wfsgrad_update_etf(const parms_t* parms, const powfs_t* powfs, int ipow
 	set_etf(p, ipowfs, &p->etfsim[0], 0);
 	if(p->etfsim2){
 		set_etf(p, ipowfs, &p->etfsim2[0], 1);
-		const int dtrat=parms->powfs[ipowfs].llt->coldtrat>0?parms->powfs[ipowfs].llt->coldtrat
+		/* the interpolation period as maos/wfsints.c:218 picks it */
+		const int dtrat=parms->powfs[ipowfs].llt->coldtrat?parms->powfs[ipowfs].llt->coldtrat
 			:parms->powfs[ipowfs].zoomdtrat;
 		chk(shwfs_powfs_set_etf_dtrat(g_ctx, g_ipowfs[ipowfs], dtrat), "set_etf_dtrat");
 	}

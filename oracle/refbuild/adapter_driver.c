@@ -42,6 +42,12 @@ int oadp_init(int noisy, double dt){
 	return parms->nwfs;
 }
 
+/* New ETF pair of powfs 0 through gpu_wfsgrad_update_etf, as sim_update_etf does
+   (maos/sim_utils.c:338) after the reference's setup made etfsim2 (oref_setup_etf2). */
+void oadp_update_etf(void){
+	gpu_wfsgrad_update_etf(oref_parms(), oref_powfs(), 0);
+}
+
 /* Seeds the noise of every WFS through gpu_wfsgrad_seeding from a reference MT19937 stream. */
 void oadp_seed(unsigned int seed){
 	rand_t rs;

@@ -63,3 +63,24 @@ def test_adapter_frames_match_reference(ref_lib, cfg_name, isims, wfs):
             assert np.isfinite(gk).all()
             err = grad_rel_err(gk, g_ref)
             assert err <= 1e-4, (cfg_name, isim, k, err)
+
+
+@pytest.mark.parametrize("isim", [5, 6])
+def test_adapter_etf_update_matches_reference(ref_lib, isim):
+    """gpu_wfsgrad_update_etf with the reference's second ETF (sodium layer 1.5 km higher) and
+    coldtrat 4: frame isim blends the pair with weight (isim mod 4)/4, on both sides."""
+    from maos_b200.configs import LGS30
+    from tests.helpers import grad_rel_err
+    screens, layers = _screens(LGS30)
+    r = ref_lib.RefPowfs(LGS30)
+    r.setup_etf2(1500.0, 4)
+    ref_lib.atm_set(screens, layers)
+    A = _adapter(ref_lib)
+    nwfs = A.oadp_init(0, LGS30["dt"])
+    A.oadp_update_etf()
+    g = np.zeros(nwfs * 2 * r.nsa)
+    assert A.oadp_frame(isim, 0, nwfs, g.ctypes.data_as(C.POINTER(C.c_double))) == 0
+    for k in (0, 4):
+        _, g_ref, _ = ref_lib.frame_full_mt(r, k, isim, LGS30["dt"], noisy=False)
+        err = grad_rel_err(g[k * 2 * r.nsa:(k + 1) * 2 * r.nsa], g_ref)
+        assert err <= 1e-4, (isim, k, err)
