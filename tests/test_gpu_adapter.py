@@ -84,3 +84,32 @@ def test_adapter_etf_update_matches_reference(ref_lib, isim):
         _, g_ref, _ = ref_lib.frame_full_mt(r, k, isim, LGS30["dt"], noisy=False)
         err = grad_rel_err(g[k * 2 * r.nsa:(k + 1) * 2 * r.nsa], g_ref)
         assert err <= 1e-4, (isim, k, err)
+
+
+def test_adapter_seeding_keys_the_noise(ref_lib):
+    """gpu_wfsgrad_seeding gives each WFS one lrand() of the simulator's stream: the same stream
+    seed gives the same noisy frame bit for bit, another seed another frame, and the noisy
+    gradients are finite and differ from the noise-free ones."""
+    from maos_b200.configs import NGS8
+    from tests.helpers import grad_rel_err
+    screens, layers = _screens(NGS8)
+    r = ref_lib.RefPowfs(NGS8)
+    ref_lib.atm_set(screens, layers)
+    A = _adapter(ref_lib)
+    A.oadp_seed.argtypes = [C.c_uint]
+    ptr = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    n = 2 * r.nsa
+    g0, g1, g2, g3 = (np.zeros(n) for _ in range(4))
+    A.oadp_init(0, NGS8["dt"])
+    A.oadp_frame(5, 0, 1, ptr(g0))
+    A.oadp_init(1, NGS8["dt"])
+    A.oadp_seed(1)
+    A.oadp_frame(5, 0, 1, ptr(g1))
+    A.oadp_seed(1)
+    A.oadp_frame(5, 0, 1, ptr(g2))
+    A.oadp_seed(2)
+    A.oadp_frame(5, 0, 1, ptr(g3))
+    assert np.array_equal(g1, g2)
+    assert not np.array_equal(g1, g3)
+    assert np.isfinite(g1).all()
+    assert grad_rel_err(g1, g0) > 1e-3
