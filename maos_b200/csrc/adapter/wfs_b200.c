@@ -16,6 +16,9 @@
  *   gpu_wfsgrad_sync        cuda/sim/wfsgrad.cu:747   gradients into simu->gradcl
  *   gpu_wfs_init_sim, gpu_save_pistat, gpu_wfssurf2gpu: no device state to reset, and the
  *                           pistat diagnostics and NCPA surfaces are not on this path.
+ *   gpu_perfevl_init, gpu_perfevl_init_sim, gpu_perfevl_queue, gpu_perfevl_sync
+ *                           cuda/sim/perfevl.cu: the open-loop science evaluation (olep, olmp
+ *                           and the PSF sums); DM terms are refused.
  *
  * The reference aborts on errors (error()); a nonzero status from the library is reported the
  * same way, with the library's message. One context serves every WFS. The simulator queues and
@@ -26,14 +29,21 @@
 #include <string.h>
 #include "gpu_sim.h"
 #include "shwfs_b200.h"
+#include "shwfs_evl.h"
 
 static shwfs_ctx* g_ctx;
 static int g_ipowfs[64];   /* MAOS ipowfs -> context powfs */
 static pthread_mutex_t g_lock=PTHREAD_MUTEX_INITIALIZER;
 
-static void chk(int rc, const char* what){
-	if(rc) error("shwfs %s: %s\n", what, shwfs_last_error(g_ctx));
+static shwfs_ctx* g_evl;   /* science path (gpu_perfevl_*): a context of its own */
+static double* g_evl_wfe;  /* nevl x 3 {PR, TT, PTTR} of the last synced frame */
+static double* g_evl_coeff;/* nevl x 3 {piston, tip, tilt} */
+static int g_evl_synced=1; /* the queued frame's results are in g_evl_wfe/coeff */
+
+static void chk_ctx(const shwfs_ctx* ctx, int rc, const char* what){
+	if(rc) error("shwfs %s: %s\n", what, shwfs_last_error(ctx));
 }
+static void chk(int rc, const char* what){ chk_ctx(g_ctx, rc, what); }
 
 /* dtf.si (npix x notf^2, CSC, bilinear: at most four entries per pixel row) -> 4-tap map */
 static void si_taps(const dsp* si, int* idx, double* wt){
@@ -183,7 +193,10 @@ void gpu_atm2gpu(const mapcell* atm, const dmat* atmscale, const parms_t* parms,
 		s[i]=P(m);
 	}
 	pthread_mutex_lock(&g_lock);
-	chk(shwfs_atm_set(g_ctx, n, L, s), "atm_set");
+	/* the WFS and the science contexts each keep the screens, as the reference keeps them on
+	   every GPU that traces them */
+	if(g_ctx) chk(shwfs_atm_set(g_ctx, n, L, s), "atm_set");
+	if(g_evl) chk_ctx(g_evl, shwfs_atm_set(g_evl, n, L, s), "atm_set");
 	pthread_mutex_unlock(&g_lock);
 	free(L); free(s);
 }
@@ -212,4 +225,94 @@ void gpu_save_pistat(sim_t* simu){
 
 void gpu_wfssurf2gpu(const parms_t* parms, powfs_t* powfs){
 	(void)parms; (void)powfs; /* NCPA surfaces are not on this path */
+}
+
+/* ---- science path, open loop (cuda/sim/perfevl.cu) ---- */
+
+void gpu_perfevl_init(const parms_t* parms, aper_t* aper){
+	const int nevl=parms->evl.nevl;
+	if(parms->ndm>0) error("shwfs: the science path has no DM terms (parms->ndm=%d)\n", parms->ndm);
+	if(parms->evl.nmod!=3) error("shwfs: the science path forms piston/tip/tilt only (evl.nmod=%d)\n",
+		parms->evl.nmod);
+	for(int i=1; i<nevl; i++){
+		if(P(parms->evl.pttr, i)!=P(parms->evl.pttr, 0)) error("shwfs: evl.pttr must be the same for every direction\n");
+	}
+	pthread_mutex_lock(&g_lock);
+	if(g_evl){
+		shwfs_destroy(g_evl);
+		g_evl=NULL;
+	}
+	chk_ctx(g_evl, shwfs_create(&g_evl, 0), "create");
+	chk_ctx(g_evl, shwfs_set_dt(g_evl, parms->sim.dt), "set_dt");
+	const loc_t* locs=aper->locs;
+	chk_ctx(g_evl, shwfs_evl_set_aper(g_evl, locs->nloc, locs->locx, locs->locy, locs->dx, P(aper->amp)),
+		"evl_set_aper");
+	for(int ievl=0; ievl<nevl; ievl++){
+		int k;
+		chk_ctx(g_evl, shwfs_evl_add_dir(g_evl, P(parms->evl.thetax, ievl), P(parms->evl.thetay, ievl),
+			P(parms->evl.hs, ievl), &k), "evl_add_dir");
+	}
+	if(parms->evl.psfmean && aper->locfft){
+		const int nwvl=parms->evl.nwvl;
+		int* nembed=mycalloc(nwvl, int);
+		int* psfsize=mycalloc(nwvl, int);
+		for(int i=0; i<nwvl; i++){
+			nembed[i]=(int)P(aper->locfft->nembed, i);
+			psfsize[i]=(int)P(parms->evl.psfsize, i);
+		}
+		chk_ctx(g_evl, shwfs_evl_set_psf(g_evl, nwvl, P(parms->evl.wvl), nembed, psfsize,
+			(int)P(parms->evl.pttr, 0)), "evl_set_psf");
+		free(nembed);
+		free(psfsize);
+	}
+	free(g_evl_wfe);
+	free(g_evl_coeff);
+	g_evl_wfe=mycalloc(3*nevl, double);
+	g_evl_coeff=mycalloc(3*nevl, double);
+	g_evl_synced=1;
+	pthread_mutex_unlock(&g_lock);
+}
+
+void gpu_perfevl_init_sim(const parms_t* parms, aper_t* aper){
+	(void)parms; (void)aper;
+	pthread_mutex_lock(&g_lock);
+	if(g_evl) chk_ctx(g_evl, shwfs_evl_psf_reset(g_evl), "evl_psf_reset");
+	pthread_mutex_unlock(&g_lock);
+}
+
+/* The simulator splits the directions over threads (info->start..end). One queue call runs every
+   direction, so the thread holding direction 0 queues the frame; the syncs of all threads follow
+   the queues (maos/sim.c runs perfevl_pre before perfevl_post). */
+void* gpu_perfevl_queue(thread_t* info){
+	sim_t* simu=(sim_t*)info->data;
+	const parms_t* parms=simu->parms;
+	if(info->start!=0) return NULL;
+	const int do_psf=parms->evl.psfmean && simu->perfisim>=parms->evl.psfisim;
+	pthread_mutex_lock(&g_lock);
+	chk_ctx(g_evl, shwfs_evl_queue(g_evl, simu->perfisim, do_psf), "evl_queue");
+	g_evl_synced=0;
+	pthread_mutex_unlock(&g_lock);
+	return NULL;
+}
+
+/* Open-loop results of frame perfisim into simu->olep (PR, TT, PTTR) and simu->olmp (piston,
+   tip, tilt), column perfisim, for the thread's directions. */
+void* gpu_perfevl_sync(thread_t* info){
+	sim_t* simu=(sim_t*)info->data;
+	const int isim=simu->perfisim;
+	pthread_mutex_lock(&g_lock);
+	if(!g_evl_synced){
+		chk_ctx(g_evl, shwfs_evl_sync(g_evl, g_evl_wfe, g_evl_coeff), "evl_sync");
+		g_evl_synced=1;
+	}
+	for(long ievl=info->start; ievl<info->end; ievl++){
+		real* pe=PCOL(P(simu->olep, ievl), isim);
+		real* pm=PCOL(P(simu->olmp, ievl), isim);
+		for(int k=0; k<3; k++){
+			pe[k]=g_evl_wfe[3*ievl+k];
+			pm[k]=g_evl_coeff[3*ievl+k];
+		}
+	}
+	pthread_mutex_unlock(&g_lock);
+	return NULL;
 }

@@ -14,6 +14,7 @@
 parms_t* oref_parms(void);
 powfs_t* oref_powfs(void);
 map_t** oref_atm(int* nlayer);
+void oref_evl_aper(loc_t** locs, dmat** amp, locfft_t** locfft);
 
 static sim_t* g_sim=NULL;
 
@@ -70,6 +71,80 @@ int oadp_frame(int isim, int iwfs0, int iwfs1, double* grad){
 	for(int iwfs=iwfs0; iwfs<iwfs1; iwfs++){
 		gpu_wfsgrad_sync(g_sim, iwfs);
 		memcpy(grad+(iwfs-iwfs0)*ng, P(P(g_sim->gradcl, iwfs)), sizeof(double)*ng);
+	}
+	return 0;
+}
+
+/* ---- science path (gpu_perfevl_*), on the aperture of oref_evl_setup ---- */
+static parms_t* g_eparms=NULL;
+static aper_t* g_eaper=NULL;
+static sim_t* g_esim=NULL;
+
+static dmat* dvec(int n, const double* v){
+	dmat* d=dnew(n, 1);
+	for(int i=0; i<n; i++) P(d, i)=v[i];
+	return d;
+}
+
+/* Setup as maos/setup.c does it for an open-loop run with nsim frames: gpu_perfevl_init,
+   gpu_atm2gpu, gpu_perfevl_init_sim. psfsize per wavelength; pttr for every direction. */
+int oadp_evl_init(int nevl, const double* thetax, const double* thetay, const double* hs, int nwvl,
+	const double* wvl, const long* psfsize, int pttr, double dt, int nsim){
+	parms_t* parms=g_eparms=mycalloc(1, parms_t);
+	parms->evl.nevl=nevl;
+	parms->evl.thetax=dvec(nevl, thetax);
+	parms->evl.thetay=dvec(nevl, thetay);
+	parms->evl.hs=dvec(nevl, hs);
+	parms->evl.nwvl=nwvl;
+	parms->evl.wvl=dvec(nwvl, wvl);
+	parms->evl.psfsize=lnew(nwvl, 1);
+	for(int i=0; i<nwvl; i++) P(parms->evl.psfsize, i)=psfsize[i];
+	parms->evl.pttr=lnew(nevl, 1);
+	for(int i=0; i<nevl; i++) P(parms->evl.pttr, i)=pttr;
+	parms->evl.nmod=3;
+	parms->evl.psfmean=nwvl>0;
+	parms->evl.psfisim=0;
+	parms->sim.dt=dt;
+	aper_t* aper=g_eaper=mycalloc(1, aper_t);
+	oref_evl_aper(&aper->locs, &aper->amp, &aper->locfft);
+	gpu_perfevl_init(parms, aper);
+	int n=0;
+	map_t** atm=oref_atm(&n);
+	mapcell* ac=mapcellnew(n, 1);
+	for(int i=0; i<n; i++) P(ac, i)=mapref(atm[i]);
+	gpu_atm2gpu(ac, NULL, parms, 0, 0);
+	cellfree(ac);
+	gpu_perfevl_init_sim(parms, aper);
+	sim_t* simu=g_esim=mycalloc(1, sim_t);
+	simu->parms=parms;
+	simu->aper=aper;
+	simu->olep=dcellnew(nevl, 1);
+	simu->olmp=dcellnew(nevl, 1);
+	for(int i=0; i<nevl; i++){
+		P(simu->olep, i)=dnew(3, nsim);
+		P(simu->olmp, i)=dnew(3, nsim);
+	}
+	return nevl;
+}
+
+/* Frame isim of every direction, queued and synced over two "threads" as the simulator splits
+   the directions; wfe and coeff receive nevl x 3 from simu->olep and simu->olmp. */
+int oadp_evl_frame(int isim, double* wfe, double* coeff){
+	sim_t* simu=g_esim;
+	if(!simu) return -1;
+	const int nevl=simu->parms->evl.nevl;
+	simu->perfisim=isim;
+	const long half=nevl/2;
+	thread_t t[2]={{0}, {0}};
+	t[0].start=0; t[0].end=half; t[0].data=simu;
+	t[1].start=half; t[1].end=nevl; t[1].data=simu;
+	gpu_perfevl_queue(&t[0]);
+	gpu_perfevl_queue(&t[1]);
+	gpu_perfevl_sync(&t[1]);
+	gpu_perfevl_sync(&t[0]);
+	for(int i=0; i<nevl; i++){
+		memcpy(wfe+3*i, PCOL(P(simu->olep, i), isim), sizeof(double)*3);
+		memcpy(coeff+3*i, PCOL(P(simu->olmp, i), isim), sizeof(double)*3);
 	}
 	return 0;
 }

@@ -654,6 +654,10 @@ long oref_evl_setup(double D, double Din, double dx, int nwvl, const double* wvl
 	}
 	return g_elocs->nloc;
 }
+/* The aperture built by oref_evl_setup, for the adapter driver (adapter_driver.c). */
+void oref_evl_aper(loc_t** locs, dmat** amp, locfft_t** locfft){
+	*locs=g_elocs; *amp=g_eamp; *locfft=g_elocfft;
+}
 void oref_evl_get_aper(double* locx, double* locy, double* amp){
 	copy_vec(locx, g_elocs->locx, g_elocs->nloc);
 	copy_vec(locy, g_elocs->locy, g_elocs->nloc);

@@ -1,7 +1,8 @@
 """The MAOS-side adapter compiles against the reference's headers and links.
 
 `maos_b200/csrc/adapter/wfs_b200.c` defines the ten functions of MAOS's GPU wavefront-sensor seam
-(`cuda/sim/gpu_sim.h:35-49`) over the flat ABI of `include/shwfs_b200.h`. This test compiles it with
+and four of its science-evaluation seam (`cuda/sim/gpu_sim.h:35-55`) over the flat ABI of
+`include/shwfs_b200.h` and `include/shwfs_evl.h`. This test compiles it with
 the reference's own `maos/` and `cuda/sim/` headers (the struct layouts and field names it reads),
 with warnings as errors, then links it into a shared object with no undefined symbol allowed against
 `libshwfs_b200.so` and the reference's C compiled as the oracle (`oracle/_ref/libmaosref.so`: the
@@ -18,7 +19,8 @@ REF = "/root/reference"
 ADAPTER = os.path.join(ROOT, "maos_b200", "csrc", "adapter", "wfs_b200.c")
 SEAM = ["gpu_wfsgrad_init", "gpu_wfs_init_sim", "gpu_wfsgrad_update_etf", "gpu_wfsgrad_update_ref",
         "gpu_wfsgrad_seeding", "gpu_wfsgrad_queue", "gpu_wfsgrad_sync", "gpu_save_pistat",
-        "gpu_wfssurf2gpu", "gpu_atm2gpu"]
+        "gpu_wfssurf2gpu", "gpu_atm2gpu", "gpu_perfevl_init", "gpu_perfevl_init_sim",
+        "gpu_perfevl_queue", "gpu_perfevl_sync"]
 
 
 @pytest.fixture(scope="module")
@@ -53,10 +55,11 @@ def test_adapter_defines_the_seam(adapter_so):
 
 
 def test_adapter_calls_only_declared_abi(adapter_so):
-    """Every shwfs_* symbol the adapter needs is one that include/shwfs_b200.h declares."""
+    """Every shwfs_* symbol the adapter needs is one that a header under include/ declares."""
     out = subprocess.run(["nm", "-u", adapter_so], capture_output=True, text=True, check=True).stdout
     used = {ln.split()[-1] for ln in out.splitlines() if ln.split()[-1].startswith("shwfs_")}
-    header = open(os.path.join(ROOT, "include", "shwfs_b200.h")).read()
+    inc = os.path.join(ROOT, "include")
+    header = "".join(open(os.path.join(inc, f)).read() for f in sorted(os.listdir(inc)) if f.endswith(".h"))
     assert used, "the adapter calls no library entry point"
     for s in used:
         assert s + "(" in header, s

@@ -113,3 +113,46 @@ def test_adapter_seeding_keys_the_noise(ref_lib):
     assert not np.array_equal(g1, g3)
     assert np.isfinite(g1).all()
     assert grad_rel_err(g1, g0) > 1e-3
+
+
+@pytest.mark.parametrize("pttr", [0, 1])
+def test_adapter_science_matches_reference(ref_lib, pttr):
+    """gpu_perfevl_init / init_sim / queue / sync on the reference's 8 m science aperture and its
+    PSF grid (locfft), three directions split over two threads: simu->olep (PR, TT, PTTR) and
+    simu->olmp (piston, tip, tilt) of each frame against the reference's loc_calc_ptt on its own
+    ray trace, within 1e-4 relative. The PSF sums run in the same frames."""
+    import math
+    from maos_b200.configs import LGS30
+    from maos_b200.setup import screens
+    from maos_b200.workload import wind
+    as2rad = math.pi / 180 / 3600
+    nx, seed, dt = 1024, 7, 1 / 800
+    cfg = dict(LGS30, atm=dict(LGS30["atm"], nx=nx, dx=1 / 32))
+    at = cfg["atm"]
+    scr = screens(nx, nx, at["dx"], at["r0"], at["L0"], at["wt"], seed)
+    vx, vy = wind(cfg, seed)
+    o = -nx / 2 * at["dx"]
+    layers = [dict(nx=nx, ny=nx, dx=at["dx"], ox=o, oy=o, ht=float(h), vx=float(vx[i]), vy=float(vy[i]),
+                   alpha=1.0) for i, h in enumerate(at["ht"])]
+    ref_lib.atm_set(scr, layers)
+    wvl, nembed, psfsize = [1.25e-6], [512], [128]
+    e = ref_lib.RefEvl(8.0, 1.2, 1 / 32, wvl=wvl, nembed=nembed)
+    dirs = [(0.0, 0.0, math.inf), (20 * as2rad, -10 * as2rad, math.inf), (5 * as2rad, 5 * as2rad, 90e3)]
+    A = _adapter(ref_lib)
+    dp = C.POINTER(C.c_double)
+    A.oadp_evl_init.argtypes = [C.c_int, dp, dp, dp, C.c_int, dp, C.POINTER(C.c_long), C.c_int, C.c_double,
+                                C.c_int]
+    A.oadp_evl_frame.argtypes = [C.c_int, dp, dp]
+    arr = lambda v: np.ascontiguousarray(v, dtype=np.float64)
+    tx, ty, hs = (arr([d[i] for d in dirs]) for i in range(3))
+    w, ps = arr(wvl), np.ascontiguousarray(psfsize, dtype=np.int64)
+    ptr = lambda a: a.ctypes.data_as(dp)
+    assert A.oadp_evl_init(len(dirs), ptr(tx), ptr(ty), ptr(hs), 1, ptr(w), ps.ctypes.data_as(C.POINTER(C.c_long)),
+                           pttr, dt, 16) == len(dirs)
+    wfe, coeff = np.zeros(3 * len(dirs)), np.zeros(3 * len(dirs))
+    for isim in (3, 11):
+        assert A.oadp_evl_frame(isim, ptr(wfe), ptr(coeff)) == 0
+        for k, d in enumerate(dirs):
+            _, wfe_r, coeff_r, _ = e.frame(*d, isim, dt, pttr=pttr, psfsize=psfsize)
+            assert np.all(np.abs(wfe[3 * k:3 * k + 3] - wfe_r) <= 1e-4 * np.abs(wfe_r)), (isim, k)
+            assert np.abs(coeff[3 * k:3 * k + 3] - coeff_r).max() <= 1e-4 * np.abs(coeff_r).max(), (isim, k)
