@@ -285,8 +285,10 @@ int shwfs_copy_counters(shwfs_ctx* ctx, uint64_t* h2d, uint64_t* d2h);
    forbid allocation after start-up, stream capture into a CUDA graph,
    externally managed memory).  ints (nsa*npix) and grad (2*nsa) are device
    pointers owned by the caller; either may be NULL, not both.  Limits: at
-   most SHWFS_NOALLOC_MAX_NSA subapertures of at most 16x16 OPD points;
-   larger WFS are rejected with SHWFS_EINVAL.  The first call on a device
+   most SHWFS_NOALLOC_MAX_NSA subapertures, each of 16x16 OPD points padded
+   to a 32x32 FFT (the 32-point form, at most 128 pixels); any other powfs
+   (64-point and larger FFTs, geometric sensors, dtrat > 1, sigmatch 2) is
+   rejected with SHWFS_EINVAL before anything is launched.  The first call on a device
    looks up the array's device address (cudaGetSymbolAddress), so make it
    before any stream capture.  Calls share the array: calls whose work
    overlaps on the GPU race; queue them on one stream. */

@@ -2127,9 +2127,14 @@ int shwfs_frame_noalloc(shwfs_ctx* ctx, int iwfs, int isim, float* ints, float* 
 	if (p.d.nsa > SHWFS_NOALLOC_MAX_NSA)
 		return fail(ctx, SHWFS_EINVAL, "frame_noalloc: %d subapertures exceed the allocation-free maximum of %d",
 			p.d.nsa, SHWFS_NOALLOC_MAX_NSA);
-	if (p.d.nopd * p.d.nopd > 256)
-		return fail(ctx, SHWFS_EINVAL, "frame_noalloc: %dx%d OPD points per subaperture exceed the maximum of 16x16",
-			p.d.nopd, p.d.nopd);
+	// the scratch offsets, the 32x32 image tile of ints_n32_kernel and the fused
+	// uplink all assume the 32-point form: 16x16 OPD points padded to a 32x32 FFT
+	if (!(p.d.nopd == 16 && p.d.nopd * p.d.embfac == 32 && p.d.notf == 32))
+		return fail(ctx, SHWFS_EINVAL,
+			"frame_noalloc: only 16x16 OPD points with a 32x32 FFT are served (this powfs: n_opd=%d n_w=%d n_f=%d)",
+			p.d.nopd, p.d.nopd * p.d.embfac, p.d.notf);
+	if (p.d.pixpsax * p.d.pixpsay > 128)
+		return fail(ctx, SHWFS_EINVAL, "frame_noalloc: at most 128 pixels per subaperture");
 	int r = set_device(ctx);
 	if (r) return r;
 	if ((r = check_ready(ctx, p, *w))) return r;

@@ -61,3 +61,37 @@ def test_noalloc_rejects_oversized_wfs():
     with pytest.raises(shwfs.ShwfsError, match="exceed the allocation-free maximum"):
         ctx.frame_noalloc(iw, 0, None, grad)  # rejected on the host before any launch
     ctx.close()
+
+
+def _small_powfs(ctx, **over):
+    from maos_b200 import shwfs
+    kw = dict(nsa=4, nopd=16, embfac=2, notf=32, pixpsax=6, pixpsay=6, pixthetax=4.8e-6, pixthetay=4.8e-6,
+              wvl=0.589e-6, dsa=0.5, dx=1 / 32, areascale=1.0, hs=float("inf"), gradtype=shwfs.SHWFS_GRAD_COG,
+              sigmatch=1, saat=0.3, sigtot_cog=500.0)
+    kw.update(over)
+    ip = ctx.powfs_add(**kw)
+    return ip, ctx.wfs_add(ipowfs=ip, hs=float("inf"), sigsim=500.0, wvlwt=1.0)
+
+
+@pytest.mark.parametrize("form", ["fft64_opd16", "fft64_opd8", "dtrat2"])
+def test_noalloc_rejects_other_forms(form):
+    """Only the 32-point form (16x16 OPD points, 32x32 FFT) runs without
+    allocation; a 64-point powfs whose pupil still fits 16x16 points and a
+    powfs integrating over frames are refused on the host, before any launch."""
+    import torch
+    from maos_b200 import shwfs
+    ctx = shwfs.Context(0)
+    if form == "fft64_opd16":
+        ip, iw = _small_powfs(ctx, nopd=16, embfac=4, notf=64)
+        msg = "only 16x16 OPD points with a 32x32 FFT"
+    elif form == "fft64_opd8":
+        ip, iw = _small_powfs(ctx, nopd=8, embfac=8, notf=64)
+        msg = "only 16x16 OPD points with a 32x32 FFT"
+    else:
+        ip, iw = _small_powfs(ctx)
+        ctx.powfs_set_dtrat(ip, 2)
+        msg = "dtrat > 1"
+    grad = torch.zeros(8, dtype=torch.float32, device="cuda")
+    with pytest.raises(shwfs.ShwfsError, match=msg):
+        ctx.frame_noalloc(iw, 0, None, grad)
+    ctx.close()
