@@ -38,6 +38,23 @@ import numpy as np  # noqa: E402
 
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
 
+_OUT_FD = None
+
+
+def emit(line: dict):
+    """Write the one JSON result line to the real standard output.  Everything
+    else the process writes to file descriptor 1 (the reference library's
+    progress messages included) goes to standard error."""
+    fd = _OUT_FD if _OUT_FD is not None else 1
+    os.write(fd, (json.dumps(line) + "\n").encode())
+
+
+def _stdout_to_stderr():
+    global _OUT_FD
+    sys.stdout.flush()
+    _OUT_FD = os.dup(1)
+    os.dup2(2, 1)
+
 
 def _peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -141,111 +158,108 @@ def tc_mma_flops_per_image():
     return tile / 4
 
 
+FFT_BACKEND = ("the oracle's FFT stand-in (oracle/refbuild/fftw_standin.c, FFTW's conventions in double): "
+               "FFTW is absent from this image (no libfftw3 in the dynamic linker cache)")
+
+
+def ref_frame(r, cfg, isim, seed, noisy=True):
+    """One frame of every WFS of the config on the reference's CPU path; seconds."""
+    from oracle import ref
+    dt = cfg.get("dt", 1.0 / 800)
+    return sum(ref.frame_full_mt(r, iwfs, isim, dt, seed=seed * 1000003 + iwfs, noisy=noisy)[2]
+               for iwfs in range(cfg["nwfs"]))
+
+
+def ref_workload(cfg, seed=1):
+    """The reference's own setup and screens of a config (oracle/_ref only):
+    RefPowfs (maos/powfs.c setup), genscreen (lib/turbulence.c) and the same
+    winds as the B200 arm."""
+    from oracle import ref
+    from maos_b200.configs import layers_of
+    ncpu = os.cpu_count() or 1
+    r = ref.RefPowfs(cfg, nthread=ncpu)
+    a = cfg["atm"]
+    scr = ref.genscreen(a["nx"], a["nx"], a["dx"], a["r0"], a["L0"], a["wt"], seed)
+    ref.atm_set(scr, layers_of(cfg, seed))
+    return r, ncpu
+
+
 def cpu_baseline(cfg, wl_layers, screens, seconds=15.0, max_frames=40):
+    """The reference's CPU frame of every WFS, timed on this host's cores for a
+    bounded sample of frames (about `seconds` of CPU work)."""
     from oracle import ref
     ncpu = os.cpu_count() or 1
     r = ref.RefPowfs(cfg, nthread=ncpu)
     ref.atm_set(screens, wl_layers)
-    dt = cfg.get("dt", 1.0 / 800)
-    ref.frame_full_mt(r, 0, 0, dt)  # warm plans and caches
+    ref_frame(r, cfg, 0, 1)  # warm plans and caches
     t = 0.0
     n = 0
     while t < seconds and n < max_frames:
-        _, _, dt_s = ref.frame_full_mt(r, n % cfg["nwfs"], n + 1, dt, seed=n + 1, noisy=True)
-        t += dt_s
+        t += ref_frame(r, cfg, n + 1, n + 1)
         n += 1
-    return {"value": r.nsa * n / t, "unit": "subap-images/s", "cores": ncpu, "kind": "reference",
-            "sample": f"{n} single-WFS frames of {cfg['name']} ({r.nsa} subapertures each): 7-layer ray trace, "
-                      f"LLT uplink, wfsints, addnoise, matched filter; reference C (oracle/_ref), FFT stand-in "
-                      f"for FFTW, NTHREAD={ncpu}"}
+    return {"value": r.nsa * cfg["nwfs"] * n / t, "unit": "subap-images/s", "cores": ncpu, "kind": "reference",
+            "fft_backend": FFT_BACKEND,
+            "sample": f"{n} frames of all {cfg['nwfs']} WFS of {cfg['name']} ({r.nsa} subapertures each): 7-layer "
+                      f"ray trace, LLT uplink, wfsints, addnoise, matched filter; reference C (oracle/_ref), "
+                      f"NTHREAD={ncpu}"}
 
 
 def run_reference(args, cfg):
-    ws, rank, local = dist_init()
-    if rank != 0:
+    """The reference's own CPU path (oracle/_ref: its maos/lib/math/sys C) on the
+    same workload and config as the B200 arm: one step is one frame of every
+    WFS.  Loads no library of this repository."""
+    if int(os.environ.get("RANK", "0")) != 0:
         return 0
     from oracle import ref
-    from maos_b200.setup import screens as mkscreens
-    from maos_b200.workload import wind
+    from maos_b200.configs import workload_desc
     if not ref.available():
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libmaosref.so is not built"}))
+        emit({"impl": "reference", "unavailable": "oracle/_ref/libmaosref.so is not built"})
         return 0
-    ncpu = os.cpu_count() or 1
-    r = ref.RefPowfs(cfg, nthread=ncpu)
-    a = cfg["atm"]
-    n = a["nx"]
-    scr = mkscreens(n, n, a["dx"], a["r0"], a["L0"], a["wt"], 1)
-    vx, vy = wind(cfg, 1)
-    o = -n / 2 * a["dx"]
-    layers = [dict(nx=n, ny=n, dx=a["dx"], ox=o, oy=o, ht=float(h), vx=float(vx[i]), vy=float(vy[i]))
-              for i, h in enumerate(a["ht"])]
-    ref.atm_set(scr, layers)
-    dt = cfg.get("dt", 1.0 / 800)
+    r, ncpu = ref_workload(cfg, seed=1)
     for i in range(args.warmup):
-        ref.frame_full_mt(r, i % cfg["nwfs"], i, dt, seed=i + 1)
-    times = []
-    for k in range(args.steps):
-        _, _, t = ref.frame_full_mt(r, k % cfg["nwfs"], args.warmup + k, dt, seed=k + 7)
-        times.append(t)
+        ref_frame(r, cfg, i, i + 1)
+    times = [ref_frame(r, cfg, args.warmup + k, k + 7) for k in range(args.steps)]
     tot = sum(times)
-    value = r.nsa * args.steps / tot
+    units = r.nsa * cfg["nwfs"]
+    value = units * args.steps / tot
     line = {
         "impl": "reference", "metric": "subaperture images/s", "value": value, "unit": "subap-images/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": cfg["name"], "step": "one single-WFS frame (reference CPU path)"},
+        "config": workload_desc(cfg, r.nsa, r.notf, r.npix),
         "cpu_baseline": {"value": value, "unit": "subap-images/s", "cores": ncpu, "kind": "reference",
-                         "sample": f"{args.steps} single-WFS frames of {cfg['name']} ({r.nsa} subapertures)"},
+                         "fft_backend": FFT_BACKEND,
+                         "sample": f"{args.steps} frames of all {cfg['nwfs']} WFS of {cfg['name']} "
+                                   f"({r.nsa} subapertures each), NTHREAD={ncpu}"},
         "e2e": {"value": value, "unit": "subap-images/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    print(json.dumps(line))
+    emit(line)
     return 0
 
 
-def run_b200(args, cfg):
+def _time_frames(wl, ext, flush, isim, steps):
+    """Device time of `steps` frames (CUDA events on the context stream, L2
+    flushed before each, the flush untimed); returns (per-step ms, next isim)."""
     import torch
-    from maos_b200 import shwfs
-    from maos_b200.workload import build
-    ws, rank, local = dist_init()
-    dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
-    form = shwfs.SHWFS_FORM_TC if args.form == "tc" else shwfs.SHWFS_FORM_FFT
-    wl = build(cfg, device=local, seed=1 + rank, noisy=True, form=form)
-    ctx = wl.ctx
-    nwfs = len(wl.wfs)
-    units_per_step = nwfs * wl.nsa
-    ext = torch.cuda.ExternalStream(ctx.stream, device=dev)
-    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
-    variant = ctx.autotune(wl.wfs[0], wl.wfs[-1] + 1, nrep=5)
-    isim = 0
-    for _ in range(args.warmup):
-        wl.frame(isim)
-        isim += 1
-    ctx.sync()
-    barrier(ws, dev)
-    clk = ClockSampler(local)
-    clk.start()
-    time.sleep(0.5)
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
     with torch.cuda.stream(ext):
-        for k in range(args.steps):
+        for k in range(steps):
             flush.zero_()  # L2 flush between timed steps (not timed)
             starts[k].record(ext)
             wl.frame(isim)
             ends[k].record(ext)
             isim += 1
-    ctx.sync()
-    torch.cuda.synchronize(dev)
-    clocks = clk.stop()
-    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    tot_ms = allreduce_max(sum(step_ms), ws, dev)
-    barrier(ws, dev)
-    value = units_per_step * args.steps * ws / (tot_ms * 1e-3)
+    wl.ctx.sync()
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in zip(starts, ends)], isim
 
-    # stage timing of the same frames (profiled pass, separate from the timed one)
+
+def _stage_profile(wl, ext, flush, isim, nprof):
+    """Per-stage device time of nprof frames (stage events on, separate from the timed frames)."""
+    import torch
+    ctx = wl.ctx
     ctx.profile_enable(True)
-    nprof = min(args.steps, 20)
     with torch.cuda.stream(ext):
         for k in range(nprof):
             flush.zero_()
@@ -254,10 +268,102 @@ def run_b200(args, cfg):
     ctx.sync()
     stages = ctx.profile_read()
     ctx.profile_enable(False)
-    launches_per_step = sum(n for _, n in stages.values()) / nprof
+    st = {k: dict(ms_per_launch=(ms / n if n else 0.0), launches_per_step=n / nprof, ms_per_step=ms / nprof)
+          for k, (ms, n) in stages.items()}
+    return st, sum(n for _, n in stages.values()) / nprof, isim
 
-    # end to end through the C ABI: queue + sync with host gradients each step,
-    # into one host buffer the loop owns (as a C caller passes its own)
+
+def _roofline(form, cfg, wl, st, units_per_step):
+    """Roofline of the form's dominant kernel from its live per-launch time."""
+    hbm, bf16, src = _peaks()
+    src_note = f"{src} (MEASURED_PEAKS.json)" if src == "measured" else "fallback"
+    nwfs = len(wl.wfs)
+    nlayer = len(cfg["atm"]["ht"])
+    ints_bytes, ray_bytes = algorithmic_traffic(cfg, wl.nsa, wl.npix, wl.setup.nopd, wl.setup.notf, nwfs, nlayer)
+    ints_ms = st["ints"]["ms_per_launch"]
+    ray_ms = st["raytrace"]["ms_per_step"]  # the WFS pupils, plus any LLT pupils traced in a second launch
+    ints_gbs = ints_bytes / (ints_ms * 1e-3) / 1e9 if ints_ms else 0.0
+    ray_gbs = ray_bytes / (ray_ms * 1e-3) / 1e9 if ray_ms else 0.0
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            traffic = json.load(f).get(f"{cfg['name']}:{form}:ints")
+    raytrace = {"kernel": "geom_kernel", "bound": "hbm", "achieved": ray_gbs, "peak": hbm, "unit": "GB/s",
+                "frac": ray_gbs / hbm, "algorithmic_bytes_per_launch": ray_bytes,
+                "note": "algorithmic bytes: one 4-byte screen read per point and layer plus the OPD write"}
+    hbm_sub = {"achieved": ints_gbs, "peak": hbm, "unit": "GB/s", "frac": ints_gbs / hbm,
+               "peak_source": src_note + " hbm_gbs", "algorithmic_bytes_per_launch": ints_bytes}
+    if form == "tc":
+        tflops = units_per_step * tc_mma_flops_per_image() / (ints_ms * 1e-3) / 1e12 if ints_ms else 0.0
+        return {"kernel": "ints_tc_kernel (tcgen05 BF16x3 DFT imaging)", "bound": "tensor",
+                "achieved": tflops, "peak": bf16, "unit": "TFLOP/s", "frac": tflops / bf16,
+                "peak_source": src_note + " bf16_tflops, burst", "traffic": traffic,
+                "flops_per_launch": units_per_step * tc_mma_flops_per_image(),
+                "hbm": hbm_sub, "post": {"kernel": "noise_grad_kernel", "ms_per_launch": st["post"]["ms_per_launch"]},
+                "raytrace": raytrace}
+    flops = fft_flops_per_image(wl.setup.notf) * units_per_step
+    fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal FP32 CUDA-core peak, TFLOP/s
+    ints_tf = flops / (ints_ms * 1e-3) / 1e12 if ints_ms else 0.0
+    if wl.setup.notf == 64:
+        kname = "ints_n64_kernel (fused imaging, noise, gradients; half-spectrum transforms)"
+    else:
+        kname = "ints_n32_kernel (fused imaging, noise, gradients)"
+    return {"kernel": kname, "bound": "fp32", "achieved": ints_tf, "peak": fp32_peak, "unit": "TFLOP/s",
+            "frac": ints_tf / fp32_peak, "traffic": traffic,
+            "peak_source": "nominal FP32 CUDA-core peak (148 SM x 128 lanes x 2 x 1.965 GHz); no measured FP32 peak",
+            "flops_per_launch": flops,
+            "note": "nominal FFT flops (3 x 5 N^2 log2 N^2 per image); the kernel issues FP32 work and moves its "
+                    "algorithmic bytes well below the HBM roof (sub-object hbm)",
+            "hbm": hbm_sub, "raytrace": raytrace}
+
+
+def run_b200(args, cfg):
+    """Both imaging forms on one workload: the plain FP32 FFT form and the
+    tensor-core BF16x3 DFT form; the line's value is the faster form's."""
+    import torch
+    from maos_b200 import shwfs
+    from maos_b200.configs import workload_desc
+    from maos_b200.workload import build
+    ws, rank, local = dist_init()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    wl = build(cfg, device=local, seed=1 + rank, noisy=True, form=shwfs.SHWFS_FORM_FFT)
+    ctx = wl.ctx
+    nwfs = len(wl.wfs)
+    units_per_step = nwfs * wl.nsa
+    ext = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    variant = ctx.autotune(wl.wfs[0], wl.wfs[-1] + 1, nrep=5)
+    forms = [args.form] if args.form != "both" else ["fft", "tc"]
+    isim = 0
+    res = {}
+    clk = ClockSampler(local)
+    clk.start()
+    for form in forms:
+        ctx.set_form(shwfs.SHWFS_FORM_TC if form == "tc" else shwfs.SHWFS_FORM_FFT)
+        for _ in range(args.warmup):
+            wl.frame(isim)
+            isim += 1
+        ctx.sync()
+        barrier(ws, dev)
+        if not res:
+            time.sleep(0.5)
+        step_ms, isim = _time_frames(wl, ext, flush, isim, args.steps)
+        tot_ms = allreduce_max(sum(step_ms), ws, dev)
+        barrier(ws, dev)
+        st, lps, isim = _stage_profile(wl, ext, flush, isim, min(args.steps, 20))
+        res[form] = dict(value=units_per_step * args.steps * ws / (tot_ms * 1e-3), tot_ms=tot_ms, step_ms=step_ms,
+                         stages=st, launches_per_step=lps, roofline=_roofline(form, cfg, wl, st, units_per_step))
+    clocks = clk.stop()
+    best = max(forms, key=lambda f: res[f]["value"])
+    ctx.set_form(shwfs.SHWFS_FORM_TC if best == "tc" else shwfs.SHWFS_FORM_FFT)
+    # end to end through the C ABI in the headline form: queue + sync with host
+    # gradients each step, into one host buffer the loop owns (as a C caller passes its own)
+    for _ in range(args.warmup):
+        wl.frame(isim)
+        isim += 1
+    wl.frame_sync()
     ctx.copy_counters()
     gbuf = np.empty(sum(2 * ctx.wfs_nsa[i] for i in wl.wfs))
     e2e_s = 0.0
@@ -273,84 +379,36 @@ def run_b200(args, cfg):
     h2d, d2h = ctx.copy_counters()
     e2e_s = allreduce_max(e2e_s, ws, dev)
     e2e = units_per_step * args.steps * ws / e2e_s
-
-    # roofline of the dominant kernel
-    hbm, bf16, src = _peaks()
-    nlayer = len(cfg["atm"]["ht"])
-    ints_bytes, ray_bytes = algorithmic_traffic(cfg, wl.nsa, wl.npix, wl.setup.nopd, wl.setup.notf, nwfs, nlayer)
-    st = {k: dict(ms_per_launch=(ms / n if n else 0.0), launches_per_step=n / nprof, ms_per_step=ms / nprof)
-          for k, (ms, n) in stages.items()}
-    ints_ms = st["ints"]["ms_per_launch"]
-    ray_ms = st["raytrace"]["ms_per_step"]  # the WFS pupils, plus any LLT pupils traced in a second launch
-    ints_gbs = ints_bytes / (ints_ms * 1e-3) / 1e9 if ints_ms else 0.0
-    ray_gbs = ray_bytes / (ray_ms * 1e-3) / 1e9 if ray_ms else 0.0
-    flops = fft_flops_per_image(wl.setup.notf) * units_per_step
-    fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal FP32 CUDA-core peak, TFLOP/s
-    ints_tf = flops / (ints_ms * 1e-3) / 1e12 if ints_ms else 0.0
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tp):
-        with open(tp) as f:
-            traffic = json.load(f).get(f"{cfg['name']}:{args.form}:ints")
-    src_note = f"{src} (MEASURED_PEAKS.json)" if src == "measured" else "fallback"
-    raytrace = {"kernel": "geom_kernel", "achieved": ray_gbs, "peak": hbm, "unit": "GB/s", "frac": ray_gbs / hbm,
-                "algorithmic_bytes_per_launch": ray_bytes}
-    if args.form == "tc":
-        tflops = units_per_step * tc_mma_flops_per_image() / (ints_ms * 1e-3) / 1e12 if ints_ms else 0.0
-        post_ms = st["post"]["ms_per_launch"]
-        roofline = {"kernel": "ints_tc_kernel (tcgen05 BF16x3 DFT imaging)", "bound": "tensor",
-                    "achieved": tflops, "peak": bf16, "unit": "TFLOP/s", "frac": tflops / bf16,
-                    "peak_source": src_note + " bf16_tflops, burst", "traffic": traffic,
-                    "flops_per_launch": units_per_step * tc_mma_flops_per_image(),
-                    "hbm": {"achieved": ints_gbs, "peak": hbm, "unit": "GB/s", "frac": ints_gbs / hbm,
-                            "algorithmic_bytes_per_launch": ints_bytes},
-                    "post": {"kernel": "noise_grad_kernel", "ms_per_launch": post_ms},
-                    "raytrace": raytrace}
-    else:
-        if wl.setup.notf == 64:
-            kname = "ints_n64_kernel (fused imaging, noise, gradients; half-spectrum transforms)"
-            knote = ("the kernel moves its algorithmic bytes at this rate but is bound by shared-memory traffic "
-                     "and issue (ncu: issue active 66 %, L1/shared 73 %, HBM 3 %); compute gives its FFT flop rate")
-        else:
-            kname = "ints_n32_kernel (fused imaging, noise, gradients)"
-            knote = ("the kernel moves its algorithmic bytes at this rate but is bound by FP32 issue "
-                     "(ncu: issue active 61 %, HBM 5 %); compute gives its FFT flop rate")
-        roofline = {"kernel": kname, "bound": "hbm",
-                    "achieved": ints_gbs, "peak": hbm, "unit": "GB/s", "frac": ints_gbs / hbm,
-                    "peak_source": src_note + " hbm_gbs", "traffic": traffic,
-                    "note": knote,
-                    "algorithmic_bytes_per_launch": ints_bytes,
-                    "compute": {"achieved": ints_tf, "peak": fp32_peak, "unit": "TFLOP/s",
-                                "frac": ints_tf / fp32_peak,
-                                "note": "nominal FFT flops (3 x 5 N^2 log2 N^2 per image) vs nominal FP32 CUDA-core peak"},
-                    "raytrace": raytrace}
-    p50 = float(np.percentile(step_ms, 50))
-    p99 = float(np.percentile(step_ms, 99))
+    head = res[best]
     line = {
-        "metric": "subaperture images/s", "value": value, "unit": "subap-images/s", "n_gpus": ws,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": cfg["name"], "wfs": nwfs, "subapertures_per_wfs": wl.nsa,
-                   "fft": wl.setup.notf, "pixels": f"{wl.setup.npix}", "layers": nlayer,
-                   "screen": f"{cfg['atm']['nx']}^2 FP32", "form": args.form, "noise": True,
-                   "gradients": "matched filter" if cfg["phytype"] == 1 else "CoG",
-                   "imaging_variant": variant,
-                   "l2": "flushed (256 MiB write) before every timed step", "parallelism": f"replicas x{ws}"},
-        "frame_latency_ms": {"p50": p50, "p99": p99},
-        "stages": st,
-        "gpu_launches": int(round(launches_per_step * args.steps)),
+        "metric": "subaperture images/s", "value": head["value"], "unit": "subap-images/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["tot_ms"] / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_desc(cfg, wl.nsa, wl.setup.notf, wl.npix),
+        "form": best, "imaging_variant": variant, "noise": True,
+        "l2": "flushed (256 MiB write) before every timed step", "parallelism": f"replicas x{ws}",
+        "frame_latency_ms": {"p50": float(np.percentile(head["step_ms"], 50)),
+                             "max": float(np.max(head["step_ms"])),
+                             "note": "device time per frame over the timed steps (the serving loop's p99 is its own "
+                                     "bench mode)"},
+        "stages": head["stages"],
+        "gpu_launches": int(round(head["launches_per_step"] * args.steps)),
         "e2e": {"value": e2e, "unit": "subap-images/s", "h2d_bytes_per_step": h2d // args.steps,
-                "d2h_bytes_per_step": d2h // args.steps},
-        "roofline": roofline,
+                "d2h_bytes_per_step": d2h // args.steps, "form": best},
+        "roofline": head["roofline"],
         "clocks": clocks,
     }
+    if len(forms) == 2:
+        line["forms"] = {f: {"value": res[f]["value"], "ms_per_step": res[f]["tot_ms"] / args.steps,
+                             "stages": res[f]["stages"], "roofline": res[f]["roofline"]} for f in forms}
+        line["tc_over_fft"] = res["tc"]["value"] / res["fft"]["value"]
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(cfg, wl.layers, wl.screens)
         except Exception as e:  # the oracle library may be absent on a foreign host
             line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
     if rank == 0:
-        print(json.dumps(line))
+        emit(line)
     wl.close()
     if ws > 1:
         import torch.distributed as dist
@@ -366,7 +424,8 @@ def run_batch(args, bcfg):
     ws, rank, local = dist_init()
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    form = shwfs.SHWFS_FORM_TC if args.form == "tc" else shwfs.SHWFS_FORM_FFT
+    form_name = "tc" if args.form == "tc" else "fft"
+    form = shwfs.SHWFS_FORM_TC if form_name == "tc" else shwfs.SHWFS_FORM_FFT
     wl = build_batch(bcfg["members"], device=local, seed=1 + rank, noisy=True, form=form, graph=True)
     ctx = wl.ctx
     units_per_step = wl.images_per_frame
@@ -446,7 +505,7 @@ def run_batch(args, bcfg):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": bcfg["name"], "members": members, "layers": nlayer,
-                   "screen": f"{lcfg['atm']['nx']}^2 FP32", "form": args.form, "noise": True,
+                   "screen": f"{lcfg['atm']['nx']}^2 FP32", "form": form_name, "noise": True,
                    "frame": "one CUDA graph per frame, one branch per sensor type", "imaging_variant": variant,
                    "l2": "flushed (256 MiB write) before every timed step", "parallelism": f"replicas x{ws}"},
         "frame_latency_ms": {"p50": p50, "p99": p99},
@@ -467,7 +526,7 @@ def run_batch(args, bcfg):
         except Exception as e:
             line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
     if rank == 0:
-        print(json.dumps(line))
+        emit(line)
     wl.close()
     if ws > 1:
         import torch.distributed as dist
@@ -517,7 +576,7 @@ def run_serving(args):
         "clocks": clocks,
     }
     if rank == 0:
-        print(json.dumps(line))
+        emit(line)
     return 0
 
 
@@ -575,35 +634,32 @@ def science_cpu(scfg, layers, scr, seconds=20.0, max_frames=4):
 
 def run_science(args, scfg):
     """Science path: every direction of a frame (ray trace, WFE, PSFs)."""
+    if args.impl == "reference":
+        if int(os.environ.get("RANK", "0")) != 0:
+            return 0
+        from oracle import ref
+        from maos_b200.configs import layers_of
+        at = scfg["atm"]
+        n = at["nx"]
+        scr = ref.genscreen(n, n, at["dx"], at["r0"], at["L0"], at["wt"], 1)
+        layers = layers_of(scfg, 1)
+        v, nfr, cores = science_cpu(scfg, layers, scr, seconds=30.0, max_frames=max(args.steps, 1))
+        sample = (f"{nfr} direction-frames of {scfg['name']}: prop of 7 layers onto aper->locs, loc_calc_ptt, "
+                  f"locfft_psf at 3 wavelengths (reference C, FFT stand-in for FFTW)")
+        emit({"impl": "reference", "metric": "science direction-frames/s", "value": v,
+              "unit": "direction-frames/s", "n_gpus": args.gpus, "steps": nfr, "warmup": 0,
+              "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
+              "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+              "config": {"workload": scfg["name"], "step": "one direction-frame (reference CPU path)"},
+              "cpu_baseline": {"value": v, "unit": "direction-frames/s", "cores": cores,
+                               "kind": "reference", "sample": sample},
+              "e2e": {"value": v, "unit": "direction-frames/s", "h2d_bytes_per_step": 0,
+                      "d2h_bytes_per_step": 0}})
+        return 0
     import torch
     ws, rank, local = dist_init()
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    if args.impl == "reference":
-        if rank != 0:
-            return 0
-        from maos_b200.setup import screens
-        from maos_b200.workload import wind
-        at = scfg["atm"]
-        n = at["nx"]
-        scr = screens(n, n, at["dx"], at["r0"], at["L0"], at["wt"], 1)
-        vx, vy = wind(scfg, 1)
-        o = -n / 2 * at["dx"]
-        layers = [dict(nx=n, ny=n, dx=at["dx"], ox=o, oy=o, ht=float(h), vx=float(vx[i]), vy=float(vy[i]))
-                  for i, h in enumerate(at["ht"])]
-        v, nfr, cores = science_cpu(scfg, layers, scr, seconds=30.0, max_frames=max(args.steps, 1))
-        sample = (f"{nfr} direction-frames of {scfg['name']}: prop of 7 layers onto aper->locs, loc_calc_ptt, "
-                  f"locfft_psf at 3 wavelengths (reference C, FFT stand-in for FFTW)")
-        print(json.dumps({"impl": "reference", "metric": "science direction-frames/s", "value": v,
-                          "unit": "direction-frames/s", "n_gpus": args.gpus, "steps": nfr, "warmup": 0,
-                          "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
-                          "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                          "config": {"workload": scfg["name"], "step": "one direction-frame (reference CPU path)"},
-                          "cpu_baseline": {"value": v, "unit": "direction-frames/s", "cores": cores,
-                                           "kind": "reference", "sample": sample},
-                          "e2e": {"value": v, "unit": "direction-frames/s", "h2d_bytes_per_step": 0,
-                                  "d2h_bytes_per_step": 0}}))
-        return 0
     ctx, nloc, layers, scr, npts_traced = _science_ctx(scfg, local, 1 + rank)
     nevl = len(scfg["dirs"])
     ext = torch.cuda.ExternalStream(ctx.stream, device=dev)
@@ -702,7 +758,7 @@ def run_science(args, scfg):
         except Exception as e:
             line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
     if rank == 0:
-        print(json.dumps(line))
+        emit(line)
     ctx.close()
     if ws > 1:
         import torch.distributed as dist
@@ -717,10 +773,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="lgs30_6x60x60_mf")
-    ap.add_argument("--form", default="fft", choices=["fft", "tc"])
+    ap.add_argument("--form", default="both", choices=["both", "fft", "tc"],
+                    help="imaging form(s) to time; both: the FFT and tensor-core forms, value = the faster")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=0.5, help="serving: seconds of requests per rate")
     args = ap.parse_args()
+    _stdout_to_stderr()
     from maos_b200.configs import CONFIGS, BATCHES, SCIENCE
     if args.warmup < 3:
         args.warmup = 3
@@ -728,7 +786,7 @@ def main():
         return run_science(args, SCIENCE[args.config])
     if args.config == "serving_32sims":
         if args.impl == "reference":
-            print(json.dumps({"impl": "reference", "unavailable": "the reference has no serving loop"}))
+            emit({"impl": "reference", "unavailable": "the reference has no serving loop"})
             return 0
         return run_serving(args)
     if args.config in BATCHES:

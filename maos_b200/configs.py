@@ -129,3 +129,41 @@ SCIENCE = {SCIENCE30["name"]: SCIENCE30}
 # two tip-tilt sensors (FFT 256) in one frame, on the LGS30 atmosphere.
 UNEVEN_BATCH = dict(name="uneven_batch_lgs6_ngs1_tt2", members=[LGS30, NGS30_2X2, TT30])
 BATCHES = {UNEVEN_BATCH["name"]: UNEVEN_BATCH}
+
+
+def wind(cfg: dict, seed: int):
+    """Per-layer wind vectors (vx, vy): speeds from the config, directions
+    from a seeded generator unless the config fixes them."""
+    import numpy as np
+    a = cfg["atm"]
+    rng = np.random.default_rng(seed)
+    nl = len(a["ht"])
+    if a.get("wdir_deg") is not None:
+        ang = np.deg2rad(np.asarray(a["wdir_deg"], dtype=float))
+    else:
+        ang = rng.uniform(0, 2 * math.pi, nl)
+    ws = np.asarray(a["ws"], dtype=float)
+    return ws * np.cos(ang), ws * np.sin(ang)
+
+
+def layers_of(cfg: dict, seed: int, nx: int = None):
+    """Layer descriptors (screen size and origin, height, wind) of a config's
+    atmosphere on nx x nx screens centred on the telescope."""
+    a = cfg["atm"]
+    n = nx or a["nx"]
+    dx = a["dx"]
+    vx, vy = wind(cfg, seed)
+    o = -n / 2 * dx
+    return [dict(nx=n, ny=n, dx=dx, ox=o, oy=o, ht=float(h), vx=float(vx[i]), vy=float(vy[i]), alpha=1.0)
+            for i, h in enumerate(a["ht"])]
+
+
+def workload_desc(cfg: dict, nsa: int, notf: int, npix: int) -> dict:
+    """The workload of one frame of a config, as both bench arms name it."""
+    a = cfg["atm"]
+    return {"workload": cfg["name"], "wfs": cfg["nwfs"], "subapertures_per_wfs": nsa, "fft": notf,
+            "pixels": npix, "layers": len(a["ht"]), "screen": f"{a['nx']}^2",
+            "photons": cfg["siglev"], "read_noise_e": cfg["rne"],
+            "gradients": "matched filter" if cfg["phytype"] == 1 else "CoG",
+            "step": f"one frame of all {cfg['nwfs']} WFS: ray trace, uplink, imaging, noise, gradients"}
+

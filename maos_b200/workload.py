@@ -15,6 +15,7 @@ from typing import List
 import numpy as np
 
 from . import shwfs
+from .configs import layers_of, wind  # noqa: F401  (wind is re-exported)
 from .setup import Setup, screens
 
 
@@ -53,19 +54,6 @@ class Workload:
         self.setup.close()
 
 
-def wind(cfg: dict, seed: int):
-    """Per-layer wind vectors: speeds from the config, directions seeded."""
-    a = cfg["atm"]
-    rng = np.random.default_rng(seed)
-    nl = len(a["ht"])
-    if a.get("wdir_deg") is not None:
-        ang = np.deg2rad(np.asarray(a["wdir_deg"], dtype=float))
-    else:
-        ang = rng.uniform(0, 2 * math.pi, nl)
-    ws = np.asarray(a["ws"], dtype=float)
-    return ws * np.cos(ang), ws * np.sin(ang)
-
-
 def build(cfg: dict, device: int = 0, seed: int = 1, noisy: bool = True, nx: int = None,
           form: int = shwfs.SHWFS_FORM_FFT) -> Workload:
     return build_from_setup(cfg, Setup(cfg), device=device, seed=seed, noisy=noisy, nx=nx, form=form)
@@ -87,12 +75,8 @@ def build_from_setup(cfg: dict, setup: Setup, device: int = 0, seed: int = 1, no
         wl.append(i)
     a = cfg["atm"]
     n = nx or a["nx"]
-    dx = a["dx"]
-    scr = screens(n, n, dx, a["r0"], a["L0"], a["wt"], seed)
-    vx, vy = wind(cfg, seed)
-    o = -n / 2 * dx
-    layers = [dict(nx=n, ny=n, dx=dx, ox=o, oy=o, ht=float(h), vx=float(vx[i]), vy=float(vy[i]), alpha=1.0)
-              for i, h in enumerate(a["ht"])]
+    scr = screens(n, n, a["dx"], a["r0"], a["L0"], a["wt"], seed)
+    layers = layers_of(cfg, seed, n)
     ctx.atm_set(layers, scr)
     return Workload(cfg=cfg, ctx=ctx, setup=setup, ipowfs=ip, wfs=wl, layers=layers, screens=scr)
 
@@ -162,11 +146,7 @@ def build_batch(cfgs, device: int = 0, seed: int = 1, noisy: bool = True, nx: in
         members.append((cfg, setup, ip, wl))
     a = cfgs[0]["atm"]
     n = nx or a["nx"]
-    dx = a["dx"]
-    scr = screens(n, n, dx, a["r0"], a["L0"], a["wt"], seed)
-    vx, vy = wind(cfgs[0], seed)
-    o = -n / 2 * dx
-    layers = [dict(nx=n, ny=n, dx=dx, ox=o, oy=o, ht=float(h), vx=float(vx[i]), vy=float(vy[i]), alpha=1.0)
-              for i, h in enumerate(a["ht"])]
+    scr = screens(n, n, a["dx"], a["r0"], a["L0"], a["wt"], seed)
+    layers = layers_of(cfgs[0], seed, n)
     ctx.atm_set(layers, scr)
     return BatchWorkload(ctx=ctx, members=members, layers=layers, screens=scr, graph=graph)

@@ -300,6 +300,17 @@ def genatm_simple(r0, L0, slope, dx, n, seed):
     return out.reshape(n, n)
 
 
+def genscreen(nx, ny, dx, r0, L0, wt, seed):
+    """Von Karman screens from the reference's genscreen: a list of (ny, nx) arrays, one per weight."""
+    n = len(wt)
+    outs = [np.zeros((ny, nx)) for _ in range(n)]
+    ptrs = (C.c_void_p * n)(*[o.ctypes.data for o in outs])
+    w = np.ascontiguousarray(wt, dtype=np.float64)
+    lib().oref_genscreen(C.c_int(n), C.c_long(nx), C.c_long(ny), C.c_double(dx), C.c_double(r0), C.c_double(L0),
+                         _p(w), C.c_uint(int(seed) & 0xFFFFFFFF), ptrs)
+    return outs
+
+
 class RefEvl:
     """The reference's science aperture and open-loop evaluation (setup_aper
     for an annulus; prop onto aper->locs, loc_calc_ptt, locfft_psf)."""

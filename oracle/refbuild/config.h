@@ -17,7 +17,10 @@
 #define MAC_INTEGRATION 0
 #define COMPILER "gcc"
 #define LDSUFFIX "so"
-#define SRCDIR "/root/reference"
+/* SRCDIR (the reference tree) comes from the oracle Makefile's REF */
+#ifndef SRCDIR
+#define SRCDIR "."
+#endif
 #define BUILDDIR "/tmp"
 #define DEBUG 0
 #define PACKAGE_VERSION "oracle"

@@ -354,6 +354,25 @@ void oref_genatm_simple(double r0, double L0, double slope, double dx, long n, u
 	dfree(s);
 }
 
+/* Von Karman screens of nlayer layers with weights wt from one seed, made by the
+   reference's genscreen (lib/turbulence.c:214, spect_screen_do :70-168): the
+   layers come in pairs from one complex transform, every layer with outer
+   scale L0.  out[i] receives the nx*ny values of layer i (x fastest). */
+void oref_genscreen(int nlayer, long nx, long ny, double dx, double r0, double L0, const double* wt,
+	unsigned int seed, double* const* out){
+	rand_t rstat;
+	seed_rand(&rstat, seed);
+	real* w=mycalloc(nlayer, real);
+	real* l0=mycalloc(nlayer, real);
+	for(int i=0; i<nlayer; i++){ w[i]=wt[i]; l0[i]=L0; }
+	genatm_t cfg={&rstat, w, r0, l0, dx, 0, 0, -11./3., nx, ny, nlayer, 0, 0, 0, 0};
+	mapcell* screens=genscreen(&cfg);
+	for(int i=0; i<nlayer; i++) copy_vec(out[i], P(P(screens, i)), nx*ny);
+	cellfree(screens);
+	free(w);
+	free(l0);
+}
+
 /* Uniform and normal draws from the reference's RNG, for checking a restatement. */
 void oref_rand_stream(unsigned int seed, long n, double* u, double* g, long* pois, double pois_mean){
 	rand_t rstat;

@@ -151,7 +151,8 @@ def test_gzip_and_multiple_arrays(tmp_path):
 
 def test_reference_data_file_reads(ref_lib):
     """A data file shipped with the reference, when its tree is present."""
-    p = "/root/reference/config/maos/bin/NapMean.bin"
+    from oracle import REF_TREE
+    p = os.path.join(REF_TREE, "config", "maos", "bin", "NapMean.bin")
     if not os.path.exists(p):
         pytest.skip("reference tree absent")
     from maos_b200.binio import read_bin

@@ -15,7 +15,7 @@ import subprocess
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF = "/root/reference"
+from oracle import REF_TREE as REF
 ADAPTER = os.path.join(ROOT, "maos_b200", "csrc", "adapter", "wfs_b200.c")
 SEAM = ["gpu_wfsgrad_init", "gpu_wfs_init_sim", "gpu_wfsgrad_update_etf", "gpu_wfsgrad_update_ref",
         "gpu_wfsgrad_seeding", "gpu_wfsgrad_queue", "gpu_wfsgrad_sync", "gpu_save_pistat",

@@ -60,6 +60,19 @@ def test_screen_generator_bit_exact_and_kat(ref_lib):
     assert abs(np.sqrt((b ** 2).mean()) * 1e9 - 169.648) < 1e-3
 
 
+def test_seven_layer_screens_bit_exact(ref_lib):
+    """The 7-layer atmosphere of the LGS configs against the reference's own
+    genscreen (lib/turbulence.c:214) from the same seed: every layer equal."""
+    from maos_b200.configs import LGS30
+    from maos_b200.setup import screens
+    a = LGS30["atm"]
+    ref = ref_lib.genscreen(128, 128, a["dx"], a["r0"], a["L0"], a["wt"], 3)
+    own = screens(128, 128, a["dx"], a["r0"], a["L0"], a["wt"], 3)
+    assert len(ref) == len(own) == 7
+    for x, y in zip(ref, own):
+        assert np.array_equal(x, y)
+
+
 def test_two_layer_screens_pairing(ref_lib):
     """Layers come in pairs from one complex transform (real, imaginary)."""
     from maos_b200.setup import screens
