@@ -190,6 +190,42 @@ int shwfs_wfs_seed(shwfs_ctx* ctx, int iwfs, uint64_t seed);
    host screens converted to FP32 device screens (screens[i] has nx*ny). */
 int shwfs_atm_set(shwfs_ctx* ctx, int nlayer, const shwfs_layer_desc* layers, const double* const* screens);
 
+/* ---- closed loop and static surfaces (maos/wfsgrad.c:200-262,
+        cuda/sim/wfsgrad.cu:531-605) ---- */
+/* Deformable-mirror surfaces (gpu_dmreal2gpu, cuda/sim/atm.cu:315): ndm grids
+   (x fastest, FP64 host values stored FP32) with their sampling, origin,
+   conjugation height and weight alpha (-1 subtracts the mirror, as
+   mapcell2loc(..., -1) does at cuda/sim/wfsgrad.cu:564-567; vx, vy are
+   ignored).  A WFS that uses them (shwfs_wfs_set_opd_terms) traces them after
+   the turbulence with its cone and misregistration, without wind and without
+   wrap: a point whose bilinear cell leaves a grid gets nothing from it
+   (map2loc_linear, cuda/sim/accphi.cu:24-38).  The first call allocates the
+   grids; later calls with the same sizes only copy the new surfaces,
+   asynchronously on the context stream (counted by shwfs_copy_counters), and
+   apply to the frames queued after them.  ndm = 0 removes the mirrors.  The
+   layers and mirrors together are at most 16. */
+int shwfs_dm_set(shwfs_ctx* ctx, int ndm, const shwfs_layer_desc* dms, const double* const* surfaces);
+/* Per-WFS terms of the OPD of the frames queued from now on (they persist
+   until changed):
+     use_dm     subtract the mirror grids of shwfs_dm_set (sim.closeloop);
+     ptt        ptt[0] + ptt[1] x + ptt[2] y on the pupil points (loc_add_ptt,
+                math/loc.c:762-789): -ttmreal and -fsmreal in closed loop,
+                the telescope wind shake; NULL for none;
+     focus_tel  f (x^2 + y^2) less its mean over the pupil points
+                (loc_add_focus, math/loc.c:1247): -telfocusreal;
+     focus_llt  the same about the LLT position llt_ox, llt_oy of the powfs
+                descriptor (loc_add_focus_offset, math/loc.c:1226-1246):
+                zoomfocusadj (maos/utils.c:865-879);
+     lltptt     tip/tilt of the LLT pupil (wfsgrad_llt_tt,
+                maos/wfsgrad.c:89-116, added at :373-377); NULL for none.
+   LLT tip/tilt on a powfs without an LLT is refused. */
+int shwfs_wfs_set_opd_terms(shwfs_ctx* ctx, int iwfs, int use_dm, const double* ptt, double focus_tel,
+	double focus_llt, const double* lltptt);
+/* Static surface added to WFS iwfs's OPD every frame (powfs.opdadd[wfsind],
+   maos/wfsgrad.c:230-233; gpu_wfssurf2gpu, cuda/sim/wfsinit.cu:514-524):
+   nsa*nopd^2 FP64 values on the pupil points, or NULL to remove it. */
+int shwfs_wfs_set_opdadd(shwfs_ctx* ctx, int iwfs, const double* opd);
+
 /* Imaging form used by the frame calls (default SHWFS_FORM_FFT). */
 int shwfs_set_form(shwfs_ctx* ctx, int form);
 /* Wind shift time step: frame isim shifts layer l by -v*dt*isim. */

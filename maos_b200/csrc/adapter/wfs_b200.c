@@ -14,14 +14,19 @@
  *   gpu_atm2gpu             cuda/sim/atm.cu:106       turbulence screens
  *   gpu_wfsgrad_queue       cuda/sim/wfsgrad.cu:483   queue the frame of info->start..end
  *   gpu_wfsgrad_sync        cuda/sim/wfsgrad.cu:747   gradients into simu->gradcl
- *   gpu_wfs_init_sim, gpu_save_pistat, gpu_wfssurf2gpu: no device state to reset, and the
- *                           pistat diagnostics and NCPA surfaces are not on this path.
+ *   gpu_dmreal2gpu          cuda/sim/atm.cu:315       DM surfaces, subtracted in closed loop
+ *   gpu_wfssurf2gpu         cuda/sim/wfsinit.cu:514   NCPA surfaces (powfs.opdadd)
+ *   gpu_wfs_init_sim, gpu_save_pistat: no device state to reset; pistatout is refused.
+ *   gpu_dmproj2gpu: DM-projected turbulence (idealwfs, wfsalias) is refused.
  *   gpu_perfevl_init, gpu_perfevl_init_sim, gpu_perfevl_queue, gpu_perfevl_sync
  *                           cuda/sim/perfevl.cu: the open-loop science evaluation (olep, olmp
  *                           and the PSF sums); DM terms are refused.
  *
  * The reference aborts on errors (error()); a nonzero status from the library is reported the
- * same way, with the library's message. One context serves every WFS. The simulator queues and
+ * same way, with the library's message.  Options of the reference's WFS path that the library
+ * does not serve (several wavelengths, sodium sublayers, per-WFS amplitude maps, cubic DMs,
+ * MOAO, field stops, dithering, ...) are refused with error() at gpu_wfsgrad_init, so the
+ * adapter never returns gradients that differ from MAOS's in silence. One context serves every WFS. The simulator queues and
  * syncs WFS from several host threads at once, and calls on one context must not overlap, so
  * every call goes through one mutex.
  */
@@ -32,7 +37,13 @@
 #include "shwfs_evl.h"
 
 static shwfs_ctx* g_ctx;
-static int g_ipowfs[64];   /* MAOS ipowfs -> context powfs */
+static int g_ipowfs[64];   /* MAOS ipowfs -> context powfs (physical optics, or the geometric sensor) */
+static int g_ipowfs_geo[64];/* MAOS ipowfs -> context geometric powfs before phystep, or -1 */
+static int* g_wfs_phy;     /* MAOS iwfs -> context WFS with physical optics, or -1 */
+static int* g_wfs_geo;     /* MAOS iwfs -> context geometric WFS, or -1 */
+static int* g_wfs_cur;     /* MAOS iwfs -> the context WFS its last queued frame ran, or -1 */
+static int g_nwfs;
+static int g_ndm;          /* mirror grids held by the context (gpu_dmreal2gpu) */
 static pthread_mutex_t g_lock=PTHREAD_MUTEX_INITIALIZER;
 
 static shwfs_ctx* g_evl;   /* science path (gpu_perfevl_*): a context of its own */
@@ -73,18 +84,122 @@ static void set_etf(const powfs_t* p, int ip, const etf_t* etf, int slot){
 /* intstat->mtche is nsa x nwfs cells of 2 x npix; pack the WFS's column subaperture-major. */
 static void set_mtche(const parms_t* parms, const powfs_t* p, int ip, int iwfs){
 	const intstat_t* st=p->intstat;
-	if(!st || !st->mtche) return;
+	if(!st || !st->mtche || g_wfs_phy[iwfs]<0) return;
 	const long wfsind=P(parms->powfs[ip].wfsind, iwfs);
 	const long nsa=p->saloc->nloc, npix=(long)p->pixpsax*p->pixpsay;
 	const long icol=NY(st->mtche)>1?wfsind:0;
 	dmat* mt=dnew(2*npix, nsa);
 	for(long isa=0; isa<nsa; isa++) memcpy(PCOL(mt, isa), P(P(st->mtche, isa, icol)), sizeof(real)*2*npix);
 	const long ii0=NY(st->i0sum)>1?wfsind:0;
-	chk(shwfs_wfs_set_mtche(g_ctx, iwfs, P(mt), PCOL(st->i0sum, ii0), P(st->i0sumsum, ii0)), "set_mtche");
+	chk(shwfs_wfs_set_mtche(g_ctx, g_wfs_phy[iwfs], P(mt), PCOL(st->i0sum, ii0), P(st->i0sumsum, ii0)),
+		"set_mtche");
 	dfree(mt);
 }
 
+/* Options of the reference's WFS path that this library does not serve: refused at set-up, so
+   that a run never returns gradients that differ from MAOS's without an error. */
+static void refuse_unsupported(const parms_t* parms, const powfs_t* powfs){
+	if(parms->sim.idealwfs || parms->sim.wfsalias)
+		error("shwfs: sim.idealwfs/sim.wfsalias (DM-projected turbulence) are not supported\n");
+	if(parms->atm.dtrat>0) error("shwfs: atm.dtrat (screens played back in time) is not supported\n");
+	if(parms->tomo.ahst_idealngs) error("shwfs: tomo.ahst_idealngs is not supported\n");
+	for(int idm=0; idm<parms->ndm; idm++){
+		if(parms->dm[idm].iac) error("shwfs: DM %d uses a cubic influence function (dm.iac); only linear DMs\n", idm);
+	}
+	for(int ip=0; ip<parms->npowfs; ip++){
+		const powfs_cfg_t* pc=&parms->powfs[ip];
+		const powfs_t* p=&powfs[ip];
+		if(pc->type!=WFS_SH) error("shwfs: powfs %d is not a Shack-Hartmann WFS\n", ip);
+		if(pc->nwvl>1) error("shwfs: powfs %d has %d wavelengths; one band only\n", ip, pc->nwvl);
+		if(pc->moao>-1) error("shwfs: powfs %d uses MOAO\n", ip);
+		if(pc->fieldstop>0) error("shwfs: powfs %d has a field stop\n", ip);
+		if(pc->dither) error("shwfs: powfs %d dithers\n", ip);
+		if(pc->pistatout || pc->psfout) error("shwfs: powfs %d asks for pistatout/psfout diagnostics\n", ip);
+		if(PN(p->amp)>1 || (p->saa && PN(p->saa)>1))
+			error("shwfs: powfs %d has one amplitude map per WFS (misregistration); one shared map only\n", ip);
+		if(pc->llt){
+			if(pc->llt->nhs>1) error("shwfs: powfs %d simulates %d sodium sublayers (llt.nhs)\n", ip, pc->llt->nhs);
+			if(PN(pc->llt->ox)>1) error("shwfs: powfs %d has %ld launch telescopes; one only\n", ip, PN(pc->llt->ox));
+			if(p->llt && p->llt->ncpa) error("shwfs: powfs %d has an LLT surface (llt.ncpa)\n", ip);
+		}
+		if(pc->usephy){
+			if(pc->phytype_sim!=PTYPE_MF && pc->phytype_sim!=PTYPE_COG)
+				error("shwfs: powfs %d gradient type %d; matched filter or CoG only\n", ip, pc->phytype_sim);
+			const dtf_t* dtf=&p->dtf[0];
+			if(NY(dtf->si)>1 || NY(dtf->nominal)>1)
+				error("shwfs: powfs %d has pixel maps per WFS (pixoffx/pixoffy per WFS)\n", ip);
+		}
+	}
+}
+
+/* The physical-optics powfs of MAOS powfs ip; *ipl receives its index. */
+static void add_phy_powfs(const parms_t* parms, const powfs_t* p, int ip, int* ipl){
+	const powfs_cfg_t* pc=&parms->powfs[ip];
+	const int llt=p->llt!=NULL;
+	shwfs_powfs_desc d={
+		.nsa=(int)p->saloc->nloc, .nopd=(int)p->pts->nxsa, .embfac=pc->embfac,
+		.notf=p->notfx, .pixpsax=p->pixpsax, .pixpsay=p->pixpsay,
+		.pixthetax=pc->radpixtheta, .pixthetay=pc->pixtheta,
+		.wvl=P(pc->wvl, 0), .dsa=p->pts->dsa, .dx=p->pts->dx,
+		.areascale=p->areascale, .hs=pc->hs,
+		.has_etf=llt, .has_llt=llt, .llt_nx=llt?(int)p->llt->pts->nxsa:0,
+		.llt_ox=llt?P(pc->llt->ox, 0):0, .llt_oy=llt?P(pc->llt->oy, 0):0,
+		.llt_origx=llt?p->llt->pts->origx[0]:0, .llt_origy=llt?p->llt->pts->origy[0]:0,
+		.gradtype=pc->phytype_sim, .sigmatch=pc->sigmatch,
+		.cogthres=pc->cogthres, .cogoff=pc->cogoff, .rne=pc->rne,
+		.bkgrnd=pc->bkgrnd*pc->dtrat, .bkgrndc=pc->bkgrnd*pc->dtrat*pc->bkgrndc,
+		.saat=pc->saat, .sigtot_cog=pc->siglev*pc->dtrat};
+	chk(shwfs_powfs_add(g_ctx, &d, ipl), "powfs_add");
+	chk(shwfs_powfs_set_geom(g_ctx, *ipl, p->pts->origx, p->pts->origy, P(P(p->amp, 0)), 1, P(P(p->saa, 0))),
+		"set_geom");
+	chk(shwfs_powfs_set_saasum(g_ctx, *ipl, P(p->saasum, 0)), "set_saasum");
+	/* dtf.si and dtf.nominal: one map shared by every subaperture, or one per subaperture
+	   (lib/mkdtf.c:116-161: radpix or pixoffx) */
+	const dspcell* si=p->dtf[0].si;
+	const long nmap=PN(si);
+	const long npix=(long)p->pixpsax*p->pixpsay;
+	int* idx=mymalloc(nmap*npix*4, int);
+	double* wt=mymalloc(nmap*npix*4, double);
+	for(long m=0; m<nmap; m++) si_taps(P(si, m), idx+m*npix*4, wt+m*npix*4);
+	chk(shwfs_powfs_set_simap(g_ctx, *ipl, idx, wt, (int)nmap), "set_simap");
+	free(idx); free(wt);
+	if(llt){
+		set_etf(p, ip, &p->etfsim[0], 0);
+		chk(shwfs_powfs_set_lltamp(g_ctx, *ipl, P(p->llt->amp)), "set_lltamp");
+	}else{
+		/* nominal is real-valued in MAOS's FFT layout */
+		const dcell* nom=p->dtf[0].nominal;
+		const long nn=PN(nom), n2=(long)p->notfx*p->notfy;
+		dmat* all=dnew(n2, nn);
+		for(long m=0; m<nn; m++) memcpy(PCOL(all, m), P(P(nom, m)), sizeof(real)*n2);
+		chk(shwfs_powfs_set_nominal(g_ctx, *ipl, P(all), (int)nn), "set_nominal");
+		dfree(all);
+	}
+	if(pc->dtrat>1) chk(shwfs_powfs_set_dtrat(g_ctx, *ipl, pc->dtrat), "set_dtrat");
+}
+
+/* The geometric sensor of MAOS powfs ip (gtype_sim: z-tilt, or G-tilt through powfs.GS0):
+   the sensor itself when usephy is 0, else the gradients before phystep. */
+static void add_geo_powfs(const parms_t* parms, const powfs_t* p, int ip, int* ipl){
+	const powfs_cfg_t* pc=&parms->powfs[ip];
+	const int gtype=pc->gtype_sim==GTYPE_Z?SHWFS_GRAD_ZTILT:SHWFS_GRAD_GTILT;
+	const int llt=p->llt!=NULL;  /* its position centres the trombone focus (loc_add_focus_offset) */
+	shwfs_powfs_desc d={.nsa=(int)p->saloc->nloc, .nopd=(int)p->pts->nxsa, .embfac=1, .notf=1,
+		.dsa=p->pts->dsa, .dx=p->pts->dx, .areascale=p->areascale, .hs=pc->hs, .gradtype=gtype,
+		.saat=pc->saat, .llt_ox=llt?P(pc->llt->ox, 0):0, .llt_oy=llt?P(pc->llt->oy, 0):0};
+	chk(shwfs_powfs_add(g_ctx, &d, ipl), "powfs_add");
+	chk(shwfs_powfs_set_geom(g_ctx, *ipl, p->pts->origx, p->pts->origy, P(P(p->amp, 0)), 1, P(P(p->saa, 0))),
+		"set_geom");
+	if(gtype==SHWFS_GRAD_GTILT){
+		const dsp* gs0=p->GS0?P(p->GS0, 0):NULL;
+		if(!gs0) error("shwfs: powfs %d uses G-tilt gradients but powfs.GS0 is not set\n", ip);
+		chk(shwfs_powfs_set_gs0(g_ctx, *ipl, 0, gs0->nx, gs0->ny, gs0->pp, gs0->pi, gs0->px), "set_gs0");
+	}
+	if(pc->dtrat>1) chk(shwfs_powfs_set_dtrat(g_ctx, *ipl, pc->dtrat), "set_dtrat");
+}
+
 void gpu_wfsgrad_init(const parms_t* parms, const powfs_t* powfs){
+	refuse_unsupported(parms, powfs);
 	pthread_mutex_lock(&g_lock);
 	if(g_ctx){ /* a new simulation in the same process */
 		shwfs_destroy(g_ctx);
@@ -92,52 +207,47 @@ void gpu_wfsgrad_init(const parms_t* parms, const powfs_t* powfs){
 	}
 	chk(shwfs_create(&g_ctx, 0), "create");
 	if(parms->npowfs>64) error("shwfs: at most 64 powfs\n");
+	g_ndm=0;
 	for(int ip=0; ip<parms->npowfs; ip++){
-		const powfs_t* p=&powfs[ip];
 		const powfs_cfg_t* pc=&parms->powfs[ip];
-		const int llt=p->llt!=NULL;
-		shwfs_powfs_desc d={
-			.nsa=(int)p->saloc->nloc, .nopd=(int)p->pts->nxsa, .embfac=pc->embfac,
-			.notf=p->notfx, .pixpsax=p->pixpsax, .pixpsay=p->pixpsay,
-			.pixthetax=pc->radpixtheta, .pixthetay=pc->pixtheta,
-			.wvl=P(pc->wvl, 0), .dsa=p->pts->dsa, .dx=p->pts->dx,
-			.areascale=p->areascale, .hs=pc->hs,
-			.has_etf=llt, .has_llt=llt, .llt_nx=llt?(int)p->llt->pts->nxsa:0,
-			.llt_ox=llt?P(pc->llt->ox, 0):0, .llt_oy=llt?P(pc->llt->oy, 0):0,
-			.llt_origx=llt?p->llt->pts->origx[0]:0, .llt_origy=llt?p->llt->pts->origy[0]:0,
-			.gradtype=pc->phytype_sim, .sigmatch=pc->sigmatch,
-			.cogthres=pc->cogthres, .cogoff=pc->cogoff, .rne=pc->rne,
-			.bkgrnd=pc->bkgrnd*pc->dtrat, .bkgrndc=pc->bkgrnd*pc->dtrat*pc->bkgrndc,
-			.saat=pc->saat, .sigtot_cog=pc->siglev*pc->dtrat};
-		chk(shwfs_powfs_add(g_ctx, &d, &g_ipowfs[ip]), "powfs_add");
-		chk(shwfs_powfs_set_geom(g_ctx, g_ipowfs[ip], p->pts->origx, p->pts->origy,
-			P(P(p->amp, 0)), 1, P(P(p->saa, 0))), "set_geom"); /* one amplitude map for every WFS */
-		chk(shwfs_powfs_set_saasum(g_ctx, g_ipowfs[ip], P(p->saasum, 0)), "set_saasum");
-		const long npix=(long)p->pixpsax*p->pixpsay;
-		int* idx=mymalloc(npix*4, int);
-		double* wt=mymalloc(npix*4, double);
-		si_taps(P(p->dtf[0].si, 0), idx, wt);
-		chk(shwfs_powfs_set_simap(g_ctx, g_ipowfs[ip], idx, wt, 1), "set_simap");
-		free(idx); free(wt);
-		if(llt){
-			set_etf(p, ip, &p->etfsim[0], 0);
-			chk(shwfs_powfs_set_lltamp(g_ctx, g_ipowfs[ip], P(p->llt->amp)), "set_lltamp");
+		g_ipowfs_geo[ip]=-1;
+		if(pc->usephy){
+			add_phy_powfs(parms, &powfs[ip], ip, &g_ipowfs[ip]);
+			if(pc->phystep>0) add_geo_powfs(parms, &powfs[ip], ip, &g_ipowfs_geo[ip]);
 		}else{
-			/* nominal is real-valued in MAOS's FFT layout; one shared by every subaperture */
-			chk(shwfs_powfs_set_nominal(g_ctx, g_ipowfs[ip], P(P(p->dtf[0].nominal, 0)), 1), "set_nominal");
+			add_geo_powfs(parms, &powfs[ip], ip, &g_ipowfs[ip]);
+			g_ipowfs_geo[ip]=g_ipowfs[ip];
 		}
-		if(pc->dtrat>1) chk(shwfs_powfs_set_dtrat(g_ctx, g_ipowfs[ip], pc->dtrat), "set_dtrat");
 	}
+	free(g_wfs_phy); free(g_wfs_geo); free(g_wfs_cur);
+	g_nwfs=parms->nwfs;
+	g_wfs_phy=mymalloc(g_nwfs, int);
+	g_wfs_geo=mymalloc(g_nwfs, int);
+	g_wfs_cur=mymalloc(g_nwfs, int);
 	for(int iwfs=0; iwfs<parms->nwfs; iwfs++){
 		const int ip=parms->wfs[iwfs].powfs;
+		const powfs_cfg_t* pc=&parms->powfs[ip];
 		const wfs_cfg_t* wc=&parms->wfs[iwfs];
-		shwfs_wfs_desc w={.ipowfs=g_ipowfs[ip], .thetax=wc->thetax, .thetay=wc->thetay,
-			.hs=wc->hs, .hc=wc->hc, .misregx=wc->misregx, .misregy=wc->misregy,
-			.sigsim=wc->sigsim, .wvlwt=P(wc->wvlwts, 0), .noisy=parms->powfs[ip].noisy};
-		int i;
-		chk(shwfs_wfs_add(g_ctx, &w, &i), "wfs_add");
-		if(i!=iwfs) error("shwfs: WFS %d registered as %d\n", iwfs, i);
-		set_mtche(parms, &powfs[ip], ip, iwfs);
+		const long wfsind=P(pc->wfsind, iwfs);
+		g_wfs_phy[iwfs]=g_wfs_geo[iwfs]=g_wfs_cur[iwfs]=-1;
+		if(pc->usephy){
+			shwfs_wfs_desc w={.ipowfs=g_ipowfs[ip], .thetax=wc->thetax, .thetay=wc->thetay,
+				.hs=wc->hs, .hc=wc->hc, .misregx=wc->misregx, .misregy=wc->misregy,
+				.sigsim=wc->sigsim, .wvlwt=P(wc->wvlwts, 0), .noisy=pc->noisy};
+			chk(shwfs_wfs_add(g_ctx, &w, &g_wfs_phy[iwfs]), "wfs_add");
+			set_mtche(parms, &powfs[ip], ip, iwfs);
+		}
+		if(g_ipowfs_geo[ip]>=0){
+			/* noise on geometric gradients only for a geometric sensor, not before phystep
+			   (cuda/sim/wfsgrad.cu:709-712) */
+			const int noisy=pc->noisy && !pc->usephy;
+			shwfs_wfs_desc w={.ipowfs=g_ipowfs_geo[ip], .thetax=wc->thetax, .thetay=wc->thetay,
+				.hs=wc->hs, .hc=wc->hc, .misregx=wc->misregx, .misregy=wc->misregy,
+				.sigsim=wc->sigsim, .wvlwt=1, .noisy=noisy};
+			chk(shwfs_wfs_add(g_ctx, &w, &g_wfs_geo[iwfs]), "wfs_add");
+			const dmat* nea=powfs[ip].neasim?PR(powfs[ip].neasim, wfsind, 0):NULL;
+			if(noisy && nea) chk(shwfs_wfs_set_neasim(g_ctx, g_wfs_geo[iwfs], P(nea)), "set_neasim");
+		}
 	}
 	chk(shwfs_set_dt(g_ctx, parms->sim.dt), "set_dt");
 	pthread_mutex_unlock(&g_lock);
@@ -149,7 +259,7 @@ void gpu_wfs_init_sim(const parms_t* parms, powfs_t* powfs){
 
 void gpu_wfsgrad_update_etf(const parms_t* parms, const powfs_t* powfs, int ipowfs){
 	const powfs_t* p=&powfs[ipowfs];
-	if(!p->llt) return;
+	if(!p->llt || !parms->powfs[ipowfs].usephy) return;
 	pthread_mutex_lock(&g_lock);
 	set_etf(p, ipowfs, &p->etfsim[0], 0);
 	if(p->etfsim2){
@@ -158,6 +268,9 @@ void gpu_wfsgrad_update_etf(const parms_t* parms, const powfs_t* powfs, int ipow
 		const int dtrat=parms->powfs[ipowfs].llt->coldtrat?parms->powfs[ipowfs].llt->coldtrat
 			:parms->powfs[ipowfs].zoomdtrat;
 		chk(shwfs_powfs_set_etf_dtrat(g_ctx, g_ipowfs[ipowfs], dtrat), "set_etf_dtrat");
+	}else{
+		/* slot 0 alone: no interpolation left over from an earlier pair */
+		chk(shwfs_powfs_set_etf_dtrat(g_ctx, g_ipowfs[ipowfs], 0), "set_etf_dtrat");
 	}
 	pthread_mutex_unlock(&g_lock);
 }
@@ -174,7 +287,11 @@ void gpu_wfsgrad_update_ref(const parms_t* parms, const powfs_t* powfs, int ipow
 void gpu_wfsgrad_seeding(const parms_t* parms, const powfs_t* powfs, rand_t* rstat){
 	(void)powfs;
 	pthread_mutex_lock(&g_lock);
-	for(int iwfs=0; iwfs<parms->nwfs; iwfs++) chk(shwfs_wfs_seed(g_ctx, iwfs, lrand(rstat)), "seed");
+	for(int iwfs=0; iwfs<parms->nwfs; iwfs++){
+		const long seed=lrand(rstat); /* one draw per WFS, as cuda/sim/wfsinit.cu:536 */
+		if(g_wfs_phy[iwfs]>=0) chk(shwfs_wfs_seed(g_ctx, g_wfs_phy[iwfs], seed), "seed");
+		if(g_wfs_geo[iwfs]>=0) chk(shwfs_wfs_seed(g_ctx, g_wfs_geo[iwfs], seed), "seed");
+	}
 	pthread_mutex_unlock(&g_lock);
 }
 
@@ -201,30 +318,124 @@ void gpu_atm2gpu(const mapcell* atm, const dmat* atmscale, const parms_t* parms,
 	free(L); free(s);
 }
 
+/* The DM surfaces embedded in square maps (simu->dmrealsq, NaN outside the actuators), once per
+   step after the servo (maos/filter.c:561, maos/sim_utils.c:1268).  Subtracted from the OPD of
+   every WFS in closed loop. */
+void gpu_dmreal2gpu(mapcell* dmreal){
+	if(!dmreal) return;
+	const int n=(int)PN(dmreal);
+	shwfs_layer_desc* L=mycalloc(n, shwfs_layer_desc);
+	const double** s=mycalloc(n, const double*);
+	for(int i=0; i<n; i++){
+		const map_t* m=P(dmreal, i);
+		if(m->iac) error("shwfs: DM %d uses a cubic influence function; only linear DMs\n", i);
+		L[i]=(shwfs_layer_desc){.nx=m->nx, .ny=m->ny, .dx=m->dx, .ox=m->ox, .oy=m->oy, .ht=m->ht, .alpha=-1};
+		s[i]=P(m);
+	}
+	pthread_mutex_lock(&g_lock);
+	if(g_ctx){
+		chk(shwfs_dm_set(g_ctx, n, L, s), "dm_set");
+		g_ndm=n;
+	}
+	pthread_mutex_unlock(&g_lock);
+	free(L); free(s);
+}
+
+void gpu_dmproj2gpu(mapcell* dmproj){
+	(void)dmproj;
+	error("shwfs: sim.idealwfs/sim.wfsalias (DM-projected turbulence) are not supported\n");
+}
+
+/* The terms MAOS adds to a WFS OPD besides the turbulence (maos/wfsgrad.c:200-262, 373-377;
+   cuda/sim/wfsgrad.cu:548-605), for the frame of step isim. */
+static void set_opd_terms(const sim_t* simu, int iwfs, int lib_wfs, int isim){
+	const parms_t* parms=simu->parms;
+	const int ip=parms->wfs[iwfs].powfs;
+	const int CL=parms->sim.closeloop;
+	const int llt=simu->powfs[ip].llt!=NULL;
+	double ptt[3]={0, 0, 0};
+	if(simu->telws){ /* wind shake */
+		const real tmp=P(simu->telws, isim);
+		const real angle=simu->winddir?P(simu->winddir, 0):0;
+		ptt[1]+=tmp*cos(angle);
+		ptt[2]+=tmp*sin(angle);
+	}
+	if(CL){
+		if(simu->ttmreal){
+			ptt[1]-=P(simu->ttmreal, 0);
+			ptt[2]-=P(simu->ttmreal, 1);
+		}
+		if(simu->fsmreal && P(simu->fsmreal, iwfs) && !llt){
+			ptt[1]-=P(P(simu->fsmreal, iwfs), 0);
+			ptt[2]-=P(P(simu->fsmreal, iwfs), 1);
+		}
+	}
+	double ftel=0, fllt=0;
+	if(simu->telfocusreal) ftel=-P(P(simu->telfocusreal, 0), 0);
+	if(llt && (simu->zoomint || simu->powfs[ip].focus)){
+		fllt=simu->zoomint?zoomfocusadj((sim_t*)simu, iwfs):PR(simu->powfs[ip].focus, isim, P(parms->powfs[ip].wfsind, iwfs));
+	}
+	/* the uplink tip/tilt reaches only the physical-optics frame (the LLT OPD, maos/wfsgrad.c:373-377) */
+	const int phy=lib_wfs==g_wfs_phy[iwfs];
+	real lt[2]={0, 0};
+	if(llt && phy) wfsgrad_llt_tt(&lt[0], &lt[1], (sim_t*)simu, iwfs, isim);
+	const double lltptt[2]={lt[0], lt[1]};
+	chk(shwfs_wfs_set_opd_terms(g_ctx, lib_wfs, CL && g_ndm>0, ptt, ftel, fllt, (llt && phy)?lltptt:NULL),
+		"set_opd_terms");
+}
+
 void* gpu_wfsgrad_queue(thread_t* info){
 	sim_t* simu=(sim_t*)info->data;
+	const parms_t* parms=simu->parms;
+	const int isim=simu->wfsisim;
 	pthread_mutex_lock(&g_lock);
-	for(int iwfs=info->start; iwfs<info->end; iwfs++)
-		chk(shwfs_frame_queue(g_ctx, simu->wfsisim, iwfs, iwfs+1), "frame_queue");
+	for(int iwfs=info->start; iwfs<info->end; iwfs++){
+		const int ip=parms->wfs[iwfs].powfs;
+		const powfs_cfg_t* pc=&parms->powfs[ip];
+		g_wfs_cur[iwfs]=-1;
+		if(isim<pc->step) continue; /* the WFS starts at powfs.step (cuda/sim/wfsgrad.cu:492) */
+		const int do_phy=pc->usephy && isim>=pc->phystep;
+		const int lw=do_phy?g_wfs_phy[iwfs]:g_wfs_geo[iwfs];
+		set_opd_terms(simu, iwfs, lw, isim);
+		chk(shwfs_frame_queue(g_ctx, isim, lw, lw+1), "frame_queue");
+		g_wfs_cur[iwfs]=lw;
+	}
 	pthread_mutex_unlock(&g_lock);
 	return NULL;
 }
 
+/* Gradients of the frame into simu->gradcl on the WFS's output frames ((isim+1) mod dtrat = 0,
+   cuda/sim/wfsgrad.cu:747-776); other frames leave it as it was. */
 void gpu_wfsgrad_sync(sim_t* simu, int iwfs){
 	const int ip=simu->parms->wfs[iwfs].powfs;
-	dmat** pg=&P(simu->gradcl, iwfs);
-	if(!*pg) *pg=dnew(simu->powfs[ip].saloc->nloc*2, 1);
+	const int dtrat=simu->parms->powfs[ip].dtrat;
 	pthread_mutex_lock(&g_lock);
-	chk(shwfs_frame_sync(g_ctx, iwfs, P(*pg), NULL), "frame_sync");
+	const int lw=g_wfs_cur[iwfs];
+	if(lw>=0 && (simu->wfsisim+1)%dtrat==0){
+		dmat** pg=&P(simu->gradcl, iwfs);
+		if(!*pg) *pg=dnew(simu->powfs[ip].saloc->nloc*2, 1);
+		chk(shwfs_frame_sync(g_ctx, lw, P(*pg), NULL), "frame_sync");
+	}else if(lw>=0){
+		chk(shwfs_sync(g_ctx), "sync");
+	}
 	pthread_mutex_unlock(&g_lock);
 }
 
 void gpu_save_pistat(sim_t* simu){
-	(void)simu; /* pistat diagnostics are not formed on this path */
+	(void)simu; /* pistatout is refused at set-up */
 }
 
+/* NCPA surfaces of every WFS (powfs.opdadd, cuda/sim/wfsinit.cu:514-524). */
 void gpu_wfssurf2gpu(const parms_t* parms, powfs_t* powfs){
-	(void)parms; (void)powfs; /* NCPA surfaces are not on this path */
+	pthread_mutex_lock(&g_lock);
+	for(int iwfs=0; iwfs<parms->nwfs; iwfs++){
+		const int ip=parms->wfs[iwfs].powfs;
+		const int wfsind=P(parms->powfs[ip].wfsind, iwfs);
+		const dmat* add=powfs[ip].opdadd?P(powfs[ip].opdadd, wfsind):NULL;
+		if(g_wfs_phy[iwfs]>=0) chk(shwfs_wfs_set_opdadd(g_ctx, g_wfs_phy[iwfs], add?P(add):NULL), "set_opdadd");
+		if(g_wfs_geo[iwfs]>=0) chk(shwfs_wfs_set_opdadd(g_ctx, g_wfs_geo[iwfs], add?P(add):NULL), "set_opdadd");
+	}
+	pthread_mutex_unlock(&g_lock);
 }
 
 /* ---- science path, open loop (cuda/sim/perfevl.cu) ---- */

@@ -80,6 +80,12 @@ struct WfsState {
 	DevBuf<float> neasim;  // geometric gradient noise: Cholesky factor, 3 nsa
 	DevBuf<double> i1sum;  // sigmatch 2: total intensity of the frame
 	uint64_t seed = 1;
+	// closed-loop and static OPD terms (shwfs_wfs_set_opd_terms, shwfs_wfs_set_opdadd)
+	DevBuf<float> opdadd;     // NCPA surface on the pupil points, or empty
+	int use_dm = 0;           // subtract the mirror grids (shwfs_dm_set) from this WFS's OPD
+	int has_poly = 0, has_lltpoly = 0;
+	double poly[4] = {0, 0, 0, 0};     // c0 + c1 x + c2 y + c3 (x^2 + y^2) on the pupil points
+	double lltpoly[4] = {0, 0, 0, 0};  // the same on the LLT pupil (uplink tip/tilt)
 	int garena = -1;          // gradient arena chunk holding grad and grad_h (shwfs_ctx::garena)
 	float* grad_h = nullptr;  // pinned staging
 	float* ints_h = nullptr;
@@ -103,6 +109,10 @@ struct shwfs_ctx {
 	std::vector<PowfsState> powfs;
 	std::vector<WfsState> wfs;
 	std::vector<LayerState> atm;
+	std::vector<LayerState> dm;          // deformable-mirror grids (shwfs_dm_set), traced after the layers
+	float* dm_stage = nullptr;           // pinned FP32 staging of the mirror surfaces
+	size_t dm_stage_n = 0;
+	cudaEvent_t ev_dm = nullptr;         // the last staging copy has left the host buffer
 	double dt = 1.0 / 800;
 	int form = SHWFS_FORM_FFT;
 	DevBuf<WfsDev> wfsdev;  // staging for per-launch WFS descriptors
@@ -336,6 +346,10 @@ int shwfs_destroy(shwfs_ctx* ctx) {
 	}
 	if (ctx->errflag_h) cudaFreeHost(ctx->errflag_h);
 	for (auto& l : ctx->atm) l.screen.free_();
+	for (auto& l : ctx->dm) l.screen.free_();
+	if (ctx->dm_stage) cudaFreeHost(ctx->dm_stage);
+	if (ctx->ev_dm) cudaEventDestroy(ctx->ev_dm);
+	for (auto& w : ctx->wfs) w.opdadd.free_();
 	for (auto& m : ctx->marks) {
 		cudaEventDestroy(m.a);
 		cudaEventDestroy(m.b);
@@ -581,6 +595,9 @@ int shwfs_wfs_seed(shwfs_ctx* ctx, int iwfs, uint64_t seed) {
 int shwfs_atm_set(shwfs_ctx* ctx, int nlayer, const shwfs_layer_desc* layers, const double* const* screens) {
 	if (!ctx || nlayer < 0 || nlayer > SHWFS_MAX_LAYERS || (nlayer && (!layers || !screens)))
 		return ctx ? fail(ctx, SHWFS_EINVAL, "atm_set: 0..%d layers", SHWFS_MAX_LAYERS) : SHWFS_EINVAL;
+	if (nlayer + (int)ctx->dm.size() > SHWFS_MAX_LAYERS)
+		return fail(ctx, SHWFS_EINVAL, "atm_set: %d layers and %d mirror grids exceed %d", nlayer, (int)ctx->dm.size(),
+			SHWFS_MAX_LAYERS);
 	int r = set_device(ctx);
 	if (r) return r;
 	for (auto& l : ctx->atm) l.screen.free_();
@@ -595,6 +612,115 @@ int shwfs_atm_set(shwfs_ctx* ctx, int nlayer, const shwfs_layer_desc* layers, co
 	return 0;
 }
 
+int shwfs_dm_set(shwfs_ctx* ctx, int ndm, const shwfs_layer_desc* dms, const double* const* surfaces) {
+	if (!ctx || ndm < 0 || (ndm && (!dms || !surfaces))) return ctx ? fail(ctx, SHWFS_EINVAL, "dm_set: bad arguments") : SHWFS_EINVAL;
+	if ((int)ctx->atm.size() + ndm > SHWFS_MAX_LAYERS)
+		return fail(ctx, SHWFS_EINVAL, "dm_set: %d layers and %d mirror grids exceed %d", (int)ctx->atm.size(), ndm,
+			SHWFS_MAX_LAYERS);
+	size_t total = 0;
+	for (int i = 0; i < ndm; i++) {
+		const shwfs_layer_desc& d = dms[i];
+		if (d.nx < 2 || d.ny < 2 || !(d.dx > 0) || !surfaces[i] || !isfinite(d.ht) || !isfinite(d.alpha))
+			return fail(ctx, SHWFS_EINVAL, "dm_set: mirror %d is invalid", i);
+		total += (size_t)d.nx * d.ny;
+	}
+	int r = set_device(ctx);
+	if (r) return r;
+	if (!ctx->ev_dm) CK(cudaEventCreateWithFlags(&ctx->ev_dm, cudaEventDisableTiming));
+	// the previous frame's surfaces may still be on their way out of the staging buffer
+	CK(cudaEventSynchronize(ctx->ev_dm));
+	if (ndm == 0) {
+		for (auto& m : ctx->dm) m.screen.free_();
+		ctx->dm.clear();
+		return 0;
+	}
+	if ((int)ctx->dm.size() != ndm) {
+		for (auto& m : ctx->dm) m.screen.free_();
+		ctx->dm.clear();
+		ctx->dm.resize(ndm);
+	}
+	if (ctx->dm_stage_n < total) {
+		if (ctx->dm_stage) cudaFreeHost(ctx->dm_stage);
+		ctx->dm_stage = nullptr;
+		ctx->dm_stage_n = 0;
+		CK(cudaMallocHost(&ctx->dm_stage, total * sizeof(float)));
+		ctx->dm_stage_n = total;
+	}
+	size_t off = 0;
+	for (int i = 0; i < ndm; i++) {
+		const size_t n = (size_t)dms[i].nx * dms[i].ny;
+		if ((r = dev_alloc(ctx, ctx->dm[i].screen, n))) return r;
+		ctx->dm[i].d = dms[i];
+		float* st = ctx->dm_stage + off;
+		for (size_t k = 0; k < n; k++) st[k] = (float)surfaces[i][k];
+		CK(cudaMemcpyAsync(ctx->dm[i].screen.p, st, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+		ctx->h2d_bytes += n * sizeof(float);
+		off += n;
+	}
+	CK(cudaEventRecord(ctx->ev_dm, ctx->stream));
+	return 0;
+}
+
+int shwfs_wfs_set_opd_terms(shwfs_ctx* ctx, int iwfs, int use_dm, const double* ptt, double focus_tel,
+	double focus_llt, const double* lltptt) {
+	WfsState* w = get_wfs(ctx, iwfs);
+	if (!w) return ctx ? fail(ctx, SHWFS_EINVAL, "set_opd_terms: unknown wfs %d", iwfs) : SHWFS_EINVAL;
+	const PowfsState& p = ctx->powfs[w->d.ipowfs];
+	if (lltptt && (lltptt[0] != 0 || lltptt[1] != 0) && !p.d.has_llt)
+		return fail(ctx, SHWFS_EINVAL, "set_opd_terms: LLT tip/tilt for WFS %d, whose powfs has no LLT", iwfs);
+	const double t0 = ptt ? ptt[0] : 0, t1 = ptt ? ptt[1] : 0, t2 = ptt ? ptt[2] : 0;
+	if (!isfinite(t0) || !isfinite(t1) || !isfinite(t2) || !isfinite(focus_tel) || !isfinite(focus_llt))
+		return fail(ctx, SHWFS_EINVAL, "set_opd_terms: terms must be finite");
+	if ((focus_tel != 0 || focus_llt != 0) && p.origx_h.empty())
+		return fail(ctx, SHWFS_ESTATE, "set_opd_terms: powfs geometry not set");
+	w->use_dm = use_dm ? 1 : 0;
+	// loc_add_ptt (math/loc.c:762-789): ptt[0] + ptt[1] x + ptt[2] y.
+	// loc_add_focus_offset (math/loc.c:1226-1246): f ((x-a)^2 + (y-b)^2) less its
+	// mean over the pupil points, for the telescope focus (a = b = 0) and the LLT
+	// zoom focus (a, b = the LLT position); expanded about the origin in FP64.
+	double c[4] = {t0, t1, t2, focus_tel + focus_llt};
+	if (focus_tel != 0 || focus_llt != 0) {
+		const int nopd = p.d.nopd;
+		const double n = (double)p.d.nsa * nopd * nopd;
+		double sx = 0, sy = 0, sr = 0;
+		for (int isa = 0; isa < p.d.nsa; isa++)
+			for (int iy = 0; iy < nopd; iy++)
+				for (int ix = 0; ix < nopd; ix++) {
+					const double x = p.origx_h[isa] + ix * p.d.dx, y = p.origy_h[isa] + iy * p.d.dx;
+					sx += x;
+					sy += y;
+					sr += x * x + y * y;
+				}
+		const double a = p.d.llt_ox, b = p.d.llt_oy;
+		c[0] -= focus_tel * sr / n;
+		c[0] += focus_llt * (a * a + b * b) - focus_llt * (sr - 2 * a * sx - 2 * b * sy + n * (a * a + b * b)) / n;
+		c[1] -= 2 * focus_llt * a;
+		c[2] -= 2 * focus_llt * b;
+	}
+	w->has_poly = c[0] != 0 || c[1] != 0 || c[2] != 0 || c[3] != 0;
+	memcpy(w->poly, c, sizeof(c));
+	w->lltpoly[0] = 0;
+	w->lltpoly[1] = lltptt ? lltptt[0] : 0;
+	w->lltpoly[2] = lltptt ? lltptt[1] : 0;
+	w->lltpoly[3] = 0;
+	w->has_lltpoly = w->lltpoly[1] != 0 || w->lltpoly[2] != 0;
+	return 0;
+}
+
+int shwfs_wfs_set_opdadd(shwfs_ctx* ctx, int iwfs, const double* opd) {
+	WfsState* w = get_wfs(ctx, iwfs);
+	if (!w) return ctx ? fail(ctx, SHWFS_EINVAL, "set_opdadd: unknown wfs %d", iwfs) : SHWFS_EINVAL;
+	int r = set_device(ctx);
+	if (r) return r;
+	if (!opd) {
+		CK(cudaStreamSynchronize(ctx->stream));
+		w->opdadd.free_();
+		return 0;
+	}
+	const PowfsState& p = ctx->powfs[w->d.ipowfs];
+	return dev_upload_f(ctx, w->opdadd, opd, (size_t)p.d.nsa * p.d.nopd * p.d.nopd);
+}
+
 }  // extern "C"
 
 // ---- frame machinery ----
@@ -606,7 +732,7 @@ static int launch_geom_wfs(shwfs_ctx* ctx, GeomParams& gp, bool split = true);
 // (lib/accphi_grid_do.c:408-434), FP64 on the host.
 static int add_geom_entry(shwfs_ctx* ctx, GeomParams& gp, double thetax, double thetay, double hs, double hc,
 	double misregx, double misregy, double extra_shiftx, double extra_shifty, int isim, const double* origx,
-	const double* origy, int nsa, int nopd, double dx, float* out) {
+	const double* origy, int nsa, int nopd, double dx, float* out, bool mirrors = false) {
 	if (gp.nentry >= SHWFS_MAX_ENTRIES) return fail(ctx, SHWFS_EINVAL, "too many pupils in one ray-trace launch");
 	GeomEntry& e = gp.e[gp.nentry++];
 	memset(&e, 0, sizeof(e));
@@ -634,6 +760,22 @@ static int add_geom_entry(shwfs_ctx* ctx, GeomParams& gp, double thetax, double 
 		e.dispy[l] = (displacey - a.oy) * dx_in1;
 		e.use |= 1u << l;
 	}
+	// mirror grids after the layers: the WFS's cone, misregistration, no wind
+	// (mapcell2loc, cuda/sim/accphi.cu:238-249; maos/sim_utils.c:1034-1052)
+	const int na = (int)ctx->atm.size();
+	for (int k = 0; mirrors && k < (int)ctx->dm.size(); k++) {
+		const shwfs_layer_desc& a = ctx->dm[k].d;
+		const int l = na + k;
+		const double ht = a.ht;
+		const bool finite_hs = isfinite(hs) && hs != 0;
+		const double scale = finite_hs ? 1. - (ht - hc) / (hs - hc) : 1.;
+		if (scale < 0) continue;
+		const double dx_in1 = 1. / a.dx;
+		e.sx[l] = scale * dx_in1;
+		e.dispx[l] = (ht * thetax + scale * misregx - a.ox) * dx_in1;
+		e.dispy[l] = (ht * thetay + scale * misregy - a.oy) * dx_in1;
+		e.use |= 1u << l;
+	}
 	return 0;
 }
 
@@ -645,6 +787,14 @@ static void geom_init(shwfs_ctx* ctx, GeomParams& gp) {
 		gp.nx[l] = (int)ctx->atm[l].d.nx;
 		gp.ny[l] = (int)ctx->atm[l].d.ny;
 		gp.alpha[l] = (float)ctx->atm[l].d.alpha;
+	}
+	for (const LayerState& m : ctx->dm) {  // mirror grids last (shwfs_dm_set)
+		const int l = gp.nlayer++;
+		gp.screen[l] = m.screen.p;
+		gp.nx[l] = (int)m.d.nx;
+		gp.ny[l] = (int)m.d.ny;
+		gp.alpha[l] = (float)m.d.alpha;
+		gp.nmirror++;
 	}
 }
 
@@ -737,13 +887,19 @@ static int launch_geom_wfs(shwfs_ctx* ctx, GeomParams& gp, bool split) {
 		StageMark m(ctx, SHWFS_STAGE_RAYTRACE);
 		const size_t smem = (size_t)gp.nlayer * nopd * 2 * sizeof(int4);
 		if (smem > 160 * 1024) return fail(ctx, SHWFS_EINVAL, "ray trace: %d layers x %d points too large", gp.nlayer, nopd);
-		if (smem > 48 * 1024) CK(cudaFuncSetAttribute(geom_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+		bool extra = gp.nmirror > 0;
+		for (int i = 0; i < gp.nentry; i++) extra = extra || gp.e[i].opdadd || gp.e[i].has_poly;
+		if (smem > 48 * 1024) {
+			CK(cudaFuncSetAttribute(geom_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+			CK(cudaFuncSetAttribute(geom_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+		}
 		// GEOM_PTS points per thread with no idle slot where the pupil allows it:
 		// 16x16 pupils 64 threads, 32x32 256, larger ones split over blocks of 256
 		const int np = nopd * nopd;
 		const int bd = std::min(256, std::max(32, ((np + GEOM_PTS - 1) / GEOM_PTS + 31) / 32 * 32));
 		const int bps = (np + GEOM_PTS * bd - 1) / (GEOM_PTS * bd);  // blocks per subaperture
-		geom_kernel<<<(unsigned)nblk * bps, bd, smem, ctx->stream>>>(gp, nopd, nitem, bps);
+		if (extra) geom_kernel<true><<<(unsigned)nblk * bps, bd, smem, ctx->stream>>>(gp, nopd, nitem, bps);
+		else geom_kernel<false><<<(unsigned)nblk * bps, bd, smem, ctx->stream>>>(gp, nopd, nitem, bps);
 	}
 	CK(cudaGetLastError());
 	return 0;
@@ -752,8 +908,18 @@ static int launch_geom_wfs(shwfs_ctx* ctx, GeomParams& gp, bool split) {
 // The ray-trace entry of one WFS.
 static int add_wfs_entry(shwfs_ctx* ctx, GeomParams& gp, WfsState& w, int isim, float* opd) {
 	PowfsState& p = ctx->powfs[w.d.ipowfs];
-	return add_geom_entry(ctx, gp, w.d.thetax, w.d.thetay, w.d.hs, w.d.hc, w.d.misregx, w.d.misregy, 0, 0, isim,
-		p.origx.p, p.origy.p, p.d.nsa, p.d.nopd, p.d.dx, opd);
+	int r = add_geom_entry(ctx, gp, w.d.thetax, w.d.thetay, w.d.hs, w.d.hc, w.d.misregx, w.d.misregy, 0, 0, isim,
+		p.origx.p, p.origy.p, p.d.nsa, p.d.nopd, p.d.dx, opd, w.use_dm != 0);
+	if (r) return r;
+	GeomEntry& e = gp.e[gp.nentry - 1];
+	e.opdadd = w.opdadd.p;
+	e.has_poly = w.has_poly;
+	memcpy(e.poly, w.poly, sizeof(e.poly));
+	return 0;
+}
+static void set_llt_poly(GeomEntry& e, const WfsState& w) {
+	e.has_poly = w.has_lltpoly;
+	memcpy(e.poly, w.lltpoly, sizeof(e.poly));
 }
 // The LLT pupil of one LGS WFS (maos/wfsgrad.c:337-365): direction
 // theta - llt_o/hs, shift llt_o - v*dt*isim, cone of the star, wrap; the
@@ -763,8 +929,9 @@ static int add_llt_entry(shwfs_ctx* ctx, GeomParams& gp, WfsState& w, int isim) 
 	int r = add_geom_entry(ctx, gp, w.d.thetax - p.d.llt_ox / w.d.hs, w.d.thetay - p.d.llt_oy / w.d.hs, w.d.hs, 0, 0,
 		0, p.d.llt_ox, p.d.llt_oy, isim, p.lltorig.p, p.lltorig.p + 1, 1, p.d.llt_nx, p.d.dx, w.lltopd.p);
 	if (r) return r;
-	if (p.d.notf != 32) return 0;  // the uplink OTF follows from the traced OPD (launch_uplink_gen)
 	GeomEntry& e = gp.e[gp.nentry - 1];
+	set_llt_poly(e, w);
+	if (p.d.notf != 32) return 0;  // the uplink OTF follows from the traced OPD (launch_uplink_gen)
 	e.lltamp = p.lltamp.p;
 	e.lotfT = w.lotfT.p;
 	e.twoinvwvl = (float)(2.0 / p.d.wvl);
@@ -2160,6 +2327,7 @@ int shwfs_frame_noalloc(shwfs_ctx* ctx, int iwfs, int isim, float* ints, float* 
 				 0, 0, 0, p.d.llt_ox, p.d.llt_oy, isim, p.lltorig.p, p.lltorig.p + 1, 1, p.d.llt_nx, p.d.dx, lltopd)))
 			return r;
 		GeomEntry& e = gp.e[gp.nentry - 1];
+		set_llt_poly(e, *w);
 		e.lltamp = p.lltamp.p;
 		e.lotfT = lotfT;
 		e.twoinvwvl = (float)(2.0 / p.d.wvl);

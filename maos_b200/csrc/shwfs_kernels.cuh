@@ -152,10 +152,19 @@ struct GeomEntry {
 	const float* lltamp;   // nopd^2, or null for a WFS entry
 	float2* lotfT;
 	float twoinvwvl, lltnorm;
+	// closed-loop and static terms of the pupil's OPD (maos/wfsgrad.c:200-262)
+	const float* opdadd;   // nsa*nopd^2 surface added at every point (NCPA), or null
+	int has_poly;          // add poly[0] + poly[1] x + poly[2] y + poly[3] (x^2 + y^2) at point (x, y)
+	double poly[4];        // tip/tilt, piston and focus terms gathered on the host (FP64)
 };
 struct GeomParams {
 	int nentry, nlayer;
 	int interleave;  // items are (subaperture, entry) pairs, entry fastest (all entries have the same nsa)
+	// the last nmirror of the nlayer layers are deformable-mirror grids: no wind,
+	// no wrap (prop with wrap=0, maos/sim_utils.c:1042; map2loc_linear,
+	// cuda/sim/accphi.cu:24-38): a point whose bilinear cell leaves the grid gets
+	// nothing from it
+	int nmirror;
 	const float* screen[SHWFS_MAX_LAYERS];
 	int nx[SHWFS_MAX_LAYERS], ny[SHWFS_MAX_LAYERS];
 	float alpha[SHWFS_MAX_LAYERS];
@@ -330,12 +339,19 @@ constexpr int GEOM_PTS = 4;
 // false) or y, in FP64 from the subaperture origin: first screen index j0 and
 // FP32 fraction f0, wrapped into the screen (prop_grid_pts,
 // lib/accphi_grid_do.c:424-434, wrap=1).
+template <bool EXTRA>
 __device__ __forceinline__ void geom_origin(const GeomParams& P, const GeomEntry& E, int isa, int l, bool isy, int& j0,
 	float& f0) {
 	const int n = isy ? P.ny[l] : P.nx[l];
 	double x0 = (isy ? E.origy[isa] : E.origx[isa]) * E.sx[l] + (isy ? E.dispy[l] : E.dispx[l]);
 	if (!isfinite(x0) || !isfinite((isy ? E.origx[isa] : E.origy[isa]) * E.sx[l] + (isy ? E.dispx[l] : E.dispy[l])))
 		x0 = 0;
+	if (EXTRA && l >= P.nlayer - P.nmirror) {  // mirror grid: no wrap; the origin may lie off the grid
+		x0 = fmin(fmax(x0, -1e9), 1e9);
+		j0 = (int)floor(x0);
+		f0 = (float)(x0 - j0);
+		return;
+	}
 	x0 -= floor(x0 / n) * n;
 	j0 = (int)floor(x0);
 	f0 = (float)(x0 - j0);
@@ -352,12 +368,37 @@ __device__ __forceinline__ void geom_point(int j0, float f0, int i, float step, 
 	j1 = j == n - 1 ? 0 : j + 1;
 	w = f - fl;
 }
+// The same on a mirror grid (no wrap): *valid is 0 when the point's cell
+// [j, j+1] leaves the grid, and j, j1 are then 0.
+__device__ __forceinline__ void geom_point_clip(int j0, float f0, int i, float step, int n, int& j, int& j1, float& w,
+	int& valid) {
+	const float f = f0 + i * step;
+	const float fl = floorf(f);
+	j = j0 + (int)fl;
+	w = f - fl;
+	valid = j >= 0 && j < n - 1;
+	if (!valid) j = 0;
+	j1 = valid ? j + 1 : 0;
+}
+// The OPD terms of a pupil point that are not ray traced: the NCPA surface and
+// the tip/tilt/piston/focus polynomial (x, y: the point's pupil coordinate).
+__device__ __forceinline__ float geom_extra(const GeomEntry& E, int isa, int ipt, int ix, int iy, int np, float acc) {
+	if (E.opdadd) acc += E.opdadd[(size_t)isa * np + ipt];
+	if (E.has_poly) {
+		const double x = E.origx[isa] + ix * E.dx, y = E.origy[isa] + iy * E.dx;
+		acc += (float)(E.poly[0] + E.poly[1] * x + E.poly[2] * y + E.poly[3] * (x * x + y * y));
+	}
+	return acc;
+}
 // acc + al * bilinear(m00, m10, m01, m11; wx, wy)
 __device__ __forceinline__ float geom_bilerp(float al, float m00, float m10, float m01, float m11, float wx, float wy,
 	float acc) {
 	return fmaf(al, (m00 + (m10 - m00) * wx) * (1.f - wy) + (m01 + (m11 - m01) * wx) * wy, acc);
 }
 
+// EXTRA: the launch has mirror grids, NCPA surfaces or polynomial terms (a
+// closed-loop frame); the open-loop launch compiles without their code.
+template <bool EXTRA>
 __global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomParams P, int nopd, int nitem, int bps) {
 	extern __shared__ int4 s_tab[];
 	const int item = blockIdx.x / bps, part = blockIdx.x - item * bps;
@@ -379,7 +420,7 @@ __global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomP
 	if (tid < 2 * nl) {
 		int j0;
 		float f0;
-		geom_origin(P, E, isa, tid >> 1, tid & 1, j0, f0);
+		geom_origin<EXTRA>(P, E, isa, tid >> 1, tid & 1, j0, f0);
 		s_j0[tid] = j0;
 		s_f0[tid] = f0;
 		if (!(tid & 1)) s_step[tid >> 1] = (float)(E.dx * E.sx[tid >> 1]);
@@ -390,11 +431,14 @@ __global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomP
 		const bool isy = r >= nopd;
 		const int i = isy ? r - nopd : r;
 		const int n = isy ? P.ny[l] : P.nx[l];
-		int j, j1;
+		int j, j1, valid = 1;
 		float w;
-		geom_point(s_j0[2 * l + isy], s_f0[2 * l + isy], i, s_step[l], n, j, j1, w);
+		if (!EXTRA || l < nl - P.nmirror)
+			geom_point(s_j0[2 * l + isy], s_f0[2 * l + isy], i, s_step[l], n, j, j1, w);
+		else
+			geom_point_clip(s_j0[2 * l + isy], s_f0[2 * l + isy], i, s_step[l], n, j, j1, w, valid);
 		const int m = isy ? P.nx[l] : 1;
-		s_tab[k] = make_int4(j * m, j1 * m, __float_as_int(w), 0);
+		s_tab[k] = make_int4(j * m, j1 * m, __float_as_int(w), valid);
 	}
 	__syncthreads();
 	// up to GEOM_PTS points per thread, layers outermost so that the gathers of the points are in flight
@@ -410,7 +454,8 @@ __global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomP
 		ixu[u] = ip % nopd;
 		iyu[u] = ip / nopd;
 	}
-	for (int l = 0; l < nl; l++) {
+	const int nwrap = EXTRA ? nl - P.nmirror : nl;
+	for (int l = 0; l < nwrap; l++) {
 		if (!((E.use >> l) & 1u)) continue;
 		const float* __restrict__ sc = P.screen[l];
 		const float al = P.alpha[l];
@@ -423,6 +468,30 @@ __global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomP
 				acc[u] = geom_bilerp(al, m00, m10, m01, m11, __int_as_float(tx.z), __int_as_float(ty.z), acc[u]);
 			}
 		}
+	}
+	for (int l = nwrap; EXTRA && l < nl; l++) {  // mirror grids: only points whose cell lies on the grid and is valid
+		if (!((E.use >> l) & 1u)) continue;
+		const float* __restrict__ sc = P.screen[l];
+		const float al = P.alpha[l];
+#pragma unroll
+		for (int u = 0; u < GEOM_PTS; u++) {
+			if (p0 + tid + bd * u < p1) {
+				const int4 tx = s_tab[l * 2 * nopd + ixu[u]], ty = s_tab[l * 2 * nopd + nopd + iyu[u]];
+				if (tx.w & ty.w) {
+					const float m00 = __ldg(sc + (ty.x + tx.x)), m10 = __ldg(sc + (ty.x + tx.y));
+					const float m01 = __ldg(sc + (ty.y + tx.x)), m11 = __ldg(sc + (ty.y + tx.y));
+					const float wx = __int_as_float(tx.z), wy = __int_as_float(ty.z);
+					const float v = (m00 + (m10 - m00) * wx) * (1.f - wy) + (m01 + (m11 - m01) * wx) * wy;
+					// NaN marks grid points outside the mirror (add_valid, math/numtype.h:40)
+					if (!isnan(v)) acc[u] = fmaf(al, v, acc[u]);
+				}
+			}
+		}
+	}
+	if (EXTRA && (E.opdadd || E.has_poly)) {
+#pragma unroll
+		for (int u = 0; u < GEOM_PTS; u++)
+			if (p0 + tid + bd * u < p1) acc[u] = geom_extra(E, isa, p0 + tid + bd * u, ixu[u], iyu[u], np, acc[u]);
 	}
 #pragma unroll
 	for (int u = 0; u < GEOM_PTS; u++)
@@ -441,7 +510,7 @@ __global__ void __launch_bounds__(256) llt_uplink_kernel(const __grid_constant__
 	const int ip = threadIdx.x;
 	const int ix = ip & 15, iy = ip >> 4;
 	// the pupil's FP64 origin in each layer once (thread l), -1 where it is not finite
-	if (ip < P.nlayer) {
+	if (ip < P.nlayer - P.nmirror) {
 		const int l = ip, nx = P.nx[l], ny = P.ny[l];
 		double x0 = E.origx[0] * E.sx[l] + E.dispx[l];
 		double y0 = E.origy[0] * E.sx[l] + E.dispy[l];
@@ -460,7 +529,7 @@ __global__ void __launch_bounds__(256) llt_uplink_kernel(const __grid_constant__
 	}
 	__syncthreads();
 	float acc = 0.f;
-	for (int l = 0; l < P.nlayer; l++) {
+	for (int l = 0; l < P.nlayer - P.nmirror; l++) {
 		if (!((E.use >> l) & 1u) || s_i0[l][0] < 0) continue;
 		const int nx = P.nx[l], ny = P.ny[l];
 		const int ix0 = s_i0[l][0], iy0 = s_i0[l][1];
@@ -477,6 +546,7 @@ __global__ void __launch_bounds__(256) llt_uplink_kernel(const __grid_constant__
 		const float m01 = __ldg(sc + jx + (size_t)nx * jy1), m11 = __ldg(sc + jx1 + (size_t)nx * jy1);
 		acc += P.alpha[l] * ((m00 + (m10 - m00) * wx) * (1.f - wy) + (m01 + (m11 - m01) * wx) * wy);
 	}
+	if (E.has_poly) acc = geom_extra(E, 0, ip, ix, iy, 256, acc);  // uplink tip/tilt (maos/wfsgrad.c:373-377)
 	s_opd[ip] = acc;
 	if (E.opd) E.opd[ip] = acc;
 	__syncthreads();

@@ -128,6 +128,9 @@ def _load() -> C.CDLL:
         "shwfs_evl_psf_reset": [vp],
         "shwfs_evl_opd_dev": [vp, i, vp],
         "shwfs_grad_gtilt_dev": [vp, i, vp, vp],
+        "shwfs_dm_set": [vp, i, C.POINTER(LayerDesc), C.POINTER(dp)],
+        "shwfs_wfs_set_opd_terms": [vp, i, i, dp, C.c_double, C.c_double, dp],
+        "shwfs_wfs_set_opdadd": [vp, i, dp],
     }
     for name, args in sig.items():
         f = getattr(lib, name)
@@ -308,6 +311,29 @@ class Context:
         keep = [_f64(s) for s in screens]
         ptrs = (C.POINTER(C.c_double) * max(n, 1))(*[_dptr(s) for s in keep])
         self._check(self._L.shwfs_atm_set(self._h, n, descs, ptrs), "atm_set")
+
+    def dm_set(self, mirrors: Sequence[dict], surfaces: Sequence[np.ndarray]):
+        """Deformable-mirror grids subtracted from the OPD of WFS that use them
+        (layer dicts: nx, ny, dx, ox, oy, ht, alpha = weight, -1 to subtract;
+        surfaces (ny, nx)); later calls with the same sizes copy new surfaces."""
+        n = len(mirrors)
+        descs = (LayerDesc * max(n, 1))(*[LayerDesc(**{**dict(vx=0.0, vy=0.0), **m}) for m in mirrors])
+        keep = [_f64(s) for s in surfaces]
+        ptrs = (C.POINTER(C.c_double) * max(n, 1))(*[_dptr(s) for s in keep])
+        self._check(self._L.shwfs_dm_set(self._h, n, descs, ptrs), "dm_set")
+
+    def wfs_set_opd_terms(self, iwfs: int, use_dm: bool = False, ptt=(0.0, 0.0, 0.0), focus_tel: float = 0.0,
+                          focus_llt: float = 0.0, lltptt=(0.0, 0.0)):
+        """Closed-loop terms of WFS iwfs's OPD for the frames queued from now on."""
+        p = _f64(ptt)
+        lp = _f64(lltptt)
+        self._check(self._L.shwfs_wfs_set_opd_terms(self._h, iwfs, int(bool(use_dm)), _dptr(p), float(focus_tel),
+                                                    float(focus_llt), _dptr(lp)), "wfs_set_opd_terms")
+
+    def wfs_set_opdadd(self, iwfs: int, opd: Optional[np.ndarray]):
+        """NCPA surface (nsa*nopd^2 on the pupil points) added to WFS iwfs's OPD; None removes it."""
+        a = _f64(opd).ravel() if opd is not None else None
+        self._check(self._L.shwfs_wfs_set_opdadd(self._h, iwfs, _dptr(a)), "wfs_set_opdadd")
 
     def set_form(self, form: int):
         self._check(self._L.shwfs_set_form(self._h, form), "set_form")

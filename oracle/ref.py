@@ -264,6 +264,30 @@ def atm_set(screens, layers):
     lib().oref_atm_set(C.c_int(n), ptrs, _p(nx), _p(ny), _p(dx), _p(ox), _p(oy), _p(ht), _p(vx), _p(vy))
 
 
+def cl_set(mirrors=(), surfaces=(), use_dm=False, ptt=(0.0, 0.0, 0.0), focus_tel=0.0, focus_llt=0.0,
+           lltptt=(0.0, 0.0), opdadd=None):
+    """Closed-loop terms of the full-frame path (mirror dicts: nx, ny, dx, ox, oy, ht)."""
+    n = len(mirrors)
+    keep = [np.ascontiguousarray(s, dtype=np.float64) for s in surfaces]
+    ptrs = (C.c_void_p * max(n, 1))(*[k.ctypes.data for k in keep])
+    arr = lambda key, t=np.float64: np.ascontiguousarray([m[key] for m in mirrors] or [0], dtype=t)
+    nx, ny = arr("nx", np.int64), arr("ny", np.int64)
+    dx, ox, oy, ht = (arr(k) for k in ("dx", "ox", "oy", "ht"))
+    p = np.ascontiguousarray(ptt, dtype=np.float64)
+    lp = np.ascontiguousarray(lltptt, dtype=np.float64)
+    oa = None if opdadd is None else np.ascontiguousarray(opdadd, dtype=np.float64).ravel()
+    lib().oref_cl_set(C.c_int(n), ptrs, _p(nx), _p(ny), _p(dx), _p(ox), _p(oy), _p(ht), C.c_int(int(bool(use_dm))),
+                      _p(p), C.c_double(focus_tel), C.c_double(focus_llt), _p(lp), _p(oa))
+
+
+def frame_opd(ref: "RefPowfs", iwfs: int, isim: int, dt: float):
+    """(OPD, LLT OPD or None) of WFS iwfs at step isim on the full-frame path."""
+    opd = np.zeros(ref.nsa * ref.nopd ** 2)
+    llt = np.zeros(ref.llt_nx ** 2) if ref.llt_nx else None
+    lib().oref_frame_opd(C.c_int(iwfs), C.c_int(isim), C.c_double(dt), _p(opd), _p(llt))
+    return opd, llt
+
+
 def frame_full_mt(ref: "RefPowfs", iwfs: int, isim: int, dt: float, seed: int = 1, noisy: bool = True):
     """One complete WFS frame of the reference CPU path; returns (ints, grad, seconds)."""
     ints = np.zeros(ref.nsa * ref.npix)

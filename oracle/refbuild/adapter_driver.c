@@ -39,6 +39,8 @@ int oadp_init(int noisy, double dt){
 	g_sim=mycalloc(1, sim_t);
 	g_sim->parms=parms;
 	g_sim->powfs=powfs;
+	g_sim->save=mycalloc(1, sim_save_t);
+	parms->sim.closeloop=0;
 	g_sim->gradcl=dcellnew(parms->nwfs, 1);
 	return parms->nwfs;
 }
@@ -70,7 +72,118 @@ int oadp_frame(int isim, int iwfs0, int iwfs1, double* grad){
 	gpu_wfsgrad_queue(&t);
 	for(int iwfs=iwfs0; iwfs<iwfs1; iwfs++){
 		gpu_wfsgrad_sync(g_sim, iwfs);
-		memcpy(grad+(iwfs-iwfs0)*ng, P(P(g_sim->gradcl, iwfs)), sizeof(double)*ng);
+		const dmat* g=P(g_sim->gradcl, iwfs);  /* still NULL before the WFS's first output */
+		if(g) memcpy(grad+(iwfs-iwfs0)*ng, P(g), sizeof(double)*ng);
+		else memset(grad+(iwfs-iwfs0)*ng, 0, sizeof(double)*ng);
+	}
+	return 0;
+}
+
+/* Closed-loop state of the simulation as the adapter reads it from sim_t: the DM surfaces
+   (simu->dmrealsq, uploaded through gpu_dmreal2gpu as maos/filter.c:561 does), the tip/tilt
+   mirror (simu->ttmreal), the per-WFS FSM (simu->fsmreal: downlink for NGS, uplink for LGS),
+   the telescope focus (simu->telfocusreal) and the LGS trombone (simu->zoomint, one per WFS).
+   closeloop sets parms->sim.closeloop. */
+int oadp_set_cl(int closeloop, int ndm, const double* const* surf, const long* nx, const long* ny, const double* dx,
+	const double* ox, const double* oy, const double* ht, const double* ttm, const double* fsm, double telfocus,
+	const double* zoomint){
+	sim_t* simu=g_sim;
+	if(!simu) return -1;
+	parms_t* parms=(parms_t*)simu->parms;
+	parms->sim.closeloop=closeloop;
+	cellfree(simu->dmrealsq);
+	simu->dmrealsq=NULL;
+	if(ndm){
+		simu->dmrealsq=mapcellnew(ndm, 1);
+		for(int i=0; i<ndm; i++){
+			map_t* m=P(simu->dmrealsq, i)=mapnew(nx[i], ny[i], dx[i], dx[i]);
+			memcpy(P(m), surf[i], sizeof(double)*nx[i]*ny[i]);
+			m->ox=ox[i]; m->oy=oy[i]; m->ht=ht[i];
+		}
+	}
+	dfree(simu->ttmreal);
+	simu->ttmreal=NULL;
+	if(ttm){ simu->ttmreal=dnew(2, 1); P(simu->ttmreal, 0)=ttm[0]; P(simu->ttmreal, 1)=ttm[1]; }
+	dcellfree(simu->fsmreal);
+	simu->fsmreal=NULL;
+	if(fsm){
+		simu->fsmreal=dcellnew(parms->nwfs, 1);
+		for(int i=0; i<parms->nwfs; i++){
+			P(simu->fsmreal, i)=dnew(2, 1);
+			P(P(simu->fsmreal, i), 0)=fsm[2*i];
+			P(P(simu->fsmreal, i), 1)=fsm[2*i+1];
+		}
+	}
+	dcellfree(simu->telfocusreal);
+	simu->telfocusreal=NULL;
+	if(telfocus!=0){ simu->telfocusreal=dcellnew(1, 1); P(simu->telfocusreal, 0)=dnew(1, 1); P(P(simu->telfocusreal, 0), 0)=telfocus; }
+	dfree(simu->zoomint);
+	simu->zoomint=NULL;
+	if(zoomint){ simu->zoomint=dnew(parms->nwfs, 1); for(int i=0; i<parms->nwfs; i++) P(simu->zoomint, i)=zoomint[i]; }
+	if(simu->dmrealsq) gpu_dmreal2gpu(simu->dmrealsq);
+	return 0;
+}
+
+/* The NCPA surface of every WFS of powfs 0 (powfs.opdadd, nsa*nopd^2 values, the same for all WFS)
+   through gpu_wfssurf2gpu, as maos/setup.c:202 does; NULL removes it. */
+int oadp_set_opdadd(const double* opd){
+	parms_t* parms=oref_parms();
+	powfs_t* powfs=oref_powfs();
+	dcellfree(powfs[0].opdadd);
+	powfs[0].opdadd=NULL;
+	if(opd){
+		const long n=powfs[0].saloc->nloc*powfs[0].pts->nxsa*powfs[0].pts->nxsa;
+		powfs[0].opdadd=dcellnew(parms->powfs[0].nwfs, 1);
+		for(int i=0; i<parms->powfs[0].nwfs; i++){
+			P(powfs[0].opdadd, i)=dnew(n, 1);
+			memcpy(P(P(powfs[0].opdadd, i)), opd, sizeof(double)*n);
+		}
+	}
+	gpu_wfssurf2gpu(parms, powfs);
+	return 0;
+}
+
+/* Sets one option of the reference's parms_t/powfs_t (powfs 0) before oadp_init, for the tests of
+   the options the adapter serves or refuses:
+     1 powfs.nwvl   2 llt.nhs   3 one amplitude map per WFS   4 powfs.phytype_sim   5 powfs.moao
+     6 powfs.fieldstop   7 powfs.dither   8 powfs.pistatout   9 sim.idealwfs   10 a cubic DM (dm.iac)
+     11 atm.dtrat   12 powfs.type   13 powfs.usephy   14 powfs.gtype_sim   15 powfs.phystep
+     16 powfs.step   17 powfs.dtrat */
+int oadp_poke(int what, double v){
+	parms_t* parms=oref_parms();
+	powfs_t* powfs=oref_powfs();
+	if(!parms || !powfs) return -1;
+	powfs_cfg_t* pc=&parms->powfs[0];
+	switch(what){
+	case 1: pc->nwvl=(int)v; break;
+	case 2: if(!pc->llt) return -1; pc->llt->nhs=(int)v; break;
+	case 3:{
+		dcell* a=dcellnew(2, 1);
+		P(a, 0)=dref(P(powfs[0].amp, 0));
+		P(a, 1)=dref(P(powfs[0].amp, 0));
+		dcellfree(powfs[0].amp);
+		powfs[0].amp=a;
+		break;
+	}
+	case 4: pc->phytype_sim=(int)v; break;
+	case 5: pc->moao=(int)v; break;
+	case 6: pc->fieldstop=v; break;
+	case 7: pc->dither=(int)v; break;
+	case 8: pc->pistatout=(int)v; break;
+	case 9: parms->sim.idealwfs=(int)v; break;
+	case 10:
+		parms->ndm=1;
+		parms->dm=mycalloc(1, dm_cfg_t);
+		parms->dm[0].iac=v;
+		break;
+	case 11: parms->atm.dtrat=(int)v; break;
+	case 12: pc->type=(int)v; break;
+	case 13: pc->usephy=(int)v; break;
+	case 14: pc->gtype_sim=(int)v; break;
+	case 15: pc->phystep=(int)v; break;
+	case 16: pc->step=(int)v; break;
+	case 17: pc->dtrat=(int)v; break;
+	default: return -1;
 	}
 	return 0;
 }

@@ -71,9 +71,14 @@ static lmat* lvec(long n, long start){
 
 /* Builds parms_t/powfs_t for one powfs with cfg->nwfs WFS and runs the
    reference's SH setup. Returns the number of valid subapertures. */
+void oref_cl_set(int ndm, const double* const* surf, const long* nx, const long* ny, const double* dx,
+	const double* ox, const double* oy, const double* ht, int use_dm, const double* ptt, double focus_tel,
+	double focus_llt, const double* lltptt, const double* opdadd);
 int oref_setup(const oref_cfg_t* c){
 	dspfree(g_gs0);
 	g_gs0=NULL;
+	/* a new powfs starts with no closed-loop terms */
+	oref_cl_set(0, NULL, NULL, NULL, NULL, NULL, NULL, NULL, 0, NULL, 0, 0, NULL, NULL);
 	if(!global) global=mycalloc(1, global_t);
 	NTHREAD=c->nthread>0?c->nthread:1;
 	omp_set_num_threads(NTHREAD);
@@ -123,6 +128,7 @@ int oref_setup(const oref_cfg_t* c){
 	p->r0=c->r0;
 	p->L0=c->L0;
 	p->dtrat=1;
+	p->moao=-1;   /* no MOAO (the configuration default) */
 	p->usephy=1;
 	p->noisy=1;
 	p->nwfs=c->nwfs;
@@ -476,6 +482,61 @@ void oref_atm_set(int nlayer, const double* const* screens, const long* nx, cons
 }
 map_t** oref_atm(int* nlayer){ *nlayer=g_natm; return g_atm; }
 
+/* Closed-loop and static terms of the full frame's OPD (maos/wfsgrad.c:200-262
+   and 373-377): mirror grids subtracted with prop (wrap=0, alpha=-1, as
+   maos/sim_utils.c:1034-1052 sets up wfs_propdata_dm), loc_add_ptt,
+   loc_add_focus (telescope) and loc_add_focus_offset (LLT zoom), the NCPA
+   surface (powfs.opdadd) and the uplink tip/tilt on the LLT OPD.  ndm = 0 and
+   zeros remove them. */
+static map_t** g_dm=NULL;
+static int g_ndm=0;
+static int g_cl_use_dm=0;
+static real g_cl_ptt[3]={0,0,0}, g_cl_focus_tel=0, g_cl_focus_llt=0, g_cl_lltptt[3]={0,0,0};
+static dmat* g_cl_opdadd=NULL;
+void oref_cl_set(int ndm, const double* const* surf, const long* nx, const long* ny, const double* dx,
+	const double* ox, const double* oy, const double* ht, int use_dm, const double* ptt, double focus_tel,
+	double focus_llt, const double* lltptt, const double* opdadd){
+	for(int i=0; i<g_ndm; i++) mapfree(g_dm[i]);
+	free(g_dm);
+	g_ndm=ndm;
+	g_dm=ndm?mycalloc(ndm, map_t*):NULL;
+	for(int i=0; i<ndm; i++){
+		map_t* m=g_dm[i]=mapnew(nx[i], ny[i], dx[i], dx[i]);
+		memcpy(P(m), surf[i], sizeof(double)*nx[i]*ny[i]);
+		m->ox=ox[i]; m->oy=oy[i]; m->ht=ht[i];
+	}
+	g_cl_use_dm=use_dm;
+	for(int k=0; k<3; k++) g_cl_ptt[k]=ptt?ptt[k]:0;
+	g_cl_focus_tel=focus_tel;
+	g_cl_focus_llt=focus_llt;
+	g_cl_lltptt[0]=0;
+	g_cl_lltptt[1]=lltptt?lltptt[0]:0;
+	g_cl_lltptt[2]=lltptt?lltptt[1]:0;
+	dfree(g_cl_opdadd);
+	g_cl_opdadd=NULL;
+	if(opdadd){
+		const long n=g_powfs[0].saloc->nloc*g_powfs[0].pts->nxsa*g_powfs[0].pts->nxsa;
+		g_cl_opdadd=dnew(n, 1);
+		memcpy(P(g_cl_opdadd), opdadd, sizeof(double)*n);
+	}
+}
+static void cl_apply(dmat* opd, int iwfs){
+	const parms_t* parms=g_parms;
+	powfs_t* powfs=g_powfs;
+	const real hs=parms->wfs[iwfs].hs;
+	if(g_cl_focus_tel) loc_add_focus(opd, powfs[0].loc, g_cl_focus_tel);
+	if(g_cl_focus_llt) loc_add_focus_offset(opd, powfs[0].loc, g_cl_focus_llt,
+		P(parms->powfs[0].llt->ox, 0), P(parms->powfs[0].llt->oy, 0));
+	if(g_cl_opdadd) dadd(&opd, 1, g_cl_opdadd, 1);
+	if(g_cl_use_dm){
+		for(int idm=0; idm<g_ndm; idm++){
+			prop(&(propdata_t){.mapin=g_dm[idm], .ptsout=powfs[0].pts, .phiout=P(opd), .alpha=-1,
+				.hs=hs, .thetax=parms->wfs[iwfs].thetax, .thetay=parms->wfs[iwfs].thetay, .wrap=0});
+		}
+	}
+	if(g_cl_ptt[0]||g_cl_ptt[1]||g_cl_ptt[2]) loc_add_ptt(opd, g_cl_ptt, powfs[0].loc);
+}
+
 /* One complete WFS frame of the reference CPU path at step isim, as
    wfsgrad_iwfs runs it (maos/wfsgrad.c:170-194, 330-473): the ray trace of
    every layer split over 8 threads (LGS) or 2 (NGS) per layer
@@ -506,6 +567,7 @@ double oref_frame_full_mt(int iwfs, int isim, double dt, double* ints, double* g
 		CALL_THREAD(thd, 1);
 		free(thd);
 	}
+	cl_apply(opd, iwfs);
 	dmat* lltopd=NULL;
 	if(powfs[0].llt){
 		lltopd=dnew(powfs[0].llt->pts->nxsa, powfs[0].llt->pts->nysa);
@@ -518,6 +580,7 @@ double oref_frame_full_mt(int iwfs, int isim, double dt, double* ints, double* g
 				.hs=hs, .thetax=parms->wfs[iwfs].thetax-ox/hs, .thetay=parms->wfs[iwfs].thetay-oy/hs,
 				.shiftx=ox-g_atm[ips]->vx*isim*dt, .shifty=oy-g_atm[ips]->vy*isim*dt, .wrap=1});
 		}
+		if(g_cl_lltptt[1]||g_cl_lltptt[2]) loc_add_ptt(lltopd, g_cl_lltptt, powfs[0].llt->loc);
 	}
 	double t1=omp_get_wtime();
 	g_frame_isim=isim;
@@ -526,6 +589,40 @@ double oref_frame_full_mt(int iwfs, int isim, double dt, double* ints, double* g
 	dfree(opd);
 	dfree(lltopd);
 	return (t1-t0)+t;
+}
+
+/* The OPD (nsa*nopd^2) and LLT OPD (llt_nx^2, if any) of WFS iwfs at step isim
+   as oref_frame_full_mt forms them, closed-loop terms included. */
+void oref_frame_opd(int iwfs, int isim, double dt, double* opdout, double* lltout){
+	const parms_t* parms=g_parms;
+	powfs_t* powfs=g_powfs;
+	const long nsa=powfs[0].saloc->nloc;
+	const long nopd=powfs[0].pts->nxsa;
+	const real hs=parms->wfs[iwfs].hs;
+	dmat* opd=dnew_do(nsa*nopd*nopd, 1, opdout, 0);
+	dzero(opd);
+	for(int ips=0; ips<g_natm; ips++){
+		prop(&(propdata_t){.mapin=g_atm[ips], .ptsout=powfs[0].pts, .phiout=P(opd), .alpha=1, .hs=hs,
+			.thetax=parms->wfs[iwfs].thetax, .thetay=parms->wfs[iwfs].thetay,
+			.shiftx=-g_atm[ips]->vx*dt*isim, .shifty=-g_atm[ips]->vy*dt*isim, .wrap=1});
+	}
+	cl_apply(opd, iwfs);
+	dfree(opd);
+	if(lltout && powfs[0].llt){
+		dmat* lltopd=dnew_do(powfs[0].llt->pts->nxsa, powfs[0].llt->pts->nysa, lltout, 0);
+		dzero(lltopd);
+		const real ox=P(parms->powfs[0].llt->ox, 0);
+		const real oy=P(parms->powfs[0].llt->oy, 0);
+		for(int ips=0; ips<g_natm; ips++){
+			const real scale=1.-g_atm[ips]->ht/hs;
+			if(scale<0) continue;
+			prop(&(propdata_t){.mapin=g_atm[ips], .ptsout=powfs[0].llt->pts, .phiout=P(lltopd), .alpha=1,
+				.hs=hs, .thetax=parms->wfs[iwfs].thetax-ox/hs, .thetay=parms->wfs[iwfs].thetay-oy/hs,
+				.shiftx=ox-g_atm[ips]->vx*isim*dt, .shifty=oy-g_atm[ips]->vy*isim*dt, .wrap=1});
+		}
+		if(g_cl_lltptt[1]||g_cl_lltptt[2]) loc_add_ptt(lltopd, g_cl_lltptt, powfs[0].llt->loc);
+		dfree(lltopd);
+	}
 }
 
 /* The second ETF of the time interpolation: the reference's own

@@ -20,7 +20,7 @@ ADAPTER = os.path.join(ROOT, "maos_b200", "csrc", "adapter", "wfs_b200.c")
 SEAM = ["gpu_wfsgrad_init", "gpu_wfs_init_sim", "gpu_wfsgrad_update_etf", "gpu_wfsgrad_update_ref",
         "gpu_wfsgrad_seeding", "gpu_wfsgrad_queue", "gpu_wfsgrad_sync", "gpu_save_pistat",
         "gpu_wfssurf2gpu", "gpu_atm2gpu", "gpu_perfevl_init", "gpu_perfevl_init_sim",
-        "gpu_perfevl_queue", "gpu_perfevl_sync"]
+        "gpu_perfevl_queue", "gpu_perfevl_sync", "gpu_dmreal2gpu", "gpu_dmproj2gpu"]
 
 
 @pytest.fixture(scope="module")
@@ -40,7 +40,7 @@ def adapter_so(tmp_path_factory, ref_lib):
     assert r.returncode == 0, r.stderr[-4000:]
     ld = ["gcc", "-shared", "-o", so, obj, "-L" + os.path.join(ROOT, "oracle", "_ref"),
           "-l:libmaosref.so", "-L" + os.path.dirname(lib), "-l:libshwfs_b200.so",
-          "-Wl,--no-undefined", "-lpthread"]
+          "-Wl,--no-undefined", "-lpthread", "-lm"]
     r = subprocess.run(ld, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-4000:]
     return so

@@ -156,3 +156,102 @@ def test_adapter_science_matches_reference(ref_lib, pttr):
             _, wfe_r, coeff_r, _ = e.frame(*d, isim, dt, pttr=pttr, psfsize=psfsize)
             assert np.all(np.abs(wfe[3 * k:3 * k + 3] - wfe_r) <= 1e-4 * np.abs(wfe_r)), (isim, k)
             assert np.abs(coeff[3 * k:3 * k + 3] - coeff_r).max() <= 1e-4 * np.abs(coeff_r).max(), (isim, k)
+
+
+def _adapter_full(ref_lib):
+    A = _adapter(ref_lib)
+    dp, lp = C.POINTER(C.c_double), C.POINTER(C.c_long)
+    A.oadp_set_cl.argtypes = [C.c_int, C.c_int, C.POINTER(dp), lp, lp, dp, dp, dp, dp, dp, dp, C.c_double, dp]
+    A.oadp_set_opdadd.argtypes = [dp]
+    A.oadp_poke.argtypes = [C.c_int, C.c_double]
+    return A
+
+
+@pytest.mark.parametrize("cfg_name,isim", [("LGS8_N32", 9), ("NGS8", 4)])
+def test_adapter_closed_loop_matches_reference(ref_lib, cfg_name, isim):
+    """sim.closeloop with DM surfaces (simu->dmrealsq through gpu_dmreal2gpu), the tip/tilt mirror,
+    the FSM (downlink for NGS, uplink for LGS), the telescope focus, the LGS trombone and an NCPA
+    surface (powfs.opdadd through gpu_wfssurf2gpu): the adapter's gradients against the reference's
+    CPU frame with the same terms (maos/wfsgrad.c:200-262, 373-377), within 1e-4 relative."""
+    from maos_b200 import configs
+    from tests.helpers import grad_rel_err
+    from tests.test_gpu_closedloop import _mirrors
+    cfg = getattr(configs, cfg_name)
+    llt = bool(cfg.get("has_llt"))
+    screens, layers = _screens(cfg)
+    r = ref_lib.RefPowfs(cfg)
+    ref_lib.atm_set(screens, layers)
+    A = _adapter_full(ref_lib)
+    nwfs = A.oadp_init(0, cfg["dt"])
+    mir, surf = _mirrors(cfg["D"], seed=21)
+    keep = [np.ascontiguousarray(x, dtype=np.float64) for x in surf]
+    dp = C.POINTER(C.c_double)
+    sp = (dp * len(keep))(*[k.ctypes.data_as(dp) for k in keep])
+    col = lambda key, t=np.float64: np.ascontiguousarray([m[key] for m in mir], dtype=t)
+    nx, ny = col("nx", np.int64), col("ny", np.int64)
+    dxs, ox, oy, ht = col("dx"), col("ox"), col("oy"), col("ht")
+    ttm = np.array([2.5e-7, -1.5e-7])
+    fsm = np.array([[1.0e-7 * (k + 1), -6e-8 * (k + 1)] for k in range(nwfs)]).ravel()
+    telfocus = 3e-9
+    zoomint = np.array([1.5e-9 * (k + 1) for k in range(nwfs)])
+    ptr = lambda a: a.ctypes.data_as(dp)
+    lptr = lambda a: a.ctypes.data_as(C.POINTER(C.c_long))
+    assert A.oadp_set_cl(1, len(mir), sp, lptr(nx), lptr(ny), ptr(dxs), ptr(ox), ptr(oy), ptr(ht), ptr(ttm),
+                         ptr(fsm), telfocus, ptr(zoomint) if llt else None) == 0
+    opdadd = np.random.default_rng(22).normal(0, 2e-8, r.nsa * r.nopd ** 2)
+    assert A.oadp_set_opdadd(ptr(opdadd)) == 0
+    g = np.zeros(nwfs * 2 * r.nsa)
+    assert A.oadp_frame(isim, 0, nwfs, ptr(g)) == 0
+    for k in range(nwfs):
+        f = fsm[2 * k:2 * k + 2]
+        ptt = (0.0, -ttm[0] - (0 if llt else f[0]), -ttm[1] - (0 if llt else f[1]))
+        ref_lib.cl_set(mir, surf, use_dm=True, ptt=ptt, focus_tel=-telfocus,
+                       focus_llt=-zoomint[k] if llt else 0.0, lltptt=tuple(f) if llt else (0.0, 0.0), opdadd=opdadd)
+        _, g_ref, _ = ref_lib.frame_full_mt(r, k, isim, cfg["dt"], noisy=False)
+        err = grad_rel_err(g[k * 2 * r.nsa:(k + 1) * 2 * r.nsa], g_ref)
+        assert err <= 1e-4, (cfg_name, k, err)
+    ref_lib.cl_set()
+    A.oadp_set_opdadd(None)
+
+
+def test_adapter_geometric_sensor_and_phystep(ref_lib):
+    """A geometric powfs (usephy 0, gtype_sim z-tilt) returns the z-tilt of the frame's OPD
+    (pts_ztilt); a physical-optics powfs with phystep 3 returns z-tilt gradients (without noise,
+    cuda/sim/wfsgrad.cu:709-712) before frame 3 and physical-optics ones from it; a powfs with
+    step 2 leaves simu->gradcl unset before frame 2."""
+    from maos_b200.configs import NGS8
+    from tests.helpers import grad_rel_err
+    screens, layers = _screens(NGS8)
+    r = ref_lib.RefPowfs(NGS8)
+    ref_lib.atm_set(screens, layers)
+    A = _adapter_full(ref_lib)
+    dp = C.POINTER(C.c_double)
+    n = 2 * r.nsa
+    g = np.zeros(n)
+    # geometric sensor (noisy, but without neasim no noise is drawn)
+    assert A.oadp_poke(13, 0) == 0 and A.oadp_poke(14, 1) == 0
+    A.oadp_init(1, NGS8["dt"])
+    A.oadp_frame(6, 0, 1, g.ctypes.data_as(dp))
+    opd, _ = ref_lib.frame_opd(r, 0, 6, NGS8["dt"])
+    assert grad_rel_err(g, r.ztilt(opd)) <= 1e-4
+    # physical optics from frame 3 on
+    assert A.oadp_poke(13, 1) == 0 and A.oadp_poke(15, 3) == 0
+    A.oadp_init(1, NGS8["dt"])
+    A.oadp_frame(1, 0, 1, g.ctypes.data_as(dp))
+    opd, _ = ref_lib.frame_opd(r, 0, 1, NGS8["dt"])
+    assert grad_rel_err(g, r.ztilt(opd)) <= 1e-4
+    A.oadp_init(0, NGS8["dt"])
+    A.oadp_frame(4, 0, 1, g.ctypes.data_as(dp))
+    _, g_ref, _ = ref_lib.frame_full_mt(r, 0, 4, NGS8["dt"], noisy=False)
+    assert grad_rel_err(g, g_ref) <= 1e-4
+    # the WFS starts at frame 2
+    assert A.oadp_poke(15, 0) == 0 and A.oadp_poke(16, 2) == 0
+    A.oadp_init(0, NGS8["dt"])
+    g[:] = 1.0
+    A.oadp_frame(1, 0, 1, g.ctypes.data_as(dp))
+    assert not g.any()
+    A.oadp_frame(2, 0, 1, g.ctypes.data_as(dp))
+    _, g_ref, _ = ref_lib.frame_full_mt(r, 0, 2, NGS8["dt"], noisy=False)
+    assert grad_rel_err(g, g_ref) <= 1e-4
+    A.oadp_poke(16, 0)
+
