@@ -136,6 +136,14 @@ int shwfs_powfs_set_simap(shwfs_ctx* ctx, int ipowfs, const int* idx, const doub
 int shwfs_powfs_set_etf(shwfs_ctx* ctx, int ipowfs, const double* etf, int slot);
 /* LLT pupil amplitude (llt->amp, llt_nx^2). */
 int shwfs_powfs_set_lltamp(shwfs_ctx* ctx, int ipowfs, const double* lltamp);
+/* Short-exposure OTF of every subaperture (nsa x notf^2 complex, peak in the
+   corner, x fastest), from which shwfs_wfs_update_mtche forms i0, gx and gy:
+   the OTF of the p/t/t-removed turbulence (genseotf, lib/gensei.c:81-111)
+   times the conjugate uplink OTF, to the PSF times saa/n^2 (intstat.sepsf,
+   gensepsf :135-209), back to the OTF times 1/n^2 (gensei :327-335).
+   shwfs_setup_load uploads the setup's (SHWFS_SETUP_SEOTF); NULL removes it,
+   and update_mtche then uses the flat-wavefront OTF. */
+int shwfs_powfs_set_seotf(shwfs_ctx* ctx, int ipowfs, const double* seotf);
 
 /* Declares a WFS; *iwfs receives its index. */
 int shwfs_wfs_add(shwfs_ctx* ctx, const shwfs_wfs_desc* desc, int* iwfs);
@@ -143,9 +151,15 @@ int shwfs_wfs_add(shwfs_ctx* ctx, const shwfs_wfs_desc* desc, int* iwfs);
    column-major block), i0sum (nsa) and i0sumsum (gpu_wfsgrad_update_ref,
    cuda/sim/wfsinit.cu:107). i0sum may be NULL for CoG. */
 int shwfs_wfs_set_mtche(shwfs_ctx* ctx, int iwfs, const double* mtche, const double* i0sum, double i0sumsum);
+/* The matched filter, i0 sums and their total held for WFS iwfs (set by
+   shwfs_wfs_set_mtche or formed by shwfs_wfs_update_mtche), copied to host
+   memory in the layout of shwfs_wfs_set_mtche; any pointer may be NULL.
+   The reverse of gpu_wfsgrad_update_ref (cuda/sim/wfsinit.cu:107). */
+int shwfs_wfs_get_mtche(shwfs_ctx* ctx, int iwfs, double* mtche, double* i0sum, double* i0sumsum);
 /* The matched filter of WFS iwfs regenerated on the device from the powfs's
-   current amplitude, ETF (with its interpolation weights) or DTF nominal,
-   flat uplink OTF and pixel map, in place of a host-built one (the reference
+   short-exposure OTF (shwfs_powfs_set_seotf; else the OTF of a flat wavefront
+   and flat uplink), current ETF (with its interpolation weights) or DTF
+   nominal and pixel map, in place of a host-built one (the reference
    builds it on the host, lib/gensei.c:213-419 and lib/mtch.c:93-335, and
    copies it with gpu_wfsgrad_update_ref, cuda/sim/gpu_sim.h:42): i0 and its
    x/y derivatives of a flat wavefront, then the weighted pseudo-inverse with

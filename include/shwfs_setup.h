@@ -7,8 +7,11 @@
  * reference routine cited beside it; geometry, valid-subaperture selection and
  * pixel-sampling maps are bit-for-bit the reference's.
  *
- * The matched filter is built from the diffraction-limited short-exposure
- * image (no turbulence OTF), then inverted exactly as lib/mtch.c does.
+ * The matched filter is built as the reference builds it: i0 and its
+ * derivatives from the short-exposure OTF of the turbulence and the uplink
+ * (genseotf/genotf with piston, tip and tilt removed, lib/gensei.c:41-111,
+ * lib/genotf.c:46-330; gensepsf, lib/gensei.c:135-209) times the ETF or the
+ * DTF nominal (gensei, :213-419), then inverted as lib/mtch.c does.
  */
 #ifndef SHWFS_SETUP_H
 #define SHWFS_SETUP_H
@@ -40,6 +43,8 @@ typedef struct shwfs_setup_cfg {
 	int na_n;           /* evenly sampled sodium profile */
 	const double* na_h;
 	const double* na_p;
+	double r0, L0;      /* powfs.r0 (at 0.5 um) and powfs.L0 of the matched filter's short-exposure OTF;
+	                       r0 <= 0 or infinite: no turbulence (diffraction-limited) */
 } shwfs_setup_cfg;
 
 typedef struct shwfs_setup shwfs_setup;
@@ -80,6 +85,8 @@ double shwfs_setup_saasum(const shwfs_setup* s);
 #define SHWFS_SETUP_I0 15     /* [nsa*npix] */
 #define SHWFS_SETUP_GX 16     /* [nsa*npix] */
 #define SHWFS_SETUP_GY 17     /* [nsa*npix] */
+#define SHWFS_SETUP_SEPSF 18  /* [nsa*notf^2] short-exposure PSF, peak in the centre (intstat.sepsf) */
+#define SHWFS_SETUP_SEOTF 19  /* [2*nsa*notf^2] its OTF, peak in the corner, interleaved complex */
 int shwfs_setup_get(const shwfs_setup* s, int what, double* out);
 /* [npix*4] pixel-map tap indices into the notf^2 PSF, -1 for unused */
 int shwfs_setup_get_simap_idx(const shwfs_setup* s, int* out);

@@ -29,6 +29,8 @@ struct shwfs_setup {
 	double* lltamp;    /* llt_nx^2 */
 	double llt_orig;
 	double *mtche, *i0sum, *i0, *gx, *gy;
+	double* sepsf;     /* nsa*notf^2 short-exposure PSF (matched filter only) */
+	hcplx* seotf;      /* nsa*notf^2 its OTF / notf^2, peak in the corner */
 };
 
 static int serr(shwfs_setup* s, const char* fmt, ...) {
@@ -434,6 +436,231 @@ static int setup_llt(shwfs_setup* s) {
 	return 0;
 }
 
+/* ---- short-exposure OTF of the turbulence (lib/genotf.c, lib/gensei.c:41-209) ---- */
+
+/* Modified Bessel function of the second kind K_nu(x), x > 0, from its
+   integral representation K_nu(x) = int_0^inf exp(-x cosh t) cosh(nu t) dt
+   (DLMF 10.32.9) by the trapezoidal rule: the integrand is analytic in the
+   strip |Im t| < pi/2 and decays double-exponentially, so the rule converges
+   exponentially (error ~ exp(-pi^2 / h)); h = 1/32 is far below double
+   precision. */
+static double bessel_k(double nu, double x) {
+	const double h = 1. / 32;
+	double s = 0.5 * exp(-x);
+	for (int k = 1; k < 1000000; k++) {
+		const double t = k * h;
+		const double term = exp(-x * cosh(t)) * cosh(nu * t);
+		s += term;
+		if (term < 1e-20 * s) break;
+	}
+	return s * h;
+}
+
+/* Phase covariance (m^2 of OPD, r0 at 0.5 um) at separation r, as turbcov
+   (lib/turbulence.c:400-435) defines it with rmax = 0: von Karman for finite
+   L0, Kolmogorov structure function otherwise. */
+static double turb_cov(double r, double r0, double L0) {
+	const double k05 = pow(2 * M_PI / 0.5e-6, -2);
+	if (!isfinite(L0)) return -0.5 * 6.88 * k05 * pow(r0, -5. / 3.) * pow(r, 5. / 3.);
+	const double tg1 = tgamma(11. / 6) * pow(24. / 5 * tgamma(6. / 5.), 5. / 6.) * k05 / pow(M_PI, 8. / 3.);
+	const double f0 = 1. / L0, r0f0p = pow(r0 * f0, -5. / 3.);
+	if (fabs(r) < EPS_REF) return tg1 * tgamma(5. / 6.) / 2 * r0f0p;
+	const double x = r * 2 * M_PI * f0;
+	return tg1 / pow(2, 5. / 6.) * r0f0p * pow(x, 5. / 6.) * bessel_k(5. / 6., x);
+}
+
+/* Inverse of a symmetric matrix by its eigen-decomposition with the
+   thresholds of svd_pow(A, -1) (math/blas.c:441-481: 1e-7 absolute, 1e-3
+   relative to the previous kept value). a is destroyed. */
+static void pinv_sym(double* a, int n, double* out) {
+	double w[16], v[256];
+	int order[16];
+	hsyev_jacobi(a, n, w, v);
+	for (int i = 0; i < n; i++) order[i] = i;
+	for (int i = 0; i < n; i++)
+		for (int j = i + 1; j < n; j++)
+			if (fabs(w[order[j]]) > fabs(w[order[i]])) {
+				const int t = order[i];
+				order[i] = order[j];
+				order[j] = t;
+			}
+	const double maxeig = fabs(w[order[0]]);
+	double thres2 = 1e-3 * maxeig, sinv[16] = {0};
+	for (int k = 0; k < n; k++) {
+		const double sv = fabs(w[order[k]]);
+		if (sv > 1e-7 * maxeig && sv > thres2) {
+			thres2 = sv * 1e-3;
+			sinv[k] = 1. / w[order[k]];
+		} else {
+			break;
+		}
+	}
+	for (int i = 0; i < n; i++)
+		for (int j = 0; j < n; j++) {
+			double s = 0;
+			for (int k = 0; k < n; k++) s += v[i + order[k] * n] * sinv[k] * v[j + order[k] * n];
+			out[i + j * n] = s;
+		}
+}
+
+/* The tip/tilt-removed short-exposure OTF of one pupil of nx x nx points
+   (spacing dx, amplitude a) for a Kolmogorov/von Karman covariance B of the
+   pupil points (nloc x nloc): genotf_do (lib/genotf.c:46-108) with pttr.
+   Piston, tip and tilt are removed from both sides of B with the amplitude
+   weighting (loc_remove_ptt with cov, math/loc.c:794-826), then
+   OTF(m) = sum over point pairs (i, i+m) of a_i a_{i+m} e^{k^2 B'_{i,i+m}}
+   / sqrt(e^{k^2 B'_ii} e^{k^2 B'_jj}) / sum a^2, on npsf x npsf separations
+   with the zero separation at (npsf/2, npsf/2).  out: npsf^2, x fastest. */
+static void genotf_pupil(const double* B, int nx, double dx, const double* a, double wvl, int npsf, double* out) {
+	const int nloc = nx * nx;
+	double* BP = malloc(sizeof(double) * nloc * nloc);
+	memcpy(BP, B, sizeof(double) * nloc * nloc);
+	double* X = malloc(sizeof(double) * nloc);
+	double* Y = malloc(sizeof(double) * nloc);
+	for (int iy = 0; iy < nx; iy++)
+		for (int ix = 0; ix < nx; ix++) {  /* mksqloc_auto (math/loc.c:526-528) */
+			X[ix + iy * nx] = ix * dx - nx / 2 * dx;
+			Y[ix + iy * nx] = iy * dx - nx / 2 * dx;
+		}
+	double mcc[9] = {0}, imcc[9];
+	for (int i = 0; i < nloc; i++) {
+		const double m[3] = {1, X[i], Y[i]};
+		for (int r = 0; r < 3; r++)
+			for (int c = 0; c < 3; c++) mcc[r + 3 * c] += m[r] * m[c] * a[i];
+	}
+	pinv_sym(mcc, 3, imcc);
+	for (int pass = 0; pass < 2; pass++) {  /* columns, then rows */
+		for (int ic = 0; ic < nloc; ic++) {
+			const long s0 = pass ? ic : (long)ic * nloc, st = pass ? nloc : 1;
+			double c[3] = {0, 0, 0};
+			for (int i = 0; i < nloc; i++) {
+				const double v = BP[s0 + i * st] * a[i];
+				c[0] += v;
+				c[1] += v * X[i];
+				c[2] += v * Y[i];
+			}
+			double t[3];
+			for (int r = 0; r < 3; r++) t[r] = imcc[r] * c[0] + imcc[r + 3] * c[1] + imcc[r + 6] * c[2];
+			for (int i = 0; i < nloc; i++) BP[s0 + i * st] -= t[0] + t[1] * X[i] + t[2] * Y[i];
+		}
+	}
+	const double k2 = pow(2 * M_PI / wvl, 2);
+	double* D = malloc(sizeof(double) * nloc);
+	for (long k = 0; k < (long)nloc * nloc; k++) BP[k] = exp(k2 * BP[k]);
+	for (int i = 0; i < nloc; i++) D[i] = pow(BP[i + (long)i * nloc], -0.5);
+	double an = 0;
+	for (int i = 0; i < nloc; i++) an += a[i] * a[i];
+	an = 1. / an;
+	const int h = npsf / 2;
+	for (int jm = 0; jm < npsf; jm++)
+		for (int im = 0; im < npsf; im++) {
+			const int sx = im - h, sy = jm - h;
+			double acc = 0;
+			for (int iy = 0; iy < nx; iy++) {
+				const int jy = iy + sy;
+				if (jy < 0 || jy >= nx) continue;
+				for (int ix = 0; ix < nx; ix++) {
+					const int jx = ix + sx;
+					if (jx < 0 || jx >= nx) continue;
+					const int i1 = ix + iy * nx, i2 = jx + jy * nx;
+					acc += D[i1] * D[i2] * BP[i2 + (long)i1 * nloc] * a[i1] * a[i2];
+				}
+			}
+			out[im + jm * npsf] = acc * an;
+		}
+	free(BP); free(X); free(Y); free(D);
+}
+
+/* Short-exposure PSF and OTF of every subaperture for the matched filter:
+   genseotf (lib/gensei.c:41-111: a subaperture of area saa > 1 - 1e-10 takes
+   the OTF of the first fullest one, one of area <= 0.01 none), the LLT's OTF
+   (genseotf of the LLT pupil), gensepsf (lib/gensei.c:135-209: OTF times the
+   conjugate uplink OTF, to the PSF, real part times saa / n^2) and the first
+   steps of gensei (:327-335: back to the OTF, times 1/n^2). */
+static int setup_seotf(shwfs_setup* s) {
+	const shwfs_setup_cfg* c = &s->cfg;
+	const int nopd = s->nopd, n = s->notf, nsa = s->nsa, nloc = nopd * nopd;
+	const int npsf = nopd * c->embfac;
+	if (npsf != n) return serr(s, "matched-filter setup needs notf == nopd*embfac");
+	if (nloc > 4096) return serr(s, "matched-filter setup: at most 64x64 OPD points per subaperture");
+	const int turb = c->r0 > 0 && isfinite(c->r0);
+	/* the covariance of the pupil points (loc_sep + turbcov, lib/genotf.c:216-227) */
+	double* B = calloc((size_t)nloc * nloc, sizeof(double));
+	if (turb) {
+		double* cov = malloc(sizeof(double) * nopd * nopd);  /* by |dx|, |dy| in points */
+		for (int dy = 0; dy < nopd; dy++)
+			for (int dx = 0; dx < nopd; dx++)
+				cov[dx + dy * nopd] = turb_cov(sqrt(pow(dx * s->dx, 2) + pow(dy * s->dx, 2)), c->r0, c->L0);
+		for (int j = 0; j < nloc; j++)
+			for (int i = 0; i < nloc; i++)
+				B[i + (long)j * nloc] = cov[abs(i % nopd - j % nopd) + abs(i / nopd - j / nopd) * nopd];
+		free(cov);
+	}
+	double* otf = calloc((size_t)nsa * n * n, sizeof(double));
+	int isafull = -1;
+	double maxarea = 0;
+	for (int isa = 0; isa < nsa; isa++)
+		if (s->saa[isa] > maxarea) {
+			maxarea = s->saa[isa];
+			isafull = isa;
+		}
+	double* full = NULL;
+	if (isafull > 0) {  /* as lib/genotf.c:248: the first subaperture cannot be the template */
+		full = malloc(sizeof(double) * n * n);
+		genotf_pupil(B, nopd, s->dx, s->amp + (size_t)isafull * nloc, c->wvl, n, full);
+	}
+	const double thres = 1 - 1e-10;
+	for (int isa = 0; isa < nsa; isa++) {
+		double* o = otf + (size_t)isa * n * n;
+		if (full && s->saa[isa] > thres) memcpy(o, full, sizeof(double) * n * n);
+		else if (s->saa[isa] > 0.01) genotf_pupil(B, nopd, s->dx, s->amp + (size_t)isa * nloc, c->wvl, n, o);
+	}
+	free(full);
+	free(B);
+	double* lotf = NULL;
+	if (c->has_llt) {
+		const int nl = s->llt_nx, nll = nl * nl;
+		if (nl * c->embfac != n) {
+			free(otf);
+			return serr(s, "LLT pupil size incompatible with notf");
+		}
+		double* BL = calloc((size_t)nll * nll, sizeof(double));
+		if (turb)
+			for (int j = 0; j < nll; j++)
+				for (int i = 0; i < nll; i++) {
+					const double ddx = (i % nl - j % nl) * s->dx, ddy = (i / nl - j / nl) * s->dx;
+					BL[i + (long)j * nll] = turb_cov(sqrt(ddx * ddx + ddy * ddy), c->r0, c->L0);
+				}
+		lotf = malloc(sizeof(double) * n * n);
+		genotf_pupil(BL, nl, s->dx, s->lltamp, c->wvl, n, lotf);
+		free(BL);
+	}
+	s->sepsf = calloc((size_t)nsa * n * n, sizeof(double));
+	s->seotf = malloc(sizeof(hcplx) * nsa * n * n);
+	hcplx* t = malloc(sizeof(hcplx) * n * n);
+	const double n2 = (double)n * n;
+	for (int isa = 0; isa < nsa; isa++) {
+		const double* o = otf + (size_t)isa * n * n;
+		/* the OTFs are real (no static aberration): o * conj(lotf) */
+		for (int i = 0; i < n * n; i++) t[i] = o[i] * (lotf ? lotf[i] : 1.);
+		hfftshift(t, n, n);
+		hfft2(t, n, n, 1);
+		hfftshift(t, n, n);
+		double* ps = s->sepsf + (size_t)isa * n * n;
+		const double norm = s->saa[isa] / n2;
+		for (int i = 0; i < n * n; i++) ps[i] = creal(t[i]) * norm;
+		hcplx* so = s->seotf + (size_t)isa * n * n;
+		for (int i = 0; i < n * n; i++) so[i] = ps[i];
+		hfftshift(so, n, n);
+		hfft2(so, n, n, -1);
+		for (int i = 0; i < n * n; i++) so[i] *= 1. / n2;
+	}
+	free(t);
+	free(otf);
+	free(lotf);
+	return 0;
+}
+
 /* |FFT(embed(amp))|^2 scaled, then FFT: the OTF of a flat wavefront
    (maos/wfsints.c:233-260 with zero OPD). a: nopd^2; out: n^2, peak in corner. */
 static void flat_otf(const double* a, int nopd, int n, double scale, hcplx* out) {
@@ -475,10 +702,17 @@ static int setup_mtch(shwfs_setup* s) {
 	s->gy = calloc((size_t)nsa * npix, sizeof(double));
 	hcplx* otf = malloc(sizeof(hcplx) * n * n);
 	hcplx* t = malloc(sizeof(hcplx) * n * n);
+	/* the matched filter starts from the short-exposure OTF (gensei, lib/gensei.c:327-366), scaled
+	   by the signal level; the CoG's i0 sums from the diffraction-limited frame */
+	const double scale = s->seotf ? c->siglev : norm_ints;
 	for (int isa = 0; isa < nsa; isa++) {
-		flat_otf(s->amp + (size_t)isa * nopd * nopd, nopd, n, 1, otf);
-		if (lotf)
-			for (int i = 0; i < n * n; i++) otf[i] *= conj(lotf[i]);
+		if (s->seotf) {
+			memcpy(otf, s->seotf + (size_t)isa * n * n, sizeof(hcplx) * n * n);
+		} else {
+			flat_otf(s->amp + (size_t)isa * nopd * nopd, nopd, n, 1, otf);
+			if (lotf)
+				for (int i = 0; i < n * n; i++) otf[i] *= conj(lotf[i]);
+		}
 		if (s->etf) {
 			const hcplx* e = s->etf + (size_t)isa * n * n;
 			for (int i = 0; i < n * n; i++) otf[i] *= e[i];
@@ -500,7 +734,7 @@ static int setup_mtch(shwfs_setup* s) {
 					const int id = s->simap_idx[4 * p + k];
 					if (id >= 0) v += s->simap_wt[4 * p + k] * creal(t[id]);
 				}
-				out[p] = v * norm_ints;
+				out[p] = v * scale;
 			}
 		}
 	}
@@ -671,6 +905,7 @@ int shwfs_setup_create(shwfs_setup** ps, const shwfs_setup_cfg* cfg) {
 		if (cfg->has_llt) {
 			if (!((r = setup_etf(s)) == 0 && (r = setup_llt(s)) == 0)) goto out;
 		}
+		if (cfg->gradtype == SHWFS_GRAD_MF && (r = setup_seotf(s)) != 0) goto out;
 		r = setup_mtch(s);
 	}
 out:
@@ -683,6 +918,7 @@ void shwfs_setup_destroy(shwfs_setup* s) {
 	free(s->salocx); free(s->salocy); free(s->origx); free(s->origy); free(s->amp); free(s->saa);
 	free(s->nominal); free(s->simap_idx); free(s->simap_wt); free(s->srot); free(s->srsa); free(s->etf);
 	free(s->lltamp); free(s->mtche); free(s->i0sum); free(s->i0); free(s->gx); free(s->gy);
+	free(s->sepsf); free(s->seotf);
 	free(s);
 }
 const char* shwfs_setup_error(const shwfs_setup* s) { return s ? s->err : "null setup"; }
@@ -720,6 +956,8 @@ int shwfs_setup_get(const shwfs_setup* s, int what, double* out) {
 	case SHWFS_SETUP_I0: src = s->i0; n = nsa * np; break;
 	case SHWFS_SETUP_GX: src = s->gx; n = nsa * np; break;
 	case SHWFS_SETUP_GY: src = s->gy; n = nsa * np; break;
+	case SHWFS_SETUP_SEPSF: src = s->sepsf; n = nsa * n2; break;
+	case SHWFS_SETUP_SEOTF: src = (const double*)s->seotf; n = 2 * nsa * n2; break;
 	default: return SHWFS_EINVAL;
 	}
 	if (!src) return SHWFS_EINVAL;
@@ -776,6 +1014,7 @@ int shwfs_setup_load(const shwfs_setup* s, shwfs_ctx* ctx, int* ipowfs) {
 	} else {
 		if ((r = shwfs_powfs_set_nominal(ctx, *ipowfs, s->nominal, 1))) return r;
 	}
+	if (s->seotf && (r = shwfs_powfs_set_seotf(ctx, *ipowfs, (const double*)s->seotf))) return r;
 	return 0;
 }
 

@@ -62,6 +62,7 @@ struct PowfsState {
 	DevBuf<uint4> tc_bmat;            // tensor-core B operands (bf16 images)
 	DevBuf<float2> gen_buf, gen_lbuf, gen_tw;  // generic-size chain: scratch images (WFS, LLT), twiddles
 	DevBuf<float2> lotf_flat;         // uplink OTF of a flat LLT wavefront (matched-filter regeneration)
+	DevBuf<float2> seotfT;            // short-exposure OTF per subaperture (matched-filter regeneration), transposed
 	DevBuf<float> mtch_img, zero_opd;  // i0/gx/gy scratch; zeros for flat wavefronts
 	DevBuf<double> mtch_red;          // i0 sum total, max i0 sum (float bits)
 	int tc_ready = 0;
@@ -309,6 +310,7 @@ int shwfs_destroy(shwfs_ctx* ctx) {
 		p.gen_lbuf.free_();
 		p.gen_tw.free_();
 		p.lotf_flat.free_();
+		p.seotfT.free_();
 		p.mtch_img.free_();
 		p.zero_opd.free_();
 		p.mtch_red.free_();
@@ -519,6 +521,22 @@ int shwfs_powfs_set_etf(shwfs_ctx* ctx, int ipowfs, const double* etf, int slot)
 	return 0;
 }
 
+int shwfs_powfs_set_seotf(shwfs_ctx* ctx, int ipowfs, const double* seotf) {
+	PowfsState* p = get_powfs(ctx, ipowfs);
+	if (!p || is_geom(p->d.gradtype)) return ctx ? fail(ctx, SHWFS_EINVAL, "set_seotf: bad arguments") : SHWFS_EINVAL;
+	int r = set_device(ctx);
+	if (r) return r;
+	if (!seotf) {
+		CK(cudaStreamSynchronize(ctx->stream));
+		p->seotfT.free_();
+		return 0;
+	}
+	const int n = p->d.notf;
+	std::vector<float2> t((size_t)p->d.nsa * n * n);
+	transpose_blocks_cplx(seotf, t.data(), p->d.nsa, n);
+	return dev_upload(ctx, p->seotfT, t.data(), t.size());
+}
+
 int shwfs_powfs_set_lltamp(shwfs_ctx* ctx, int ipowfs, const double* lltamp) {
 	PowfsState* p = get_powfs(ctx, ipowfs);
 	if (!p || !lltamp || !p->d.has_llt) return ctx ? fail(ctx, SHWFS_EINVAL, "set_lltamp: bad arguments") : SHWFS_EINVAL;
@@ -582,6 +600,30 @@ int shwfs_wfs_set_mtche(shwfs_ctx* ctx, int iwfs, const double* mtche, const dou
 	if (mtche && (r = dev_upload_f(ctx, w->mtche, mtche, (size_t)nsa * 2 * npix))) return r;
 	if (i0sum && (r = dev_upload_f(ctx, w->i0sum, i0sum, nsa))) return r;
 	w->i0sumsum = i0sumsum;
+	return 0;
+}
+
+int shwfs_wfs_get_mtche(shwfs_ctx* ctx, int iwfs, double* mtche, double* i0sum, double* i0sumsum) {
+	WfsState* w = get_wfs(ctx, iwfs);
+	if (!w) return ctx ? fail(ctx, SHWFS_EINVAL, "get_mtche: unknown wfs %d", iwfs) : SHWFS_EINVAL;
+	PowfsState& p = ctx->powfs[w->d.ipowfs];
+	const size_t nsa = p.d.nsa, n = nsa * 2 * p.d.pixpsax * p.d.pixpsay;
+	if ((mtche && !w->mtche.p) || (i0sum && !w->i0sum.p))
+		return fail(ctx, SHWFS_ESTATE, "get_mtche: WFS %d has no matched filter", iwfs);
+	int r = set_device(ctx);
+	if (r) return r;
+	std::vector<float> t(std::max(n, nsa));
+	if (mtche) {
+		CK(cudaMemcpyAsync(t.data(), w->mtche.p, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+		CK(cudaStreamSynchronize(ctx->stream));
+		for (size_t k = 0; k < n; k++) mtche[k] = t[k];
+	}
+	if (i0sum) {
+		CK(cudaMemcpyAsync(t.data(), w->i0sum.p, nsa * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+		CK(cudaStreamSynchronize(ctx->stream));
+		for (size_t k = 0; k < nsa; k++) i0sum[k] = t[k];
+	}
+	if (i0sumsum) *i0sumsum = w->i0sumsum;
 	return 0;
 }
 
@@ -1910,7 +1952,8 @@ int shwfs_wfs_update_mtche(shwfs_ctx* ctx, int iwfs, int mtchcr) {
 		std::vector<float> z(256, 0.f);
 		if ((r = dev_upload(ctx, p.zero_opd, z.data(), z.size()))) return r;
 	}
-	if (d.has_llt && !p.lotf_flat.p) {  // flat uplink OTF, as the host setup (lib/gensei.c with lotf)
+	const bool se = p.seotfT.p != nullptr;  // the short-exposure OTF of shwfs_powfs_set_seotf
+	if (!se && d.has_llt && !p.lotf_flat.p) {  // without it: the flat uplink OTF
 		if (!p.lltamp.p) return fail(ctx, SHWFS_ESTATE, "update_mtche: LLT amplitude not set");
 		if ((r = dev_alloc(ctx, p.lotf_flat, (size_t)d.notf * d.notf))) return r;
 		DevBuf<const float*> in;
@@ -1945,7 +1988,9 @@ int shwfs_wfs_update_mtche(shwfs_ctx* ctx, int iwfs, int mtchcr) {
 		M.cry = M.nmod;
 		M.nmod += 2;
 	}
-	M.norm_ints = norm_ints(p, *w);
+	// gensei (lib/gensei.c:320-366) scales the short-exposure images by the signal level alone
+	M.norm_ints = se ? (float)(w->d.sigsim * w->d.wvlwt) : norm_ints(p, *w);
+	M.seotfT = se ? p.seotfT.p : nullptr;
 	M.dux = (float)(1.0 / (d.wvl / (d.dsa * d.embfac) * d.notf));
 	M.amp = p.amp.p + (p.namp > 1 ? (size_t)w->wfsind * nsa * 256 : 0);
 	M.zero_opd = p.zero_opd.p;

@@ -3,14 +3,18 @@
 // the matched filter (lib/mtch.c:93-211 mtch, :223-335 mtch_cell) on the host
 // and copies them in (gpu_wfsgrad_update_ref, cuda/sim/gpu_sim.h:42); here
 // they are formed from the device-resident amplitude, transfer functions and
-// flat uplink OTF, so a sodium-profile or reference update needs no host
-// round trip.  As the project's host setup, the images are those of a flat
-// wavefront (the short-exposure diffraction-limited OTF).
+// short-exposure OTF, so a sodium-profile or reference update needs no host
+// round trip.  The short-exposure OTF of each subaperture (turbulence with
+// piston/tip/tilt removed times the conjugate uplink OTF, as genseotf and
+// gensepsf form it, lib/gensei.c:41-209) is static and uploaded once
+// (shwfs_powfs_set_seotf); without it the images are those of a flat
+// wavefront.
 //
-//   mtch_images_kernel: one warp per subaperture; OTF of the flat field x
-//     conj(flat uplink OTF) x ETF / nominal, times 1, Ux(fx), Ux(fy) with
-//     Ux(f) = -2 pi i f' / (dtheta n) (f' the signed frequency), inverse FFT,
-//     real part, pixel map, x norm_ints -> i0, gx, gy; i0 sums and their max.
+//   mtch_images_kernel: one warp per subaperture; the short-exposure OTF (or
+//     the OTF of the flat field x conj(flat uplink OTF)) x ETF / nominal,
+//     times 1, Ux(fx), Ux(fy) with Ux(f) = -2 pi i f' / (dtheta n) (f' the
+//     signed frequency), inverse FFT, real part, pixel map, x the signal
+//     level (x norm_ints for the flat field) -> i0, gx, gy; i0 sums and max.
 //   mtch_filter_kernel: one warp per subaperture; A = [gx, gy, i0 kp + 2 bkg,
 //     (i0 shifted by +-1 pixel in x, y)], W = 1 / (rne^2 + bkg + i0), the
 //     weighted pseudo-inverse (A'WA)^-1 A'W with the eigenvalue thresholds of
@@ -33,6 +37,7 @@ struct MtchParams {
 	const float* amp;             // nsa * 256
 	const float* zero_opd;        // 256 zeros
 	const float2* lotfT;          // flat uplink OTF (transposed), or null
+	const float2* seotfT;         // nsa * 1024 short-exposure OTF (transposed), or null: flat wavefront
 	const float2* etfT1;          // nsa * 1024 transposed, or null
 	const float2* etfT2;
 	float etfwt1, etfwt2;
@@ -56,11 +61,17 @@ __global__ void __launch_bounds__(128) mtch_images_kernel(MtchParams M) {
 	if (isa >= M.nsa) return;
 	float2* tile = tiles[warp];
 	float2 F[32];
-	field_fft_n32(M.zero_opd, M.amp + (size_t)isa * 256, 0.f, tile, lane, F);
-	psf_to_otf_n32(F, 1.f, tile, lane);  // lane = fy holds OTF(fx, fy) in F[fx]
-	if (M.lotfT) {
+	if (M.seotfT) {  // the short-exposure OTF of turbulence and uplink (genseotf, gensepsf)
+		const float2* so = M.seotfT + (size_t)isa * 1024 + lane;
 #pragma unroll
-		for (int fx = 0; fx < 32; fx++) F[fx] = cmulc(F[fx], __ldg(M.lotfT + lane + 32 * fx));
+		for (int fx = 0; fx < 32; fx++) F[fx] = __ldg(so + 32 * fx);
+	} else {
+		field_fft_n32(M.zero_opd, M.amp + (size_t)isa * 256, 0.f, tile, lane, F);
+		psf_to_otf_n32(F, 1.f, tile, lane);  // lane = fy holds OTF(fx, fy) in F[fx]
+		if (M.lotfT) {
+#pragma unroll
+			for (int fx = 0; fx < 32; fx++) F[fx] = cmulc(F[fx], __ldg(M.lotfT + lane + 32 * fx));
+		}
 	}
 	if (M.etfT1) {
 		const float2* e1 = M.etfT1 + (size_t)isa * 1024 + lane;

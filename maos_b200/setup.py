@@ -18,7 +18,7 @@ from . import shwfs
 from .configs import sodium_gaussian
 
 GET = dict(salocx=1, salocy=2, origx=3, origy=4, amp=5, saa=6, nominal=7, simap_wt=8, srot=9, srsa=10, etf=11,
-           lltamp=12, mtche=13, i0sum=14, i0=15, gx=16, gy=17)
+           lltamp=12, mtche=13, i0sum=14, i0=15, gx=16, gy=17, sepsf=18, seotf=19)
 
 
 class SetupCfg(C.Structure):
@@ -29,7 +29,8 @@ class SetupCfg(C.Structure):
                 ("bkgrnd", C.c_double), ("bkgrndc", C.c_double), ("gradtype", C.c_int), ("sigmatch", C.c_int),
                 ("mtchcr", C.c_int), ("cogthres", C.c_double), ("cogoff", C.c_double), ("has_llt", C.c_int),
                 ("llt_d", C.c_double), ("llt_widthp", C.c_double), ("llt_ox", C.c_double), ("llt_oy", C.c_double),
-                ("na_n", C.c_int), ("na_h", C.c_void_p), ("na_p", C.c_void_p)]
+                ("na_n", C.c_int), ("na_h", C.c_void_p), ("na_p", C.c_void_p), ("r0", C.c_double),
+                ("L0", C.c_double)]
 
 
 _bound = False
@@ -86,7 +87,8 @@ class Setup:
                      has_llt=cfg.get("has_llt", 0), llt_d=cfg.get("llt_d", 0.0), llt_widthp=cfg.get("llt_widthp", 0.0),
                      llt_ox=cfg.get("llt_ox", 0.0), llt_oy=cfg.get("llt_oy", 0.0),
                      na_n=0 if na_h is None else len(na_h),
-                     na_h=None if na_h is None else na_h.ctypes.data, na_p=None if na_p is None else na_p.ctypes.data)
+                     na_h=None if na_h is None else na_h.ctypes.data, na_p=None if na_p is None else na_p.ctypes.data,
+                     r0=cfg.get("r0", 0.0), L0=cfg.get("L0", math.inf))
         h = C.c_void_p()
         rc = L.shwfs_setup_create(C.byref(h), C.byref(c))
         self._h = h
@@ -120,14 +122,15 @@ class Setup:
         nsa, n2, np_, no2 = self.nsa, self.notf ** 2, self.npix, self.nopd ** 2
         return dict(salocx=nsa, salocy=nsa, origx=nsa, origy=nsa, amp=nsa * no2, saa=nsa, nominal=n2,
                     simap_wt=np_ * 4, srot=nsa, srsa=nsa, etf=2 * nsa * n2, lltamp=self.llt_nx ** 2,
-                    mtche=nsa * 2 * np_, i0sum=nsa, i0=nsa * np_, gx=nsa * np_, gy=nsa * np_)[name]
+                    mtche=nsa * 2 * np_, i0sum=nsa, i0=nsa * np_, gx=nsa * np_, gy=nsa * np_, sepsf=nsa * n2,
+                    seotf=2 * nsa * n2)[name]
 
     def get(self, name: str) -> np.ndarray:
         out = np.zeros(self._size(name))
         rc = _lib().shwfs_setup_get(self._h, GET[name], out.ctypes.data_as(C.POINTER(C.c_double)))
         if rc != 0:
             raise shwfs.ShwfsError(f"setup array {name} is not available")
-        if name == "etf":
+        if name in ("etf", "seotf"):
             return (out[0::2] + 1j * out[1::2]).reshape(self.nsa, self.notf ** 2)
         return out
 

@@ -131,6 +131,8 @@ def _load() -> C.CDLL:
         "shwfs_dm_set": [vp, i, C.POINTER(LayerDesc), C.POINTER(dp)],
         "shwfs_wfs_set_opd_terms": [vp, i, i, dp, C.c_double, C.c_double, dp],
         "shwfs_wfs_set_opdadd": [vp, i, dp],
+        "shwfs_powfs_set_seotf": [vp, i, dp],
+        "shwfs_wfs_get_mtche": [vp, i, dp, dp, dp],
     }
     for name, args in sig.items():
         f = getattr(lib, name)
@@ -201,6 +203,7 @@ class Context:
         self.npix = {}
         self.nsa = {}
         self.wfs_nsa = {}  # iwfs -> subapertures of its powfs
+        self.wfs_powfs = {}  # iwfs -> its powfs
         _live.add(self)
 
     def _check(self, rc: int, what: str):
@@ -280,6 +283,15 @@ class Context:
         """powfs.saasum for sigmatch 2 CoG (default: the sum of saa)."""
         self._check(self._L.shwfs_powfs_set_saasum(self._h, ipowfs, float(saasum)), "powfs_set_saasum")
 
+    def powfs_set_seotf(self, ipowfs, seotf):
+        """Short-exposure OTF per subaperture ((nsa, notf^2) complex, peak in the corner) for the
+        device matched-filter regeneration; None removes it."""
+        if seotf is None:
+            self._check(self._L.shwfs_powfs_set_seotf(self._h, ipowfs, None), "powfs_set_seotf")
+            return
+        a = np.ascontiguousarray(seotf, dtype=np.complex128).view(np.float64)
+        self._check(self._L.shwfs_powfs_set_seotf(self._h, ipowfs, _dptr(a)), "powfs_set_seotf")
+
     def powfs_set_lltamp(self, ipowfs, lltamp):
         a = _f64(lltamp)
         self._check(self._L.shwfs_powfs_set_lltamp(self._h, ipowfs, _dptr(a)), "powfs_set_lltamp")
@@ -289,6 +301,7 @@ class Context:
         out = C.c_int()
         self._check(self._L.shwfs_wfs_add(self._h, C.byref(d), C.byref(out)), "wfs_add")
         self.wfs_nsa[out.value] = self.nsa.get(d.ipowfs, 0)
+        self.wfs_powfs[out.value] = d.ipowfs
         return out.value
 
     def wfs_set_mtche(self, iwfs, mtche, i0sum=None, i0sumsum=0.0):
@@ -366,6 +379,16 @@ class Context:
         g = np.zeros(sum(sizes))
         self._check(self._L.shwfs_frame_sync_range(self._h, iwfs0, iwfs1, _dptr(g)), "frame_sync_range")
         return np.split(g, np.cumsum(sizes)[:-1])
+
+    def wfs_get_mtche(self, iwfs: int):
+        """(mtche (nsa, 2*npix), i0sum (nsa), i0sumsum) held for WFS iwfs."""
+        nsa = self.wfs_nsa[iwfs]
+        npix = self.npix[self.wfs_powfs[iwfs]]
+        m = np.zeros(nsa * 2 * npix)
+        s = np.zeros(nsa)
+        tot = C.c_double()
+        self._check(self._L.shwfs_wfs_get_mtche(self._h, iwfs, _dptr(m), _dptr(s), C.byref(tot)), "wfs_get_mtche")
+        return m.reshape(nsa, 2 * npix), s, tot.value
 
     def wfs_update_mtche(self, iwfs: int, mtchcr: int):
         """Regenerate WFS iwfs's matched filter on the device (shwfs_wfs_update_mtche)."""

@@ -201,6 +201,18 @@ class RefPowfs:
             out[isa] = buf
         return out
 
+    def sepsf(self, isa: int):
+        n = self.notf
+        a = np.zeros(n * n)
+        lib().oref_get_sepsf(C.c_int(isa), _p(a))
+        return a
+
+    def i0(self, isa: int):
+        """(i0, gx, gy) of subaperture isa, each npix."""
+        i0, gx, gy = np.zeros(self.npix), np.zeros(self.npix), np.zeros(self.npix)
+        lib().oref_get_i0(C.c_int(isa), _p(i0), _p(gx), _p(gy))
+        return i0, gx, gy
+
     def i0sum(self):
         a = np.zeros(self.nsa); lib().oref_get_i0sum(_p(a)); return a
 
@@ -322,6 +334,14 @@ def genatm_simple(r0, L0, slope, dx, n, seed):
     lib().oref_genatm_simple(C.c_double(r0), C.c_double(L0), C.c_double(slope), C.c_double(dx), C.c_long(n),
                              C.c_uint(seed), _p(out))
     return out.reshape(n, n)
+
+
+def turbcov(r, r0, L0):
+    """The reference's turbcov (rmax 0) at separations r."""
+    r = np.ascontiguousarray(r, dtype=np.float64)
+    out = np.zeros_like(r)
+    lib().oref_turbcov(_p(r), C.c_long(r.size), C.c_double(r0), C.c_double(L0), _p(out))
+    return out
 
 
 def genscreen(nx, ny, dx, r0, L0, wt, seed):

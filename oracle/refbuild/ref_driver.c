@@ -267,6 +267,21 @@ void oref_get_i0sum(double* out){
 	for(long i=0; i<NX(s); i++) out[i]=P(s, i, 0);
 }
 double oref_get_i0sumsum(void){ return P(g_powfs[0].intstat->i0sumsum, 0); }
+/* The short-exposure PSF of subaperture isa (intstat->sepsf, gensepsf, lib/gensei.c:135-209):
+   notf^2, peak in the centre. */
+void oref_get_sepsf(int isa, double* out){
+	const dmat* p=P(P(g_powfs[0].intstat->sepsf, 0, 0), isa);
+	copy_vec(out, P(p), PN(p));
+}
+/* turbcov (lib/turbulence.c:400-435) of n separations r with rmax 0. */
+void oref_turbcov(const double* r, long n, double r0, double L0, double* out){
+	dmat* rr=dnew(n, 1);
+	memcpy(P(rr), r, sizeof(double)*n);
+	dmat* c=turbcov(rr, 0, r0, L0);
+	copy_vec(out, P(c), n);
+	dfree(c);
+	dfree(rr);
+}
 void oref_get_i0(int isa, double* i0, double* gx, double* gy){
 	intstat_t* st=g_powfs[0].intstat;
 	copy_vec(i0, P(P(st->i0, isa, 0)), PN(P(st->i0, isa, 0)));

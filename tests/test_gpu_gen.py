@@ -47,3 +47,30 @@ def test_ngs_fft128_frame_matches_reference(ref_lib):
 def test_tiptilt_fft256_frame_matches_reference(ref_lib):
     from maos_b200.configs import TT30
     _check(ref_lib, TT30, 3, use_ref_mtche=False)
+
+
+def test_stress_config_full_size_matches_reference(ref_lib):
+    """The large-sampling stress configuration at its full size: 30 m telescope, 6 LGS of
+    60x60 subapertures (2820 valid), 32x32 OPD points, FFT 64, 12x12 pixels of 0.8", the
+    two-Gaussian sodium profile (88 and 94 km) and 7 layers on 4096^2 screens at 1/64 m.
+    The product's own setup and matched filter throughout; two WFS on two frames against the
+    reference's CPU frame on the same screens, with its own setup and matched filter."""
+    import os
+    from maos_b200.configs import LGS30_N64
+    from maos_b200.workload import build
+    from tests.helpers import ints_tolerance_ok, grad_rel_err
+    cfg = LGS30_N64
+    wl = build(cfg, device=0, seed=4, noisy=False)
+    assert wl.nsa == 2820 and wl.setup.notf == 64 and wl.npix == 144 and wl.screens[0].shape == (4096, 4096)
+    r = ref_lib.RefPowfs(cfg, nthread=os.cpu_count() or 1)
+    ref_lib.atm_set(wl.screens, wl.layers)
+    for isim in (0, 17):
+        wl.frame(isim)
+        out = wl.frame_sync(want_ints=True)
+        for k in (0, 4):
+            ints_ref, g_ref, _ = ref_lib.frame_full_mt(r, k, isim, cfg["dt"], noisy=False)
+            g, ints = out[k]
+            ok, worst = ints_tolerance_ok(ints, ints_ref, r.nsa, r.npix, 1e-5)
+            assert ok, f"wfs {k}: intensity error {worst:.3e} of subaperture total"
+            assert grad_rel_err(g, g_ref) <= 1e-4, (isim, k, grad_rel_err(g, g_ref))
+    wl.close()
