@@ -331,9 +331,9 @@ int shwfs_copy_counters(shwfs_ctx* ctx, uint64_t* h2d, uint64_t* d2h);
    gradients -- that allocates no device memory: its scratch (OPD, LLT OPD,
    uplink OTF, launch descriptor) lives in one file-scope device array of
    about 4 MiB that every GPU loading the library keeps until exit.  For
-   callers that cannot call cudaMalloc once running (real-time loops that
-   forbid allocation after start-up, stream capture into a CUDA graph,
-   externally managed memory).  ints (nsa*npix) and grad (2*nsa) are device
+   callers that cannot call cudaMalloc once running: real-time loops that
+   forbid allocation after start-up (it can block and can fail), and hosts
+   whose device memory belongs to their own pool.  ints (nsa*npix) and grad (2*nsa) are device
    pointers owned by the caller; either may be NULL, not both.  Limits: at
    most SHWFS_NOALLOC_MAX_NSA subapertures, each of 16x16 OPD points padded
    to a 32x32 FFT (the 32-point form, at most 128 pixels); any other powfs

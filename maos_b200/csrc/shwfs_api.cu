@@ -2279,10 +2279,10 @@ int shwfs_sync(shwfs_ctx* ctx) {
 // Allocation-free frame.
 //
 // For callers that must not allocate device memory once they run: a
-// real-time control loop that forbids allocation after start-up, code that
-// records the frame into a CUDA graph (cudaMalloc is not allowed while a
-// stream is being captured), or a host whose memory pool is handed out by
-// someone else.  The ordinary frame keeps its scratch (the ray-traced OPD,
+// real-time control loop that forbids allocation after start-up (an
+// allocation can block for milliseconds and fail when memory is short), or a
+// host application whose device memory is handed out by its own pool.  The
+// ordinary frame keeps its scratch (the ray-traced OPD,
 // the LLT OPD, the uplink OTF and the launch descriptor) in buffers the
 // context allocates; this variant keeps them in one file-scope device array
 // instead, so a call allocates nothing.

@@ -1,9 +1,10 @@
 """The allocation-free frame (shwfs_frame_noalloc) against the ordinary frame.
 
-Some callers cannot allocate device memory once they run -- a real-time loop
-that forbids allocation after start-up, or code recording the frame into a
-CUDA graph, where cudaMalloc is not allowed during stream capture.  For them
-the C ABI has one entry point whose scratch lives in a static device array.
+Some callers cannot allocate device memory once they run: a real-time loop
+that forbids allocation after start-up (cudaMalloc can block for a long time
+and can fail when memory runs short), or a host application whose device
+memory belongs to its own pool.  For them the C ABI has one entry point whose
+scratch lives in a static device array.
 This test calls it through the C ABI twice in a row and checks each result
 against the ordinary entry point (shwfs_frame_queue + shwfs_frame_sync) with
 the tolerances of the other parity tests: intensities within 1e-5 of the
