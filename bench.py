@@ -433,6 +433,20 @@ def run_batch(args, bcfg):
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     lgs = wl.members[0]
     variant = ctx.autotune(lgs[3][0], lgs[3][-1] + 1, nrep=5)
+    # both frame layouts: the per-powfs launches (a graph branch per sensor type) and
+    # the imaging of all sensors as one persistent work-list launch
+    isim = 1000
+    layouts = {}
+    for name, on in (("branches", False), ("worklist", True)):
+        ctx.set_worklist(on)
+        for _ in range(args.warmup):
+            wl.frame(isim)
+            isim += 1
+        ctx.sync()
+        ms, isim = _time_frames(wl, ext, flush, isim, args.steps)
+        layouts[name] = {"value": units_per_step * args.steps / (sum(ms) * 1e-3), "ms_per_step": sum(ms) / args.steps}
+    choice = ctx.autotune_frame(0, wl.nwfs, nrep=5)
+    layouts["chosen"] = "branches" if choice == 0 else "worklist"
     isim = 0
     for _ in range(args.warmup):
         wl.frame(isim)
@@ -506,9 +520,12 @@ def run_batch(args, bcfg):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": bcfg["name"], "members": members, "layers": nlayer,
                    "screen": f"{lcfg['atm']['nx']}^2 FP32", "form": form_name, "noise": True,
-                   "frame": "one CUDA graph per frame, one branch per sensor type", "imaging_variant": variant,
+                   "frame": ("one CUDA graph per frame, one branch per sensor type" if choice == 0 else
+                             "one CUDA graph per frame: ray traces, then one persistent work-list imaging launch"),
+                   "imaging_variant": variant, "layout_choice": choice,
                    "l2": "flushed (256 MiB write) before every timed step", "parallelism": f"replicas x{ws}"},
         "frame_latency_ms": {"p50": p50, "p99": p99},
+        "layouts": layouts,
         "stages": st,
         "gpu_launches": int(round(launches_per_step * args.steps)),
         "e2e": {"value": e2e, "unit": "subap-images/s", "h2d_bytes_per_step": h2d // args.steps,

@@ -345,6 +345,28 @@ int shwfs_copy_counters(shwfs_ctx* ctx, uint64_t* h2d, uint64_t* d2h);
 #define SHWFS_NOALLOC_MAX_NSA 4096
 int shwfs_frame_noalloc(shwfs_ctx* ctx, int iwfs, int isim, float* ints, float* grad);
 
+/* ---- the frame's imaging as one persistent launch ----
+   With on != 0, shwfs_frame_queue and shwfs_frame_graph run the imaging
+   (field, FFTs, transfer functions, pixels, noise, gradients) of every powfs
+   of the frame in one persistent launch over a work list of (WFS,
+   subaperture, FFT size) items: groups of four 32-point images, tiles of the
+   FFT-pass chain of the 128- and 256-point images (each pass waits, bounded,
+   for its image's previous pass) and their pixel steps; ray traces and
+   uplinks stay separate launches.  Replaces the reference's per-WFS launch
+   chains and cuFFT plans (cuda/sim/wfsgrad.cu:483-745,
+   cuda/sim/wfsinit.cu:321-342).  FFT form, dtrat 1, sigmatch 0/1, at most 4
+   powfs; a frame with any other powfs runs the ordinary per-powfs launches.
+   slices (0 keeps the current value, default 7): the 32-point groups are cut
+   into that many slices placed between the passes of the large images;
+   group (0 keeps the current value, default 4, at most 64): 32-point images
+   per work item. */
+int shwfs_set_worklist(shwfs_ctx* ctx, int on, int slices, int group);
+/* Times nrep whole frames of WFS [iwfs0, iwfs1) with the per-powfs launches
+   and with the work list at (slices, group) = (7, 4), (14, 4), (28, 4),
+   (7, 8), and keeps the fastest; *choice receives 0 for the per-powfs
+   launches, 1-4 for the work-list settings in that order. */
+int shwfs_autotune_frame(shwfs_ctx* ctx, int iwfs0, int iwfs1, int nrep, int* choice);
+
 /* Synchronise the context stream; returns the first error of queued work. */
 int shwfs_sync(shwfs_ctx* ctx);
 /* The CUDA stream the context launches on (cudaStream_t as void*). */

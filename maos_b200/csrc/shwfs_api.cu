@@ -20,6 +20,7 @@
 #include "shwfs_tc.cuh"
 #include "shwfs_gen.cuh"
 #include "shwfs_mtch.cuh"
+#include "shwfs_worklist.cuh"
 
 using namespace shwfs;
 
@@ -158,6 +159,16 @@ struct shwfs_ctx {
 	std::vector<Mark> marks;
 	EvlState* evl = nullptr;
 	int sig2_inner = 0;        // launch_ints_sig2 is running the imaging part
+	// one persistent imaging launch per frame over a work list (shwfs_set_worklist)
+	int worklist = 0;
+	int wl_slices = 7;                   // slices of 32-point groups between the passes of the large images
+	int wl_group = 4;                    // 32-point images per work item
+	struct WorkCache {
+		std::vector<int4> h;
+		DevBuf<int4> d;
+	};
+	std::vector<WorkCache> wl_cache;
+	DevBuf<int> wl_cnt;                  // dispenser + per-image tile counters
 	int dtrat_inner = 0;       // launch_ints_dtrat is running the imaging part
 };
 static void evl_free(shwfs_ctx* ctx);
@@ -253,7 +264,7 @@ static int check_errflag(shwfs_ctx* ctx) {
 	CK(cudaMemcpy(&v, ctx->errflag.p, sizeof(int), cudaMemcpyDeviceToHost));
 	if (v) {
 		CK(cudaMemset(ctx->errflag.p, 0, sizeof(int)));
-		return fail(ctx, SHWFS_ETIMEOUT, "a bounded tensor-core wait expired in the imaging kernel");
+		return fail(ctx, SHWFS_ETIMEOUT, "a bounded device wait expired in an imaging kernel");
 	}
 	return 0;
 }
@@ -320,6 +331,8 @@ int shwfs_destroy(shwfs_ctx* ctx) {
 	}
 	evl_free(ctx);
 	for (auto& c : ctx->desc_cache) c.d.free_();
+	for (auto& c : ctx->wl_cache) c.d.free_();
+	ctx->wl_cnt.free_();
 	if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
 	for (size_t i = 0; i < ctx->pstream.size(); i++) {
 		cudaStreamSynchronize(ctx->pstream[i]);
@@ -1737,6 +1750,7 @@ static int launch_geom_grad(shwfs_ctx* ctx, WfsState& w, const float* opd, float
 }
 
 // The work of one powfs in a frame: ray trace (and uplink), then imaging.
+static int trace_powfs(shwfs_ctx* ctx, int ip, const std::vector<int>& wl, int isim);
 static int frame_powfs(shwfs_ctx* ctx, int ip, const std::vector<int>& wl, int isim) {
 	PowfsState& p = ctx->powfs[ip];
 	int r;
@@ -1756,7 +1770,28 @@ static int frame_powfs(shwfs_ctx* ctx, int ip, const std::vector<int>& wl, int i
 		}
 		return 0;
 	}
-	// (a) one ray-trace launch per batch of pupils (WFS + LLT)
+	if ((r = trace_powfs(ctx, ip, wl, isim))) return r;
+	// (b)-(e)
+	std::vector<const float*> opds;
+	std::vector<const float2*> lotf;
+	std::vector<float*> in, gr;
+	std::vector<int> nz;
+	for (int i : wl) {
+		WfsState& w = ctx->wfs[i];
+		opds.push_back(w.opd.p);
+		lotf.push_back(p.d.has_llt ? w.lotfT.p : nullptr);
+		in.push_back(w.ints.p);
+		gr.push_back(w.grad.p);
+		nz.push_back(w.d.noisy);
+	}
+	return launch_ints(ctx, ip, wl, isim, opds, lotf, in, gr, nz);
+}
+
+// (a) of a physical-optics powfs: one ray-trace launch per batch of pupils
+// (WFS + LLT), and the uplink OTFs of the larger sizes.
+static int trace_powfs(shwfs_ctx* ctx, int ip, const std::vector<int>& wl, int isim) {
+	PowfsState& p = ctx->powfs[ip];
+	int r;
 	const int per = p.d.has_llt ? SHWFS_MAX_ENTRIES / 2 : SHWFS_MAX_ENTRIES;
 	for (size_t b = 0; b < wl.size(); b += per) {
 		GeomParams gp;
@@ -1777,20 +1812,7 @@ static int frame_powfs(shwfs_ctx* ctx, int ip, const std::vector<int>& wl, int i
 			if ((r = launch_uplink_gen(ctx, p, bw, lo))) return r;
 		}
 	}
-	// (b)-(e)
-	std::vector<const float*> opds;
-	std::vector<const float2*> lotf;
-	std::vector<float*> in, gr;
-	std::vector<int> nz;
-	for (int i : wl) {
-		WfsState& w = ctx->wfs[i];
-		opds.push_back(w.opd.p);
-		lotf.push_back(p.d.has_llt ? w.lotfT.p : nullptr);
-		in.push_back(w.ints.p);
-		gr.push_back(w.grad.p);
-		nz.push_back(w.d.noisy);
-	}
-	return launch_ints(ctx, ip, wl, isim, opds, lotf, in, gr, nz);
+	return 0;
 }
 
 static int ensure_branches(shwfs_ctx* ctx) {
@@ -1804,6 +1826,211 @@ static int ensure_branches(shwfs_ctx* ctx) {
 		ctx->ev_pfork.push_back(a);
 		ctx->ev_pjoin.push_back(b);
 	}
+	return 0;
+}
+
+// The powfs the work-list launch serves: FFT form, physical optics, 32-point
+// (at most 128 pixels) or 128/256-point (at most 256 pixels), one frame per
+// output frame (dtrat 1), sigmatch 0 or 1.
+static bool worklist_serves(const shwfs_ctx* ctx, const PowfsState& p) {
+	if (ctx->form != SHWFS_FORM_FFT || is_geom(p.d.gradtype) || p.dtrat > 1 || p.d.sigmatch == 2) return false;
+	const int npix = p.d.pixpsax * p.d.pixpsay;
+	if (p.d.notf == 32) return p.d.nopd == 16 && npix <= 128;
+	return (p.d.notf == 128 || p.d.notf == 256) && npix <= 256;
+}
+
+// One frame of the powfs in wl as ray traces, then one persistent imaging
+// launch over a work list (worklist_kernel).  Geometric powfs run their own
+// chain first.  Returns 1 (nothing queued) when a powfs is not served.
+static int frame_worklist(shwfs_ctx* ctx, const std::vector<std::vector<int>>& wl, int isim) {
+	int nseg = 0;
+	for (size_t ip = 0; ip < wl.size(); ip++) {
+		if (wl[ip].empty() || is_geom(ctx->powfs[ip].d.gradtype)) continue;
+		if (!worklist_serves(ctx, ctx->powfs[ip])) return 1;
+		nseg++;
+	}
+	if (nseg == 0 || nseg > WL_MAX_SEG) return 1;
+	int r;
+	// the ray traces of the powfs (and the whole chain of a geometric one) run
+	// side by side: the first on the context stream, the others on the powfs
+	// branches, joined before the imaging launch
+	int nbr = 0;
+	for (size_t ip = 0; ip < wl.size(); ip++) nbr += !wl[ip].empty();
+	if (nbr > 1 && !ctx->capturing && (r = ensure_branches(ctx))) return r;
+	if (nbr > 1 && ctx->pstream.size() < ctx->powfs.size())
+		return fail(ctx, SHWFS_ESTATE, "frame graph: stream branches not created by a warm-up frame");
+	cudaStream_t main = ctx->stream;
+	bool first = true;
+	if (nbr > 1) CK(cudaEventRecord(ctx->ev_pfork[0], main));
+	for (size_t ip = 0; ip < wl.size(); ip++) {
+		if (wl[ip].empty()) continue;
+		const bool branch = nbr > 1 && !first;
+		if (branch) {
+			CK(cudaStreamWaitEvent(ctx->pstream[ip], ctx->ev_pfork[0], 0));
+			ctx->stream = ctx->pstream[ip];
+		}
+		if (is_geom(ctx->powfs[ip].d.gradtype)) r = frame_powfs(ctx, (int)ip, wl[ip], isim);
+		else r = trace_powfs(ctx, (int)ip, wl[ip], isim);
+		ctx->stream = main;
+		if (branch) {
+			CK(cudaEventRecord(ctx->ev_pjoin[ip], ctx->pstream[ip]));
+			CK(cudaStreamWaitEvent(main, ctx->ev_pjoin[ip], 0));
+		}
+		first = false;
+		if (r) return r;
+	}
+	if (!ctx->errflag.p) {
+		if ((r = dev_alloc(ctx, ctx->errflag, 1))) return r;
+		CK(cudaMemsetAsync(ctx->errflag.p, 0, sizeof(int), ctx->stream));
+	}
+	WorkParams W;
+	memset(&W, 0, sizeof(W));
+	int nimg_big = 0;
+	std::vector<int4> b_tiles[7], pix, n32;
+	for (size_t ip = 0; ip < wl.size(); ip++) {
+		if (wl[ip].empty() || is_geom(ctx->powfs[ip].d.gradtype)) continue;
+		PowfsState& p = ctx->powfs[ip];
+		const int nw = (int)wl[ip].size(), nitem = p.d.nsa * nw, si = W.nseg++;
+		WorkSeg& S = W.seg[si];
+		S.P = make_powfs_dev(p, isim);
+		std::vector<WfsDev> wd(nw);
+		for (int k = 0; k < nw; k++) {
+			WfsState& w = ctx->wfs[wl[ip][k]];
+			WfsDev& d = wd[k];
+			memset(&d, 0, sizeof(d));
+			d.opd = w.opd.p;
+			d.amp = p.amp.p + (p.namp > 1 ? (size_t)w.wfsind * p.d.nsa * p.d.nopd * p.d.nopd : 0);
+			d.lotfT = p.d.has_llt ? w.lotfT.p : nullptr;
+			d.mtche = w.mtche.p;
+			d.i0sum = w.i0sum.p;
+			d.ints = w.ints.p;
+			d.grad = w.grad.p;
+			d.alpha = norm_ints(p, w);
+			d.noisy = w.d.noisy;
+			d.wfs_id = (uint32_t)wl[ip][k];
+			d.seed = w.seed;
+		}
+		if ((r = push_wfsdev(ctx, wd, &S.wfs))) return r;
+		S.nw = nw;
+		S.nitem = nitem;
+		S.n = p.d.notf;
+		const int npix = p.d.pixpsax * p.d.pixpsay;
+		S.npq = npix <= 32 ? 1 : npix <= 64 ? 2 : npix <= 128 ? 4 : 8;
+		if (S.n == 32) {
+			const int g = std::max(1, ctx->wl_group);
+			for (int a = 0; a < nitem; a += g) n32.push_back(make_int4(WL_N32, si, a, g));
+			continue;
+		}
+		// the pass chain of the large images, as launch_gen sets it up
+		const int N = S.n;
+		if ((r = ensure_twiddles(ctx, p))) return r;
+		if (p.gen_buf.n < (size_t)nitem * N * N) {
+			if (ctx->capturing) return fail(ctx, SHWFS_ESTATE, "frame graph: scratch not allocated by a warm-up frame");
+			CK(cudaStreamSynchronize(ctx->stream));
+			if ((r = dev_alloc(ctx, p.gen_buf, (size_t)nitem * N * N))) return r;
+		}
+		GenParams& G = S.G;
+		G.nitem = nitem;
+		G.nw = nw;
+		G.nopd = p.d.nopd;
+		G.pad = (N - G.nopd) / 2;
+		G.uplink = 0;
+		G.scale = 1.f;
+		G.twoinvwvl = (float)(2.0 / p.d.wvl);
+		G.buf = p.gen_buf.p;
+		G.tw = p.gen_tw.p;
+		G.wfs = S.wfs;
+		G.etfT1 = S.P.etfT1;
+		G.etfT2 = S.P.etfT2;
+		G.etfwt1 = S.P.etfwt1;
+		G.etfwt2 = S.P.etfwt2;
+		G.nominalT = S.P.nominalT;
+		G.nominal_per_sa = S.P.nominal_per_sa;
+		const int L = gen_lines(N);
+		S.nt1 = (G.nopd + L - 1) / L;
+		S.ntf = N / L;
+		S.img0 = nimg_big;
+		nimg_big += nitem;
+		for (int i = 0; i < nitem; i++) {
+			for (int t = 0; t < S.nt1; t++) b_tiles[1].push_back(make_int4(WL_TILE, si, i, (1 << 16) | t));
+			for (int ps = 2; ps <= 6; ps++)
+				for (int t = 0; t < S.ntf; t++) b_tiles[ps].push_back(make_int4(WL_TILE, si, i, (ps << 16) | t));
+		}
+		for (int a = 0; a < nitem; a += 4) pix.push_back(make_int4(WL_PIX, si, a, 0));
+	}
+	// the list: pass 1 tiles, a slice of 32-point groups, pass 2 tiles, a slice, ...,
+	// pass 6 tiles, a slice, the large images' pixels, the rest of the 32-point groups
+	std::vector<int4> list;
+	const int ns = std::max(7, ctx->wl_slices);
+	const size_t per = (n32.size() + ns - 1) / ns;
+	size_t k = 0;
+	for (int ps = 1; ps <= 6; ps++) {
+		list.insert(list.end(), b_tiles[ps].begin(), b_tiles[ps].end());
+		for (size_t e = std::min(n32.size(), k + per); k < e; k++) list.push_back(n32[k]);
+	}
+	list.insert(list.end(), pix.begin(), pix.end());
+	for (; k < n32.size(); k++) list.push_back(n32[k]);
+	// the list repeats from frame to frame: kept on the device
+	const int4* dlist = nullptr;
+	for (auto& c : ctx->wl_cache)
+		if (c.h.size() == list.size() && !memcmp(c.h.data(), list.data(), sizeof(int4) * list.size())) dlist = c.d.p;
+	if (!dlist) {
+		if (ctx->capturing) return fail(ctx, SHWFS_ESTATE, "frame graph: work list changed since the warm-up frame");
+		if (ctx->wl_cache.size() >= 8) {
+			CK(cudaStreamSynchronize(ctx->stream));
+			for (auto& c : ctx->wl_cache) c.d.free_();
+			ctx->wl_cache.clear();
+		}
+		ctx->wl_cache.emplace_back();
+		auto& c = ctx->wl_cache.back();
+		c.h = list;
+		if ((r = dev_upload(ctx, c.d, list.data(), list.size()))) return r;
+		dlist = c.d.p;
+	}
+	const size_t ncnt = 1 + (size_t)nimg_big;
+	if (ctx->wl_cnt.n < ncnt) {
+		if (ctx->capturing) return fail(ctx, SHWFS_ESTATE, "frame graph: counters not allocated by a warm-up frame");
+		CK(cudaStreamSynchronize(ctx->stream));
+		if ((r = dev_alloc(ctx, ctx->wl_cnt, std::max(ncnt, (size_t)64)))) return r;
+	}
+	CK(cudaMemsetAsync(ctx->wl_cnt.p, 0, sizeof(int) * ncnt, ctx->stream));
+	W.nwork = (int)list.size();
+	W.work = dlist;
+	W.next = ctx->wl_cnt.p;
+	W.cnt = ctx->wl_cnt.p + 1;
+	W.errflag = ctx->errflag.p;
+	int npq32 = 1;
+	for (int i = 0; i < W.nseg; i++)
+		if (W.seg[i].n == 32) npq32 = std::max(npq32, W.seg[i].npq);
+	auto kern = npq32 == 1 ? worklist_kernel<1> : npq32 == 2 ? worklist_kernel<2> : worklist_kernel<4>;
+	const int kv = npq32 == 1 ? 0 : npq32 == 2 ? 1 : 2;
+	static int resident[64][3] = {{0}};
+	if (ctx->device >= 64) return fail(ctx, SHWFS_EINVAL, "work list: device %d out of range", ctx->device);
+	if (!resident[ctx->device][kv]) {
+		CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, WL_N32_SMEM));
+		int per_sm = 0, nsm = 0;
+		CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WL_THREADS, WL_N32_SMEM));
+		CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device));
+		resident[ctx->device][kv] = std::max(1, per_sm) * nsm;
+	}
+	// no more blocks than the device holds at once: a wait only ever depends on
+	// items already handed to running blocks
+	const int grid = std::min(W.nwork, resident[ctx->device][kv]);
+	{
+		StageMark mark(ctx, SHWFS_STAGE_INTS);
+		kern<<<grid, WL_THREADS, WL_N32_SMEM, ctx->stream>>>(W);
+	}
+	CK(cudaGetLastError());
+	return 0;
+}
+
+int shwfs_set_worklist(shwfs_ctx* ctx, int on, int slices, int group) {
+	if (!ctx || slices < 0 || group < 0 || group > 64)
+		return ctx ? fail(ctx, SHWFS_EINVAL, "set_worklist: bad arguments") : SHWFS_EINVAL;
+	ctx->worklist = on ? 1 : 0;
+	if (slices) ctx->wl_slices = slices;
+	if (group) ctx->wl_group = group;
+	ctx->g_warm = 0;  // a frame graph is captured again
 	return 0;
 }
 
@@ -1823,6 +2050,14 @@ int shwfs_frame_queue(shwfs_ctx* ctx, int isim, int iwfs0, int iwfs1) {
 		if (!wl[ip].empty()) nbranch++;
 	}
 	ctx->cache_desc = 1;
+	if (ctx->worklist) {
+		r = frame_worklist(ctx, wl, isim);
+		if (r <= 0) {
+			ctx->cache_desc = 0;
+			return r;
+		}
+		r = 0;  // a powfs the work list does not serve: the ordinary frame
+	}
 	if (nbranch <= 1) {
 		for (size_t ip = 0; ip < ctx->powfs.size() && !r; ip++)
 			if (!wl[ip].empty()) r = frame_powfs(ctx, (int)ip, wl[ip], isim);
@@ -2210,6 +2445,58 @@ int shwfs_autotune(shwfs_ctx* ctx, int iwfs0, int iwfs1, int nrep, int* chosen) 
 	if (r) return r;
 	p.variant = bestv;
 	if (chosen) *chosen = bestv;
+	return 0;
+}
+
+// The frame layouts shwfs_autotune_frame compares: per-powfs launches, then the
+// work list at these (slices, group).
+static const int kWlChoices[][2] = {{7, 4}, {14, 4}, {28, 4}, {7, 8}};
+constexpr int WL_NCHOICE = 1 + (int)(sizeof(kWlChoices) / sizeof(kWlChoices[0]));
+
+int shwfs_autotune_frame(shwfs_ctx* ctx, int iwfs0, int iwfs1, int nrep, int* choice) {
+	if (!ctx || iwfs0 < 0 || iwfs1 > (int)ctx->wfs.size() || iwfs0 >= iwfs1 || nrep <= 0)
+		return ctx ? fail(ctx, SHWFS_EINVAL, "autotune_frame: bad arguments") : SHWFS_EINVAL;
+	int r = set_device(ctx);
+	if (r) return r;
+	cudaEvent_t e0 = nullptr, e1 = nullptr;
+	CK(cudaEventCreate(&e0));
+	if (cudaEventCreate(&e1) != cudaSuccess) {
+		cudaEventDestroy(e0);
+		return fail(ctx, SHWFS_ECUDA, "autotune_frame: cudaEventCreate failed");
+	}
+	double best = 1e300;
+	int bestc = 0;
+	for (int c = 0; c < WL_NCHOICE && !r; c++) {
+		ctx->worklist = c > 0;
+		if (c > 0) {
+			ctx->wl_slices = kWlChoices[c - 1][0];
+			ctx->wl_group = kWlChoices[c - 1][1];
+		}
+		if ((r = shwfs_frame_queue(ctx, 0, iwfs0, iwfs1))) break;  // warm
+		if (cudaEventRecord(e0, ctx->stream) != cudaSuccess) { r = fail(ctx, SHWFS_ECUDA, "autotune_frame: event record failed"); break; }
+		for (int k = 0; k < nrep && !r; k++) r = shwfs_frame_queue(ctx, k, iwfs0, iwfs1);
+		if (r) break;
+		float ms = 0.f;
+		if (cudaEventRecord(e1, ctx->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+			cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+			r = fail(ctx, SHWFS_ECUDA, "autotune_frame: event timing failed");
+			break;
+		}
+		if (ms < best) {
+			best = ms;
+			bestc = c;
+		}
+	}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	if (r) return r;
+	ctx->worklist = bestc > 0;
+	if (bestc > 0) {
+		ctx->wl_slices = kWlChoices[bestc - 1][0];
+		ctx->wl_group = kWlChoices[bestc - 1][1];
+	}
+	ctx->g_warm = 0;
+	if (choice) *choice = bestc;
 	return 0;
 }
 

@@ -38,13 +38,13 @@ __host__ __device__ constexpr int ilog2c(int n) { return n <= 1 ? 0 : 1 + ilog2c
 // In-place radix-2 FFT of gen_lines(N) lines of N points in shared memory, line
 // stride N + 1 (bank-conflict free for column tiles), input in bit-reversed
 // order.  tw[k] = exp(-2 pi i k / N), k < N/2; dir -1 forward, +1 inverse.
-template <int N>
+template <int N, int NT = GEN_THREADS>
 __device__ __forceinline__ void fft_lines(float2* s, const float2* __restrict__ tw, int dir) {
 	constexpr int LOGN = ilog2c(N), LS = N + 1, NB = gen_lines(N) * N / 2;
 #pragma unroll 1
 	for (int st = 0; st < LOGN; st++) {
 		const int half = 1 << st;
-		for (int b = threadIdx.x; b < NB; b += GEN_THREADS) {
+		for (int b = threadIdx.x; b < NB; b += NT) {
 			const int line = b / (N / 2), j = b - line * (N / 2);
 			const int grp = j >> st, pos = j & (half - 1);
 			const int k0 = grp * 2 * half + pos, k1 = k0 + half;
@@ -84,26 +84,36 @@ struct GenParams {
 	int nominal_per_sa;
 };
 
-// One pass over one tile (blockIdx.y) of one image (blockIdx.x).
-template <int N, int PASS>
-__global__ void __launch_bounds__(GEN_THREADS) gen_pass_kernel(GenParams G) {
+// Shared memory of one pass tile: the lines (stride N + 1) and N/2 twiddles.
+__host__ __device__ constexpr int gen_tile_smem(int n) { return (gen_lines(n) * (n + 1) + n / 2) * (int)sizeof(float2); }
+
+// Reads of the scratch image: through L1, or from L2 only (L2ONLY) where other
+// blocks of the same launch wrote it (L1 is not coherent between SMs).
+template <bool L2ONLY>
+__device__ __forceinline__ float2 gen_ld(const float2* p) {
+	if constexpr (L2ONLY) return __ldcg(p);
+	else return *p;
+}
+
+// One pass over tile `tile` of image i by a block of NT threads; gen_s is the
+// tile's shared memory (gen_tile_smem(N) bytes).
+template <int N, int PASS, int NT, bool L2ONLY>
+__device__ __forceinline__ void gen_pass_tile(const GenParams& G, int i, int tile, float2* gen_s) {
 	constexpr int LS = N + 1, GEN_LINES = gen_lines(N);
 	constexpr bool ROWS = PASS == GEN_FIELD_ROWS || PASS == GEN_OTF_ROWS || PASS == GEN_INV_ROWS;
-	extern __shared__ float2 gen_s[];
 	float2* tw = gen_s + GEN_LINES * LS;  // N/2 twiddles
-	const int i = blockIdx.x;
 	const int isa = G.uplink ? 0 : i / G.nw;
 	const WfsDev& W = G.wfs[G.uplink ? i : i % G.nw];
 	float2* im = G.buf + (size_t)i * N * N;
 	const int tid = threadIdx.x;
-	for (int k = tid; k < N / 2; k += GEN_THREADS) tw[k] = G.tw[k];
-	int l0 = blockIdx.y * GEN_LINES, nl = GEN_LINES;  // first line and lines of the tile
+	for (int k = tid; k < N / 2; k += NT) tw[k] = G.tw[k];
+	int l0 = tile * GEN_LINES, nl = GEN_LINES;  // first line and lines of the tile
 	if (PASS == GEN_FIELD_ROWS) {
 		nl = min(GEN_LINES, G.nopd - l0);
 		l0 += G.pad;
 	}
 	// ---- load (bit-reversed along the line)
-	for (int idx = tid; idx < GEN_LINES * N; idx += GEN_THREADS) {
+	for (int idx = tid; idx < GEN_LINES * N; idx += NT) {
 		int line, k;
 		if (ROWS) {
 			line = idx / N;
@@ -124,18 +134,18 @@ __global__ void __launch_bounds__(GEN_THREADS) gen_pass_kernel(GenParams G) {
 					v = make_float2(a * cs, a * sn);
 				}
 			} else if (ROWS) {
-				v = im[(size_t)(l0 + line) * N + k];
+				v = gen_ld<L2ONLY>(im + (size_t)(l0 + line) * N + k);
 			} else if (PASS != GEN_PSF_COLS || (k >= G.pad && k < G.pad + G.nopd)) {
-				v = im[(size_t)k * N + l0 + line];  // rows outside the pupil are zero before pass 2
+				v = gen_ld<L2ONLY>(im + (size_t)k * N + l0 + line);  // rows outside the pupil are zero before pass 2
 			}
 		}
 		gen_s[line * LS + bitrev<N>(k)] = v;
 	}
 	__syncthreads();
-	fft_lines<N>(gen_s, tw, PASS >= GEN_INV_ROWS ? 1 : -1);
+	fft_lines<N, NT>(gen_s, tw, PASS >= GEN_INV_ROWS ? 1 : -1);
 	// ---- element-wise step of the chain
 	if (PASS == GEN_PSF_COLS) {
-		for (int idx = tid; idx < GEN_LINES * N; idx += GEN_THREADS) {
+		for (int idx = tid; idx < GEN_LINES * N; idx += NT) {
 			const float2 v = gen_s[(idx / N) * LS + idx % N];
 			gen_s[(idx / N) * LS + idx % N] = make_float2((v.x * v.x + v.y * v.y) * G.scale, 0.f);
 		}
@@ -143,7 +153,7 @@ __global__ void __launch_bounds__(GEN_THREADS) gen_pass_kernel(GenParams G) {
 	}
 	if (PASS == GEN_OTF_COLS) {
 		// line = fx - l0, element fy; transfer functions are [fy + N fx]: fy fastest
-		for (int idx = tid; idx < GEN_LINES * N; idx += GEN_THREADS) {
+		for (int idx = tid; idx < GEN_LINES * N; idx += NT) {
 			const int line = idx / N, fy = idx - line * N;
 			const size_t t = (size_t)fy + (size_t)N * (l0 + line);
 			float2 v = gen_s[line * LS + fy];
@@ -169,14 +179,14 @@ __global__ void __launch_bounds__(GEN_THREADS) gen_pass_kernel(GenParams G) {
 		if (G.uplink) return;
 	}
 	if (PASS == GEN_INV_COLS) {
-		for (int idx = tid; idx < GEN_LINES * N; idx += GEN_THREADS) {
+		for (int idx = tid; idx < GEN_LINES * N; idx += NT) {
 			const int line = idx / N, k = idx - line * N;
 			gen_s[line * LS + k].y = 0.f;  // real part only
 		}
 		__syncthreads();
 	}
 	// ---- store (natural order)
-	for (int idx = tid; idx < GEN_LINES * N; idx += GEN_THREADS) {
+	for (int idx = tid; idx < GEN_LINES * N; idx += NT) {
 		int line, k;
 		if (ROWS) {
 			line = idx / N;
@@ -192,15 +202,19 @@ __global__ void __launch_bounds__(GEN_THREADS) gen_pass_kernel(GenParams G) {
 	}
 }
 
+// One pass over one tile (blockIdx.y) of one image (blockIdx.x).
+template <int N, int PASS>
+__global__ void __launch_bounds__(GEN_THREADS) gen_pass_kernel(GenParams G) {
+	extern __shared__ float2 gen_s[];
+	gen_pass_tile<N, PASS, GEN_THREADS, false>(G, blockIdx.x, blockIdx.y, gen_s);
+}
+
 // Pixels, noise and gradients of generic-size images: one warp per work item
 // (item = isa * nw + k as in the imaging launch), image item of buf (n2 = N^2
 // elements each), real part.
-template <int NPQ>
-__global__ void gen_pixels_kernel(PowfsDev P, const WfsDev* __restrict__ wfs, int nw, int nitem,
-	const float2* __restrict__ buf, int n2) {
-	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	const int item = blockIdx.x * (blockDim.x >> 5) + warp;
-	if (item >= nitem) return;
+template <int NPQ, bool L2ONLY>
+__device__ __forceinline__ void gen_pixels_item(const PowfsDev& P, const WfsDev* __restrict__ wfs, int nw, int item,
+	const float2* __restrict__ buf, int n2, int lane) {
 	const int isa = item / nw;
 	const WfsDev& W = wfs[item % nw];
 	const float2* im = buf + (size_t)item * n2;
@@ -216,7 +230,7 @@ __global__ void gen_pixels_kernel(PowfsDev P, const WfsDev* __restrict__ wfs, in
 #pragma unroll
 			for (int c = 0; c < 4; c++) {
 				const int id = __ldg(sidx + 4 * p + c);
-				if (id >= 0) v = fmaf(__ldg(swt + 4 * p + c), im[id].x, v);
+				if (id >= 0) v = fmaf(__ldg(swt + 4 * p + c), gen_ld<L2ONLY>(im + id).x, v);
 			}
 			v *= W.alpha;
 			if (P.accum) v += W.ints[(size_t)isa * npix + p];  // dtrat > 1: the frames so far
@@ -243,6 +257,14 @@ __global__ void gen_pixels_kernel(PowfsDev P, const WfsDev* __restrict__ wfs, in
 	if (W.grad)
 		grad_from_pixels<NPQ>(pix, npix, P.pixpsax, P.pixpsay, P, W.mtche + (size_t)isa * 2 * npix, W.i0sum, isa, lane,
 			W.grad, P.nsa);
+}
+template <int NPQ>
+__global__ void gen_pixels_kernel(PowfsDev P, const WfsDev* __restrict__ wfs, int nw, int nitem,
+	const float2* __restrict__ buf, int n2) {
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int item = blockIdx.x * (blockDim.x >> 5) + warp;
+	if (item >= nitem) return;
+	gen_pixels_item<NPQ, false>(P, wfs, nw, item, buf, n2, lane);
 }
 
 // ---------------------------------------------------------------------------

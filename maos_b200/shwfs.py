@@ -129,6 +129,8 @@ def _load() -> C.CDLL:
         "shwfs_evl_opd_dev": [vp, i, vp],
         "shwfs_grad_gtilt_dev": [vp, i, vp, vp],
         "shwfs_dm_set": [vp, i, C.POINTER(LayerDesc), C.POINTER(dp)],
+        "shwfs_set_worklist": [vp, i, i, i],
+        "shwfs_autotune_frame": [vp, i, i, i, ip],
         "shwfs_wfs_set_opd_terms": [vp, i, i, dp, C.c_double, C.c_double, dp],
         "shwfs_wfs_set_opdadd": [vp, i, dp],
         "shwfs_powfs_set_seotf": [vp, i, dp],
@@ -348,6 +350,11 @@ class Context:
         a = _f64(opd).ravel() if opd is not None else None
         self._check(self._L.shwfs_wfs_set_opdadd(self._h, iwfs, _dptr(a)), "wfs_set_opdadd")
 
+    def set_worklist(self, on: bool = True, slices: int = 0, group: int = 0):
+        """Imaging of every powfs of a frame as one persistent work-list launch (slices, group: 0
+        keeps the current values)."""
+        self._check(self._L.shwfs_set_worklist(self._h, int(bool(on)), int(slices), int(group)), "set_worklist")
+
     def set_form(self, form: int):
         self._check(self._L.shwfs_set_form(self._h, form), "set_form")
 
@@ -495,6 +502,13 @@ class Context:
         """Pick the fastest imaging-kernel variant on the real frames; returns its index."""
         out = C.c_int()
         self._check(self._L.shwfs_autotune(self._h, iwfs0, iwfs1, nrep, C.byref(out)), "autotune")
+        return out.value
+
+    def autotune_frame(self, iwfs0: int, iwfs1: int, nrep: int = 5) -> int:
+        """Per-powfs launches or the work list (and its settings), whichever runs the frame
+        fastest; returns the choice (0: per-powfs launches)."""
+        out = C.c_int()
+        self._check(self._L.shwfs_autotune_frame(self._h, iwfs0, iwfs1, nrep, C.byref(out)), "autotune_frame")
         return out.value
 
     def set_variant(self, ipowfs: int, variant: int):

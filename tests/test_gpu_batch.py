@@ -10,10 +10,12 @@ from tests.conftest import cuda_available
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not cuda_available(), reason="needs a CUDA GPU")]
 
 
-def _frames(graph, isims, noisy):
+def _frames(graph, isims, noisy, worklist=False, slices=0):
     from maos_b200.configs import UNEVEN_BATCH
     from maos_b200.workload import build_batch
     wl = build_batch(UNEVEN_BATCH["members"], device=0, seed=6, noisy=noisy, nx=512, graph=graph)
+    if worklist:
+        wl.ctx.set_worklist(True, slices)
     out = []
     for isim in isims:
         wl.frame(isim)
@@ -84,3 +86,52 @@ def test_range_sync_into_caller_buffer():
     with pytest.raises(ValueError):
         wl.frame_sync(out=np.empty(n, dtype=np.float32))
     wl.close()
+
+
+@pytest.mark.parametrize("graph,slices", [(False, 8), (True, 8), (True, 3)])
+def test_worklist_frames_equal_branch_frames(graph, slices):
+    """The frame's imaging as one persistent work-list launch (32-point groups,
+    pass tiles of the 128- and 256-point images waiting on their previous pass,
+    pixel steps) gives the frames of the per-powfs launches, bit for bit, as a
+    stream frame and as a CUDA graph, with the passes interleaved at two slice
+    counts; noisy frames, so the noise counters are exercised too."""
+    isims = [0, 1, 4, 7]
+    a = _frames(False, isims, True)
+    b = _frames(graph, isims, True, worklist=True, slices=slices)
+    for fa, fb in zip(a, b):
+        for (ga, ia), (gb, ib) in zip(fa, fb):
+            assert np.isfinite(ga).all()
+            assert np.array_equal(ga, gb) and np.array_equal(ia, ib)
+
+
+def test_worklist_single_powfs_frames_equal():
+    """A frame of one 32-point powfs through the work list equals the ordinary launch."""
+    from maos_b200.configs import LGS8_N32
+    from maos_b200.workload import build
+    out = []
+    for wlon in (False, True):
+        wl = build(LGS8_N32, device=0, seed=2, noisy=True, nx=512)
+        wl.ctx.set_variant(wl.ipowfs, 1)
+        wl.ctx.set_worklist(wlon)
+        wl.frame(3)
+        out.append(wl.frame_sync(want_ints=True))
+        wl.close()
+    for (ga, ia), (gb, ib) in zip(*out):
+        assert np.array_equal(ga, gb) and np.array_equal(ia, ib)
+
+
+
+def test_frame_layout_autotuner_keeps_a_layout_and_its_frames():
+    """shwfs_autotune_frame times the per-powfs launches and the work list at its settings and
+    keeps one; the frames after it are the frames of every layout, bit for bit."""
+    from maos_b200.configs import UNEVEN_BATCH
+    from maos_b200.workload import build_batch
+    ref = _frames(False, [3], True)[0]
+    wl = build_batch(UNEVEN_BATCH["members"], device=0, seed=6, noisy=True, nx=512, graph=True)
+    c = wl.ctx.autotune_frame(0, wl.nwfs, nrep=2)
+    assert 0 <= c <= 4
+    wl.frame(3)
+    out = wl.frame_sync(want_ints=True)
+    wl.close()
+    for (ga, ia), (gb, ib) in zip(ref, out):
+        assert np.array_equal(ga, gb) and np.array_equal(ia, ib)
