@@ -366,6 +366,13 @@ int shwfs_set_worklist(shwfs_ctx* ctx, int on, int slices, int group);
    (7, 8), and keeps the fastest; *choice receives 0 for the per-powfs
    launches, 1-4 for the work-list settings in that order. */
 int shwfs_autotune_frame(shwfs_ctx* ctx, int iwfs0, int iwfs1, int nrep, int* choice);
+/* With on != 0 (the default), a frame of several powfs runs each powfs whose
+   images per frame are fewer than the largest powfs's on a branch stream of
+   the device's greatest priority, so their chains of small launches start as
+   the large imaging kernel's blocks retire; with 0 every branch has the
+   default priority.  Synchronises the context; the branches and the frame
+   graph are made again by the next frame.  Results do not depend on it. */
+int shwfs_set_branch_priority(shwfs_ctx* ctx, int on);
 
 /* Synchronise the context stream; returns the first error of queued work. */
 int shwfs_sync(shwfs_ctx* ctx);

@@ -163,6 +163,7 @@ struct shwfs_ctx {
 	int worklist = 0;
 	int wl_slices = 7;                   // slices of 32-point groups between the passes of the large images
 	int wl_group = 4;                    // 32-point images per work item
+	int branch_priority = 1;             // the smaller powfs' branches at the greatest stream priority
 	struct WorkCache {
 		std::vector<int4> h;
 		DevBuf<int4> d;
@@ -1815,11 +1816,23 @@ static int trace_powfs(shwfs_ctx* ctx, int ip, const std::vector<int>& wl, int i
 	return 0;
 }
 
+// The branch of a powfs with fewer images per frame than the largest powfs of
+// the context runs at the device's greatest stream priority (captured into the
+// frame graph as node priorities): the small sensors' chains of dependent
+// launches (the FFT-pass chain of one NGS image) then take SMs as the large
+// imaging kernel's blocks retire, instead of queueing behind all of them.
 static int ensure_branches(shwfs_ctx* ctx) {
+	if (ctx->pstream.size() >= ctx->powfs.size()) return 0;
+	std::vector<long> nimg(ctx->powfs.size(), 0);
+	for (const WfsState& w : ctx->wfs) nimg[w.d.ipowfs] += ctx->powfs[w.d.ipowfs].d.nsa;
+	const long nmax = *std::max_element(nimg.begin(), nimg.end());
+	int lo = 0, hi = 0;
+	CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
 	while (ctx->pstream.size() < ctx->powfs.size()) {
 		cudaStream_t st;
 		cudaEvent_t a, b;
-		CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+		const size_t ip = ctx->pstream.size();
+		CK(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, ctx->branch_priority && nimg[ip] < nmax ? hi : lo));
 		CK(cudaEventCreateWithFlags(&a, cudaEventDisableTiming));
 		CK(cudaEventCreateWithFlags(&b, cudaEventDisableTiming));
 		ctx->pstream.push_back(st);
@@ -2034,6 +2047,30 @@ int shwfs_set_worklist(shwfs_ctx* ctx, int on, int slices, int group) {
 	return 0;
 }
 
+int shwfs_set_branch_priority(shwfs_ctx* ctx, int on) {
+	if (!ctx) return SHWFS_EINVAL;
+	int r = set_device(ctx);
+	if (r) return r;
+	CK(cudaStreamSynchronize(ctx->stream));
+	// the branches are made again, at the new priorities, by the next frame
+	for (size_t i = 0; i < ctx->pstream.size(); i++) {
+		CK(cudaStreamSynchronize(ctx->pstream[i]));
+		CK(cudaStreamDestroy(ctx->pstream[i]));
+		CK(cudaEventDestroy(ctx->ev_pfork[i]));
+		CK(cudaEventDestroy(ctx->ev_pjoin[i]));
+	}
+	ctx->pstream.clear();
+	ctx->ev_pfork.clear();
+	ctx->ev_pjoin.clear();
+	if (ctx->gexec) {
+		CK(cudaGraphExecDestroy(ctx->gexec));
+		ctx->gexec = nullptr;
+	}
+	ctx->g_warm = 0;
+	ctx->branch_priority = on ? 1 : 0;
+	return 0;
+}
+
 int shwfs_frame_queue(shwfs_ctx* ctx, int isim, int iwfs0, int iwfs1) {
 	if (!ctx || iwfs0 < 0 || iwfs1 > (int)ctx->wfs.size() || iwfs0 >= iwfs1)
 		return ctx ? fail(ctx, SHWFS_EINVAL, "frame_queue: bad WFS range") : SHWFS_EINVAL;
@@ -2127,7 +2164,8 @@ int shwfs_frame_graph(shwfs_ctx* ctx, int isim, int iwfs0, int iwfs1) {
 		}
 	}
 	if (!ctx->gexec) {
-		const cudaError_t ei = cudaGraphInstantiate(&ctx->gexec, g, 0);
+		// the branches' stream priorities, captured as node priorities, hold in the graph
+		const cudaError_t ei = cudaGraphInstantiate(&ctx->gexec, g, cudaGraphInstantiateFlagUseNodePriority);
 		if (ei != cudaSuccess) {
 			cudaGraphDestroy(g);
 			ctx->gexec = nullptr;

@@ -130,6 +130,7 @@ def _load() -> C.CDLL:
         "shwfs_grad_gtilt_dev": [vp, i, vp, vp],
         "shwfs_dm_set": [vp, i, C.POINTER(LayerDesc), C.POINTER(dp)],
         "shwfs_set_worklist": [vp, i, i, i],
+        "shwfs_set_branch_priority": [vp, i],
         "shwfs_autotune_frame": [vp, i, i, i, ip],
         "shwfs_wfs_set_opd_terms": [vp, i, i, dp, C.c_double, C.c_double, dp],
         "shwfs_wfs_set_opdadd": [vp, i, dp],
@@ -354,6 +355,10 @@ class Context:
         """Imaging of every powfs of a frame as one persistent work-list launch (slices, group: 0
         keeps the current values)."""
         self._check(self._L.shwfs_set_worklist(self._h, int(bool(on)), int(slices), int(group)), "set_worklist")
+
+    def set_branch_priority(self, on: bool = True):
+        """Smaller powfs' stream branches at the greatest stream priority (default on)."""
+        self._check(self._L.shwfs_set_branch_priority(self._h, int(bool(on))), "set_branch_priority")
 
     def set_form(self, form: int):
         self._check(self._L.shwfs_set_form(self._h, form), "set_form")

@@ -10,10 +10,12 @@ from tests.conftest import cuda_available
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not cuda_available(), reason="needs a CUDA GPU")]
 
 
-def _frames(graph, isims, noisy, worklist=False, slices=0):
+def _frames(graph, isims, noisy, worklist=False, slices=0, priority=True):
     from maos_b200.configs import UNEVEN_BATCH
     from maos_b200.workload import build_batch
     wl = build_batch(UNEVEN_BATCH["members"], device=0, seed=6, noisy=noisy, nx=512, graph=graph)
+    if not priority:
+        wl.ctx.set_branch_priority(False)
     if worklist:
         wl.ctx.set_worklist(True, slices)
     out = []
@@ -135,3 +137,15 @@ def test_frame_layout_autotuner_keeps_a_layout_and_its_frames():
     wl.close()
     for (ga, ia), (gb, ib) in zip(ref, out):
         assert np.array_equal(ga, gb) and np.array_equal(ia, ib)
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_branch_priority_keeps_frames(graph):
+    """The smaller powfs' branches at the greatest stream priority change the order in which
+    blocks reach the SMs, not the frames: identical, bit for bit, with and without."""
+    isims = [2, 7]
+    a = _frames(graph, isims, True, priority=True)
+    b = _frames(graph, isims, True, priority=False)
+    for fa, fb in zip(a, b):
+        for (ga, ia), (gb, ib) in zip(fa, fb):
+            assert np.array_equal(ga, gb) and np.array_equal(ia, ib)
