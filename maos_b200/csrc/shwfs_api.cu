@@ -164,6 +164,7 @@ struct shwfs_ctx {
 	int wl_slices = 7;                   // slices of 32-point groups between the passes of the large images
 	int wl_group = 4;                    // 32-point images per work item
 	int branch_priority = 1;             // the smaller powfs' branches at the greatest stream priority
+	int priority = 0;                    // stream priority of the context (shwfs_set_stream_priority)
 	struct WorkCache {
 		std::vector<int4> h;
 		DevBuf<int4> d;
@@ -1832,7 +1833,8 @@ static int ensure_branches(shwfs_ctx* ctx) {
 		cudaStream_t st;
 		cudaEvent_t a, b;
 		const size_t ip = ctx->pstream.size();
-		CK(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, ctx->branch_priority && nimg[ip] < nmax ? hi : lo));
+		CK(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking,
+			ctx->branch_priority && nimg[ip] < nmax ? hi : std::min(lo, std::max(hi, ctx->priority))));
 		CK(cudaEventCreateWithFlags(&a, cudaEventDisableTiming));
 		CK(cudaEventCreateWithFlags(&b, cudaEventDisableTiming));
 		ctx->pstream.push_back(st);
@@ -2047,11 +2049,8 @@ int shwfs_set_worklist(shwfs_ctx* ctx, int on, int slices, int group) {
 	return 0;
 }
 
-int shwfs_set_branch_priority(shwfs_ctx* ctx, int on) {
-	if (!ctx) return SHWFS_EINVAL;
-	int r = set_device(ctx);
-	if (r) return r;
-	CK(cudaStreamSynchronize(ctx->stream));
+// Destroys the powfs branches and the frame graph (made again by the next frame).
+static int drop_branches(shwfs_ctx* ctx) {
 	// the branches are made again, at the new priorities, by the next frame
 	for (size_t i = 0; i < ctx->pstream.size(); i++) {
 		CK(cudaStreamSynchronize(ctx->pstream[i]));
@@ -2067,7 +2066,40 @@ int shwfs_set_branch_priority(shwfs_ctx* ctx, int on) {
 		ctx->gexec = nullptr;
 	}
 	ctx->g_warm = 0;
+	return 0;
+}
+
+int shwfs_set_branch_priority(shwfs_ctx* ctx, int on) {
+	if (!ctx) return SHWFS_EINVAL;
+	int r = set_device(ctx);
+	if (r) return r;
+	CK(cudaStreamSynchronize(ctx->stream));
+	if ((r = drop_branches(ctx))) return r;
 	ctx->branch_priority = on ? 1 : 0;
+	return 0;
+}
+
+int shwfs_set_stream_priority(shwfs_ctx* ctx, int priority) {
+	if (!ctx) return SHWFS_EINVAL;
+	int r = set_device(ctx);
+	if (r) return r;
+	int lo = 0, hi = 0;
+	CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+	const int p = std::min(lo, std::max(hi, priority));
+	CK(cudaStreamSynchronize(ctx->stream));
+	CK(cudaStreamSynchronize(ctx->aux));
+	if ((r = drop_branches(ctx))) return r;
+	cudaStream_t s = nullptr, a = nullptr;
+	CK(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, p));
+	if (cudaStreamCreateWithPriority(&a, cudaStreamNonBlocking, p) != cudaSuccess) {
+		cudaStreamDestroy(s);
+		return fail(ctx, SHWFS_ECUDA, "set_stream_priority: stream creation failed");
+	}
+	CK(cudaStreamDestroy(ctx->stream));
+	CK(cudaStreamDestroy(ctx->aux));
+	ctx->stream = s;
+	ctx->aux = a;
+	ctx->priority = p;
 	return 0;
 }
 

@@ -142,7 +142,7 @@ class Server:
     """Continuous-batching frame server over independent simulations on one GPU."""
 
     def __init__(self, cfgs: List[dict], device: int = 0, form: int = 0, hbm_budget: Optional[int] = None,
-                 seed: int = 1):
+                 seed: int = 1, priority: Optional[str] = None):
         import torch
         from . import shwfs
         from .setup import Setup
@@ -152,6 +152,7 @@ class Server:
         self.form = form
         self.seed = seed
         self.setups = [Setup(c) for c in cfgs]  # host setup of every sim, ahead of time
+        self.priority = priority
         self.sims: Dict[int, object] = {}
         self.isim = [0] * len(cfgs)
         free, total = torch.cuda.mem_get_info(device)
@@ -165,6 +166,28 @@ class Server:
         per_img = s.nopd ** 2 * 8 + s.npix * 4 + (s.notf ** 2 * 8 if s.notf != 32 else 0)
         return nl * nx * nx * 4 + c["nwfs"] * s.nsa * per_img + (64 << 20)
 
+    def cost(self, i: int) -> float:
+        """Relative device work of one frame of sim i: images x FFT points x log2 of the points."""
+        c, s = self.cfgs[i], self.setups[i]
+        n = s.notf
+        return c["nwfs"] * s.nsa * n * n * math.log2(n)
+
+    def stream_priority(self, i: int) -> int:
+        """CUDA stream priority of sim i under the server's policy (lower runs first):
+        "large" gives the costliest frames the greatest priority, in equal steps of the
+        cost's logarithm over the device's levels; "small" the reverse; None all 0."""
+        if self.priority is None:
+            return 0
+        lo, hi = self.torch.cuda.Stream.priority_range() if hasattr(self.torch.cuda.Stream, "priority_range") \
+            else (0, -5)
+        levels = lo - hi
+        cmin = min(self.cost(j) for j in range(len(self.cfgs)))
+        cmax = max(self.cost(j) for j in range(len(self.cfgs)))
+        f = math.log(self.cost(i) / cmin) / math.log(cmax / cmin) if cmax > cmin else 0.0
+        if self.priority == "small":
+            f = 1.0 - f
+        return lo - int(round(f * levels))
+
     def _load(self, i: int) -> int:
         from .workload import build_from_setup
         torch = self.torch
@@ -172,6 +195,8 @@ class Server:
         f0 = torch.cuda.mem_get_info(self.device)[0]
         wl = build_from_setup(self.cfgs[i], self.setups[i], device=self.device, seed=self.seed + i, noisy=True,
                               form=self.form)
+        if self.priority is not None:
+            wl.ctx.set_stream_priority(self.stream_priority(i))
         ext = torch.cuda.ExternalStream(wl.ctx.stream, device=self.device)
         self.sims[i] = (wl, ext, torch.cuda.Event())
         wl.frame(0)  # buffers made on first use belong to the footprint too

@@ -131,6 +131,7 @@ def _load() -> C.CDLL:
         "shwfs_dm_set": [vp, i, C.POINTER(LayerDesc), C.POINTER(dp)],
         "shwfs_set_worklist": [vp, i, i, i],
         "shwfs_set_branch_priority": [vp, i],
+        "shwfs_set_stream_priority": [vp, i],
         "shwfs_autotune_frame": [vp, i, i, i, ip],
         "shwfs_wfs_set_opd_terms": [vp, i, i, dp, C.c_double, C.c_double, dp],
         "shwfs_wfs_set_opdadd": [vp, i, dp],
@@ -359,6 +360,11 @@ class Context:
     def set_branch_priority(self, on: bool = True):
         """Smaller powfs' stream branches at the greatest stream priority (default on)."""
         self._check(self._L.shwfs_set_branch_priority(self._h, int(bool(on))), "set_branch_priority")
+
+    def set_stream_priority(self, priority: int):
+        """Priority of the context's streams (lower runs first; clamped to the device's range).
+        The stream handle changes: read `stream` again after the call."""
+        self._check(self._L.shwfs_set_stream_priority(self._h, int(priority)), "set_stream_priority")
 
     def set_form(self, form: int):
         self._check(self._L.shwfs_set_form(self._h, form), "set_form")
