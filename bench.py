@@ -334,7 +334,11 @@ def run_b200(args, cfg):
     units_per_step = nwfs * wl.nsa
     ext = torch.cuda.ExternalStream(ctx.stream, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
-    variant = ctx.autotune(wl.wfs[0], wl.wfs[-1] + 1, nrep=5)
+    if args.variant is None:
+        variant = ctx.autotune(wl.wfs[0], wl.wfs[-1] + 1, nrep=5)
+    else:  # a fixed imaging variant (profiling one kernel)
+        variant = args.variant
+        ctx.set_variant(wl.ipowfs, variant)
     forms = [args.form] if args.form != "both" else ["fft", "tc"]
     isim = 0
     res = {}
@@ -793,6 +797,8 @@ def main():
     ap.add_argument("--form", default="both", choices=["both", "fft", "tc"],
                     help="imaging form(s) to time; both: the FFT and tensor-core forms, value = the faster")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--variant", type=int, default=None,
+                    help="imaging-kernel variant of the 32-point FFT form (default: the autotuner's choice)")
     ap.add_argument("--serve-seconds", type=float, default=0.5, help="serving: seconds of requests per rate")
     args = ap.parse_args()
     _stdout_to_stderr()

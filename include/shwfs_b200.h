@@ -304,7 +304,8 @@ int shwfs_profile_enable(shwfs_ctx* ctx, int enable);
 int shwfs_profile_read(shwfs_ctx* ctx, double* ms, int* launches);
 
 /* ---- tuning ---- */
-#define SHWFS_NVARIANT 3 /* imaging-kernel variants: register cap for 4, 5 or 6 blocks per SM */
+#define SHWFS_NVARIANT 6 /* imaging-kernel variants: 0-2 full-spectrum transforms at a register cap
+                            for 4, 5 or 6 blocks per SM; 3-5 the half-spectrum form at the same caps */
 /* Times every imaging-kernel variant on nrep whole frames of WFS
    [iwfs0, iwfs1) (their powfs; device time of the frame on the context's
    stream) and keeps the fastest; *chosen receives its index. */

@@ -1488,17 +1488,28 @@ static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist
 	StageMark mark(ctx, SHWFS_STAGE_INTS);
 	const int v = p.variant;
 	auto go = [&](auto kern) { kern<<<nblk, 128, 0, ctx->stream>>>(P, wdev, nw, nitem); };
+	// variants 0-2: full-spectrum transforms at a register cap for 4, 5, 6
+	// blocks per SM; 3-5: the half-spectrum form at the same caps
 	if (npix <= 32) {
 		if (v == 1) go(ints_n32_kernel<1, 5>);
 		else if (v == 2) go(ints_n32_kernel<1, 6>);
+		else if (v == 3) go(ints_n32_kernel<1, 4, true>);
+		else if (v == 4) go(ints_n32_kernel<1, 5, true>);
+		else if (v == 5) go(ints_n32_kernel<1, 6, true>);
 		else go(ints_n32_kernel<1, 4>);
 	} else if (npix <= 64) {
 		if (v == 1) go(ints_n32_kernel<2, 5>);
 		else if (v == 2) go(ints_n32_kernel<2, 6>);
+		else if (v == 3) go(ints_n32_kernel<2, 4, true>);
+		else if (v == 4) go(ints_n32_kernel<2, 5, true>);
+		else if (v == 5) go(ints_n32_kernel<2, 6, true>);
 		else go(ints_n32_kernel<2, 4>);
 	} else {
 		if (v == 1) go(ints_n32_kernel<4, 5>);
 		else if (v == 2) go(ints_n32_kernel<4, 6>);
+		else if (v == 3) go(ints_n32_kernel<4, 4, true>);
+		else if (v == 4) go(ints_n32_kernel<4, 5, true>);
+		else if (v == 5) go(ints_n32_kernel<4, 6, true>);
 		else go(ints_n32_kernel<4, 4>);
 	}
 	CK(cudaGetLastError());

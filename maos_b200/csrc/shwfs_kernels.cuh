@@ -659,6 +659,10 @@ __device__ __forceinline__ void grad_from_pixels(const float (&pix)[NPQ], int np
 // (b)-(e) fused, n_opd=16, n_w=n_f=32.  Work item w -> (isa = w / nw, wfs =
 // wlist[w % nw]) so the WFS that share a subaperture's ETF run together.
 // ---------------------------------------------------------------------------
+template <int NPQ>
+__device__ __forceinline__ void ints_n32_pixels(const PowfsDev& P, const WfsDev& W, int isa, int lane,
+	const float* psf);
+
 // (c)-(e) of one subaperture image after its field transform: F from
 // field_fft_n32 (lane = kx holds F(kx, ky=0..31)); tile is the warp's scratch.
 template <int NPQ>
@@ -705,6 +709,14 @@ __device__ __forceinline__ void ints_n32_tail(const PowfsDev& P, const WfsDev& W
 #pragma unroll
 	for (int y = 0; y < 32; y++) psf[lane + 32 * y] = F[y].x;
 	__syncwarp();
+	ints_n32_pixels<NPQ>(P, W, isa, lane, psf);
+}
+
+// (c)-(e) after the image is in shared memory (psf[x + 32 y], the real part of
+// the inverse transform): pixel sampling, noise, stored intensities, gradients.
+template <int NPQ>
+__device__ __forceinline__ void ints_n32_pixels(const PowfsDev& P, const WfsDev& W, int isa, int lane,
+	const float* psf) {
 	// pixel sampling (mkh bilinear map, up to 4 taps per pixel)
 	const int npix = P.npix;
 	const int* sidx = P.simap_idx + (P.simap_per_sa ? (size_t)isa * npix * 4 : 0);
@@ -751,10 +763,218 @@ __device__ __forceinline__ void ints_n32_tail(const PowfsDev& P, const WfsDev& W
 	}
 }
 
+// ---- half-spectrum form of (c): the PSF is real, so its OTF is formed only
+// for fy = 0..16 and the image comes back through a complex-to-real inverse.
+// The columns fy = 0 and 16 (real along ky) travel packed as one complex
+// column, so 16 spectral columns remain, and lanes c and c + 16 share column
+// c: each does a 16-point transform of the even (c) or odd (c + 16) samples
+// and one exchange of 8 values forms the 32-point column.  Per image this is
+// four 16-point transforms per lane where the full spectrum takes four
+// 32-point ones, with half the transfer-function products.  The transfer
+// function (uplink OTF, ETF or DTF nominal: transforms of real kernels) is
+// Hermitian, so the half spectrum carries the whole product; the image equals
+// the real part of the full inverse (maos/wfsints.c:284-286 takes that real
+// part) up to rounding.
+
+// X[k] = sum_n x[n] w32^(kn), k = 0..16, of the real x held as z[n] = x[2n] +
+// i x[2n+1] after z = FFT16(z): X[0] and X[16] (real) packed as Q[0] = (X0,
+// X16), Q[k] = X[k] for k = 1..15.
+template <int K>
+__device__ __forceinline__ void r2c32_post(const float2 (&z)[16], float2 (&Q)[16]) {
+	if constexpr (K < 16) {
+		const float2 a = z[K], b = make_float2(z[16 - K].x, -z[16 - K].y);
+		const float2 sm = cadd(a, b), df = csub(a, b);
+		const float2 t = twmul<-1, 32, K>(make_float2(df.y, -df.x));  // w^K * (-i) * (a - b)
+		Q[K] = make_float2(0.5f * (sm.x + t.x), 0.5f * (sm.y + t.y));
+		r2c32_post<K + 1>(z, Q);
+	}
+}
+// The inverse: Z[k] = (Y[k] + Y[k+16]) + i w32^(-k) (Y[k] - Y[k+16]) with
+// Y[k+16] = conj Y[16-k], so that IFFT16(Z)[n] = y[2n] + i y[2n+1] for the
+// real y[n] = sum_k Y[k] w32^(-kn) of the Hermitian Y (Y[0], Y[16] packed).
+template <int K>
+__device__ __forceinline__ void c2r32_pre(const float2 (&Y)[16], float2 (&Z)[16]) {
+	if constexpr (K < 16) {
+		const float2 a = Y[K], b = make_float2(Y[16 - K].x, -Y[16 - K].y);
+		const float2 sm = cadd(a, b);
+		const float2 t = twmul<1, 32, K>(csub(a, b));
+		Z[K] = make_float2(sm.x - t.y, sm.y + t.x);
+		c2r32_pre<K + 1>(Y, Z);
+	}
+}
+// i * w32^(-k) (v) for k = i + 8h: the compile-time part w32^(-i), then i^h
+template <int I>
+__device__ __forceinline__ void inv_ramp8(float2 (&v)[8], int h) {
+	if constexpr (I < 8) {
+		float2 t = twmul<1, 32, I>(v[I]);
+		if (h) t = make_float2(-t.y, t.x);
+		v[I] = t;
+		inv_ramp8<I + 1>(v, h);
+	}
+}
+// v[i] times the transfer function at element e0 + stride*i (fx*32 + fy of
+// the transposed arrays): conj(uplink OTF) x (ETF, the blend of two ETFs, or
+// the DTF nominal).  The conditions are uniform over the warp and each
+// factor's NV loads are issued together.
+template <int NV>
+__device__ __forceinline__ void tf_apply(const PowfsDev& P, const WfsDev& W, int isa, int e0, int stride,
+	float2 (&v)[NV]) {
+	if (W.lotfT) {
+		float2 l[NV];
+#pragma unroll
+		for (int i = 0; i < NV; i++) l[i] = __ldg(W.lotfT + e0 + stride * i);
+#pragma unroll
+		for (int i = 0; i < NV; i++) v[i] = cmulc(v[i], l[i]);
+	}
+	if (P.etfT1) {
+		const float2* e1 = P.etfT1 + (size_t)isa * 1024 + e0;
+		float2 a[NV];
+#pragma unroll
+		for (int i = 0; i < NV; i++) a[i] = __ldg(e1 + stride * i);
+		if (P.etfT2) {
+			const float2* e2 = P.etfT2 + (size_t)isa * 1024 + e0;
+#pragma unroll
+			for (int i = 0; i < NV; i++) {
+				const float2 b = __ldg(e2 + stride * i);
+				a[i] = make_float2(a[i].x * P.etfwt1 + b.x * P.etfwt2, a[i].y * P.etfwt1 + b.y * P.etfwt2);
+			}
+		}
+#pragma unroll
+		for (int i = 0; i < NV; i++) v[i] = cmul(v[i], a[i]);
+	} else if (P.nominalT) {
+		const float* nm = P.nominalT + (P.nominal_per_sa ? (size_t)isa * 1024 : 0) + e0;
+		float d[NV];
+#pragma unroll
+		for (int i = 0; i < NV; i++) d[i] = __ldg(nm + stride * i);
+#pragma unroll
+		for (int i = 0; i < NV; i++) v[i] = make_float2(v[i].x * d[i], v[i].y * d[i]);
+	}
+}
+
+// F from field_fft_n32 (lane = kx holds F(kx, ky=0..31)) -> psf[x + 32 y] in
+// tile, the real image before pixel sampling.
+__device__ __forceinline__ void otf_tf_inverse_half_n32(const PowfsDev& P, const WfsDev& W, int isa, int lane,
+	float2* tile, const float2 (&F)[32]) {
+	// PSF row kx = lane along ky as 16 complex pairs, then its real FFT
+	float2 Q[16];
+	{
+		float2 z[16];
+#pragma unroll
+		for (int n = 0; n < 16; n++)
+			z[n] = make_float2(F[2 * n].x * F[2 * n].x + F[2 * n].y * F[2 * n].y,
+				F[2 * n + 1].x * F[2 * n + 1].x + F[2 * n + 1].y * F[2 * n + 1].y);
+		fft_reg<-1, 16>(z);
+		Q[0] = make_float2(z[0].x + z[0].y, z[0].x - z[0].y);
+		r2c32_post<1>(z, Q);
+	}
+	__syncwarp();
+#pragma unroll
+	for (int c = 0; c < 16; c++) tile[c * LD + lane] = Q[c];  // tile[c][kx]
+	__syncwarp();
+	// column c = lane & 15 along kx: h = 0 the even kx, h = 1 the odd kx
+	const int c = lane & 15, h = lane >> 4;
+	float2 A[8], B[8];  // G(fx) at fx = i + 8h (A) and i + 8h + 16 (B)
+	{
+		float2 v[16];
+#pragma unroll
+		for (int j = 0; j < 16; j++) v[j] = tile[c * LD + 2 * j + h];
+		fft_reg<-1, 16>(v);
+		if (h) twiddle_ramp<-1, 16, 32, 1>(v);  // w^k O[k]
+#pragma unroll
+		for (int i = 0; i < 8; i++) {
+			const float2 sd = h ? v[i] : v[8 + i];
+			const float2 r = make_float2(__shfl_xor_sync(0xffffffffu, sd.x, 16), __shfl_xor_sync(0xffffffffu, sd.y, 16));
+			const float2 ev = h ? r : v[i], od = h ? v[8 + i] : r;
+			A[i] = cadd(ev, od);
+			B[i] = csub(ev, od);
+		}
+	}
+	// column 0 holds Gp = G(fx, 0) + i G(fx, 16), both Hermitian in fx.  Lanes
+	// 0 and 16 put it in a scratch row; every lane then splits one fx with the
+	// mirrored value Gp(-fx), applies the transfer function at fy = 0 and 16,
+	// and packs the products again in a second row, which lanes 0 and 16 take
+	// back after the other columns' products.
+	float2* scr = tile + 16 * LD;
+	float2* scr2 = tile + 17 * LD;
+	if (c == 0) {
+#pragma unroll
+		for (int i = 0; i < 8; i++) {
+			scr[i + 8 * h] = A[i];
+			scr[i + 8 * h + 16] = B[i];
+		}
+	}
+	__syncwarp();
+	{
+		const float2 g = scr[lane], m = scr[(32 - lane) & 31];
+		float2 y0[1] = {make_float2(0.5f * (g.x + m.x), 0.5f * (g.y - m.y))};
+		float2 y16[1] = {make_float2(0.5f * (g.y + m.y), -0.5f * (g.x - m.x))};
+		tf_apply<1>(P, W, isa, lane * 32, 0, y0);
+		tf_apply<1>(P, W, isa, lane * 32 + 16, 0, y16);
+		scr2[lane] = make_float2(y0[0].x - y16[0].y, y0[0].y + y16[0].x);
+	}
+	tf_apply<8>(P, W, isa, 8 * h * 32 + c, 32, A);
+	tf_apply<8>(P, W, isa, (8 * h + 16) * 32 + c, 32, B);
+	__syncwarp();
+	if (c == 0) {
+#pragma unroll
+		for (int i = 0; i < 8; i++) {
+			A[i] = scr2[i + 8 * h];
+			B[i] = scr2[i + 8 * h + 16];
+		}
+	}
+	// inverse along fx: h = 0 forms the even x, h = 1 the odd x
+	float2 X[16];
+	{
+		float2 u[8], d[8];
+#pragma unroll
+		for (int i = 0; i < 8; i++) {
+			u[i] = cadd(A[i], B[i]);
+			d[i] = csub(A[i], B[i]);
+		}
+		inv_ramp8<0>(d, h);
+#pragma unroll
+		for (int i = 0; i < 8; i++) {
+			const float2 sd = h ? u[i] : d[i];
+			const float2 r = make_float2(__shfl_xor_sync(0xffffffffu, sd.x, 16), __shfl_xor_sync(0xffffffffu, sd.y, 16));
+			X[i] = h ? r : u[i];
+			X[8 + i] = h ? d[i] : r;
+		}
+		fft_reg<1, 16>(X);  // y(x = 2m + h, c)
+	}
+	__syncwarp();
+#pragma unroll
+	for (int m = 0; m < 16; m++) tile[(2 * m + h) * LD + c] = X[m];  // tile[x][c]
+	__syncwarp();
+	// row x = lane along fy: complex-to-real
+	{
+		float2 Y[16], Z[16];
+#pragma unroll
+		for (int k = 0; k < 16; k++) Y[k] = tile[lane * LD + k];
+		Z[0] = make_float2(Y[0].x + Y[0].y, Y[0].x - Y[0].y);
+		c2r32_pre<1>(Y, Z);
+		fft_reg<1, 16>(Z);
+		__syncwarp();
+		float* psf = reinterpret_cast<float*>(tile);
+#pragma unroll
+		for (int n = 0; n < 16; n++) {
+			psf[lane + 64 * n] = Z[n].x;
+			psf[lane + 64 * n + 32] = Z[n].y;
+		}
+	}
+	__syncwarp();
+}
+
+template <int NPQ>
+__device__ __forceinline__ void ints_n32_tail_half(const PowfsDev& P, const WfsDev& W, int isa, int lane,
+	float2* tile, const float2 (&F)[32]) {
+	otf_tf_inverse_half_n32(P, W, isa, lane, tile, F);
+	ints_n32_pixels<NPQ>(P, W, isa, lane, reinterpret_cast<const float*>(tile));
+}
+
 // NPQ: pixel slots per lane, ceil(npix/32).  MINB: resident blocks per SM the
 // register allocation must allow (occupancy/spill trade-off, picked by the
-// autotuner).
-template <int NPQ, int MINB>
+// autotuner).  HALF: the half-spectrum form of (c).
+template <int NPQ, int MINB, bool HALF = false>
 __global__ void __launch_bounds__(128, MINB) ints_n32_kernel(PowfsDev P, const WfsDev* __restrict__ wfs, int nw, int nitem) {
 	__shared__ float2 tiles[4][32 * LD];
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -771,7 +991,8 @@ __global__ void __launch_bounds__(128, MINB) ints_n32_kernel(PowfsDev P, const W
 		prefetch_l2(P.etfT1 + (size_t)isa * 1024 + 32 * lane + 16);
 	}
 	field_fft_n32(W.opd + off_opd, W.amp + off_opd, P.twoinvwvl, tile, lane, F);
-	ints_n32_tail<NPQ>(P, W, isa, lane, tile, F);
+	if (HALF) ints_n32_tail_half<NPQ>(P, W, isa, lane, tile, F);
+	else ints_n32_tail<NPQ>(P, W, isa, lane, tile, F);
 }
 
 // (d)-(e) after an imaging kernel that stored noise-free intensities (the

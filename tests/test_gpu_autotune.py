@@ -14,7 +14,7 @@ def test_autotune_keeps_a_variant_and_its_frames():
     from maos_b200.workload import build
     wl = build(LGS8_N32, device=0, seed=3, noisy=True, nx=256)
     v = wl.ctx.autotune(wl.wfs[0], wl.wfs[-1] + 1, nrep=2)
-    assert 0 <= v < 3
+    assert 0 <= v < 6  # SHWFS_NVARIANT
     wl.frame(1)
     a = wl.frame_sync(want_ints=True)
     wl.ctx.set_variant(wl.ipowfs, v)

@@ -41,11 +41,13 @@ def test_raytrace_matches_reference_prop(ref_lib, isim):
     wl.close()
 
 
-@pytest.mark.parametrize("isim", [0, 37])
-def test_lgs_full_frame_matches_reference(ref_lib, isim):
+# imaging variants: 0 full-spectrum transforms, 3 the half-spectrum form
+@pytest.mark.parametrize("isim,variant", [(0, 0), (37, 0), (0, 3), (37, 5)])
+def test_lgs_full_frame_matches_reference(ref_lib, isim, variant):
     from maos_b200.configs import LGS30
     from tests.helpers import ints_tolerance_ok, grad_rel_err
     wl = _workload(LGS30)
+    wl.ctx.set_variant(wl.ipowfs, variant)
     r = ref_lib.RefPowfs(LGS30)
     # same matched filter on both sides (the reference's, built from its turbulence OTF)
     for i in wl.wfs:
@@ -62,10 +64,12 @@ def test_lgs_full_frame_matches_reference(ref_lib, isim):
     wl.close()
 
 
-def test_ngs_full_frame_matches_reference(ref_lib):
+@pytest.mark.parametrize("variant", [0, 3])
+def test_ngs_full_frame_matches_reference(ref_lib, variant):
     from maos_b200.configs import NGS8
     from tests.helpers import ints_tolerance_ok, grad_rel_err
     wl = _workload(NGS8)
+    wl.ctx.set_variant(wl.ipowfs, variant)
     r = ref_lib.RefPowfs(NGS8)
     ref_lib.atm_set(wl.screens, wl.layers)
     wl.frame(5)

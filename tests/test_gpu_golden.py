@@ -18,7 +18,7 @@ from tests.test_golden import golden, meta
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not cuda_available(), reason="needs a CUDA GPU")]
 
 
-def _run(case, form):
+def _run(case, form, variant=None):
     import torch
     from maos_b200 import shwfs
     from maos_b200.configs import CONFIGS
@@ -30,6 +30,8 @@ def _run(case, form):
     wl = build(cfg, device=0, seed=1, noisy=False, nx=256, form=form)
     nsa, npix = wl.setup.nsa, wl.setup.npix
     iw = wl.wfs[iwfs]
+    if variant is not None:
+        wl.ctx.set_variant(wl.ipowfs, variant)
     if cfg["phytype"] == 1:
         mt = golden(case, "mtche")
         mtche = np.stack([mt[i, 0].ravel() for i in range(nsa)])
@@ -57,6 +59,15 @@ def _run(case, form):
 def test_fft_form_matches_golden(case):
     from maos_b200 import shwfs
     _run(case, shwfs.SHWFS_FORM_FFT)
+
+
+@pytest.mark.parametrize("case", ["ngs8", "lgs8_n32"])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5])
+def test_fft_form_variants_match_golden(case, variant):
+    """Every imaging-kernel variant of the 32-point FFT form (register caps of the full-spectrum
+    transforms; the half-spectrum form) against the same fixtures."""
+    from maos_b200 import shwfs
+    _run(case, shwfs.SHWFS_FORM_FFT, variant)
 
 
 @pytest.mark.parametrize("case", ["ngs8", "lgs8_n32"])
