@@ -57,7 +57,10 @@ struct PowfsState {
 	int dtrat = 1;      // frames integrated per output frame (powfs.dtrat)
 	DevBuf<float> lltamp;
 	DevBuf<double> lltorig;  // {llt origx, llt origy}
-	int variant = 0;         // imaging-kernel variant chosen by shwfs_autotune
+	// imaging-kernel variant chosen by shwfs_autotune: 0-2 full-spectrum, 3-5
+	// half-spectrum 32-point transforms; the half-spectrum form at 5 blocks per
+	// SM until the autotuner has run
+	int variant = 4;
 	std::vector<int> simap_idx_h;     // host copies of the pixel map (TC tables)
 	std::vector<double> simap_wt_h;
 	DevBuf<uint4> tc_bmat;            // tensor-core B operands (bf16 images)
@@ -1855,6 +1858,8 @@ static int ensure_branches(shwfs_ctx* ctx) {
 	return 0;
 }
 
+static bool variant_half(int v) { return v >= 3; }
+
 // The powfs the work-list launch serves: FFT form, physical optics, 32-point
 // (at most 128 pixels) or 128/256-point (at most 256 pixels), one frame per
 // output frame (dtrat 1), sigmatch 0 or 1.
@@ -1869,12 +1874,16 @@ static bool worklist_serves(const shwfs_ctx* ctx, const PowfsState& p) {
 // launch over a work list (worklist_kernel).  Geometric powfs run their own
 // chain first.  Returns 1 (nothing queued) when a powfs is not served.
 static int frame_worklist(shwfs_ctx* ctx, const std::vector<std::vector<int>>& wl, int isim) {
-	int nseg = 0;
+	int nseg = 0, nhalf = 0, nfull = 0;
 	for (size_t ip = 0; ip < wl.size(); ip++) {
 		if (wl[ip].empty() || is_geom(ctx->powfs[ip].d.gradtype)) continue;
 		if (!worklist_serves(ctx, ctx->powfs[ip])) return 1;
 		nseg++;
+		if (ctx->powfs[ip].d.notf == 32) (variant_half(ctx->powfs[ip].variant) ? nhalf : nfull)++;
 	}
+	// one form for the frame's 32-point images: that of their powfs' variants
+	if (nhalf && nfull) return 1;
+	const bool half32 = nhalf > 0;
 	if (nseg == 0 || nseg > WL_MAX_SEG) return 1;
 	int r;
 	// the ray traces of the powfs (and the whole chain of a geometric one) run
@@ -2028,9 +2037,12 @@ static int frame_worklist(shwfs_ctx* ctx, const std::vector<std::vector<int>>& w
 	int npq32 = 1;
 	for (int i = 0; i < W.nseg; i++)
 		if (W.seg[i].n == 32) npq32 = std::max(npq32, W.seg[i].npq);
-	auto kern = npq32 == 1 ? worklist_kernel<1> : npq32 == 2 ? worklist_kernel<2> : worklist_kernel<4>;
-	const int kv = npq32 == 1 ? 0 : npq32 == 2 ? 1 : 2;
-	static int resident[64][3] = {{0}};
+	using WlKernel = void (*)(const WorkParams);
+	const WlKernel kern = half32
+		? (npq32 == 1 ? (WlKernel)worklist_kernel<1, true> : npq32 == 2 ? (WlKernel)worklist_kernel<2, true> : (WlKernel)worklist_kernel<4, true>)
+		: (npq32 == 1 ? (WlKernel)worklist_kernel<1, false> : npq32 == 2 ? (WlKernel)worklist_kernel<2, false> : (WlKernel)worklist_kernel<4, false>);
+	const int kv = (npq32 == 1 ? 0 : npq32 == 2 ? 1 : 2) + (half32 ? 3 : 0);
+	static int resident[64][6] = {{0}};
 	if (ctx->device >= 64) return fail(ctx, SHWFS_EINVAL, "work list: device %d out of range", ctx->device);
 	if (!resident[ctx->device][kv]) {
 		CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, WL_N32_SMEM));
@@ -2766,11 +2778,11 @@ int shwfs_frame_noalloc(shwfs_ctx* ctx, int iwfs, int isim, float* ints, float* 
 	PowfsDev P = make_powfs_dev(p, isim);
 	const int nitem = p.d.nsa, nblk = (nitem + 3) / 4;
 	if (P.npix <= 32)
-		ints_n32_kernel<1, 4><<<nblk, 128, 0, ctx->stream>>>(P, desc, 1, nitem);
+		ints_n32_kernel<1, 5, true><<<nblk, 128, 0, ctx->stream>>>(P, desc, 1, nitem);
 	else if (P.npix <= 64)
-		ints_n32_kernel<2, 4><<<nblk, 128, 0, ctx->stream>>>(P, desc, 1, nitem);
+		ints_n32_kernel<2, 5, true><<<nblk, 128, 0, ctx->stream>>>(P, desc, 1, nitem);
 	else
-		ints_n32_kernel<4, 4><<<nblk, 128, 0, ctx->stream>>>(P, desc, 1, nitem);
+		ints_n32_kernel<4, 5, true><<<nblk, 128, 0, ctx->stream>>>(P, desc, 1, nitem);
 	CK(cudaGetLastError());
 	return 0;
 }

@@ -112,8 +112,11 @@ __device__ __noinline__ void wl_pixels(const WorkSeg& S, int item, int lane) {
 }
 
 // NPQ: pixel slots per lane of the 32-point items (the largest of the frame's
-// 32-point powfs; fewer pixels are handled by the same code).
-template <int NPQ>
+// 32-point powfs; fewer pixels are handled by the same code).  HALF: the
+// 32-point images in the half-spectrum form (the imaging variants 3-5 of
+// ints_n32_kernel), else the full-spectrum form, so that the frames equal
+// those of the powfs' own launches.
+template <int NPQ, bool HALF>
 __global__ void __launch_bounds__(WL_THREADS, 4) worklist_kernel(const __grid_constant__ WorkParams W) {
 	extern __shared__ float2 wl_s[];
 	__shared__ int s_it[2], s_ok;
@@ -140,7 +143,12 @@ __global__ void __launch_bounds__(WL_THREADS, 4) worklist_kernel(const __grid_co
 				}
 				float2 F[32];
 				field_fft_n32(Wd.opd + (size_t)isa * 256, Wd.amp + (size_t)isa * 256, S.P.twoinvwvl, tile, lane, F);
-				ints_n32_tail<NPQ>(S.P, Wd, isa, lane, tile, F);
+				if (HALF) {
+					otf_tf_inverse_half_n32(S.P, Wd, isa, lane, tile, F);
+					ints_n32_pixels<NPQ>(S.P, Wd, isa, lane, reinterpret_cast<const float*>(tile));
+				} else {
+					ints_n32_tail<NPQ>(S.P, Wd, isa, lane, tile, F);
+				}
 			}
 		} else if (w.x == WL_TILE) {
 			const int pass = w.w >> 16, tile = w.w & 0xffff;

@@ -81,9 +81,11 @@ def test_ngs_full_frame_matches_reference(ref_lib, variant):
     wl.close()
 
 
-def test_noise_statistics_match_reference(ref_lib):
+@pytest.mark.parametrize("variant", [0, 4])
+def test_noise_statistics_match_reference(ref_lib, variant):
     """10^4 noisy frames: per-pixel mean and variance, and the distribution of
-    normalised residuals against the reference's addnoise on the same image."""
+    normalised residuals against the reference's addnoise on the same image;
+    full-spectrum (variant 0) and half-spectrum (variant 4) imaging."""
     import torch
     from scipy import stats
     from maos_b200.configs import NGS8
@@ -91,6 +93,7 @@ def test_noise_statistics_match_reference(ref_lib):
     r = ref_lib.RefPowfs(NGS8)
     opd, _ = turbulent_opd(r, seed=11)
     ctx, ip, iw = context_from_ref(r, NGS8, noisy=1)
+    ctx.set_variant(ip, variant)
     dev = torch.device("cuda", 0)
     o = torch.tensor(opd, dtype=torch.float32, device=dev)
     nf = torch.zeros(r.nsa * r.npix, dtype=torch.float32, device=dev)
