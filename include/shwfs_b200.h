@@ -374,9 +374,10 @@ int shwfs_autotune_frame(shwfs_ctx* ctx, int iwfs0, int iwfs1, int nrep, int* ch
    default priority.  Synchronises the context; the branches and the frame
    graph are made again by the next frame.  Results do not depend on it. */
 int shwfs_set_branch_priority(shwfs_ctx* ctx, int on);
-/* Stream priority of the context's streams (CUDA's scale: lower numbers run
-   first; clamped to the device's range, 0 the default).  Synchronises the
-   context and makes its streams again: shwfs_stream returns the new handle.
+/* Stream priority of the context's stream (CUDA's scale: lower numbers run
+   first; clamped to the device's range, 0 the default; the context's uplink
+   stream stays at the greatest priority).  Synchronises the context and makes
+   its streams again: shwfs_stream returns the new handle.
    A server of many contexts on one GPU uses it to let some contexts' blocks
    reach the SMs first.  Results do not depend on it. */
 int shwfs_set_stream_priority(shwfs_ctx* ctx, int priority);

@@ -141,6 +141,7 @@ struct shwfs_ctx {
 	DevBuf<float2*> llt_out;
 	DevBuf<int> errflag;                 // bounded device waits record expiry here
 	int* errflag_h = nullptr;            // pinned copy read by the frame syncs
+	int errflag_armed = 0;               // a kernel that can set errflag ran since the last check
 	// gradients of the WFS in consecutive slices of a few chunks (device and
 	// pinned host at the same offsets), so that a range of WFS crosses to the
 	// host in one copy
@@ -264,7 +265,8 @@ static void f32_to_f64(const float* __restrict__ src, double* __restrict__ dst, 
 }
 
 static int check_errflag(shwfs_ctx* ctx) {
-	if (!ctx->errflag.p) return 0;
+	if (!ctx->errflag.p || !ctx->errflag_armed) return 0;
+	ctx->errflag_armed = 0;
 	int v = 0;
 	CK(cudaMemcpy(&v, ctx->errflag.p, sizeof(int), cudaMemcpyDeviceToHost));
 	if (v) {
@@ -294,8 +296,10 @@ int shwfs_create(shwfs_ctx** pctx, int device) {
 		delete ctx;
 		return SHWFS_ECUDA;
 	}
-	if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
-		cudaStreamCreateWithFlags(&ctx->aux, cudaStreamNonBlocking) != cudaSuccess ||
+	int prio_lo = 0, prio_hi = 0;
+	if (cudaSetDevice(device) != cudaSuccess || cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi) != cudaSuccess ||
+		cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+		cudaStreamCreateWithPriority(&ctx->aux, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
 		cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
 		cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming) != cudaSuccess) {
 		delete ctx;
@@ -869,8 +873,12 @@ static int launch_geom(shwfs_ctx* ctx, GeomParams& all) {
 		if (all.e[i].lltamp) lp.e[lp.nentry++] = all.e[i];
 		else gp.e[gp.nentry++] = all.e[i];
 	}
+	// the subaperture trace (the frame's critical path) is launched first; the
+	// uplink follows on the aux stream, whose greater priority lets its few
+	// blocks start as the trace's first blocks retire
+	if (lp.nentry) CK(cudaEventRecord(ctx->ev_fork, ctx->stream));
+	int r = launch_geom_wfs(ctx, gp);
 	if (lp.nentry) {
-		CK(cudaEventRecord(ctx->ev_fork, ctx->stream));
 		CK(cudaStreamWaitEvent(ctx->aux, ctx->ev_fork, 0));
 		{
 			StageMark m(ctx, SHWFS_STAGE_UPLINK, ctx->aux);
@@ -878,9 +886,8 @@ static int launch_geom(shwfs_ctx* ctx, GeomParams& all) {
 		}
 		CK(cudaGetLastError());
 		CK(cudaEventRecord(ctx->ev_join, ctx->aux));
+		CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
 	}
-	int r = launch_geom_wfs(ctx, gp);
-	if (lp.nentry) CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
 	return r;
 }
 
@@ -1476,6 +1483,7 @@ static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist
 			StageMark mark(ctx, SHWFS_STAGE_INTS);
 			ints_tc_kernel<<<grid, TC_THREADS, tc_smem_bytes(nlotf), ctx->stream>>>(P, wdev, nw, nitem, nlotf, T,
 				ctx->errflag.p);
+			ctx->errflag_armed = 1;
 		}
 		CK(cudaGetLastError());
 		bool post = false;
@@ -2057,6 +2065,7 @@ static int frame_worklist(shwfs_ctx* ctx, const std::vector<std::vector<int>>& w
 	{
 		StageMark mark(ctx, SHWFS_STAGE_INTS);
 		kern<<<grid, WL_THREADS, WL_N32_SMEM, ctx->stream>>>(W);
+		ctx->errflag_armed = 1;
 	}
 	CK(cudaGetLastError());
 	return 0;
@@ -2114,7 +2123,7 @@ int shwfs_set_stream_priority(shwfs_ctx* ctx, int priority) {
 	if ((r = drop_branches(ctx))) return r;
 	cudaStream_t s = nullptr, a = nullptr;
 	CK(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, p));
-	if (cudaStreamCreateWithPriority(&a, cudaStreamNonBlocking, p) != cudaSuccess) {
+	if (cudaStreamCreateWithPriority(&a, cudaStreamNonBlocking, hi) != cudaSuccess) {
 		cudaStreamDestroy(s);
 		return fail(ctx, SHWFS_ECUDA, "set_stream_priority: stream creation failed");
 	}
@@ -2248,15 +2257,20 @@ int shwfs_frame_sync(shwfs_ctx* ctx, int iwfs, double* grad, double* ints) {
 		CK(cudaMemcpyAsync(w->ints_h, w->ints.p, sizeof(float) * nsa * npix, cudaMemcpyDeviceToHost, ctx->stream));
 		ctx->d2h_bytes += sizeof(float) * nsa * npix;
 	}
-	if (ctx->errflag.p) {
+	// the error flag travels only when a kernel that can set it ran since the last check
+	const bool chk = ctx->errflag.p && ctx->errflag_armed;
+	if (chk) {
 		if (!ctx->errflag_h) CK(cudaMallocHost(&ctx->errflag_h, sizeof(int)));
 		CK(cudaMemcpyAsync(ctx->errflag_h, ctx->errflag.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
 	}
 	CK(cudaStreamSynchronize(ctx->stream));
 	ctx->wfsdev_h.clear();
-	if (ctx->errflag.p && *ctx->errflag_h) {
-		CK(cudaMemset(ctx->errflag.p, 0, sizeof(int)));
-		return fail(ctx, SHWFS_ETIMEOUT, "a bounded tensor-core wait expired in the imaging kernel");
+	if (chk) {
+		ctx->errflag_armed = 0;
+		if (*ctx->errflag_h) {
+			CK(cudaMemset(ctx->errflag.p, 0, sizeof(int)));
+			return fail(ctx, SHWFS_ETIMEOUT, "a bounded device wait expired in an imaging kernel");
+		}
 	}
 	if (grad) f32_to_f64(w->grad_h, grad, (size_t)2 * nsa);
 	if (ints) f32_to_f64(w->ints_h, ints, (size_t)nsa * npix);
@@ -2482,15 +2496,20 @@ int shwfs_frame_sync_range(shwfs_ctx* ctx, int iwfs0, int iwfs1, double* grad) {
 		ctx->d2h_bytes += sizeof(float) * n;
 		i = j;
 	}
-	if (ctx->errflag.p) {
+	// the error flag travels only when a kernel that can set it ran since the last check
+	const bool chk = ctx->errflag.p && ctx->errflag_armed;
+	if (chk) {
 		if (!ctx->errflag_h) CK(cudaMallocHost(&ctx->errflag_h, sizeof(int)));
 		CK(cudaMemcpyAsync(ctx->errflag_h, ctx->errflag.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
 	}
 	CK(cudaStreamSynchronize(ctx->stream));
 	ctx->wfsdev_h.clear();
-	if (ctx->errflag.p && *ctx->errflag_h) {
-		CK(cudaMemset(ctx->errflag.p, 0, sizeof(int)));
-		return fail(ctx, SHWFS_ETIMEOUT, "a bounded tensor-core wait expired in the imaging kernel");
+	if (chk) {
+		ctx->errflag_armed = 0;
+		if (*ctx->errflag_h) {
+			CK(cudaMemset(ctx->errflag.p, 0, sizeof(int)));
+			return fail(ctx, SHWFS_ETIMEOUT, "a bounded device wait expired in an imaging kernel");
+		}
 	}
 	for (int i = iwfs0; i < iwfs1; i++) {
 		const size_t n = ctx->wfs[i].grad.n;
