@@ -14,6 +14,7 @@
 #include <string.h>
 #include <string>
 #include <algorithm>
+#include <mutex>
 #include <vector>
 #include "../../include/shwfs_b200.h"
 #include "shwfs_kernels.cuh"
@@ -304,6 +305,21 @@ int shwfs_create(shwfs_ctx** pctx, int device) {
 		cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming) != cudaSuccess) {
 		delete ctx;
 		return SHWFS_ECUDA;
+	}
+	// the log-factorial table of the Poisson sampler, once per device
+	{
+		static std::mutex mu;
+		static bool done[64] = {false};
+		std::lock_guard<std::mutex> lock(mu);
+		if (device >= 64 || !done[device]) {
+			static float t[SHWFS_LOGFACT_N];
+			for (int k = 0; k < SHWFS_LOGFACT_N; k++) t[k] = (float)lgamma(k + 1.0);
+			if (cudaMemcpyToSymbol(g_logfact, t, sizeof(t)) != cudaSuccess) {
+				delete ctx;
+				return SHWFS_ECUDA;
+			}
+			if (device < 64) done[device] = true;
+		}
 	}
 	*pctx = ctx;
 	return 0;
@@ -959,6 +975,7 @@ static int launch_geom_wfs(shwfs_ctx* ctx, GeomParams& gp, bool split) {
 		if (smem > 48 * 1024) {
 			CK(cudaFuncSetAttribute(geom_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 			CK(cudaFuncSetAttribute(geom_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+			CK(cudaFuncSetAttribute(geom_kernel<false, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 		}
 		// GEOM_PTS points per thread with no idle slot where the pupil allows it:
 		// 16x16 pupils 64 threads, 32x32 256, larger ones split over blocks of 256
@@ -966,6 +983,7 @@ static int launch_geom_wfs(shwfs_ctx* ctx, GeomParams& gp, bool split) {
 		const int bd = std::min(256, std::max(32, ((np + GEOM_PTS - 1) / GEOM_PTS + 31) / 32 * 32));
 		const int bps = (np + GEOM_PTS * bd - 1) / (GEOM_PTS * bd);  // blocks per subaperture
 		if (extra) geom_kernel<true><<<(unsigned)nblk * bps, bd, smem, ctx->stream>>>(gp, nopd, nitem, bps);
+		else if (nopd == 16) geom_kernel<false, 16><<<(unsigned)nblk * bps, bd, smem, ctx->stream>>>(gp, nopd, nitem, bps);
 		else geom_kernel<false><<<(unsigned)nblk * bps, bd, smem, ctx->stream>>>(gp, nopd, nitem, bps);
 	}
 	CK(cudaGetLastError());

@@ -92,6 +92,14 @@ struct InvTableF {
 };
 __constant__ InvTableF c_invkf = InvTableF();
 
+// log(k!) for k < SHWFS_LOGFACT_N, filled from the host (double lgamma,
+// rounded) when the first context of a device is created
+#define SHWFS_LOGFACT_N 1024
+__device__ float g_logfact[SHWFS_LOGFACT_N];
+__device__ __forceinline__ float log_factorial(float k) {
+	return k < (float)SHWFS_LOGFACT_N ? __ldg(&g_logfact[(int)k]) : lgammaf(k + 1.f);
+}
+
 __device__ __forceinline__ float poisson_ptrs(PixelRng& rng, float lam) {
 	const float slam = sqrtf(lam), loglam = logf(lam);
 	const float b = 0.931f + 2.53f * slam;
@@ -105,7 +113,8 @@ __device__ __forceinline__ float poisson_ptrs(PixelRng& rng, float lam) {
 		const float k = floorf((2.f * a / us + b) * U + lam + 0.43f);
 		if (us >= 0.07f && V <= vr) return k;
 		if (k < 0.f || (us < 0.013f && V > us)) continue;
-		if (logf(V) + logf(invalpha) - logf(a / (us * us) + b) <= -lam + k * loglam - lgammaf(k + 1.f)) return k;
+		// log V + log(1/alpha) - log(a/us^2 + b) as one logarithm
+		if (logf(V * invalpha / (a / (us * us) + b)) <= -lam + k * loglam - log_factorial(k)) return k;
 	}
 	return rintf(lam);  // 64 rejections in a row: probability below 1e-60
 }
@@ -398,8 +407,10 @@ __device__ __forceinline__ float geom_bilerp(float al, float m00, float m10, flo
 
 // EXTRA: the launch has mirror grids, NCPA surfaces or polynomial terms (a
 // closed-loop frame); the open-loop launch compiles without their code.
-template <bool EXTRA>
-__global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomParams P, int nopd, int nitem, int bps) {
+// NOPD: the pupil side at compile time (0: the nopd argument).
+template <bool EXTRA, int NOPD = 0>
+__global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomParams P, int nopd_arg, int nitem, int bps) {
+	const int nopd = NOPD ? NOPD : nopd_arg;
 	extern __shared__ int4 s_tab[];
 	const int item = blockIdx.x / bps, part = blockIdx.x - item * bps;
 	if (item >= nitem) return;
