@@ -918,6 +918,25 @@ static int l2_bytes(shwfs_ctx* ctx) {
 	return v;
 }
 
+// The open-loop trace kernel for 16x16 or 32x32 pupils and 1-8 layers (their
+// tables stay below the 48 KB default of dynamic shared memory).
+using GeomKernel = void (*)(const GeomParams, int, int, int);
+template <int NOPD>
+static GeomKernel geom_pick_n(int nl) {
+	switch (nl) {
+	case 1: return geom_kernel<false, NOPD, 1>;
+	case 2: return geom_kernel<false, NOPD, 2>;
+	case 3: return geom_kernel<false, NOPD, 3>;
+	case 4: return geom_kernel<false, NOPD, 4>;
+	case 5: return geom_kernel<false, NOPD, 5>;
+	case 6: return geom_kernel<false, NOPD, 6>;
+	case 7: return geom_kernel<false, NOPD, 7>;
+	case 8: return geom_kernel<false, NOPD, 8>;
+	default: return geom_kernel<false, NOPD, 0>;
+	}
+}
+static GeomKernel geom_pick(int nopd, int nl) { return nopd == 16 ? geom_pick_n<16>(nl) : geom_pick_n<32>(nl); }
+
 // split: when the launch's screens exceed L2, the pupils of the largest size
 // are traced interleaved (each screen row their footprints share is fetched
 // from DRAM once while in L2) and any other pupils in a second launch.  With
@@ -975,7 +994,6 @@ static int launch_geom_wfs(shwfs_ctx* ctx, GeomParams& gp, bool split) {
 		if (smem > 48 * 1024) {
 			CK(cudaFuncSetAttribute(geom_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 			CK(cudaFuncSetAttribute(geom_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-			CK(cudaFuncSetAttribute(geom_kernel<false, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 		}
 		// GEOM_PTS points per thread with no idle slot where the pupil allows it:
 		// 16x16 pupils 64 threads, 32x32 256, larger ones split over blocks of 256
@@ -983,7 +1001,8 @@ static int launch_geom_wfs(shwfs_ctx* ctx, GeomParams& gp, bool split) {
 		const int bd = std::min(256, std::max(32, ((np + GEOM_PTS - 1) / GEOM_PTS + 31) / 32 * 32));
 		const int bps = (np + GEOM_PTS * bd - 1) / (GEOM_PTS * bd);  // blocks per subaperture
 		if (extra) geom_kernel<true><<<(unsigned)nblk * bps, bd, smem, ctx->stream>>>(gp, nopd, nitem, bps);
-		else if (nopd == 16) geom_kernel<false, 16><<<(unsigned)nblk * bps, bd, smem, ctx->stream>>>(gp, nopd, nitem, bps);
+		else if ((nopd == 16 || nopd == 32) && gp.nlayer <= 8)  // pupil side and layer count fixed at compile time
+			geom_pick(nopd, gp.nlayer)<<<(unsigned)nblk * bps, bd, smem, ctx->stream>>>(gp, nopd, nitem, bps);
 		else geom_kernel<false><<<(unsigned)nblk * bps, bd, smem, ctx->stream>>>(gp, nopd, nitem, bps);
 	}
 	CK(cudaGetLastError());

@@ -407,8 +407,10 @@ __device__ __forceinline__ float geom_bilerp(float al, float m00, float m10, flo
 
 // EXTRA: the launch has mirror grids, NCPA surfaces or polynomial terms (a
 // closed-loop frame); the open-loop launch compiles without their code.
-// NOPD: the pupil side at compile time (0: the nopd argument).
-template <bool EXTRA, int NOPD = 0>
+// NOPD: the pupil side at compile time (0: the nopd argument; 16 launches
+// 64-thread blocks, 32 256-thread blocks); NL: the layer count at compile time
+// (0: P.nlayer).
+template <bool EXTRA, int NOPD = 0, int NL = 0>
 __global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomParams P, int nopd_arg, int nitem, int bps) {
 	const int nopd = NOPD ? NOPD : nopd_arg;
 	extern __shared__ int4 s_tab[];
@@ -423,7 +425,8 @@ __global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomP
 		isa = item - P.e[ie].item0;
 	}
 	const GeomEntry& E = P.e[ie];
-	const int tid = threadIdx.x, nl = P.nlayer;
+	const int tid = threadIdx.x, nl = NL ? NL : P.nlayer;
+	const int bdim = NOPD == 16 ? 64 : NOPD == 32 ? 256 : (int)blockDim.x;
 	// the footprint origin of each (layer, axis) once, in FP64; then the
 	// entries of the nopd points of each line from it in FP32
 	__shared__ int s_j0[2 * SHWFS_MAX_LAYERS];
@@ -437,7 +440,7 @@ __global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomP
 		if (!(tid & 1)) s_step[tid >> 1] = (float)(E.dx * E.sx[tid >> 1]);
 	}
 	__syncthreads();
-	for (int k = tid; k < nl * 2 * nopd; k += blockDim.x) {
+	for (int k = tid; k < nl * 2 * nopd; k += bdim) {
 		const int l = k / (2 * nopd), r = k - l * 2 * nopd;
 		const bool isy = r >= nopd;
 		const int i = isy ? r - nopd : r;
@@ -454,7 +457,7 @@ __global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomP
 	__syncthreads();
 	// up to GEOM_PTS points per thread, layers outermost so that the gathers of the points are in flight
 	// together; every point still sums its layers in order
-	const int bd = blockDim.x;
+	const int bd = bdim;
 	const int np = nopd * nopd, p0 = GEOM_PTS * bd * part, p1 = min(np, p0 + GEOM_PTS * bd);
 	float acc[GEOM_PTS];
 	int ixu[GEOM_PTS], iyu[GEOM_PTS];
@@ -466,6 +469,7 @@ __global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomP
 		iyu[u] = ip / nopd;
 	}
 	const int nwrap = EXTRA ? nl - P.nmirror : nl;
+#pragma unroll
 	for (int l = 0; l < nwrap; l++) {
 		if (!((E.use >> l) & 1u)) continue;
 		const float* __restrict__ sc = P.screen[l];
