@@ -145,6 +145,23 @@ int shwfs_powfs_set_lltamp(shwfs_ctx* ctx, int ipowfs, const double* lltamp);
    and update_mtche then uses the flat-wavefront OTF. */
 int shwfs_powfs_set_seotf(shwfs_ctx* ctx, int ipowfs, const double* seotf);
 
+/* Another wavelength band of powfs ipowfs (the reference images every
+   wavelength of powfs.wvl, maos/wfsints.c:145-288; cuda/sim/wfsints.cu).  desc
+   describes the band: the subapertures, sampling, sizes, pixels, LLT and
+   gradient options of ipowfs, its own wvl; wvlwt is its weight
+   (powfs.wvlwts[iwvl]); the main band's weight is the WFS's wvlwt.  *iband
+   receives the band's powfs index: give the band its transfer functions and
+   pixel map with shwfs_powfs_set_nominal / set_simap / set_etf (and
+   set_lltamp to replace the LLT pupil copied from ipowfs).  The band copies
+   the geometry of ipowfs as set at the call (set it first).  A frame of
+   ipowfs's WFS traces the OPD once, images it in every band (the uplink OTF at
+   each band's wavelength), sums the intensities, then adds noise and forms
+   gradients once.  Matched filters come from the host for such a powfs
+   (shwfs_wfs_update_mtche refuses it), and the work-list and allocation-free
+   paths do not serve it.  At most SHWFS_MAX_BANDS extra bands. */
+#define SHWFS_MAX_BANDS 8
+int shwfs_powfs_add_band(shwfs_ctx* ctx, int ipowfs, const shwfs_powfs_desc* desc, double wvlwt, int* iband);
+
 /* Declares a WFS; *iwfs receives its index. */
 int shwfs_wfs_add(shwfs_ctx* ctx, const shwfs_wfs_desc* desc, int* iwfs);
 /* Matched filter mtche (nsa x 2 x npix, each subaperture a 2 x npix

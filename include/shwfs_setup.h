@@ -95,6 +95,11 @@ int shwfs_setup_get_simap_idx(const shwfs_setup* s, int* out);
    its index.  WFS are added separately (shwfs_wfs_add); the matched filter of
    the setup is available for shwfs_wfs_set_mtche via shwfs_setup_get. */
 int shwfs_setup_load(const shwfs_setup* s, shwfs_ctx* ctx, int* ipowfs);
+/* Declares the setup as another wavelength band of powfs ipowfs
+   (shwfs_powfs_add_band, weight wvlwt) and uploads its pixel map and its ETF
+   or DTF nominal; *iband receives the band's powfs index.  The setup is that
+   of the same powfs configuration at the band's wavelength. */
+int shwfs_setup_load_band(const shwfs_setup* s, shwfs_ctx* ctx, int ipowfs, double wvlwt, int* iband);
 /* Loads the setup's matched filter (or CoG i0sum) into WFS iwfs. */
 int shwfs_setup_load_wfs(const shwfs_setup* s, shwfs_ctx* ctx, int iwfs);
 

@@ -971,8 +971,40 @@ int shwfs_setup_get_simap_idx(const shwfs_setup* s, int* out) {
 	return 0;
 }
 
+static void setup_desc(const shwfs_setup* s, shwfs_powfs_desc* pd);
+
 int shwfs_setup_load(const shwfs_setup* s, shwfs_ctx* ctx, int* ipowfs) {
 	if (!s || !ctx || !ipowfs) return SHWFS_EINVAL;
+	const shwfs_setup_cfg* c = &s->cfg;
+	shwfs_powfs_desc d;
+	setup_desc(s, &d);
+	int r = shwfs_powfs_add(ctx, &d, ipowfs);
+	if (r) return r;
+	if ((r = shwfs_powfs_set_geom(ctx, *ipowfs, s->origx, s->origy, s->amp, 1, s->saa))) return r;
+	if ((r = shwfs_powfs_set_saasum(ctx, *ipowfs, s->saasum))) return r;
+	if ((r = shwfs_powfs_set_simap(ctx, *ipowfs, s->simap_idx, s->simap_wt, 1))) return r;
+	if (c->has_llt) {
+		if ((r = shwfs_powfs_set_etf(ctx, *ipowfs, (const double*)s->etf, 0))) return r;
+		if ((r = shwfs_powfs_set_lltamp(ctx, *ipowfs, s->lltamp))) return r;
+	} else {
+		if ((r = shwfs_powfs_set_nominal(ctx, *ipowfs, s->nominal, 1))) return r;
+	}
+	if (s->seotf && (r = shwfs_powfs_set_seotf(ctx, *ipowfs, (const double*)s->seotf))) return r;
+	return 0;
+}
+
+int shwfs_setup_load_band(const shwfs_setup* s, shwfs_ctx* ctx, int ipowfs, double wvlwt, int* iband) {
+	if (!s || !ctx || !iband) return SHWFS_EINVAL;
+	shwfs_powfs_desc d;
+	setup_desc(s, &d);
+	int r = shwfs_powfs_add_band(ctx, ipowfs, &d, wvlwt, iband);
+	if (r) return r;
+	if ((r = shwfs_powfs_set_simap(ctx, *iband, s->simap_idx, s->simap_wt, 1))) return r;
+	if (s->cfg.has_llt) return shwfs_powfs_set_etf(ctx, *iband, (const double*)s->etf, 0);
+	return shwfs_powfs_set_nominal(ctx, *iband, s->nominal, 1);
+}
+
+static void setup_desc(const shwfs_setup* s, shwfs_powfs_desc* pd) {
 	const shwfs_setup_cfg* c = &s->cfg;
 	shwfs_powfs_desc d;
 	memset(&d, 0, sizeof(d));
@@ -1003,19 +1035,7 @@ int shwfs_setup_load(const shwfs_setup* s, shwfs_ctx* ctx, int* ipowfs) {
 	d.bkgrndc = c->bkgrnd * c->bkgrndc;
 	d.saat = c->saat;
 	d.sigtot_cog = c->siglev;
-	int r = shwfs_powfs_add(ctx, &d, ipowfs);
-	if (r) return r;
-	if ((r = shwfs_powfs_set_geom(ctx, *ipowfs, s->origx, s->origy, s->amp, 1, s->saa))) return r;
-	if ((r = shwfs_powfs_set_saasum(ctx, *ipowfs, s->saasum))) return r;
-	if ((r = shwfs_powfs_set_simap(ctx, *ipowfs, s->simap_idx, s->simap_wt, 1))) return r;
-	if (c->has_llt) {
-		if ((r = shwfs_powfs_set_etf(ctx, *ipowfs, (const double*)s->etf, 0))) return r;
-		if ((r = shwfs_powfs_set_lltamp(ctx, *ipowfs, s->lltamp))) return r;
-	} else {
-		if ((r = shwfs_powfs_set_nominal(ctx, *ipowfs, s->nominal, 1))) return r;
-	}
-	if (s->seotf && (r = shwfs_powfs_set_seotf(ctx, *ipowfs, (const double*)s->seotf))) return r;
-	return 0;
+	*pd = d;
 }
 
 int shwfs_setup_load_wfs(const shwfs_setup* s, shwfs_ctx* ctx, int iwfs) {

@@ -74,6 +74,12 @@ struct PowfsState {
 	std::vector<double> origx_h, origy_h;
 	std::vector<DevBuf<int>> gs0_ptr, gs0_col;  // G-tilt operators in CSR, one per amplitude
 	std::vector<DevBuf<float>> gs0_val;
+	// wavelength bands (shwfs_powfs_add_band): a band powfs names its main
+	// powfs and weight; the main powfs lists its bands
+	int band_of = -1;
+	double band_wvlwt = 1;
+	std::vector<int> bands;
+	std::vector<DevBuf<float2>> band_lotf;  // a band's uplink OTF per WFS (by WFS index)
 };
 
 struct WfsState {
@@ -177,6 +183,8 @@ struct shwfs_ctx {
 	std::vector<WorkCache> wl_cache;
 	DevBuf<int> wl_cnt;                  // dispenser + per-image tile counters
 	int dtrat_inner = 0;       // launch_ints_dtrat is running the imaging part
+	int band_inner = 0;        // launch_ints_bands is running one band
+	int band_accum = 0;        // the band adds to the intensities of the bands before it
 };
 static void evl_free(shwfs_ctx* ctx);
 
@@ -239,6 +247,18 @@ static int dev_alloc(shwfs_ctx* ctx, DevBuf<T>& b, size_t n) {
 	b.n = n;
 	return 0;
 }
+template <typename T>
+static int dev_copy(shwfs_ctx* ctx, DevBuf<T>& dst, const DevBuf<T>& src) {
+	if (!src.p) {
+		dst.free_();
+		return 0;
+	}
+	int r = dev_alloc(ctx, dst, src.n);
+	if (r) return r;
+	CK(cudaMemcpyAsync(dst.p, src.p, src.n * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream));
+	return 0;
+}
+
 template <typename T>
 static int dev_upload(shwfs_ctx* ctx, DevBuf<T>& b, const T* h, size_t n) {
 	int r = dev_alloc(ctx, b, n);
@@ -585,10 +605,49 @@ int shwfs_powfs_set_lltamp(shwfs_ctx* ctx, int ipowfs, const double* lltamp) {
 	return dev_upload_f(ctx, p->lltamp, lltamp, (size_t)p->d.llt_nx * p->d.llt_nx);
 }
 
+int shwfs_powfs_add_band(shwfs_ctx* ctx, int ipowfs, const shwfs_powfs_desc* d, double wvlwt, int* iband) {
+	PowfsState* m = get_powfs(ctx, ipowfs);
+	if (!m || !d || !iband || !(wvlwt >= 0)) return ctx ? fail(ctx, SHWFS_EINVAL, "add_band: bad arguments") : SHWFS_EINVAL;
+	if (m->band_of >= 0) return fail(ctx, SHWFS_EINVAL, "add_band: powfs %d is itself a band", ipowfs);
+	if (is_geom(m->d.gradtype)) return fail(ctx, SHWFS_EINVAL, "add_band: a geometric sensor forms no images");
+	if (m->bands.size() >= SHWFS_MAX_BANDS) return fail(ctx, SHWFS_EINVAL, "add_band: at most %d bands", SHWFS_MAX_BANDS);
+	if (!m->amp.p || !m->origx.p) return fail(ctx, SHWFS_ESTATE, "add_band: set the geometry of powfs %d first", ipowfs);
+	const shwfs_powfs_desc& a = m->d;
+	if (d->nsa != a.nsa || d->nopd != a.nopd || d->embfac != a.embfac || d->notf != a.notf || d->pixpsax != a.pixpsax ||
+		d->pixpsay != a.pixpsay || d->has_etf != a.has_etf || d->has_llt != a.has_llt || d->llt_nx != a.llt_nx ||
+		d->gradtype != a.gradtype || d->sigmatch != a.sigmatch || d->dsa != a.dsa || d->dx != a.dx || !(d->wvl > 0))
+		return fail(ctx, SHWFS_EINVAL,
+			"add_band: a band keeps its powfs' subapertures, sampling, sizes, pixels, LLT and gradient options; only the "
+			"wavelength and the transfer functions differ");
+	int ib = -1, r = shwfs_powfs_add(ctx, d, &ib);
+	if (r) return r;
+	PowfsState& M = ctx->powfs[ipowfs];  // the powfs vector may have grown
+	PowfsState& B = ctx->powfs[ib];
+	B.band_of = ipowfs;
+	B.band_wvlwt = wvlwt;
+	// the band images the main powfs' subapertures: its geometry, as set now
+	if ((r = dev_copy(ctx, B.origx, M.origx)) || (r = dev_copy(ctx, B.origy, M.origy)) ||
+		(r = dev_copy(ctx, B.amp, M.amp)) || (r = dev_copy(ctx, B.saa, M.saa)) ||
+		(r = dev_copy(ctx, B.lltamp, M.lltamp)) || (r = dev_copy(ctx, B.lltorig, M.lltorig)))
+		return r;
+	CK(cudaStreamSynchronize(ctx->stream));
+	B.namp = M.namp;
+	B.saasum = M.saasum;
+	B.origx_h = M.origx_h;
+	B.origy_h = M.origy_h;
+	B.dtrat = 1;
+	M.bands.push_back(ib);
+	*iband = ib;
+	return 0;
+}
+
 int shwfs_wfs_add(shwfs_ctx* ctx, const shwfs_wfs_desc* d, int* iwfs) {
 	if (!ctx || !d || !iwfs) return SHWFS_EINVAL;
 	PowfsState* p = get_powfs(ctx, d->ipowfs);
 	if (!p) return fail(ctx, SHWFS_EINVAL, "wfs_add: unknown powfs %d", d->ipowfs);
+	if (p->band_of >= 0)
+		return fail(ctx, SHWFS_EINVAL, "wfs_add: powfs %d is a wavelength band of powfs %d; add the WFS there", d->ipowfs,
+			p->band_of);
 	int r = set_device(ctx);
 	if (r) return r;
 	ctx->wfs.emplace_back();
@@ -1043,10 +1102,27 @@ static int add_llt_entry(shwfs_ctx* ctx, GeomParams& gp, WfsState& w, int isim) 
 	return 0;
 }
 
+// The LLT pupil of WFS w once more for wavelength band pb: the uplink OTF at
+// the band's wavelength into lotf (the traced OPD is that of the main band's entry).
+static int add_llt_band_entry(shwfs_ctx* ctx, GeomParams& gp, WfsState& w, int isim, const PowfsState& pb, float2* lotf) {
+	PowfsState& p = ctx->powfs[w.d.ipowfs];
+	int r = add_geom_entry(ctx, gp, w.d.thetax - p.d.llt_ox / w.d.hs, w.d.thetay - p.d.llt_oy / w.d.hs, w.d.hs, 0, 0,
+		0, p.d.llt_ox, p.d.llt_oy, isim, p.lltorig.p, p.lltorig.p + 1, 1, p.d.llt_nx, p.d.dx, nullptr);
+	if (r) return r;
+	GeomEntry& e = gp.e[gp.nentry - 1];
+	set_llt_poly(e, w);
+	e.lltamp = pb.lltamp.p;
+	e.lotfT = lotf;
+	e.twoinvwvl = (float)(2.0 / pb.d.wvl);
+	e.lltnorm = (float)(1.0 / ((double)pb.d.llt_nx * pb.d.embfac * pb.d.llt_nx * pb.d.embfac));
+	return 0;
+}
+
 static float norm_ints(const PowfsState& p, const WfsState& w) {
 	const double nwvf = (double)p.d.nopd * p.d.embfac;
 	const double norm_psf = sqrt(p.d.areascale) / ((double)p.d.nopd * nwvf);
-	return (float)(w.d.sigsim * w.d.wvlwt * norm_psf * norm_psf / ((double)p.d.notf * p.d.notf));
+	const double wt = p.band_of >= 0 ? p.band_wvlwt : w.d.wvlwt;  // powfs.wvlwts[iwvl]
+	return (float)(w.d.sigsim * wt * norm_psf * norm_psf / ((double)p.d.notf * p.d.notf));
 }
 
 static PowfsDev make_powfs_dev(const PowfsState& p, int isim) {
@@ -1391,13 +1467,13 @@ static int launch_gen(shwfs_ctx* ctx, PowfsState& p, const WfsDev* wdev, int nw,
 // Uplink OTFs of the LLT pupils of a generic-size powfs from their traced
 // OPDs (maos/wfsints.c:149-199).
 static int launch_uplink_gen(shwfs_ctx* ctx, PowfsState& p, const std::vector<int>& wlist,
-	const std::vector<const float*>& lltopd) {
+	const std::vector<const float*>& lltopd, const std::vector<float2*>* out = nullptr) {
 	std::vector<WfsDev> wd(wlist.size());
 	for (size_t k = 0; k < wlist.size(); k++) {
 		memset(&wd[k], 0, sizeof(WfsDev));
 		wd[k].opd = lltopd[k];
 		wd[k].amp = p.lltamp.p;
-		wd[k].lotfT = ctx->wfs[wlist[k]].lotfT.p;
+		wd[k].lotfT = out ? (*out)[k] : ctx->wfs[wlist[k]].lotfT.p;
 	}
 	const WfsDev* wdev = nullptr;
 	int r = push_wfsdev(ctx, wd, &wdev);
@@ -1415,6 +1491,9 @@ static int launch_ints_sig2(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& 
 static int launch_ints_dtrat(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist, int isim,
 	const std::vector<const float*>& opds, const std::vector<const float2*>& lotfs, const std::vector<float*>& ints,
 	const std::vector<float*>& grads, const std::vector<int>& noisy);
+static int launch_ints_bands(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist, int isim,
+	const std::vector<const float*>& opds, const std::vector<const float2*>& lotfs, const std::vector<float*>& ints,
+	const std::vector<float*>& grads, const std::vector<int>& noisy);
 static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist, int isim,
 	const std::vector<const float*>& opds, const std::vector<const float2*>& lotfs, const std::vector<float*>& ints,
 	const std::vector<float*>& grads, const std::vector<int>& noisy) {
@@ -1426,6 +1505,8 @@ static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist
 		return launch_ints_dtrat(ctx, ipowfs, wlist, isim, opds, lotfs, ints, grads, noisy);
 	if (p.d.sigmatch == 2 && !ctx->sig2_inner)
 		return launch_ints_sig2(ctx, ipowfs, wlist, isim, opds, lotfs, ints, grads, noisy);
+	if (!p.bands.empty() && !ctx->band_inner)
+		return launch_ints_bands(ctx, ipowfs, wlist, isim, opds, lotfs, ints, grads, noisy);
 	if (ctx->form == SHWFS_FORM_TC && nw > TC_MAX_WFS) {
 		// the tensor-core launch holds at most TC_MAX_WFS WFS descriptors in shared memory
 		for (int k0 = 0; k0 < nw; k0 += TC_MAX_WFS) {
@@ -1437,6 +1518,7 @@ static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist
 		return 0;
 	}
 	PowfsDev P = make_powfs_dev(p, isim);
+	if (ctx->band_accum) P.accum = 1;
 	std::vector<WfsDev> wd(nw);
 	for (int k = 0; k < nw; k++) {
 		WfsState& w = ctx->wfs[wlist[k]];
@@ -1534,7 +1616,7 @@ static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist
 		return 0;
 	}
 	StageMark mark(ctx, SHWFS_STAGE_INTS);
-	const int v = p.variant;
+	const int v = p.band_of >= 0 ? ctx->powfs[p.band_of].variant : p.variant;  // a band follows its main powfs
 	auto go = [&](auto kern) { kern<<<nblk, 128, 0, ctx->stream>>>(P, wdev, nw, nitem); };
 	// variants 0-2: full-spectrum transforms at a register cap for 4, 5, 6
 	// blocks per SM; 3-5: the half-spectrum form at the same caps
@@ -1631,6 +1713,41 @@ static int launch_ints_dtrat(shwfs_ctx* ctx, int ipowfs, const std::vector<int>&
 				CK(cudaMemcpyAsync(ints[k], acc[k], sizeof(float) * p.d.nsa * p.d.pixpsax * p.d.pixpsay,
 					cudaMemcpyDeviceToDevice, ctx->stream));
 	return 0;
+}
+
+// Imaging of a powfs with wavelength bands (maos/wfsints.c:145-288, the loop
+// over powfs.wvl): every band images the same OPD with its own wavelength,
+// uplink OTF, transfer function and pixel map, and adds its intensities, times
+// its weight, to those of the bands before it; noise and gradients follow on
+// the sum, in the launch of the last band.
+static int launch_ints_bands(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist, int isim,
+	const std::vector<const float*>& opds, const std::vector<const float2*>& lotfs, const std::vector<float*>& ints,
+	const std::vector<float*>& grads, const std::vector<int>& noisy) {
+	const int nw = (int)wlist.size();
+	std::vector<int> order(1, ipowfs);
+	for (int b : ctx->powfs[ipowfs].bands) order.push_back(b);
+	std::vector<float*> acc(nw), none(nw, nullptr);
+	std::vector<int> quiet(nw, 0);
+	for (int k = 0; k < nw; k++) {
+		acc[k] = ints[k] ? ints[k] : ctx->wfs[wlist[k]].ints.p;
+		if (!acc[k]) return fail(ctx, SHWFS_ESTATE, "bands: WFS %d has no intensity buffer", wlist[k]);
+	}
+	const int accum0 = ctx->band_accum;
+	int r = 0;
+	ctx->band_inner = 1;
+	for (size_t j = 0; j < order.size() && !r; j++) {
+		const bool last = j + 1 == order.size();
+		std::vector<const float2*> lj(nw, nullptr);
+		for (int k = 0; k < nw; k++) {
+			if (j == 0) lj[k] = lotfs[k];
+			else if (ctx->powfs[order[j]].d.has_llt) lj[k] = ctx->powfs[order[j]].band_lotf[wlist[k]].p;
+		}
+		ctx->band_accum = j > 0 ? 1 : accum0;
+		r = launch_ints(ctx, order[j], wlist, isim, opds, lj, acc, last ? grads : none, last ? noisy : quiet);
+	}
+	ctx->band_inner = 0;
+	ctx->band_accum = accum0;
+	return r;
 }
 
 // Imaging of a sigmatch-2 powfs (normalisation by the frame's total
@@ -1853,7 +1970,20 @@ static int frame_powfs(shwfs_ctx* ctx, int ip, const std::vector<int>& wl, int i
 static int trace_powfs(shwfs_ctx* ctx, int ip, const std::vector<int>& wl, int isim) {
 	PowfsState& p = ctx->powfs[ip];
 	int r;
-	const int per = p.d.has_llt ? SHWFS_MAX_ENTRIES / 2 : SHWFS_MAX_ENTRIES;
+	// each wavelength band of an LGS powfs forms its own uplink OTF per WFS
+	const int nb = (int)p.bands.size();
+	if (p.d.has_llt && nb) {
+		for (int ib : p.bands) {
+			PowfsState& pb = ctx->powfs[ib];
+			if (pb.band_lotf.size() < ctx->wfs.size()) pb.band_lotf.resize(ctx->wfs.size());
+			for (int i : wl) {
+				if (pb.band_lotf[i].p) continue;
+				if (ctx->capturing) return fail(ctx, SHWFS_ESTATE, "frame graph: band buffers not allocated by a warm-up frame");
+				if ((r = dev_alloc(ctx, pb.band_lotf[i], (size_t)pb.d.notf * pb.d.notf))) return r;
+			}
+		}
+	}
+	const int per = p.d.has_llt ? SHWFS_MAX_ENTRIES / (2 + (p.d.notf == 32 ? nb : 0)) : SHWFS_MAX_ENTRIES;
 	for (size_t b = 0; b < wl.size(); b += per) {
 		GeomParams gp;
 		geom_init(ctx, gp);
@@ -1861,6 +1991,10 @@ static int trace_powfs(shwfs_ctx* ctx, int ip, const std::vector<int>& wl, int i
 			WfsState& w = ctx->wfs[wl[k]];
 			if ((r = add_wfs_entry(ctx, gp, w, isim, w.opd.p))) return r;
 			if (p.d.has_llt && (r = add_llt_entry(ctx, gp, w, isim))) return r;
+			if (p.d.has_llt && p.d.notf == 32)
+				for (int ib : p.bands)
+					if ((r = add_llt_band_entry(ctx, gp, w, isim, ctx->powfs[ib], ctx->powfs[ib].band_lotf[wl[k]].p)))
+						return r;
 		}
 		if ((r = launch_geom(ctx, gp))) return r;
 		if (p.d.has_llt && p.d.notf != 32) {
@@ -1871,6 +2005,11 @@ static int trace_powfs(shwfs_ctx* ctx, int ip, const std::vector<int>& wl, int i
 				lo.push_back(ctx->wfs[wl[k]].lltopd.p);
 			}
 			if ((r = launch_uplink_gen(ctx, p, bw, lo))) return r;
+			for (int ib : p.bands) {
+				std::vector<float2*> out;
+				for (int i : bw) out.push_back(ctx->powfs[ib].band_lotf[i].p);
+				if ((r = launch_uplink_gen(ctx, ctx->powfs[ib], bw, lo, &out))) return r;
+			}
 		}
 	}
 	return 0;
@@ -1909,7 +2048,8 @@ static bool variant_half(int v) { return v >= 3; }
 // (at most 128 pixels) or 128/256-point (at most 256 pixels), one frame per
 // output frame (dtrat 1), sigmatch 0 or 1.
 static bool worklist_serves(const shwfs_ctx* ctx, const PowfsState& p) {
-	if (ctx->form != SHWFS_FORM_FFT || is_geom(p.d.gradtype) || p.dtrat > 1 || p.d.sigmatch == 2) return false;
+	if (ctx->form != SHWFS_FORM_FFT || is_geom(p.d.gradtype) || p.dtrat > 1 || p.d.sigmatch == 2 || !p.bands.empty())
+		return false;
 	const int npix = p.d.pixpsax * p.d.pixpsay;
 	if (p.d.notf == 32) return p.d.nopd == 16 && npix <= 128;
 	return (p.d.notf == 128 || p.d.notf == 256) && npix <= 256;
@@ -2324,6 +2464,7 @@ int shwfs_wfs_update_mtche(shwfs_ctx* ctx, int iwfs, int mtchcr) {
 	const int nsa = d.nsa, npix = d.pixpsax * d.pixpsay;
 	if (!(d.nopd == 16 && d.notf == 32)) return fail(ctx, SHWFS_EINVAL, "update_mtche: needs 16x16 OPD points and FFT 32");
 	if (d.gradtype != SHWFS_GRAD_MF) return fail(ctx, SHWFS_EINVAL, "update_mtche: the powfs uses CoG gradients");
+	if (!p.bands.empty()) return fail(ctx, SHWFS_EINVAL, "update_mtche: a powfs of several wavelength bands takes its filter from the host");
 	if (p.nsimap != 1 || npix > 128) return fail(ctx, SHWFS_EINVAL, "update_mtche: needs one pixel map of at most 128 pixels");
 	if (!p.amp.p || !p.simap_idx.p) return fail(ctx, SHWFS_ESTATE, "update_mtche: geometry or pixel map not set");
 	if (d.has_etf ? !p.etfT[0].p : !p.nominalT.p) return fail(ctx, SHWFS_ESTATE, "update_mtche: ETF / DTF not set");
@@ -2425,6 +2566,7 @@ int shwfs_powfs_set_dtrat(shwfs_ctx* ctx, int ipowfs, int dtrat) {
 	if (!p || dtrat < 1 || dtrat > 100000) return ctx ? fail(ctx, SHWFS_EINVAL, "set_dtrat: bad arguments") : SHWFS_EINVAL;
 	if (is_geom(p->d.gradtype) && dtrat > 1) return fail(ctx, SHWFS_EINVAL, "set_dtrat: geometric sensors form every frame");
 	if (p->d.sigmatch == 2 && dtrat > 1) return fail(ctx, SHWFS_EINVAL, "set_dtrat: sigmatch 2 with dtrat > 1 is not supported");
+	if (p->band_of >= 0) return fail(ctx, SHWFS_EINVAL, "set_dtrat: a wavelength band integrates with its powfs %d", p->band_of);
 	p->dtrat = dtrat;
 	return 0;
 }
@@ -2772,6 +2914,7 @@ int shwfs_frame_noalloc(shwfs_ctx* ctx, int iwfs, int isim, float* ints, float* 
 	if (is_geom(p.d.gradtype)) return fail(ctx, SHWFS_EINVAL, "frame_noalloc: geometric sensor");
 	if (p.d.sigmatch == 2) return fail(ctx, SHWFS_EINVAL, "frame_noalloc: sigmatch 2 needs the frame path");
 	if (p.dtrat > 1) return fail(ctx, SHWFS_EINVAL, "frame_noalloc: dtrat > 1 needs the frame path");
+	if (!p.bands.empty()) return fail(ctx, SHWFS_EINVAL, "frame_noalloc: wavelength bands need the frame path");
 	if (p.d.nsa > SHWFS_NOALLOC_MAX_NSA)
 		return fail(ctx, SHWFS_EINVAL, "frame_noalloc: %d subapertures exceed the allocation-free maximum of %d",
 			p.d.nsa, SHWFS_NOALLOC_MAX_NSA);

@@ -58,6 +58,7 @@ def _lib():
         L.shwfs_setup_get_simap_idx.argtypes = [vp, C.POINTER(C.c_int)]
         L.shwfs_setup_load.argtypes = [vp, vp, C.POINTER(i)]
         L.shwfs_setup_load_wfs.argtypes = [vp, vp, i]
+        L.shwfs_setup_load_band.argtypes = [vp, vp, i, C.c_double, C.POINTER(i)]
         L.shwfs_screens_vonkarman.argtypes = [C.POINTER(dp), i, C.c_long, C.c_long, C.c_double, C.c_double, C.c_double,
                                              dp, C.c_uint32]
         L.shwfs_aper_build.argtypes = [C.c_double, C.c_double, C.c_double, C.POINTER(C.c_long), dp, dp, dp]
@@ -147,6 +148,15 @@ class Setup:
         ctx.npix[ip.value] = self.npix
         ctx.nsa[ip.value] = self.nsa
         return ip.value
+
+    def load_band(self, ctx: "shwfs.Context", ipowfs: int, wvlwt: float) -> int:
+        """This setup as a further wavelength band of powfs ipowfs (weight wvlwt);
+        returns the band's powfs index."""
+        ib = C.c_int()
+        ctx._check(_lib().shwfs_setup_load_band(self._h, ctx._h, ipowfs, float(wvlwt), C.byref(ib)), "setup_load_band")
+        ctx.npix[ib.value] = self.npix
+        ctx.nsa[ib.value] = self.nsa
+        return ib.value
 
     def load_wfs(self, ctx: "shwfs.Context", iwfs: int):
         ctx._check(_lib().shwfs_setup_load_wfs(self._h, ctx._h, iwfs), "setup_load_wfs")

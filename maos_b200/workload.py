@@ -66,10 +66,17 @@ def build_from_setup(cfg: dict, setup: Setup, device: int = 0, seed: int = 1, no
     ctx.set_form(form)
     ctx.set_dt(cfg.get("dt", 1.0 / 800))
     ip = setup.load(ctx)
+    # further wavelengths (cfg["wvls"][1:], weights cfg["wvlwts"]): one band each, set up at its wavelength
+    wvls = list(cfg.get("wvls", [cfg["wvl"]]))
+    wts = list(cfg.get("wvlwts", [1.0] * len(wvls)))
+    for wv, wt in zip(wvls[1:], wts[1:]):
+        sb = Setup(dict(cfg, wvl=wv))
+        sb.load_band(ctx, ip, wt)
+        sb.close()
     wl = []
     for k in range(cfg["nwfs"]):
         i = ctx.wfs_add(ipowfs=ip, thetax=cfg["thetax"][k], thetay=cfg["thetay"][k], hs=cfg["hs"], hc=0.0,
-                        misregx=0.0, misregy=0.0, sigsim=cfg["siglev"], wvlwt=1.0, noisy=1 if noisy else 0)
+                        misregx=0.0, misregy=0.0, sigsim=cfg["siglev"], wvlwt=wts[0], noisy=1 if noisy else 0)
         setup.load_wfs(ctx, i)
         ctx.wfs_seed(i, seed * 1000003 + k)
         wl.append(i)

@@ -30,7 +30,7 @@ class OrefCfg(C.Structure):
                 ("L0", C.c_double), ("has_llt", C.c_int), ("llt_d", C.c_double), ("llt_widthp", C.c_double),
                 ("llt_ox", C.c_double), ("llt_oy", C.c_double), ("na_n", C.c_int), ("na_h", C.c_void_p),
                 ("na_p", C.c_void_p), ("nwfs", C.c_int), ("thetax", C.c_void_p), ("thetay", C.c_void_p),
-                ("nthread", C.c_int)]
+                ("nthread", C.c_int), ("nwvl", C.c_int), ("wvls", C.c_void_p), ("wvlwts", C.c_void_p)]
 
 
 _lib = None
@@ -75,6 +75,10 @@ class RefPowfs:
         tx = np.asarray(cfg["thetax"], dtype=np.float64)
         ty = np.asarray(cfg["thetay"], dtype=np.float64)
         keep += [tx, ty]
+        # several wavelengths: cfg["wvls"] with weights cfg["wvlwts"] (powfs.wvl, powfs.wvlwts)
+        wv = np.ascontiguousarray(cfg.get("wvls", [cfg["wvl"]]), dtype=np.float64)
+        ww = np.ascontiguousarray(cfg.get("wvlwts", [1.0] * len(wv)), dtype=np.float64)
+        keep += [wv, ww]
         c = OrefCfg(D=cfg["D"], Din=cfg["Din"], amp_binary=cfg.get("amp_binary", 0), order=cfg["order"],
                     dsa=cfg["dsa"], dx=cfg["dx"], saat=cfg["saat"], embfac=cfg["embfac"], notf=cfg["notf"],
                     pixpsa=cfg["pixpsa"], pixtheta=cfg["pixtheta"], pixblur=cfg["pixblur"], wvl=cfg["wvl"],
@@ -84,7 +88,8 @@ class RefPowfs:
                     r0=cfg["r0"], L0=cfg["L0"], has_llt=cfg.get("has_llt", 0), llt_d=cfg.get("llt_d", 0.0),
                     llt_widthp=cfg.get("llt_widthp", 0.0), llt_ox=cfg.get("llt_ox", 0.0),
                     llt_oy=cfg.get("llt_oy", 0.0), na_n=0 if na_h is None else len(na_h), na_h=_p(na_h),
-                    na_p=_p(na_p), nwfs=cfg["nwfs"], thetax=_p(tx), thetay=_p(ty), nthread=nthread)
+                    na_p=_p(na_p), nwfs=cfg["nwfs"], thetax=_p(tx), thetay=_p(ty), nthread=nthread,
+                    nwvl=len(wv), wvls=_p(wv), wvlwts=_p(ww))
         self._keep = keep
         self.nsa = L.oref_setup(C.byref(c))
         self.nopd = L.oref_nopd()
@@ -122,6 +127,11 @@ class RefPowfs:
         a = np.zeros(self.nsa)
         lib().oref_get_saa(_p(a))
         return a
+
+    def select_wvl(self, iwvl: int):
+        """The wavelength whose DTF nominal, pixel map, ETF and dtheta the getters return."""
+        lib().oref_select_wvl(C.c_int(iwvl))
+        self.dtheta = lib().oref_dtheta()
 
     def nominal(self, isa: int = 0):
         a = np.zeros(self.notf ** 2)

@@ -56,6 +56,9 @@ typedef struct oref_cfg_t{
 	const double* thetax; /* rad */
 	const double* thetay; /* rad */
 	int nthread;          /* NTHREAD for the reference's own threading */
+	int nwvl;             /* wavelengths (0 or 1: wvl alone) */
+	const double* wvls;   /* nwvl wavelengths (m) */
+	const double* wvlwts; /* nwvl weights */
 }oref_cfg_t;
 
 static parms_t* g_parms=NULL;
@@ -74,7 +77,9 @@ static lmat* lvec(long n, long start){
 void oref_cl_set(int ndm, const double* const* surf, const long* nx, const long* ny, const double* dx,
 	const double* ox, const double* oy, const double* ht, int use_dm, const double* ptt, double focus_tel,
 	double focus_llt, const double* lltptt, const double* opdadd);
+static int g_iwvl;
 int oref_setup(const oref_cfg_t* c){
+	g_iwvl=0;
 	dspfree(g_gs0);
 	g_gs0=NULL;
 	/* a new powfs starts with no closed-loop terms */
@@ -97,11 +102,21 @@ int oref_setup(const oref_cfg_t* c){
 	parms->dbg.wfslinearity=-1;
 	parms->save.gradnf=lnew(c->nwfs, 1);
 	powfs_cfg_t* p=parms->powfs;
-	g_wvl=dnew(1, 1); P(g_wvl, 0)=c->wvl;
-	p->wvl=g_wvl;
-	p->wvlwts=dnew(1, 1); P(p->wvlwts, 0)=1;
-	p->nwvl=1;
-	p->wvlmean=c->wvl;
+	{
+		/* powfs.wvl, powfs.wvlwts and wvlmean as maos/parms.c:266-283 reads them */
+		const int nwvl=(c->nwvl>1&&c->wvls)?c->nwvl:1;
+		g_wvl=dnew(nwvl, 1);
+		p->wvlwts=dnew(nwvl, 1);
+		real wm=0;
+		for(int i=0; i<nwvl; i++){
+			P(g_wvl, i)=nwvl>1?c->wvls[i]:c->wvl;
+			P(p->wvlwts, i)=(nwvl>1&&c->wvlwts)?c->wvlwts[i]:1;
+			wm+=P(g_wvl, i);
+		}
+		p->wvl=g_wvl;
+		p->nwvl=nwvl;
+		p->wvlmean=wm/nwvl;
+	}
 	p->order=c->order;
 	p->dsa=c->dsa;
 	p->dx=c->dx;
@@ -213,7 +228,10 @@ int oref_notf(void){ return g_powfs[0].notfx; }
 int oref_pixpsax(void){ return g_powfs[0].pixpsax; }
 int oref_pixpsay(void){ return g_powfs[0].pixpsay; }
 double oref_areascale(void){ return g_powfs[0].areascale; }
-double oref_dtheta(void){ return g_powfs[0].dtf[0].dtheta; }
+/* the wavelength whose DTF, pixel map and ETF the getters below return */
+static int g_iwvl=0;
+void oref_select_wvl(int iwvl){ g_iwvl=(iwvl>=0&&iwvl<g_parms->powfs[0].nwvl)?iwvl:0; }
+double oref_dtheta(void){ return g_powfs[0].dtf[g_iwvl].dtheta; }
 int oref_llt_nx(void){ return g_powfs[0].llt?(int)g_powfs[0].llt->pts->nxsa:0; }
 
 static void copy_vec(double* out, const double* in, long n){ memcpy(out, in, sizeof(double)*n); }
@@ -233,13 +251,13 @@ void oref_get_saa(double* saa){ dmat* a=P(g_powfs[0].saa, 0); copy_vec(saa, P(a)
 double oref_get_saasum(void){ return P(g_powfs[0].saasum, 0); }
 /* nominal DTF (treated, peak in corner with chess pattern) for subaperture isa */
 void oref_get_nominal(int isa, double* out){
-	dcell* nom=g_powfs[0].dtf[0].nominal;
+	dcell* nom=g_powfs[0].dtf[g_iwvl].nominal;
 	dmat* n=PN(nom)==1?P(nom, 0):P(nom, isa);
 	copy_vec(out, P(n), PN(n));
 }
 /* pixel sampling matrix si (npix x notf^2) of subaperture isa, dense, column-major */
 void oref_get_si_dense(int isa, double* out){
-	dspcell* sis=g_powfs[0].dtf[0].si;
+	dspcell* sis=g_powfs[0].dtf[g_iwvl].si;
 	dsp* si=PN(sis)==1?P(sis, 0):P(sis, isa);
 	long nr=si->nx, nc=si->ny;
 	memset(out, 0, sizeof(double)*nr*nc);
@@ -251,7 +269,7 @@ void oref_get_si_dense(int isa, double* out){
 }
 /* ETF with the nominal fused in, subaperture isa, interleaved complex notf^2 */
 void oref_get_etf(int isa, double* out){
-	cmat* e=P(g_powfs[0].etfsim[0].etf, isa, 0);
+	cmat* e=P(g_powfs[0].etfsim[g_iwvl].etf, isa, 0);
 	copy_vec(out, (double*)P(e), 2*PN(e));
 }
 void oref_get_srot(double* out){ dmat* a=P(g_powfs[0].srot, 0); copy_vec(out, P(a), PN(a)); }

@@ -5,7 +5,7 @@ screens are compared bit for bit."""
 import numpy as np
 import pytest
 
-from maos_b200.configs import NGS8, LGS30, LGS8_N64, NGS30_2X2, TT30
+from maos_b200.configs import NGS8, LGS30, LGS8_N64, NGS30_2X2, TT30, NGS8_2WVL, LGS8_N32_2WVL
 
 
 def _setup(cfg):
@@ -40,6 +40,37 @@ def test_dtf_and_pixel_map_bit_exact(ref_lib, cfg):
         a = {int(k): v for k, v in zip(ri[p], rw[p]) if k >= 0}
         b = {int(k): v for k, v in zip(si[p], sw[p]) if k >= 0}
         assert a == b, (p, a, b)
+
+
+@pytest.mark.parametrize("cfg", [NGS8_2WVL, LGS8_N32_2WVL], ids=lambda c: c["name"])
+def test_wavelength_bands_bit_exact(ref_lib, cfg):
+    """A polychromatic powfs: the product's setup at each band's wavelength gives the
+    reference's DTF nominal, pixel map and ETF of that wavelength (powfs.dtf[iwvl],
+    etfsim[iwvl]) bit for bit, with the OTF size of the first wavelength."""
+    from oracle.ref import si_to_taps
+    r = ref_lib.RefPowfs(cfg)
+    for iw, wv in enumerate(cfg["wvls"]):
+        r.select_wvl(iw)
+        s = _setup(dict(cfg, wvl=wv))
+        assert s.notf == r.notf and s.nsa == r.nsa
+        assert s.dtheta == r.dtheta
+        if cfg.get("has_llt"):
+            assert np.array_equal(r.etf(), s.get("etf")), iw
+        else:
+            assert np.array_equal(r.nominal(0), s.get("nominal")), iw
+        ri, rw = si_to_taps(r.si_dense(0))
+        si = s.simap_idx().reshape(-1, 4)
+        sw = s.get("simap_wt").reshape(-1, 4)
+        for p in range(len(ri)):
+            a = {int(k): v for k, v in zip(ri[p], rw[p]) if k >= 0}
+            b = {int(k): v for k, v in zip(si[p], sw[p]) if k >= 0}
+            assert a == b, (iw, p, a, b)
+        s.close()
+    # the two wavelengths sample differently
+    r.select_wvl(0)
+    d0 = r.dtheta
+    r.select_wvl(1)
+    assert r.dtheta > d0
 
 
 def test_lgs_etf_llt_bit_exact(ref_lib):
