@@ -24,7 +24,7 @@
  *
  * The reference aborts on errors (error()); a nonzero status from the library is reported the
  * same way, with the library's message.  Options of the reference's WFS path that the library
- * does not serve (several wavelengths, sodium sublayers, per-WFS amplitude maps, cubic DMs,
+ * does not serve (more than SHWFS_MAX_BANDS + 1 wavelengths, sodium sublayers, per-WFS amplitude maps, cubic DMs,
  * MOAO, field stops, dithering, ...) are refused with error() at gpu_wfsgrad_init, so the
  * adapter never returns gradients that differ from MAOS's in silence. One context serves every WFS. The simulator queues and
  * syncs WFS from several host threads at once, and calls on one context must not overlap, so
@@ -39,6 +39,7 @@
 static shwfs_ctx* g_ctx;
 static int g_ipowfs[64];   /* MAOS ipowfs -> context powfs (physical optics, or the geometric sensor) */
 static int g_ipowfs_geo[64];/* MAOS ipowfs -> context geometric powfs before phystep, or -1 */
+static int g_band[64][SHWFS_MAX_BANDS+1];/* MAOS ipowfs, wavelength -> context powfs of that band */
 static int* g_wfs_phy;     /* MAOS iwfs -> context WFS with physical optics, or -1 */
 static int* g_wfs_geo;     /* MAOS iwfs -> context geometric WFS, or -1 */
 static int* g_wfs_cur;     /* MAOS iwfs -> the context WFS its last queued frame ran, or -1 */
@@ -73,12 +74,38 @@ static void si_taps(const dsp* si, int* idx, double* wt){
 
 /* etf.etf is a cell of nsa (x 1 or x nllt) notf x notf complex arrays; pack the first LLT's
    column subaperture-major, as shwfs_powfs_set_etf takes it. */
-static void set_etf(const powfs_t* p, int ip, const etf_t* etf, int slot){
+static void set_etf(const powfs_t* p, int ipl, const etf_t* etf, int slot){
 	const long nsa=p->saloc->nloc, n2=(long)p->notfx*p->notfy;
 	cmat* e=cnew(n2, nsa);
 	for(long isa=0; isa<nsa; isa++) memcpy(PCOL(e, isa), P(P(etf->etf, isa, 0)), sizeof(comp)*n2);
-	chk(shwfs_powfs_set_etf(g_ctx, g_ipowfs[ip], (const double*)P(e), slot), "set_etf");
+	chk(shwfs_powfs_set_etf(g_ctx, ipl, (const double*)P(e), slot), "set_etf");
 	cfree(e);
+}
+
+/* Wavelength iwvl's pixel map and ETF (LGS) or DTF nominal (powfs.dtf[iwvl], etfsim[iwvl])
+   into context powfs ipl. */
+static void load_band_data(const powfs_t* p, int iwvl, int ipl){
+	/* dtf.si and dtf.nominal: one map shared by every subaperture, or one per subaperture
+	   (lib/mkdtf.c:116-161: radpix or pixoffx) */
+	const dspcell* si=p->dtf[iwvl].si;
+	const long nmap=PN(si);
+	const long npix=(long)p->pixpsax*p->pixpsay;
+	int* idx=mymalloc(nmap*npix*4, int);
+	double* wt=mymalloc(nmap*npix*4, double);
+	for(long m=0; m<nmap; m++) si_taps(P(si, m), idx+m*npix*4, wt+m*npix*4);
+	chk(shwfs_powfs_set_simap(g_ctx, ipl, idx, wt, (int)nmap), "set_simap");
+	free(idx); free(wt);
+	if(p->llt){
+		set_etf(p, ipl, &p->etfsim[iwvl], 0);
+	}else{
+		/* nominal is real-valued in MAOS's FFT layout */
+		const dcell* nom=p->dtf[iwvl].nominal;
+		const long nn=PN(nom), n2=(long)p->notfx*p->notfy;
+		dmat* all=dnew(n2, nn);
+		for(long m=0; m<nn; m++) memcpy(PCOL(all, m), P(P(nom, m)), sizeof(real)*n2);
+		chk(shwfs_powfs_set_nominal(g_ctx, ipl, P(all), (int)nn), "set_nominal");
+		dfree(all);
+	}
 }
 
 /* intstat->mtche is nsa x nwfs cells of 2 x npix; pack the WFS's column subaperture-major. */
@@ -110,7 +137,15 @@ static void refuse_unsupported(const parms_t* parms, const powfs_t* powfs){
 		const powfs_cfg_t* pc=&parms->powfs[ip];
 		const powfs_t* p=&powfs[ip];
 		if(pc->type!=WFS_SH) error("shwfs: powfs %d is not a Shack-Hartmann WFS\n", ip);
-		if(pc->nwvl>1) error("shwfs: powfs %d has %d wavelengths; one band only\n", ip, pc->nwvl);
+		if(pc->nwvl>SHWFS_MAX_BANDS+1) error("shwfs: powfs %d has %d wavelengths; at most %d\n", ip, pc->nwvl,
+			SHWFS_MAX_BANDS+1);
+		/* the weights of the further wavelengths belong to the band, shared by the powfs' WFS */
+		for(int jw=1; jw<pc->nwfs; jw++){
+			const dmat* w0=parms->wfs[P(pc->wfs, 0)].wvlwts, * wj=parms->wfs[P(pc->wfs, jw)].wvlwts;
+			for(int iwvl=1; iwvl<pc->nwvl; iwvl++)
+				if(P(wj, iwvl)!=P(w0, iwvl))
+					error("shwfs: powfs %d: WFS weights of wavelength %d differ between WFS\n", ip, iwvl);
+		}
 		if(pc->moao>-1) error("shwfs: powfs %d uses MOAO\n", ip);
 		if(pc->fieldstop>0) error("shwfs: powfs %d has a field stop\n", ip);
 		if(pc->dither) error("shwfs: powfs %d dithers\n", ip);
@@ -125,9 +160,11 @@ static void refuse_unsupported(const parms_t* parms, const powfs_t* powfs){
 		if(pc->usephy){
 			if(pc->phytype_sim!=PTYPE_MF && pc->phytype_sim!=PTYPE_COG)
 				error("shwfs: powfs %d gradient type %d; matched filter or CoG only\n", ip, pc->phytype_sim);
-			const dtf_t* dtf=&p->dtf[0];
-			if(NY(dtf->si)>1 || NY(dtf->nominal)>1)
-				error("shwfs: powfs %d has pixel maps per WFS (pixoffx/pixoffy per WFS)\n", ip);
+			for(int iwvl=0; iwvl<pc->nwvl; iwvl++){
+				const dtf_t* dtf=&p->dtf[iwvl];
+				if(NY(dtf->si)>1 || NY(dtf->nominal)>1)
+					error("shwfs: powfs %d has pixel maps per WFS (pixoffx/pixoffy per WFS)\n", ip);
+			}
 		}
 	}
 }
@@ -153,27 +190,17 @@ static void add_phy_powfs(const parms_t* parms, const powfs_t* p, int ip, int* i
 	chk(shwfs_powfs_set_geom(g_ctx, *ipl, p->pts->origx, p->pts->origy, P(P(p->amp, 0)), 1, P(P(p->saa, 0))),
 		"set_geom");
 	chk(shwfs_powfs_set_saasum(g_ctx, *ipl, P(p->saasum, 0)), "set_saasum");
-	/* dtf.si and dtf.nominal: one map shared by every subaperture, or one per subaperture
-	   (lib/mkdtf.c:116-161: radpix or pixoffx) */
-	const dspcell* si=p->dtf[0].si;
-	const long nmap=PN(si);
-	const long npix=(long)p->pixpsax*p->pixpsay;
-	int* idx=mymalloc(nmap*npix*4, int);
-	double* wt=mymalloc(nmap*npix*4, double);
-	for(long m=0; m<nmap; m++) si_taps(P(si, m), idx+m*npix*4, wt+m*npix*4);
-	chk(shwfs_powfs_set_simap(g_ctx, *ipl, idx, wt, (int)nmap), "set_simap");
-	free(idx); free(wt);
-	if(llt){
-		set_etf(p, ip, &p->etfsim[0], 0);
-		chk(shwfs_powfs_set_lltamp(g_ctx, *ipl, P(p->llt->amp)), "set_lltamp");
-	}else{
-		/* nominal is real-valued in MAOS's FFT layout */
-		const dcell* nom=p->dtf[0].nominal;
-		const long nn=PN(nom), n2=(long)p->notfx*p->notfy;
-		dmat* all=dnew(n2, nn);
-		for(long m=0; m<nn; m++) memcpy(PCOL(all, m), P(P(nom, m)), sizeof(real)*n2);
-		chk(shwfs_powfs_set_nominal(g_ctx, *ipl, P(all), (int)nn), "set_nominal");
-		dfree(all);
+	if(llt) chk(shwfs_powfs_set_lltamp(g_ctx, *ipl, P(p->llt->amp)), "set_lltamp");
+	load_band_data(p, 0, *ipl);
+	g_band[ip][0]=*ipl;
+	/* further wavelengths (powfs.wvl[1..]): bands imaged from the same OPD, weighted by the
+	   WFS's wvlwts (maos/wfsints.c:145-288) */
+	for(int iwvl=1; iwvl<pc->nwvl; iwvl++){
+		shwfs_powfs_desc db=d;
+		db.wvl=P(pc->wvl, iwvl);
+		const double wt=P(parms->wfs[P(pc->wfs, 0)].wvlwts, iwvl);
+		chk(shwfs_powfs_add_band(g_ctx, *ipl, &db, wt, &g_band[ip][iwvl]), "powfs_add_band");
+		load_band_data(p, iwvl, g_band[ip][iwvl]);
 	}
 	if(pc->dtrat>1) chk(shwfs_powfs_set_dtrat(g_ctx, *ipl, pc->dtrat), "set_dtrat");
 }
@@ -261,16 +288,19 @@ void gpu_wfsgrad_update_etf(const parms_t* parms, const powfs_t* powfs, int ipow
 	const powfs_t* p=&powfs[ipowfs];
 	if(!p->llt || !parms->powfs[ipowfs].usephy) return;
 	pthread_mutex_lock(&g_lock);
-	set_etf(p, ipowfs, &p->etfsim[0], 0);
-	if(p->etfsim2){
-		set_etf(p, ipowfs, &p->etfsim2[0], 1);
-		/* the interpolation period as maos/wfsints.c:218 picks it */
-		const int dtrat=parms->powfs[ipowfs].llt->coldtrat?parms->powfs[ipowfs].llt->coldtrat
-			:parms->powfs[ipowfs].zoomdtrat;
-		chk(shwfs_powfs_set_etf_dtrat(g_ctx, g_ipowfs[ipowfs], dtrat), "set_etf_dtrat");
-	}else{
-		/* slot 0 alone: no interpolation left over from an earlier pair */
-		chk(shwfs_powfs_set_etf_dtrat(g_ctx, g_ipowfs[ipowfs], 0), "set_etf_dtrat");
+	for(int iwvl=0; iwvl<parms->powfs[ipowfs].nwvl; iwvl++){
+		const int ipl=g_band[ipowfs][iwvl];
+		set_etf(p, ipl, &p->etfsim[iwvl], 0);
+		if(p->etfsim2){
+			set_etf(p, ipl, &p->etfsim2[iwvl], 1);
+			/* the interpolation period as maos/wfsints.c:218 picks it */
+			const int dtrat=parms->powfs[ipowfs].llt->coldtrat?parms->powfs[ipowfs].llt->coldtrat
+				:parms->powfs[ipowfs].zoomdtrat;
+			chk(shwfs_powfs_set_etf_dtrat(g_ctx, ipl, dtrat), "set_etf_dtrat");
+		}else{
+			/* slot 0 alone: no interpolation left over from an earlier pair */
+			chk(shwfs_powfs_set_etf_dtrat(g_ctx, ipl, 0), "set_etf_dtrat");
+		}
 	}
 	pthread_mutex_unlock(&g_lock);
 }

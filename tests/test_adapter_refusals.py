@@ -40,7 +40,7 @@ print("NOT REFUSED")
 
 # (poke code, value, config, expected message)
 CASES = [
-    (1, 2, "NGS8", "wavelengths; one band only"),
+    (1, 10, "NGS8", "wavelengths; at most"),
     (2, 3, "LGS8_N32", "sodium sublayers"),
     (3, 0, "NGS8", "one amplitude map per WFS"),
     (4, 3, "NGS8", "matched filter or CoG only"),

@@ -43,7 +43,9 @@ def _screens(cfg):
     return screens, layers
 
 
-@pytest.mark.parametrize("cfg_name,isims,wfs", [("NGS8", (5, 6), (0,)), ("LGS30", (0, 37), (0, 3))])
+# the two-wavelength cases: one band per powfs.wvl, from powfs.dtf[iwvl] and etfsim[iwvl]
+@pytest.mark.parametrize("cfg_name,isims,wfs", [("NGS8", (5, 6), (0,)), ("LGS30", (0, 37), (0, 3)),
+                                                 ("NGS8_2WVL", (4,), (0,)), ("LGS8_N32_2WVL", (3,), (0, 1))])
 def test_adapter_frames_match_reference(ref_lib, cfg_name, isims, wfs):
     from maos_b200 import configs
     from tests.helpers import grad_rel_err
