@@ -411,7 +411,8 @@ __device__ __forceinline__ float geom_bilerp(float al, float m00, float m10, flo
 // 64-thread blocks, 32 256-thread blocks); NL: the layer count at compile time
 // (0: P.nlayer).
 template <bool EXTRA, int NOPD = 0, int NL = 0>
-__global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomParams P, int nopd_arg, int nitem, int bps) {
+__global__ void __launch_bounds__(NOPD == 16 ? 64 : 256, NOPD == 16 ? 32 : NOPD == 32 ? 8 : 1)
+	geom_kernel(const __grid_constant__ GeomParams P, int nopd_arg, int nitem, int bps) {
 	const int nopd = NOPD ? NOPD : nopd_arg;
 	extern __shared__ int4 s_tab[];
 	const int item = blockIdx.x / bps, part = blockIdx.x - item * bps;
@@ -469,15 +470,20 @@ __global__ void __launch_bounds__(256) geom_kernel(const __grid_constant__ GeomP
 		iyu[u] = ip / nopd;
 	}
 	const int nwrap = EXTRA ? nl - P.nmirror : nl;
+	// 16x16 and 32x32 pupils: a thread's points fill whole rows of one column
+	// (64 or 256 threads, four rows apart), so they share the column entry and
+	// need no bounds test
+	constexpr bool ONECOL = NOPD == 16 || NOPD == 32;
 #pragma unroll
 	for (int l = 0; l < nwrap; l++) {
 		if (!((E.use >> l) & 1u)) continue;
 		const float* __restrict__ sc = P.screen[l];
 		const float al = P.alpha[l];
+		const int4 tx0 = s_tab[l * 2 * nopd + ixu[0]];
 #pragma unroll
 		for (int u = 0; u < GEOM_PTS; u++) {
-			if (p0 + tid + bd * u < p1) {
-				const int4 tx = s_tab[l * 2 * nopd + ixu[u]], ty = s_tab[l * 2 * nopd + nopd + iyu[u]];
+			if (ONECOL || p0 + tid + bd * u < p1) {
+				const int4 tx = ONECOL ? tx0 : s_tab[l * 2 * nopd + ixu[u]], ty = s_tab[l * 2 * nopd + nopd + iyu[u]];
 				const float m00 = __ldg(sc + (ty.x + tx.x)), m10 = __ldg(sc + (ty.x + tx.y));
 				const float m01 = __ldg(sc + (ty.y + tx.x)), m11 = __ldg(sc + (ty.y + tx.y));
 				acc[u] = geom_bilerp(al, m00, m10, m01, m11, __int_as_float(tx.z), __int_as_float(ty.z), acc[u]);
