@@ -340,6 +340,10 @@ def run_b200(args, cfg):
         variant = args.variant
         ctx.set_variant(wl.ipowfs, variant)
     forms = [args.form] if args.form != "both" else ["fft", "tc"]
+    if wl.setup.notf != 32 and "tc" in forms:
+        # the tensor-core form is built for the 32-point transforms only; a larger
+        # powfs runs the FFT form whichever form is asked for
+        forms = ["fft"]
     isim = 0
     res = {}
     clk = ClockSampler(local)
