@@ -198,14 +198,17 @@ class Server:
         if self.priority is not None:
             wl.ctx.set_stream_priority(self.stream_priority(i))
         ext = torch.cuda.ExternalStream(wl.ctx.stream, device=self.device)
-        self.sims[i] = (wl, ext, torch.cuda.Event())
+        # one host buffer per sim: a request's gradients land there, with no
+        # allocation per request (copied out only when a caller keeps results)
+        gbuf = np.empty(sum(2 * wl.ctx.wfs_nsa[k] for k in wl.wfs))
+        self.sims[i] = (wl, ext, torch.cuda.Event(), gbuf)
         wl.frame(0)  # buffers made on first use belong to the footprint too
         wl.frame_sync()
         torch.cuda.synchronize(self.device)
         return max(f0 - torch.cuda.mem_get_info(self.device)[0], 1)
 
     def _unload(self, i: int):
-        wl, _, _ = self.sims.pop(i)
+        wl, _, _, _ = self.sims.pop(i)
         wl.ctx.close()
 
     def prewarm(self):
@@ -218,21 +221,28 @@ class Server:
         """Imaging form of every resident sim (and of sims loaded later); one
         frame per sim builds what the form needs before anything is timed."""
         self.form = form
-        for i, (wl, _, _) in self.sims.items():
+        for i, (wl, _, _, _) in self.sims.items():
             wl.ctx.set_form(form)
             wl.frame(0)
             wl.frame_sync()
 
     def launch(self, i: int, isim: int):
-        wl, ext, ev = self.sims[i]
+        wl, ext, ev, _ = self.sims[i]
         wl.frame(isim)
         ev.record(ext)
 
     def done(self, i: int) -> bool:
         return self.sims[i][2].query()
 
-    def collect(self, i: int):
-        return self.sims[i][0].frame_sync()
+    def collect(self, i: int, keep: bool = False):
+        """The gradients of sim i's finished request, in its host buffer; with keep, a copy
+        split per WFS."""
+        wl, _, _, gbuf = self.sims[i]
+        wl.frame_sync(out=gbuf)
+        if not keep:
+            return gbuf
+        sizes = [2 * wl.ctx.wfs_nsa[k] for k in wl.wfs]
+        return [a.copy() for a in np.split(gbuf, np.cumsum(sizes)[:-1])]
 
     def run(self, arrivals, rate: float, results: Optional[dict] = None) -> Stats:
         """Serve `arrivals` [(t, sim)] in real time; returns latency statistics.
@@ -245,22 +255,15 @@ class Server:
         inflight: Dict[int, float] = {}  # sim -> arrival time of its running request
         running: Dict[int, int] = {}     # sim -> frame index of its running request
         t0 = time.perf_counter()
-        while pending or order or inflight:
-            now = time.perf_counter() - t0
-            while pending and pending[0][0] <= now:
-                t, i = pending.popleft()
-                waiting[i].append(t)
-                order.setdefault(i, None)
-            for i in [j for j in inflight if self.done(j)]:
-                out = self.collect(i)
-                if results is not None:
-                    results[(i, running[i])] = out
-                st.latencies_ms.append(1e3 * (time.perf_counter() - t0 - inflight.pop(i)))
-                st.images += self.cfgs[i]["nwfs"] * self.setups[i].nsa
+
+        def launch_ready():
+            # every waiting request whose sim is idle goes to the device now
             for i in list(order):
                 if i in inflight:
                     continue
-                if not self.adm.try_admit(i, busy=set(inflight) | set(order)):
+                if i in self.adm.resident:
+                    self.adm.touch(i)
+                elif not self.adm.try_admit(i, busy=set(inflight) | set(order)):
                     continue
                 t = waiting[i].popleft()
                 if not waiting[i]:
@@ -269,6 +272,25 @@ class Server:
                 running[i] = self.isim[i]
                 self.isim[i] += 1
                 inflight[i] = t
+
+        while pending or order or inflight:
+            now = time.perf_counter() - t0
+            while pending and pending[0][0] <= now:
+                t, i = pending.popleft()
+                waiting[i].append(t)
+                order.setdefault(i, None)
+            # launches first, so that new work reaches the device before the host
+            # spends time collecting finished frames
+            launch_ready()
+            finished = [j for j in inflight if self.done(j)]
+            for i in finished:
+                out = self.collect(i, keep=results is not None)
+                if results is not None:
+                    results[(i, running[i])] = out
+                st.latencies_ms.append(1e3 * (time.perf_counter() - t0 - inflight.pop(i)))
+                st.images += self.cfgs[i]["nwfs"] * self.setups[i].nsa
+            if finished:
+                launch_ready()
             if not inflight and pending and not order:
                 time.sleep(max(0.0, min(pending[0][0] - (time.perf_counter() - t0), 1e-3)))
         st.wall_s = time.perf_counter() - t0
