@@ -373,6 +373,7 @@ int shwfs_destroy(shwfs_ctx* ctx) {
 		for (auto& b : p.gs0_ptr) b.free_();
 		for (auto& b : p.gs0_col) b.free_();
 		for (auto& b : p.gs0_val) b.free_();
+		for (auto& b : p.band_lotf) b.free_();
 	}
 	evl_free(ctx);
 	for (auto& c : ctx->desc_cache) c.d.free_();
