@@ -440,8 +440,7 @@ __global__ void __launch_bounds__(N64_THREADS, 6) ints_n64_kernel(PowfsDev P, co
 	// forward along ky on columns 0..31 (digit-reversed inputs): natural OTF
 	fft64_lines<true, true, 32, -1>(img, 0, tw);
 	// x conj(uplink OTF) x ETF / nominal; transfer functions are [fy + 64 fx].
-	// The image is the real part of the inverse transform, which is the inverse
-	// of OTF x (TF(k) + conj TF(-k)) / 2 over the half spectrum.  Column 0 holds
+	// Column 0 holds
 	// Y = O(.,0) + i O(.,32) with O(.,0), O(.,32) the transforms of real
 	// columns; the products for kx = 0 and 32 go to column 32 as X(.,0) + i X(.,32).
 	{
@@ -467,21 +466,20 @@ __global__ void __launch_bounds__(N64_THREADS, 6) ints_n64_kernel(PowfsDev P, co
 			}
 			return o;
 		};
-		// (TF(t) + conj TF(tm)) / 2
-		auto tfh = [&](int t, int tm) -> float2 {
-			const float2 a = tf(t), b = tf(tm);
-			return make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));
-		};
+		// The transfer functions are transforms of real kernels (uplink PSF,
+		// elongated spot, pixel response), Hermitian to rounding, so each
+		// half-spectrum element takes TF(t) itself: the image is then the real
+		// part of the full inverse up to rounding.
 		for (int t = tid; t < 64 * 32; t += N64_THREADS) {
 			const int fy = t & 63, fx = t >> 6, my = (64 - fy) & 63;
 			if (fx) {
 				float2* v = img + fy * N64_LS + fx;
-				*v = cmul(*v, tfh(t, my + 64 * (64 - fx)));
+				*v = cmul(*v, tf(t));
 			} else {
 				const float2 y = img[fy * N64_LS], ym = img[my * N64_LS];
 				const float2 o0 = make_float2(0.5f * (y.x + ym.x), 0.5f * (y.y - ym.y));
 				const float2 o32 = make_float2(0.5f * (y.y + ym.y), 0.5f * (ym.x - y.x));
-				const float2 x0 = cmul(o0, tfh(fy, my)), x32 = cmul(o32, tfh(fy + 64 * 32, my + 64 * 32));
+				const float2 x0 = cmul(o0, tf(fy)), x32 = cmul(o32, tf(fy + 64 * 32));
 				img[fy * N64_LS + 32] = make_float2(x0.x - x32.y, x0.y + x32.x);
 			}
 		}
