@@ -158,7 +158,9 @@ int shwfs_powfs_set_seotf(shwfs_ctx* ctx, int ipowfs, const double* seotf);
    each band's wavelength), sums the intensities, then adds noise and forms
    gradients once.  Matched filters come from the host for such a powfs
    (shwfs_wfs_update_mtche refuses it), and the work-list and allocation-free
-   paths do not serve it.  At most SHWFS_MAX_BANDS extra bands. */
+   paths do not serve it; nor does shwfs_ints_grad_dev when ipowfs has an LGS
+   uplink, whose per-band uplink OTFs only the frame path forms.  At most
+   SHWFS_MAX_BANDS extra bands. */
 #define SHWFS_MAX_BANDS 8
 int shwfs_powfs_add_band(shwfs_ctx* ctx, int ipowfs, const shwfs_powfs_desc* desc, double wvlwt, int* iband);
 

@@ -1740,9 +1740,18 @@ static int launch_ints_bands(shwfs_ctx* ctx, int ipowfs, const std::vector<int>&
 		const bool last = j + 1 == order.size();
 		std::vector<const float2*> lj(nw, nullptr);
 		for (int k = 0; k < nw; k++) {
-			if (j == 0) lj[k] = lotfs[k];
-			else if (ctx->powfs[order[j]].d.has_llt) lj[k] = ctx->powfs[order[j]].band_lotf[wlist[k]].p;
+			if (j == 0) {
+				lj[k] = lotfs[k];
+			} else if (ctx->powfs[order[j]].d.has_llt) {
+				const auto& bl = ctx->powfs[order[j]].band_lotf;
+				if ((size_t)wlist[k] >= bl.size() || !bl[wlist[k]].p) {
+					r = fail(ctx, SHWFS_ESTATE, "bands: the uplink OTF of WFS %d is formed by the frame path", wlist[k]);
+					break;
+				}
+				lj[k] = bl[wlist[k]].p;
+			}
 		}
+		if (r) break;
 		ctx->band_accum = j > 0 ? 1 : accum0;
 		r = launch_ints(ctx, order[j], wlist, isim, opds, lj, acc, last ? grads : none, last ? noisy : quiet);
 	}
@@ -1835,6 +1844,9 @@ int shwfs_ints_grad_dev(shwfs_ctx* ctx, int iwfs, int isim, const float* opd, co
 	std::vector<const float2*> lotf{nullptr};
 	if (p.d.has_llt) {
 		if (!lltopd) return fail(ctx, SHWFS_EINVAL, "ints_grad: LGS powfs needs the LLT OPD");
+		if (!p.bands.empty())
+			return fail(ctx, SHWFS_EINVAL,
+				"ints_grad: an LGS powfs with wavelength bands forms its uplink OTFs in the frame path (shwfs_frame_queue)");
 		if (!p.lltamp.p) return fail(ctx, SHWFS_ESTATE, "LLT amplitude not set");
 		std::vector<const float*> lin{lltopd};
 		if ((r = launch_uplink(ctx, wl, lin, lotf))) return r;

@@ -84,3 +84,21 @@ def test_band_arguments_are_checked():
         finally:
             s.close()
     wl.close()
+
+
+def test_lgs_bands_refuse_the_device_input_path():
+    """An LGS powfs with bands forms each band's uplink OTF in the frame path; the single-WFS
+    device-input call refuses it before any launch and the context stays usable."""
+    import torch
+    from maos_b200 import shwfs
+    from maos_b200.configs import LGS8_N32_2WVL
+    from maos_b200.workload import build
+    wl = build(LGS8_N32_2WVL, device=0, seed=4, noisy=False, nx=512)
+    ctx = wl.ctx
+    opd = torch.zeros(1 << 16, device="cuda:0")
+    llt = torch.zeros(1 << 12, device="cuda:0")
+    with pytest.raises(shwfs.ShwfsError, match="frame path"):
+        ctx.ints_grad_dev(wl.wfs[0], 0, opd, lltopd=llt)
+    wl.frame(2)
+    assert all(np.isfinite(g).all() for g in wl.frame_sync())
+    wl.close()
