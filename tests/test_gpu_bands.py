@@ -102,3 +102,42 @@ def test_lgs_bands_refuse_the_device_input_path():
     wl.frame(2)
     assert all(np.isfinite(g).all() for g in wl.frame_sync())
     wl.close()
+
+
+@pytest.mark.parametrize("cfg_name,opts,form", [("LGS8_N32_2WVL", {"dtrat": 2}, 0),
+                                                ("LGS8_N32_2WVL", {"sigmatch": 2}, 0),
+                                                ("NGS8_2WVL", {"sigmatch": 2}, 0),
+                                                ("LGS8_N32_2WVL", {}, 1)])
+def test_bands_compose_with_integration_and_normalisation(ref_lib, cfg_name, opts, form):
+    """Bands under the other imaging layers: dtrat integration sums the band-summed frames of a
+    period, sigmatch 2 normalises by the total of the band sum, and the tensor-core form images
+    each band of an LGS powfs with that band's uplink; against the reference's own frames of the
+    same polychromatic powfs."""
+    from maos_b200 import configs
+    from maos_b200.workload import build
+    from tests.helpers import ints_tolerance_ok, grad_rel_err
+    dtrat = opts.get("dtrat", 1)
+    cfg = dict(getattr(configs, cfg_name))
+    if "sigmatch" in opts:
+        cfg.update(name=cfg["name"] + "_sig2", sigmatch=opts["sigmatch"])
+    wl = build(cfg, device=0, seed=6, noisy=False, nx=512, form=form)
+    if dtrat > 1:
+        wl.ctx.powfs_set_dtrat(wl.ipowfs, dtrat)
+    r = ref_lib.RefPowfs(cfg)
+    if cfg["phytype"] == 1:
+        for i in wl.wfs:
+            wl.ctx.wfs_set_mtche(i, r.mtche(), r.i0sum(), r.i0sumsum())
+    ref_lib.atm_set(wl.screens, wl.layers)
+    frames = list(range(4, 4 + dtrat))
+    for isim in frames:
+        wl.frame(isim)
+    out = wl.frame_sync(want_ints=True)
+    tol = 1e-4 if form == 1 else 1e-5
+    for k in range(len(wl.wfs)):
+        ints_ref = sum(ref_lib.frame_full_mt(r, k, isim, cfg["dt"], noisy=False)[0] for isim in frames)
+        g, ints = out[k]
+        ok, worst = ints_tolerance_ok(ints, ints_ref, r.nsa, r.npix, tol)
+        assert ok, f"wfs {k}: intensity error {worst:.3e} of subaperture total"
+        g_ref = r.grad(ints_ref, iwfs=k)
+        assert grad_rel_err(g, g_ref) <= 1e-4, (k, grad_rel_err(g, g_ref))
+    wl.close()
