@@ -83,7 +83,11 @@ __device__ __forceinline__ bool wl_wait(const WorkParams& W, const int* c, int n
 		*s_ok = ok;
 	}
 	__syncthreads();
-	return *s_ok != 0;
+	const bool ok = *s_ok != 0;
+	// every thread has the outcome before thread 0 may store the next wait's
+	// (the pixel items wait on four images in a row)
+	__syncthreads();
+	return ok;
 }
 
 // Tiles of pass p that must be done before it starts (pass 1 none).
