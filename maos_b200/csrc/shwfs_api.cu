@@ -559,8 +559,12 @@ int shwfs_powfs_set_simap(shwfs_ctx* ctx, int ipowfs, const int* idx, const doub
 	}
 	int r = set_device(ctx);
 	if (r) return r;
+	// a missing tap (index -1) carries weight 0, whatever the caller left there:
+	// the sampling kernels multiply it by 0 instead of branching around it
+	std::vector<float> w(m);
+	for (size_t i = 0; i < m; i++) w[i] = idx[i] < 0 ? 0.f : (float)wt[i];
 	if ((r = dev_upload(ctx, p->simap_idx, idx, m))) return r;
-	if ((r = dev_upload_f(ctx, p->simap_wt, wt, m))) return r;
+	if ((r = dev_upload(ctx, p->simap_wt, w.data(), m))) return r;
 	p->nsimap = nmap;
 	p->simap_idx_h.assign(idx, idx + m);
 	p->simap_wt_h.assign(wt, wt + m);
@@ -866,6 +870,7 @@ int shwfs_wfs_set_opdadd(shwfs_ctx* ctx, int iwfs, const double* opd) {
 // ---- frame machinery ----
 
 static int launch_geom_wfs(shwfs_ctx* ctx, GeomParams& gp, bool split = true);
+static int sm_count(shwfs_ctx* ctx);
 
 // Appends one pupil to a batched ray-trace launch: per-layer geometry of
 // prop_range (lib/accphi.c:223-244) and prop_grid_pts
@@ -1059,9 +1064,15 @@ static int launch_geom_wfs(shwfs_ctx* ctx, GeomParams& gp, bool split) {
 		// 16x16 pupils 64 threads, 32x32 256, larger ones split over blocks of 256
 		const int np = nopd * nopd;
 		const int bd = std::min(256, std::max(32, ((np + GEOM_PTS - 1) / GEOM_PTS + 31) / 32 * 32));
-		const int bps = (np + GEOM_PTS * bd - 1) / (GEOM_PTS * bd);  // blocks per subaperture
+		int bps = (np + GEOM_PTS * bd - 1) / (GEOM_PTS * bd);  // blocks per subaperture
+		const bool fixed = !extra && (nopd == 16 || nopd == 32) && gp.nlayer <= 8;
+		gp.ppt = GEOM_PTS;
+		if (!fixed && (long)nblk * bps < sm_count(ctx)) {  // a few pupils: a point per thread, more blocks
+			gp.ppt = 1;
+			bps = (np + bd - 1) / bd;
+		}
 		if (extra) geom_kernel<true><<<(unsigned)nblk * bps, bd, smem, ctx->stream>>>(gp, nopd, nitem, bps);
-		else if ((nopd == 16 || nopd == 32) && gp.nlayer <= 8)  // pupil side and layer count fixed at compile time
+		else if (fixed)  // pupil side and layer count fixed at compile time
 			geom_pick(nopd, gp.nlayer)<<<(unsigned)nblk * bps, bd, smem, ctx->stream>>>(gp, nopd, nitem, bps);
 		else geom_kernel<false><<<(unsigned)nblk * bps, bd, smem, ctx->stream>>>(gp, nopd, nitem, bps);
 	}
@@ -1341,7 +1352,7 @@ static int build_tc_tables(shwfs_ctx* ctx, PowfsState& p) {
 	return 0;
 }
 
-static int tc_sm_count(shwfs_ctx* ctx) {
+static int sm_count(shwfs_ctx* ctx) {
 	static int nsm[64] = {0};
 	if (ctx->device < 64 && nsm[ctx->device]) return nsm[ctx->device];
 	int v = 148;
@@ -1566,10 +1577,9 @@ static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist
 		int r = launch_gen(ctx, p, wdev, nw, nitem, 0, p.gen_buf, P);
 		if (r) return r;
 		const int n2 = p.d.notf * p.d.notf;
-		if (npix <= 32) gen_pixels_kernel<1><<<nblk, 128, 0, ctx->stream>>>(P, wdev, nw, nitem, p.gen_buf.p, n2);
-		else if (npix <= 64) gen_pixels_kernel<2><<<nblk, 128, 0, ctx->stream>>>(P, wdev, nw, nitem, p.gen_buf.p, n2);
-		else if (npix <= 128) gen_pixels_kernel<4><<<nblk, 128, 0, ctx->stream>>>(P, wdev, nw, nitem, p.gen_buf.p, n2);
-		else gen_pixels_kernel<8><<<nblk, 128, 0, ctx->stream>>>(P, wdev, nw, nitem, p.gen_buf.p, n2);
+		// a thread per pixel (at most GEN_PIX_THREADS: powfs_add limits these sizes to 256 pixels)
+		const int bt = (npix + 31) / 32 * 32;
+		gen_pixels_block_kernel<<<nitem, bt, 0, ctx->stream>>>(P, wdev, nw, p.gen_buf.p, n2);
 		CK(cudaGetLastError());
 		return 0;
 	}
@@ -1598,7 +1608,7 @@ static int launch_ints(shwfs_ctx* ctx, int ipowfs, const std::vector<int>& wlist
 		const int nlotf = all_lotf ? nw : 0;
 		// persistent: TC_CTAS_PER_SM CTAs of TC_GROUPS tile groups per SM
 		const int ntile = (nitem + 3) / 4;
-		const int grid = std::min((ntile + TC_GROUPS - 1) / TC_GROUPS, tc_sm_count(ctx) * TC_CTAS_PER_SM);
+		const int grid = std::min((ntile + TC_GROUPS - 1) / TC_GROUPS, sm_count(ctx) * TC_CTAS_PER_SM);
 		if (any_out) {
 			StageMark mark(ctx, SHWFS_STAGE_INTS);
 			ints_tc_kernel<<<grid, TC_THREADS, tc_smem_bytes(nlotf), ctx->stream>>>(P, wdev, nw, nitem, nlotf, T,
@@ -1910,7 +1920,7 @@ int shwfs_addnoise_dev(shwfs_ctx* ctx, float* ints, long n, const float* bkgrnd2
 	if (r) return r;
 	if (n == 0) return 0;
 	if (excess < 1) excess = 1;
-	const long nblk = std::min((n + 255) / 256, (long)tc_sm_count(ctx) * 8);
+	const long nblk = std::min((n + 255) / 256, (long)sm_count(ctx) * 8);
 	addnoise_kernel<<<(int)nblk, 256, 0, ctx->stream>>>(ints, n, bkgrnd2, bkgrnd2c, qe, (float)bkgrnd,
 		(float)bkgrndc, (float)rne, (float)excess, seed, stream, frame);
 	CK(cudaGetLastError());

@@ -11,7 +11,7 @@
 //   pass 4  columns fx:                 FFT along ky, x conj(uplink OTF) x ETF / DTF nominal
 //   pass 5  rows fy:                    inverse FFT along fx
 //   pass 6  columns x:                  inverse FFT along fy, real part
-//   pixels  one warp per image:         bilinear pixel map, noise, CoG / matched filter
+//   pixels  a thread per pixel:         bilinear pixel map, noise, CoG / matched filter
 //
 // as maos/wfsints.c:233-286 (cembed_wvf with pad (n_w - n_o)/2, cfft2 with
 // FFTW's sign and no normalisation, cabs2toreal, ccwmc with the uplink OTF,
@@ -35,26 +35,63 @@ enum GenPass { GEN_FIELD_ROWS = 1, GEN_PSF_COLS, GEN_OTF_ROWS, GEN_OTF_COLS, GEN
 
 __host__ __device__ constexpr int ilog2c(int n) { return n <= 1 ? 0 : 1 + ilog2c(n / 2); }
 
-// In-place radix-2 FFT of gen_lines(N) lines of N points in shared memory, line
-// stride N + 1 (bank-conflict free for column tiles), input in bit-reversed
-// order.  tw[k] = exp(-2 pi i k / N), k < N/2; dir -1 forward, +1 inverse.
+// Radix-2 decimation-in-time butterfly: (u, v) -> (u + w v, u - w v).
+__device__ __forceinline__ void gen_bfly(float2& u, float2& v, float2 w) {
+	const float2 t = make_float2(v.x * w.x - v.y * w.y, v.x * w.y + v.y * w.x);
+	v = make_float2(u.x - t.x, u.y - t.y);
+	u = make_float2(u.x + t.x, u.y + t.y);
+}
+
+// In-place FFT of gen_lines(N) lines of N points in shared memory, line stride
+// N + 1 (bank-conflict free for column tiles), input in bit-reversed order.
+// tw[k] = exp(-2 pi i k / N), k < N/2; dir -1 forward, +1 inverse.  The
+// log2 N radix-2 stages run two at a time: a thread takes the four points
+// k0 + {0, h, 2h, 3h} (h = 2^st) and applies stage st's butterflies (k0, k0+h)
+// and (k0+2h, k0+3h), then stage st+1's (k0, k0+2h) and (k0+h, k0+3h), with
+// those stages' twiddles -- every point sees the operations of the stage-by-
+// stage transform in the same order, with half its barriers and shared-memory
+// round trips (an odd log2 N starts with one radix-2 stage).
 template <int N, int NT = GEN_THREADS>
 __device__ __forceinline__ void fft_lines(float2* s, const float2* __restrict__ tw, int dir) {
-	constexpr int LOGN = ilog2c(N), LS = N + 1, NB = gen_lines(N) * N / 2;
-#pragma unroll 1
-	for (int st = 0; st < LOGN; st++) {
-		const int half = 1 << st;
+	constexpr int LOGN = ilog2c(N), LS = N + 1, NB = gen_lines(N) * N / 2, NQ = gen_lines(N) * N / 4;
+	int st = 0;
+	if (LOGN & 1) {  // stage 0: half = 1, twiddle tw[0]
+		float2 w0 = tw[0];
+		if (dir > 0) w0.y = -w0.y;
 		for (int b = threadIdx.x; b < NB; b += NT) {
 			const int line = b / (N / 2), j = b - line * (N / 2);
-			const int grp = j >> st, pos = j & (half - 1);
-			const int k0 = grp * 2 * half + pos, k1 = k0 + half;
-			float2 w = tw[pos << (LOGN - 1 - st)];
-			if (dir > 0) w.y = -w.y;
-			float2* a = s + line * LS;
-			const float2 u = a[k0], v = a[k1];
-			const float2 t = make_float2(v.x * w.x - v.y * w.y, v.x * w.y + v.y * w.x);
-			a[k0] = make_float2(u.x + t.x, u.y + t.y);
-			a[k1] = make_float2(u.x - t.x, u.y - t.y);
+			float2* a = s + line * LS + 2 * j;
+			float2 u = a[0], v = a[1];
+			gen_bfly(u, v, w0);
+			a[0] = u;
+			a[1] = v;
+		}
+		__syncthreads();
+		st = 1;
+	}
+#pragma unroll 1
+	for (; st < LOGN; st += 2) {
+		const int h = 1 << st;
+		for (int b = threadIdx.x; b < NQ; b += NT) {
+			const int line = b / (N / 4), j = b - line * (N / 4);
+			const int grp = j >> st, pos = j & (h - 1);
+			float2* a = s + line * LS + grp * 4 * h + pos;
+			float2 w1 = tw[pos << (LOGN - 1 - st)];
+			float2 w2 = tw[pos << (LOGN - 2 - st)], w3 = tw[(pos + h) << (LOGN - 2 - st)];
+			if (dir > 0) {
+				w1.y = -w1.y;
+				w2.y = -w2.y;
+				w3.y = -w3.y;
+			}
+			float2 x0 = a[0], x1 = a[h], x2 = a[2 * h], x3 = a[3 * h];
+			gen_bfly(x0, x1, w1);  // stage st
+			gen_bfly(x2, x3, w1);
+			gen_bfly(x0, x2, w2);  // stage st + 1
+			gen_bfly(x1, x3, w3);
+			a[0] = x0;
+			a[h] = x1;
+			a[2 * h] = x2;
+			a[3 * h] = x3;
 		}
 		__syncthreads();
 	}
@@ -219,19 +256,34 @@ __device__ __forceinline__ void gen_pixels_item(const PowfsDev& P, const WfsDev*
 	const WfsDev& W = wfs[item % nw];
 	const float2* im = buf + (size_t)item * n2;
 	const int npix = P.npix;
-	const int* sidx = P.simap_idx + (P.simap_per_sa ? (size_t)isa * npix * 4 : 0);
-	const float* swt = P.simap_wt + (P.simap_per_sa ? (size_t)isa * npix * 4 : 0);
+	// a pixel's 4 map entries are one 16-byte row (cudaMalloc'd, 4 entries per pixel)
+	const int4* sidx = reinterpret_cast<const int4*>(P.simap_idx) + (P.simap_per_sa ? (size_t)isa * npix : 0);
+	const float4* swt = reinterpret_cast<const float4*>(P.simap_wt) + (P.simap_per_sa ? (size_t)isa * npix : 0);
+	// Few warps run these images, so every load latency is exposed: the map
+	// rows, then the image taps, are each issued as one independent wave.  A
+	// missing tap (index < 0) reads as 0, and fmaf(w, 0, v) = v, so the sums
+	// equal those that skip it.
+	float x[NPQ][4];
+#pragma unroll
+	for (int q = 0; q < NPQ; q++) {
+		const int p = lane + 32 * q;
+		const int4 id = p < npix ? __ldg(sidx + p) : make_int4(-1, -1, -1, -1);
+		x[q][0] = id.x >= 0 ? gen_ld<L2ONLY>(im + id.x).x : 0.f;
+		x[q][1] = id.y >= 0 ? gen_ld<L2ONLY>(im + id.y).x : 0.f;
+		x[q][2] = id.z >= 0 ? gen_ld<L2ONLY>(im + id.z).x : 0.f;
+		x[q][3] = id.w >= 0 ? gen_ld<L2ONLY>(im + id.w).x : 0.f;
+	}
 	float pix[NPQ];
 #pragma unroll
 	for (int q = 0; q < NPQ; q++) {
 		const int p = lane + 32 * q;
 		float v = 0.f;
 		if (p < npix) {
-#pragma unroll
-			for (int c = 0; c < 4; c++) {
-				const int id = __ldg(sidx + 4 * p + c);
-				if (id >= 0) v = fmaf(__ldg(swt + 4 * p + c), gen_ld<L2ONLY>(im + id).x, v);
-			}
+			const float4 w = __ldg(swt + p);
+			v = fmaf(w.x, x[q][0], v);
+			v = fmaf(w.y, x[q][1], v);
+			v = fmaf(w.z, x[q][2], v);
+			v = fmaf(w.w, x[q][3], v);
 			v *= W.alpha;
 			if (P.accum) v += W.ints[(size_t)isa * npix + p];  // dtrat > 1: the frames so far
 		}
@@ -258,13 +310,48 @@ __device__ __forceinline__ void gen_pixels_item(const PowfsDev& P, const WfsDev*
 		grad_from_pixels<NPQ>(pix, npix, P.pixpsax, P.pixpsay, P, W.mtche + (size_t)isa * 2 * npix, W.i0sum, isa, lane,
 			W.grad, P.nsa);
 }
-template <int NPQ>
-__global__ void gen_pixels_kernel(PowfsDev P, const WfsDev* __restrict__ wfs, int nw, int nitem,
-	const float2* __restrict__ buf, int n2) {
-	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	const int item = blockIdx.x * (blockDim.x >> 5) + warp;
-	if (item >= nitem) return;
-	gen_pixels_item<NPQ, false>(P, wfs, nw, item, buf, n2, lane);
+// The same step with one block per image (blockIdx.x = item), a thread per
+// pixel (npix rounded up to whole warps): the launches of these sizes often
+// hold a few images, where a warp walking 8 pixels' noise draws in turn set
+// their latency.  The
+// image's first warp then forms the gradients from the pixels in shared
+// memory, in gen_pixels_item's lane order (pixel p = lane + 32 q), so
+// intensities, noise and gradients equal those of gen_pixels_item.
+constexpr int GEN_PIX_THREADS = 256;  // the largest pixel count of these sizes
+__global__ void __launch_bounds__(GEN_PIX_THREADS) gen_pixels_block_kernel(PowfsDev P,
+	const WfsDev* __restrict__ wfs, int nw, const float2* __restrict__ buf, int n2) {
+	__shared__ float spix[GEN_PIX_THREADS];
+	const int item = blockIdx.x, p = threadIdx.x;
+	const int isa = item / nw;
+	const WfsDev& W = wfs[item % nw];
+	const int npix = P.npix;
+	float v = 0.f;
+	if (p < npix) {
+		const float2* im = buf + (size_t)item * n2;
+		const size_t m = (P.simap_per_sa ? (size_t)isa * npix : 0) + p;
+		const int4 id = __ldg(reinterpret_cast<const int4*>(P.simap_idx) + m);
+		const float4 w = __ldg(reinterpret_cast<const float4*>(P.simap_wt) + m);
+		v = fmaf(w.x, id.x >= 0 ? im[id.x].x : 0.f, v);
+		v = fmaf(w.y, id.y >= 0 ? im[id.y].x : 0.f, v);
+		v = fmaf(w.z, id.z >= 0 ? im[id.z].x : 0.f, v);
+		v = fmaf(w.w, id.w >= 0 ? im[id.w].x : 0.f, v);
+		v *= W.alpha;
+		if (P.accum) v += W.ints[(size_t)isa * npix + p];  // dtrat > 1: the frames so far
+		if (W.noisy) {
+			PixelRng rng(W.seed, (uint32_t)(isa * npix + p), W.wfs_id, (uint32_t)P.isim);
+			v = poisson_draw(rng, v + P.bkgrnd) + P.rne * rng.normal() - P.bkgrndc;
+		}
+		if (W.ints) W.ints[(size_t)isa * npix + p] = v;
+	}
+	spix[p] = v;
+	__syncthreads();
+	if (p < 32 && W.grad) {
+		float pix[GEN_PIX_THREADS / 32];
+#pragma unroll
+		for (int q = 0; q < GEN_PIX_THREADS / 32; q++) pix[q] = p + 32 * q < npix ? spix[p + 32 * q] : 0.f;
+		grad_from_pixels<GEN_PIX_THREADS / 32>(pix, npix, P.pixpsax, P.pixpsay, P, W.mtche + (size_t)isa * 2 * npix,
+			W.i0sum, isa, p, W.grad, P.nsa);
+	}
 }
 
 // ---------------------------------------------------------------------------

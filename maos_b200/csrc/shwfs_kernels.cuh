@@ -174,6 +174,9 @@ struct GeomParams {
 	// cuda/sim/accphi.cu:24-38): a point whose bilinear cell leaves the grid gets
 	// nothing from it
 	int nmirror;
+	// points per thread of the instantiations without a fixed pupil side (0:
+	// GEOM_PTS); launches of a few large pupils take 1, for four times the blocks
+	int ppt;
 	const float* screen[SHWFS_MAX_LAYERS];
 	int nx[SHWFS_MAX_LAYERS], ny[SHWFS_MAX_LAYERS];
 	float alpha[SHWFS_MAX_LAYERS];
@@ -338,10 +341,9 @@ __device__ __forceinline__ void psf_to_otf_n32(float2 (&F)[32], float scale, flo
 //   column entry ix: (jx, jx1, wx, -)      row entry iy: (jy nx, jy1 nx, wy, -)
 // A block of bd threads (a multiple of 32, at most 256, chosen so that
 // GEOM_PTS * bd covers a pupil with no idle slot where it can) traces up to
-// GEOM_PTS * bd points of one subaperture; larger pupils split each
-// subaperture over bps blocks: block b
-// covers points [GEOM_PTS * bd (b % bps), + GEOM_PTS * bd) of subaperture
-// item b / bps.
+// pts * bd points of one subaperture (pts = GEOM_PTS, or GeomParams.ppt);
+// larger pupils split each subaperture over bps blocks: block b covers points
+// [pts * bd (b % bps), + pts * bd) of subaperture item b / bps.
 constexpr int GEOM_PTS = 4;
 
 // The footprint origin of subaperture isa of entry E in layer l along x (isy
@@ -459,7 +461,8 @@ __global__ void __launch_bounds__(NOPD == 16 ? 64 : 256, NOPD == 16 ? 32 : NOPD 
 	// up to GEOM_PTS points per thread, layers outermost so that the gathers of the points are in flight
 	// together; every point still sums its layers in order
 	const int bd = bdim;
-	const int np = nopd * nopd, p0 = GEOM_PTS * bd * part, p1 = min(np, p0 + GEOM_PTS * bd);
+	const int pts = NOPD || P.ppt <= 0 || P.ppt > GEOM_PTS ? GEOM_PTS : P.ppt;
+	const int np = nopd * nopd, p0 = pts * bd * part, p1 = min(np, p0 + pts * bd);
 	float acc[GEOM_PTS];
 	int ixu[GEOM_PTS], iyu[GEOM_PTS];
 #pragma unroll
