@@ -384,7 +384,8 @@ int shwfs_set_worklist(shwfs_ctx* ctx, int on, int slices, int group);
 /* Times nrep whole frames of WFS [iwfs0, iwfs1) with the per-powfs launches
    and with the work list at (slices, group) = (7, 4), (14, 4), (28, 4),
    (7, 8), and keeps the fastest; *choice receives 0 for the per-powfs
-   launches, 1-4 for the work-list settings in that order. */
+   launches, 1-4 for the work-list settings in that order.  The frames run as
+   CUDA graphs (shwfs_frame_graph; stream frames while stage profiling is on). */
 int shwfs_autotune_frame(shwfs_ctx* ctx, int iwfs0, int iwfs1, int nrep, int* choice);
 /* With on != 0 (the default), a frame of several powfs runs each powfs whose
    images per frame are fewer than the largest powfs's on a branch stream of

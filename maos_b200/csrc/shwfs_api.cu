@@ -2780,15 +2780,23 @@ int shwfs_autotune_frame(shwfs_ctx* ctx, int iwfs0, int iwfs1, int nrep, int* ch
 	}
 	double best = 1e300;
 	int bestc = 0;
+	// frames as CUDA graphs, the form in which a frame of several powfs runs
+	// free of host launch costs (a layout of many small launches would lose to
+	// one of few launches only through the host); stream frames while stage
+	// profiling is on, which graphs do not allow
+	auto frame = [&](int k) {
+		return ctx->profiling ? shwfs_frame_queue(ctx, k, iwfs0, iwfs1) : shwfs_frame_graph(ctx, k, iwfs0, iwfs1);
+	};
 	for (int c = 0; c < WL_NCHOICE && !r; c++) {
 		ctx->worklist = c > 0;
 		if (c > 0) {
 			ctx->wl_slices = kWlChoices[c - 1][0];
 			ctx->wl_group = kWlChoices[c - 1][1];
 		}
-		if ((r = shwfs_frame_queue(ctx, 0, iwfs0, iwfs1))) break;  // warm
+		ctx->g_warm = 0;  // the layout's own graph: a warm-up frame, then a capture
+		if ((r = frame(0)) || (r = frame(1))) break;
 		if (cudaEventRecord(e0, ctx->stream) != cudaSuccess) { r = fail(ctx, SHWFS_ECUDA, "autotune_frame: event record failed"); break; }
-		for (int k = 0; k < nrep && !r; k++) r = shwfs_frame_queue(ctx, k, iwfs0, iwfs1);
+		for (int k = 0; k < nrep && !r; k++) r = frame(2 + k);
 		if (r) break;
 		float ms = 0.f;
 		if (cudaEventRecord(e1, ctx->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
