@@ -1417,14 +1417,10 @@ static int launch_gen_n(shwfs_ctx* ctx, PowfsState& p, GenParams& G) {
 	constexpr int L = gen_lines(N);
 	const size_t smem = ((size_t)L * (N + 1) + N / 2) * sizeof(float2);
 	const dim3 full(G.nitem, N / L), field(G.nitem, (G.nopd + L - 1) / L);
-	gen_pass_kernel<N, GEN_FIELD_ROWS><<<field, GEN_THREADS, smem, ctx->stream>>>(G);
-	gen_pass_kernel<N, GEN_PSF_COLS><<<full, GEN_THREADS, smem, ctx->stream>>>(G);
-	gen_pass_kernel<N, GEN_OTF_ROWS><<<full, GEN_THREADS, smem, ctx->stream>>>(G);
-	gen_pass_kernel<N, GEN_OTF_COLS><<<full, GEN_THREADS, smem, ctx->stream>>>(G);
-	if (!G.uplink) {
-		gen_pass_kernel<N, GEN_INV_ROWS><<<full, GEN_THREADS, smem, ctx->stream>>>(G);
-		gen_pass_kernel<N, GEN_INV_COLS><<<full, GEN_THREADS, smem, ctx->stream>>>(G);
-	}
+	gen_pass_kernel<N, GEN_FIELD_COLS><<<field, GEN_THREADS, smem, ctx->stream>>>(G);
+	gen_pass_kernel<N, GEN_PSF_ROWS><<<full, GEN_THREADS, smem, ctx->stream>>>(G);
+	gen_pass_kernel<N, GEN_OTF_COLS><<<full, GEN_THREADS, smem, ctx->stream>>>(G);  // uplink mode: ends at the OTF
+	if (!G.uplink) gen_pass_kernel<N, GEN_INV_ROWS><<<full, GEN_THREADS, smem, ctx->stream>>>(G);
 	CK(cudaGetLastError());
 	(void)p;
 	return 0;
@@ -2196,18 +2192,18 @@ static int frame_worklist(shwfs_ctx* ctx, const std::vector<std::vector<int>>& w
 		nimg_big += nitem;
 		for (int i = 0; i < nitem; i++) {
 			for (int t = 0; t < S.nt1; t++) b_tiles[1].push_back(make_int4(WL_TILE, si, i, (1 << 16) | t));
-			for (int ps = 2; ps <= 6; ps++)
+			for (int ps = 2; ps <= GEN_NPASS; ps++)
 				for (int t = 0; t < S.ntf; t++) b_tiles[ps].push_back(make_int4(WL_TILE, si, i, (ps << 16) | t));
 		}
 		for (int a = 0; a < nitem; a += 4) pix.push_back(make_int4(WL_PIX, si, a, 0));
 	}
 	// the list: pass 1 tiles, a slice of 32-point groups, pass 2 tiles, a slice, ...,
-	// pass 6 tiles, a slice, the large images' pixels, the rest of the 32-point groups
+	// the last pass's tiles, a slice, the large images' pixels, the rest of the 32-point groups
 	std::vector<int4> list;
-	const int ns = std::max(7, ctx->wl_slices);
+	const int ns = std::max(GEN_NPASS + 1, ctx->wl_slices);
 	const size_t per = (n32.size() + ns - 1) / ns;
 	size_t k = 0;
-	for (int ps = 1; ps <= 6; ps++) {
+	for (int ps = 1; ps <= GEN_NPASS; ps++) {
 		list.insert(list.end(), b_tiles[ps].begin(), b_tiles[ps].end());
 		for (size_t e = std::min(n32.size(), k + per); k < e; k++) list.push_back(n32[k]);
 	}

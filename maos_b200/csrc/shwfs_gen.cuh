@@ -5,18 +5,22 @@
 // tiles of 16 rows or 16 columns of an image through shared memory, with the
 // element-wise step of the chain fused in:
 //
-//   pass 1  rows y in [pad, pad+n_o):   field E = amp exp(i 2 pi opd / lambda), FFT along x
-//   pass 2  columns kx:                 FFT along y (rows outside the pupil are zero), |.|^2 * scale
-//   pass 3  rows ky:                    FFT along kx
-//   pass 4  columns fx:                 FFT along ky, x conj(uplink OTF) x ETF / DTF nominal
-//   pass 5  rows fy:                    inverse FFT along fx
-//   pass 6  columns x:                  inverse FFT along fy, real part
-//   pixels  a thread per pixel:         bilinear pixel map, noise, CoG / matched filter
+//   pass 1  columns x in [pad, pad+n_o): field E = amp exp(i 2 pi opd / lambda), FFT along y
+//   pass 2  rows ky:                     FFT along x (columns outside the pupil are zero),
+//                                        |.|^2 * scale, FFT along x (the PSF's transform)
+//   pass 3  columns fx:                  FFT along ky (the OTF), x conj(uplink OTF) x ETF / DTF
+//                                        nominal, inverse FFT along fy
+//   pass 4  rows y:                      inverse FFT along fx, real part
+//   pixels  a thread per pixel:          bilinear pixel map, noise, CoG / matched filter
 //
+// The two-dimensional transforms are separable, so each pass takes its lines
+// through two of them where the chain allows (the PSF's rows right after the
+// field's, the inverse's columns right after the OTF's): four passes over the
+// image instead of six, with the same transforms and element-wise steps
 // as maos/wfsints.c:233-286 (cembed_wvf with pad (n_w - n_o)/2, cfft2 with
 // FFTW's sign and no normalisation, cabs2toreal, ccwmc with the uplink OTF,
-// apply_dtf_etf, cfft2 inverse, dspmulcreal).  For the LLT pupil, passes 1-4
-// without a transfer function give the uplink OTF (maos/wfsints.c:149-199).
+// apply_dtf_etf, cfft2 inverse, dspmulcreal).  For the LLT pupil, passes 1-3
+// up to the OTF give the uplink OTF (maos/wfsints.c:149-199).
 // Transfer functions are stored transposed per subaperture ([fy + N fx]), as
 // in the 32-point path; the scratch image is row-major ([row][column]).
 #pragma once
@@ -31,7 +35,8 @@ namespace shwfs {
 __host__ __device__ constexpr int gen_lines(int n) { return n >= 256 ? 4 : n >= 128 ? 8 : 16; }
 constexpr int GEN_THREADS = 256;
 
-enum GenPass { GEN_FIELD_ROWS = 1, GEN_PSF_COLS, GEN_OTF_ROWS, GEN_OTF_COLS, GEN_INV_ROWS, GEN_INV_COLS };
+enum GenPass { GEN_FIELD_COLS = 1, GEN_PSF_ROWS, GEN_OTF_COLS, GEN_INV_ROWS };
+constexpr int GEN_NPASS = 4;
 
 __host__ __device__ constexpr int ilog2c(int n) { return n <= 1 ? 0 : 1 + ilog2c(n / 2); }
 
@@ -104,7 +109,7 @@ __device__ __forceinline__ int bitrev(int k) {
 
 // A launch covers nitem images.  WFS mode: image i is subaperture i / nw of
 // wfs[i % nw] (the order of the 32-point launches).  Uplink mode: image i is
-// the LLT pupil of wfs[i] (opd = LLT OPD, amp = LLT amplitude), and pass 4
+// the LLT pupil of wfs[i] (opd = LLT OPD, amp = LLT amplitude), and pass 3
 // stores its OTF, transposed, into wfs[i].lotfT instead of applying it.
 struct GenParams {
 	int nitem, nw, nopd, pad;
@@ -132,12 +137,34 @@ __device__ __forceinline__ float2 gen_ld(const float2* p) {
 	else return *p;
 }
 
+// Element-wise step f(value, line, k) over a tile's lines in natural order,
+// the results left in bit-reversed order along each line for the line's next
+// transform (a pass that transforms its lines twice).
+template <int N, int NT, typename F>
+__device__ __forceinline__ void gen_permute(float2* s, F f) {
+	constexpr int LS = N + 1, NE = gen_lines(N) * N / NT;
+	static_assert(gen_lines(N) * N % NT == 0, "tile elements per thread");
+	float2 v[NE];
+#pragma unroll
+	for (int e = 0; e < NE; e++) {
+		const int idx = threadIdx.x + e * NT, line = idx / N, k = idx - line * N;
+		v[e] = f(s[line * LS + k], line, k);
+	}
+	__syncthreads();
+#pragma unroll
+	for (int e = 0; e < NE; e++) {
+		const int idx = threadIdx.x + e * NT, line = idx / N, k = idx - line * N;
+		s[line * LS + bitrev<N>(k)] = v[e];
+	}
+	__syncthreads();
+}
+
 // One pass over tile `tile` of image i by a block of NT threads; gen_s is the
 // tile's shared memory (gen_tile_smem(N) bytes).
 template <int N, int PASS, int NT, bool L2ONLY>
 __device__ __forceinline__ void gen_pass_tile(const GenParams& G, int i, int tile, float2* gen_s) {
 	constexpr int LS = N + 1, GEN_LINES = gen_lines(N);
-	constexpr bool ROWS = PASS == GEN_FIELD_ROWS || PASS == GEN_OTF_ROWS || PASS == GEN_INV_ROWS;
+	constexpr bool ROWS = PASS == GEN_PSF_ROWS || PASS == GEN_INV_ROWS;
 	float2* tw = gen_s + GEN_LINES * LS;  // N/2 twiddles
 	const int isa = G.uplink ? 0 : i / G.nw;
 	const WfsDev& W = G.wfs[G.uplink ? i : i % G.nw];
@@ -145,7 +172,7 @@ __device__ __forceinline__ void gen_pass_tile(const GenParams& G, int i, int til
 	const int tid = threadIdx.x;
 	for (int k = tid; k < N / 2; k += NT) tw[k] = G.tw[k];
 	int l0 = tile * GEN_LINES, nl = GEN_LINES;  // first line and lines of the tile
-	if (PASS == GEN_FIELD_ROWS) {
+	if (PASS == GEN_FIELD_COLS) {  // only the pupil's columns
 		nl = min(GEN_LINES, G.nopd - l0);
 		l0 += G.pad;
 	}
@@ -161,43 +188,42 @@ __device__ __forceinline__ void gen_pass_tile(const GenParams& G, int i, int til
 		}
 		float2 v = make_float2(0.f, 0.f);
 		if (line < nl) {
-			if (PASS == GEN_FIELD_ROWS) {
-				const int x = k - G.pad, y = l0 + line - G.pad;
-				if (x >= 0 && x < G.nopd) {
+			if (PASS == GEN_FIELD_COLS) {
+				const int x = l0 + line - G.pad, y = k - G.pad;
+				if (y >= 0 && y < G.nopd) {
 					const size_t e = (size_t)isa * G.nopd * G.nopd + (size_t)y * G.nopd + x;
 					const float o = __ldg(W.opd + e), a = __ldg(W.amp + e);
 					float sn, cs;
 					sincospif(G.twoinvwvl * o, &sn, &cs);
 					v = make_float2(a * cs, a * sn);
 				}
-			} else if (ROWS) {
-				v = gen_ld<L2ONLY>(im + (size_t)(l0 + line) * N + k);
-			} else if (PASS != GEN_PSF_COLS || (k >= G.pad && k < G.pad + G.nopd)) {
-				v = gen_ld<L2ONLY>(im + (size_t)k * N + l0 + line);  // rows outside the pupil are zero before pass 2
+			} else if (!ROWS) {
+				v = gen_ld<L2ONLY>(im + (size_t)k * N + l0 + line);
+			} else if (PASS != GEN_PSF_ROWS || (k >= G.pad && k < G.pad + G.nopd)) {
+				v = gen_ld<L2ONLY>(im + (size_t)(l0 + line) * N + k);  // columns outside the pupil are zero
 			}
 		}
 		gen_s[line * LS + bitrev<N>(k)] = v;
 	}
 	__syncthreads();
-	fft_lines<N, NT>(gen_s, tw, PASS >= GEN_INV_ROWS ? 1 : -1);
-	// ---- element-wise step of the chain
-	if (PASS == GEN_PSF_COLS) {
-		for (int idx = tid; idx < GEN_LINES * N; idx += NT) {
-			const float2 v = gen_s[(idx / N) * LS + idx % N];
-			gen_s[(idx / N) * LS + idx % N] = make_float2((v.x * v.x + v.y * v.y) * G.scale, 0.f);
-		}
-		__syncthreads();
+	fft_lines<N, NT>(gen_s, tw, PASS == GEN_INV_ROWS ? 1 : -1);
+	// ---- element-wise steps of the chain, and a pass's second transform
+	if (PASS == GEN_PSF_ROWS) {
+		// |.|^2 * scale: the PSF row, then its own transform along x (the OTF's)
+		gen_permute<N, NT>(gen_s, [&](float2 v, int, int) { return make_float2((v.x * v.x + v.y * v.y) * G.scale, 0.f); });
+		fft_lines<N, NT>(gen_s, tw, -1);
 	}
 	if (PASS == GEN_OTF_COLS) {
-		// line = fx - l0, element fy; transfer functions are [fy + N fx]: fy fastest
-		for (int idx = tid; idx < GEN_LINES * N; idx += NT) {
-			const int line = idx / N, fy = idx - line * N;
-			const size_t t = (size_t)fy + (size_t)N * (l0 + line);
-			float2 v = gen_s[line * LS + fy];
-			if (G.uplink) {
-				const_cast<float2*>(W.lotfT)[t] = v;  // the uplink OTF this launch produces
-				continue;
+		// line = fx - l0, element fy: the OTF; transfer functions are [fy + N fx], fy fastest
+		if (G.uplink) {
+			for (int idx = tid; idx < GEN_LINES * N; idx += NT) {
+				const int line = idx / N, fy = idx - line * N;
+				const_cast<float2*>(W.lotfT)[(size_t)fy + (size_t)N * (l0 + line)] = gen_s[line * LS + fy];  // the uplink OTF
 			}
+			return;
+		}
+		gen_permute<N, NT>(gen_s, [&](float2 v, int line, int fy) {
+			const size_t t = (size_t)fy + (size_t)N * (l0 + line);
 			if (W.lotfT) v = cmulc(v, __ldg(W.lotfT + t));
 			if (G.etfT1) {
 				float2 e = __ldg(G.etfT1 + (size_t)isa * N * N + t);
@@ -210,19 +236,11 @@ __device__ __forceinline__ void gen_pass_tile(const GenParams& G, int i, int til
 				const float d = __ldg(G.nominalT + (G.nominal_per_sa ? (size_t)isa * N * N : 0) + t);
 				v = make_float2(v.x * d, v.y * d);
 			}
-			gen_s[line * LS + fy] = v;
-		}
-		__syncthreads();
-		if (G.uplink) return;
+			return v;
+		});
+		fft_lines<N, NT>(gen_s, tw, 1);  // the inverse along fy
 	}
-	if (PASS == GEN_INV_COLS) {
-		for (int idx = tid; idx < GEN_LINES * N; idx += NT) {
-			const int line = idx / N, k = idx - line * N;
-			gen_s[line * LS + k].y = 0.f;  // real part only
-		}
-		__syncthreads();
-	}
-	// ---- store (natural order)
+	// ---- store (natural order; the last pass keeps the real part)
 	for (int idx = tid; idx < GEN_LINES * N; idx += NT) {
 		int line, k;
 		if (ROWS) {
@@ -233,8 +251,10 @@ __device__ __forceinline__ void gen_pass_tile(const GenParams& G, int i, int til
 			line = idx - k * GEN_LINES;
 		}
 		if (line < nl) {
-			if (ROWS) im[(size_t)(l0 + line) * N + k] = gen_s[line * LS + k];
-			else im[(size_t)k * N + l0 + line] = gen_s[line * LS + k];
+			float2 v = gen_s[line * LS + k];
+			if (PASS == GEN_INV_ROWS) v.y = 0.f;
+			if (ROWS) im[(size_t)(l0 + line) * N + k] = v;
+			else im[(size_t)k * N + l0 + line] = v;
 		}
 	}
 }

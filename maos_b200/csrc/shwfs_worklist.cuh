@@ -7,8 +7,8 @@
 //            per-warp code),
 //   WL_TILE  one tile of one pass of the FFT-pass chain of one large image
 //            (gen_pass_kernel's per-tile code),
-//   WL_PIX   four large images' pixels, noise and gradients (gen_pixels_kernel's
-//            per-warp code),
+//   WL_PIX   four large images' pixels, noise and gradients (gen_pixels_item, one
+//            warp per image),
 //
 // taken in list order by resident blocks from a global counter (each block
 // fetches its next item while it runs the current one).  The passes of
@@ -98,12 +98,10 @@ __device__ __forceinline__ int wl_need(const WorkSeg& S, int pass) { return pass
 template <int N>
 __device__ __noinline__ void wl_tile(const WorkSeg& S, int img, int pass, int tile, float2* smem) {
 	switch (pass) {
-	case GEN_FIELD_ROWS: gen_pass_tile<N, GEN_FIELD_ROWS, WL_THREADS, true>(S.G, img, tile, smem); break;
-	case GEN_PSF_COLS: gen_pass_tile<N, GEN_PSF_COLS, WL_THREADS, true>(S.G, img, tile, smem); break;
-	case GEN_OTF_ROWS: gen_pass_tile<N, GEN_OTF_ROWS, WL_THREADS, true>(S.G, img, tile, smem); break;
+	case GEN_FIELD_COLS: gen_pass_tile<N, GEN_FIELD_COLS, WL_THREADS, true>(S.G, img, tile, smem); break;
+	case GEN_PSF_ROWS: gen_pass_tile<N, GEN_PSF_ROWS, WL_THREADS, true>(S.G, img, tile, smem); break;
 	case GEN_OTF_COLS: gen_pass_tile<N, GEN_OTF_COLS, WL_THREADS, true>(S.G, img, tile, smem); break;
-	case GEN_INV_ROWS: gen_pass_tile<N, GEN_INV_ROWS, WL_THREADS, true>(S.G, img, tile, smem); break;
-	default: gen_pass_tile<N, GEN_INV_COLS, WL_THREADS, true>(S.G, img, tile, smem); break;
+	default: gen_pass_tile<N, GEN_INV_ROWS, WL_THREADS, true>(S.G, img, tile, smem); break;
 	}
 }
 
@@ -167,7 +165,7 @@ __global__ void __launch_bounds__(WL_THREADS, 4) worklist_kernel(const __grid_co
 		} else {  // WL_PIX: four images, each after its whole chain
 			const int nimg = min(4, S.nitem - w.z);
 			bool ok = true;
-			for (int k = 0; k < nimg && ok; k++) ok = wl_wait(W, W.cnt + S.img0 + w.z + k, wl_need(S, 7), &s_ok);
+			for (int k = 0; k < nimg && ok; k++) ok = wl_wait(W, W.cnt + S.img0 + w.z + k, wl_need(S, GEN_NPASS + 1), &s_ok);
 			if (ok && warp < nimg) wl_pixels(S, w.z + warp, lane);
 		}
 		__syncthreads();  // every thread is done with the shared memory; the next index is in
