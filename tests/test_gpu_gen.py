@@ -1,8 +1,8 @@
 """Full-frame parity of the larger FFT sizes (the FFT-pass chain) against the
 reference's own CPU frame (oracle/_ref) on the same screens: LGS with 32x32
 OPD points and FFT 64 (the large-sampling stress sampling, on an 8 m
-telescope), the 2x2 NGS with FFT 128 and the 1x1 tip-tilt sensors with FFT 256
-of the uneven batch.
+telescope) and FFT 128 (the same pupils embedded four times), the 2x2 NGS
+with FFT 128 and the 1x1 tip-tilt sensors with FFT 256 of the uneven batch.
 
 Tolerances as for the 32-point path: noise-free intensities within 1e-5 of the
 subaperture total, gradients within 1e-4 relative (max |dg| / max |g|)."""
@@ -37,6 +37,15 @@ def _check(ref_lib, cfg, isim, use_ref_mtche):
 def test_lgs_fft64_frame_matches_reference(ref_lib, isim):
     from maos_b200.configs import LGS8_N64
     _check(ref_lib, LGS8_N64, isim, use_ref_mtche=True)
+
+
+def test_lgs_fft128_frame_matches_reference(ref_lib):
+    """An LGS powfs through the FFT-pass chain: 32x32 OPD points embedded four times (FFT
+    128), 8x8 pixels of 0.8" -- pass 3's multiply by the elongation transfer function, and the
+    uplink OTF formed by passes 1-3 at 128 points."""
+    from maos_b200.configs import LGS8_N64
+    cfg = dict(LGS8_N64, name="lgs8_2x8x8_n128", embfac=4, notf=128, pixpsa=8)
+    _check(ref_lib, cfg, 11, use_ref_mtche=True)
 
 
 def test_ngs_fft128_frame_matches_reference(ref_lib):
