@@ -174,3 +174,37 @@ def test_etf_time_interpolation_matches_reference(ref_lib, isim):
         g0 = wl.frame_sync()[0]
         assert grad_rel_err(g0, out[0][0]) > 1e-3
     wl.close()
+
+
+@pytest.mark.parametrize("size,form", [(64, "fft"), (128, "fft"), (32, "tc")])
+def test_etf_time_interpolation_in_every_imaging_path(ref_lib, size, form):
+    """The two-slot ETF blend (maos/wfsints.c:212-221, 282) in the 64-point fused kernel, the
+    FFT-pass chain (FFT 128) and the tensor-core form, each against the reference's frame with
+    its second sodium profile, at a frame that weights both slots 1/2."""
+    from maos_b200 import shwfs
+    from maos_b200.configs import LGS8_N32, LGS8_N64
+    from maos_b200.workload import build
+    from tests.helpers import ints_tolerance_ok, grad_rel_err
+    cfg = {32: LGS8_N32, 64: LGS8_N64,
+           128: dict(LGS8_N64, name="lgs8_2x8x8_n128", embfac=4, notf=128, pixpsa=8)}[size]
+    f = shwfs.SHWFS_FORM_TC if form == "tc" else shwfs.SHWFS_FORM_FFT
+    dtrat, isim = 4, 6
+    wl = build(cfg, device=0, seed=3, noisy=False, nx=512, form=f)
+    r = ref_lib.RefPowfs(cfg)
+    r.setup_etf2(1500.0, dtrat)
+    for i in wl.wfs:
+        wl.ctx.wfs_set_mtche(i, r.mtche(), r.i0sum(), r.i0sumsum())
+    wl.ctx.powfs_set_etf(wl.ipowfs, r.etf(), slot=0)
+    wl.ctx.powfs_set_etf(wl.ipowfs, r.etf2(), slot=1)
+    wl.ctx.powfs_set_etf_dtrat(wl.ipowfs, dtrat)
+    ref_lib.atm_set(wl.screens, wl.layers)
+    wl.frame(isim)
+    out = wl.frame_sync(want_ints=True)
+    tol = 1e-4 if form == "tc" else 1e-5
+    for k in range(len(wl.wfs)):
+        ints_ref, g_ref, _ = ref_lib.frame_full_mt(r, k, isim, cfg["dt"], noisy=False)
+        g, ints = out[k]
+        ok, worst = ints_tolerance_ok(ints, ints_ref, r.nsa, r.npix, tol)
+        assert ok, f"wfs {k}: intensity error {worst:.3e} of subaperture total"
+        assert grad_rel_err(g, g_ref) <= 1e-4, (k, grad_rel_err(g, g_ref))
+    wl.close()
