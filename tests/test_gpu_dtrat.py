@@ -67,3 +67,32 @@ def test_lgs_dtrat2_frame(ref_lib):
         assert ok, worst
         assert grad_rel_err(g, r.grad(a + b, iwfs=k)) <= 1e-4
     wl.close()
+
+
+@pytest.mark.parametrize("cfg_name", ["LGS8_N64", "NGS30_2X2"])
+def test_dtrat2_larger_sizes(ref_lib, cfg_name):
+    """Integration over 2 frames in the 64-point fused kernel (LGS, matched filter) and in the
+    FFT-pass chain's pixel step (the 2x2 NGS at FFT 128, CoG): the intensities of the period
+    add up and its last frame forms the gradients of the sum."""
+    from maos_b200 import configs
+    from maos_b200.workload import build
+    from tests.helpers import ints_tolerance_ok, grad_rel_err
+    cfg = getattr(configs, cfg_name)
+    wl = build(cfg, device=0, seed=5, noisy=False, nx=512)
+    wl.ctx.powfs_set_dtrat(wl.ipowfs, 2)
+    r = ref_lib.RefPowfs(cfg)
+    if cfg["phytype"] == 1:
+        for i in wl.wfs:
+            wl.ctx.wfs_set_mtche(i, r.mtche(), r.i0sum(), r.i0sumsum())
+    ref_lib.atm_set(wl.screens, wl.layers)
+    for isim in (12, 13):
+        wl.frame(isim)
+    out = wl.frame_sync(want_ints=True)
+    for k in range(len(wl.wfs)):
+        a = ref_lib.frame_full_mt(r, k, 12, cfg["dt"], noisy=False)[0]
+        b = ref_lib.frame_full_mt(r, k, 13, cfg["dt"], noisy=False)[0]
+        g, ints = out[k]
+        ok, worst = ints_tolerance_ok(ints, a + b, r.nsa, r.npix, 1e-5)
+        assert ok, worst
+        assert grad_rel_err(g, r.grad(a + b, iwfs=k)) <= 1e-4
+    wl.close()

@@ -86,14 +86,27 @@ def test_noise_statistics_match_reference(ref_lib, variant):
     """10^4 noisy frames: per-pixel mean and variance, and the distribution of
     normalised residuals against the reference's addnoise on the same image;
     full-spectrum (variant 0) and half-spectrum (variant 4) imaging."""
+    from maos_b200.configs import NGS8
+    _noise_statistics(ref_lib, NGS8, variant)
+
+
+def test_noise_statistics_fft128_match_reference(ref_lib):
+    """The same statistics for the FFT-pass chain's pixel step (a thread per pixel): the 2x2
+    NGS at FFT 128, 256 pixels per subaperture, most of them in the wings (the inversion and
+    PTRS rules) and the core above 200 photons (the Gaussian rule)."""
+    from maos_b200.configs import NGS30_2X2
+    _noise_statistics(ref_lib, NGS30_2X2, None)
+
+
+def _noise_statistics(ref_lib, cfg, variant):
     import torch
     from scipy import stats
-    from maos_b200.configs import NGS8
     from tests.helpers import context_from_ref, turbulent_opd
-    r = ref_lib.RefPowfs(NGS8)
+    r = ref_lib.RefPowfs(cfg)
     opd, _ = turbulent_opd(r, seed=11)
-    ctx, ip, iw = context_from_ref(r, NGS8, noisy=1)
-    ctx.set_variant(ip, variant)
+    ctx, ip, iw = context_from_ref(r, cfg, noisy=1)
+    if variant is not None:
+        ctx.set_variant(ip, variant)
     dev = torch.device("cuda", 0)
     o = torch.tensor(opd, dtype=torch.float32, device=dev)
     nf = torch.zeros(r.nsa * r.npix, dtype=torch.float32, device=dev)
@@ -111,7 +124,7 @@ def test_noise_statistics_match_reference(ref_lib, variant):
     I = nf.double().cpu().numpy()
     mean = (s1 / nframe).cpu().numpy()
     var = (s2 / nframe).cpu().numpy() - mean ** 2
-    rne = NGS8["rne"]
+    rne = cfg["rne"]
     expect_var = I + rne ** 2
     # mean of the residual: 0 within 6 sigma of the mean estimate
     assert np.all(np.abs(mean) <= 6 * np.sqrt(expect_var / nframe) + 1e-3)
