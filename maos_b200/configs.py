@@ -115,9 +115,10 @@ LGS8_N32 = dict(
 # one the OTF size and the main band use.
 NGS8_2WVL = dict(NGS8, name="ngs8_16x16_2wvl", wvls=[0.7e-6, 0.9e-6], wvlwts=[0.6, 0.4])
 LGS8_N32_2WVL = dict(LGS8_N32, name="lgs8_2x16x16_mf_2wvl", wvls=[0.589e-6, 0.62e-6], wvlwts=[0.7, 0.3])
+LGS8_N64_2WVL = dict(LGS8_N64, name="lgs8_2x8x8_n64_2wvl", wvls=[0.589e-6, 0.62e-6], wvlwts=[0.7, 0.3])
 
 CONFIGS = {c["name"]: c for c in (NGS8, LGS30, LGS30_N64, NGS30_2X2, TT30, LGS8_N64, LGS8_N32, NGS8_2WVL,
-                                  LGS8_N32_2WVL)}
+                                  LGS8_N32_2WVL, LGS8_N64_2WVL)}
 
 # Science path: the 30 m aperture sampled at 1/64 m (the reference's default
 # evl.dx = atm.dx), 9 directions on a 3x3 grid over a 30" field, PSFs at J, H

@@ -14,7 +14,8 @@ from tests.conftest import cuda_available
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not cuda_available(), reason="needs a CUDA GPU")]
 
 
-@pytest.mark.parametrize("cfg_name,form,isim", [("NGS8_2WVL", 0, 3), ("LGS8_N32_2WVL", 0, 5), ("NGS8_2WVL", 1, 2)])
+@pytest.mark.parametrize("cfg_name,form,isim", [("NGS8_2WVL", 0, 3), ("LGS8_N32_2WVL", 0, 5), ("NGS8_2WVL", 1, 2),
+                                               ("LGS8_N64_2WVL", 0, 4)])
 def test_two_wavelength_frame_matches_reference(ref_lib, cfg_name, form, isim):
     from maos_b200 import configs
     from maos_b200.workload import build

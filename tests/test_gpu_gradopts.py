@@ -57,17 +57,21 @@ def test_mf_options_match_reference(ref_lib, sigmatch, mtchcr):
     _check(ref_lib, cfg)
 
 
-def test_lgs_sigmatch2_frame_matches_reference(ref_lib):
-    """A whole LGS frame (ray trace, uplink, imaging, device sum, gradients)
-    with sigmatch 2 against the reference's frame."""
-    from maos_b200.configs import LGS8_N32
+@pytest.mark.parametrize("cfg_name", ["LGS8_N32", "LGS8_N64", "NGS30_2X2"])
+def test_lgs_sigmatch2_frame_matches_reference(ref_lib, cfg_name):
+    """A whole frame (ray trace, uplink, imaging, device sum, gradients) with sigmatch 2
+    against the reference's frame: LGS at FFT 32 and 64 (matched filter), the 2x2 NGS at
+    FFT 128 (CoG)."""
+    from maos_b200 import configs
     from maos_b200.workload import build
     from tests.helpers import ints_tolerance_ok, grad_rel_err
-    cfg = dict(LGS8_N32, name="lgs8_sig2", sigmatch=2)
+    base = getattr(configs, cfg_name)
+    cfg = dict(base, name=base["name"] + "_sig2", sigmatch=2)
     wl = build(cfg, device=0, seed=3, noisy=False, nx=512)
     r = ref_lib.RefPowfs(cfg)
-    for i in wl.wfs:
-        wl.ctx.wfs_set_mtche(i, r.mtche(), r.i0sum(), r.i0sumsum())
+    if cfg["phytype"] == 1:
+        for i in wl.wfs:
+            wl.ctx.wfs_set_mtche(i, r.mtche(), r.i0sum(), r.i0sumsum())
     ref_lib.atm_set(wl.screens, wl.layers)
     wl.frame(6)
     out = wl.frame_sync(want_ints=True)
