@@ -149,3 +149,26 @@ def test_branch_priority_keeps_frames(graph):
     for fa, fb in zip(a, b):
         for (ga, ia), (gb, ib) in zip(fa, fb):
             assert np.array_equal(ga, gb) and np.array_equal(ia, ib)
+
+
+def test_tc_form_frames_in_the_batch_graph():
+    """The tensor-core form of the 32-point LGS powfs (its imaging kernel and the separate
+    noise/gradient kernel) on a graph branch beside the FFT-pass chains of the NGS and tip-tilt
+    sensors: noisy graph frames equal stream frames, bit for bit, and are finite."""
+    from maos_b200 import shwfs
+    from maos_b200.configs import UNEVEN_BATCH
+    from maos_b200.workload import build_batch
+    outs = []
+    for graph in (False, True):
+        wl = build_batch(UNEVEN_BATCH["members"], device=0, seed=6, noisy=True, nx=512, graph=graph,
+                         form=shwfs.SHWFS_FORM_TC)
+        frames = []
+        for isim in (2, 3, 4):
+            wl.frame(isim)
+            frames.append(wl.frame_sync(want_ints=True))
+        wl.close()
+        outs.append(frames)
+    for fa, fb in zip(*outs):
+        for (ga, ia), (gb, ib) in zip(fa, fb):
+            assert np.array_equal(ga, gb) and np.array_equal(ia, ib)
+            assert np.isfinite(ga).all() and np.isfinite(ia).all()
