@@ -284,13 +284,18 @@ def _roofline(form, cfg, wl, st, units_per_step):
     ray_ms = st["raytrace"]["ms_per_step"]  # the WFS pupils, plus any LLT pupils traced in a second launch
     ints_gbs = ints_bytes / (ints_ms * 1e-3) / 1e9 if ints_ms else 0.0
     ray_gbs = ray_bytes / (ray_ms * 1e-3) / 1e9 if ray_ms else 0.0
-    traffic = None
+    measured = {}
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
-            traffic = json.load(f).get(f"{cfg['name']}:{form}:ints")
+            measured = json.load(f)
+    traffic = measured.get(f"{cfg['name']}:{form}:ints")
     raytrace = {"kernel": "geom_kernel", "bound": "hbm", "achieved": ray_gbs, "peak": hbm, "unit": "GB/s",
                 "frac": ray_gbs / hbm, "algorithmic_bytes_per_launch": ray_bytes,
+                "traffic": measured.get(f"{cfg['name']}:raytrace"),
+                "limiter": "L1/L2 gather latency: the measured DRAM bytes (traffic, one launch of the WFS pupils) "
+                           "are a fraction of the algorithmic bytes, each touched screen byte crossing from DRAM "
+                           "about once",
                 "note": "algorithmic bytes: one 4-byte screen read per point and layer plus the OPD write"}
     hbm_sub = {"achieved": ints_gbs, "peak": hbm, "unit": "GB/s", "frac": ints_gbs / hbm,
                "peak_source": src_note + " hbm_gbs", "algorithmic_bytes_per_launch": ints_bytes}
