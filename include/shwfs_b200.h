@@ -359,9 +359,9 @@ int shwfs_copy_counters(shwfs_ctx* ctx, uint64_t* h2d, uint64_t* d2h);
    to a 32x32 FFT (the 32-point form, at most 128 pixels); any other powfs
    (64-point and larger FFTs, geometric sensors, dtrat > 1, sigmatch 2) is
    rejected with SHWFS_EINVAL before anything is launched.  The first call on a device
-   looks up the array's device address (cudaGetSymbolAddress), so make it
-   before any stream capture.  Calls share the array: calls whose work
-   overlaps on the GPU race; queue them on one stream. */
+   looks up the array's device address (cudaGetSymbolAddress).  Calls share
+   the array: calls whose work overlaps on the GPU race; queue them on one
+   stream. */
 #define SHWFS_NOALLOC_MAX_NSA 4096
 int shwfs_frame_noalloc(shwfs_ctx* ctx, int iwfs, int isim, float* ints, float* grad);
 
