@@ -46,7 +46,7 @@ def _terms(cfg, nsa, nopd, seed):
                 opdadd=rng.normal(0, 3e-8, nsa * nopd * nopd))
 
 
-@pytest.mark.parametrize("cfg_name,isim", [("LGS8_N32", 7), ("NGS8", 3)])
+@pytest.mark.parametrize("cfg_name,isim", [("LGS8_N32", 7), ("NGS8", 3), ("LGS8_N64", 5)])
 def test_closed_loop_frame_matches_reference(ref_lib, cfg_name, isim):
     import torch
     from maos_b200 import configs
